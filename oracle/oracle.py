@@ -1,0 +1,281 @@
+"""Test infrastructure only (the oracle).
+
+ctypes bindings for
+  * ``lib/libnkoracle.so`` - the plain-C restatement of the reference PageRank
+    path (``pagerank_oracle.c``), and
+  * ``_ref/libnkref.so`` - the reference's own PageRank compiled from the
+    reference sources (``Makefile``, ``ref/nkref_capi.cpp``), present only
+    where it was built.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module, and only as the checker / baseline. The
+product path never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "lib", "libnkoracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libnkref.so")
+
+_u64p = C.POINTER(C.c_uint64)
+_u32p = C.POINTER(C.c_uint32)
+_u8p = C.POINTER(C.c_uint8)
+_f64p = C.POINTER(C.c_double)
+
+
+class _Params(C.Structure):
+    _fields_ = [
+        ("damp", C.c_double),
+        ("tol", C.c_double),
+        ("norm", C.c_int32),
+        ("normalized", C.c_int32),
+        ("distribute_sinks", C.c_int32),
+        ("nthreads", C.c_int32),
+        ("max_iterations", C.c_uint64),
+    ]
+
+
+def build(ref: bool = True) -> None:
+    """Compile the oracle (and, when the reference sources are present, the
+    reference library)."""
+    target = "all" if ref else "oracle"
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+
+
+def _ptr(a, t):
+    if a is None:
+        return None
+    return a.ctypes.data_as(t)
+
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build(ref=False)
+        lib = C.CDLL(ORACLE_SO)
+        lib.nko_pagerank.restype = C.c_int
+        lib.nko_pagerank.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _f64p, _u32p, _u8p, _f64p,
+                                     C.POINTER(_Params), _f64p, _u64p, _f64p, _f64p, C.c_uint64]
+        lib.nko_ranking.restype = C.c_int
+        lib.nko_ranking.argtypes = [C.c_uint64, _f64p, _u8p, _u64p, _f64p]
+        lib.nko_pagerank_adjoint.restype = C.c_int64
+        lib.nko_pagerank_adjoint.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _f64p, _u32p, _f64p,
+                                             C.c_double, C.c_int, _f64p, _f64p, C.c_double,
+                                             C.c_uint64, _f64p, _f64p, _f64p]
+        _oracle = lib
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise RuntimeError("reference library not built: " + REF_SO)
+        lib = C.CDLL(REF_SO)
+        lib.nkref_last_error.restype = C.c_char_p
+        lib.nkref_graph_create.restype = C.c_int
+        lib.nkref_graph_create.argtypes = [C.POINTER(C.c_void_p), C.c_uint64, C.c_int, C.c_int,
+                                           C.c_uint64, _u32p, _u32p, _f64p, _u8p]
+        lib.nkref_graph_read.restype = C.c_int
+        lib.nkref_graph_read.argtypes = [C.POINTER(C.c_void_p), C.c_char_p, C.c_int, C.c_int]
+        lib.nkref_graph_destroy.argtypes = [C.c_void_p]
+        for f in ("nkref_graph_num_nodes", "nkref_graph_upper_node_id", "nkref_graph_num_edges"):
+            getattr(lib, f).restype = C.c_uint64
+            getattr(lib, f).argtypes = [C.c_void_p]
+        lib.nkref_graph_is_directed.argtypes = [C.c_void_p]
+        lib.nkref_graph_is_weighted.argtypes = [C.c_void_p]
+        lib.nkref_graph_arc_counts.argtypes = [C.c_void_p, _u64p, _u64p]
+        lib.nkref_graph_export.restype = C.c_int
+        lib.nkref_graph_export.argtypes = [C.c_void_p, _u64p, _u32p, _f64p, _u64p, _u32p, _f64p,
+                                           _u8p]
+        lib.nkref_pagerank.restype = C.c_int
+        lib.nkref_pagerank.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_int,
+                                       C.c_uint64, C.c_int, _f64p, _u64p, _f64p, _u64p, _f64p,
+                                       _f64p]
+        _ref = lib
+    return _ref
+
+
+@dataclass
+class OracleResult:
+    scores: np.ndarray
+    iterations: int
+    maximum: float
+    trace: np.ndarray
+
+
+def pagerank(csr, damp=0.85, tol=1e-8, norm=1, normalized=False, distribute_sinks=False,
+             max_iterations=2**64 - 1, teleport=None, nthreads=1, trace_cap=100000) -> OracleResult:
+    """Run the C restatement on an in-CSR (any object with the attributes
+    z, in_ptr, in_col, in_w, wdeg, outdeg, exists)."""
+    lib = oracle_lib()
+    z = int(csr.z)
+    scores = np.empty(z, np.float64)
+    iters = C.c_uint64(0)
+    mx = C.c_double(0.0)
+    trace = np.zeros(trace_cap, np.float64)
+    p = _Params(damp, tol, int(norm), int(bool(normalized)), int(bool(distribute_sinks)),
+                int(nthreads), int(max_iterations))
+    tele = None if teleport is None else np.ascontiguousarray(teleport, np.float64)
+    rc = lib.nko_pagerank(z, _ptr(csr.in_ptr, _u64p), _ptr(csr.in_col, _u32p),
+                          _ptr(csr.in_w, _f64p), _ptr(csr.wdeg, _f64p), _ptr(csr.outdeg, _u32p),
+                          _ptr(csr.exists, _u8p), _ptr(tele, _f64p), C.byref(p),
+                          _ptr(scores, _f64p), C.byref(iters), C.byref(mx), _ptr(trace, _f64p),
+                          trace_cap)
+    if rc != 0:
+        raise RuntimeError("oracle nko_pagerank failed")
+    it = int(iters.value)
+    return OracleResult(scores, it, float(mx.value), trace[:min(it, trace_cap)].copy())
+
+
+def ranking(scores, exists=None):
+    lib = oracle_lib()
+    z = scores.shape[0]
+    n = z if exists is None else int(np.count_nonzero(exists))
+    ids = np.empty(n, np.uint64)
+    vals = np.empty(n, np.float64)
+    sc = np.ascontiguousarray(scores, np.float64)
+    ex = None if exists is None else np.ascontiguousarray(exists, np.uint8)
+    lib.nko_ranking(z, _ptr(sc, _f64p), _ptr(ex, _u8p), _ptr(ids, _u64p), _ptr(vals, _f64p))
+    return ids, vals
+
+
+def adjoint(csr, x, g, damp=0.85, distribute_sinks=True, teleport=None, tol=1e-14,
+            max_iter=100000):
+    """FP64 host adjoint solve; returns (lam, grad_w, grad_t, sweeps)."""
+    lib = oracle_lib()
+    z = int(csr.z)
+    lam = np.empty(z, np.float64)
+    gw = np.empty(csr.in_col.shape[0], np.float64)
+    gt = np.empty(z, np.float64)
+    x = np.ascontiguousarray(x, np.float64)
+    g = np.ascontiguousarray(g, np.float64)
+    tele = None if teleport is None else np.ascontiguousarray(teleport, np.float64)
+    sweeps = lib.nko_pagerank_adjoint(z, _ptr(csr.in_ptr, _u64p), _ptr(csr.in_col, _u32p),
+                                      _ptr(csr.in_w, _f64p), _ptr(csr.wdeg, _f64p),
+                                      _ptr(csr.outdeg, _u32p), _ptr(tele, _f64p), damp,
+                                      int(bool(distribute_sinks)), _ptr(x, _f64p),
+                                      _ptr(g, _f64p), tol, max_iter, _ptr(lam, _f64p),
+                                      _ptr(gw, _f64p), _ptr(gt, _f64p))
+    if sweeps < 0:
+        raise RuntimeError("oracle adjoint failed")
+    return lam, gw, gt, int(sweeps)
+
+
+# ---------------------------------------------------------------------------
+# The reference library (oracle/_ref)
+
+
+class RefGraph:
+    """A NetworKit::Graph owned by the reference library."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    def __del__(self):
+        if getattr(self, "h", None) and _ref is not None:
+            _ref.nkref_graph_destroy(self.h)
+            self.h = None
+
+    @classmethod
+    def from_edges(cls, n, src, dst, w=None, directed=False, weighted=False, exists=None):
+        lib = ref_lib()
+        h = C.c_void_p()
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        w = None if w is None else np.ascontiguousarray(w, np.float64)
+        ex = None if exists is None else np.ascontiguousarray(exists, np.uint8)
+        rc = lib.nkref_graph_create(C.byref(h), int(n), int(bool(weighted)), int(bool(directed)),
+                                    src.shape[0], _ptr(src, _u32p), _ptr(dst, _u32p),
+                                    _ptr(w, _f64p), _ptr(ex, _u8p))
+        if rc != 0:
+            raise RuntimeError(lib.nkref_last_error().decode())
+        return cls(h)
+
+    @classmethod
+    def read(cls, path, kind, directed=False):
+        """kind: 0 = SNAP, 1 = METIS, 2 = GML (the reference readers)."""
+        lib = ref_lib()
+        h = C.c_void_p()
+        rc = lib.nkref_graph_read(C.byref(h), path.encode(), int(kind), int(bool(directed)))
+        if rc != 0:
+            raise RuntimeError(lib.nkref_last_error().decode())
+        return cls(h)
+
+    @property
+    def z(self):
+        return int(ref_lib().nkref_graph_upper_node_id(self.h))
+
+    @property
+    def n(self):
+        return int(ref_lib().nkref_graph_num_nodes(self.h))
+
+    @property
+    def m(self):
+        return int(ref_lib().nkref_graph_num_edges(self.h))
+
+    @property
+    def directed(self):
+        return bool(ref_lib().nkref_graph_is_directed(self.h))
+
+    @property
+    def weighted(self):
+        return bool(ref_lib().nkref_graph_is_weighted(self.h))
+
+    def export(self):
+        """Adjacency in storage order: dict with out_ptr, out_adj, out_w, in_ptr,
+        in_adj, in_w (directed only), exists."""
+        lib = ref_lib()
+        oa, ia = C.c_uint64(0), C.c_uint64(0)
+        lib.nkref_graph_arc_counts(self.h, C.byref(oa), C.byref(ia))
+        z = self.z
+        out_ptr = np.zeros(z + 1, np.uint64)
+        out_adj = np.zeros(oa.value, np.uint32)
+        out_w = np.zeros(oa.value, np.float64)
+        directed = self.directed
+        in_ptr = np.zeros(z + 1, np.uint64) if directed else None
+        in_adj = np.zeros(ia.value, np.uint32) if directed else None
+        in_w = np.zeros(ia.value, np.float64) if directed else None
+        exists = np.zeros(z, np.uint8)
+        rc = lib.nkref_graph_export(self.h, _ptr(out_ptr, _u64p), _ptr(out_adj, _u32p),
+                                    _ptr(out_w, _f64p), _ptr(in_ptr, _u64p), _ptr(in_adj, _u32p),
+                                    _ptr(in_w, _f64p), _ptr(exists, _u8p))
+        if rc != 0:
+            raise RuntimeError(lib.nkref_last_error().decode())
+        return dict(out_ptr=out_ptr, out_adj=out_adj, out_w=out_w, in_ptr=in_ptr, in_adj=in_adj,
+                    in_w=in_w, exists=exists, directed=directed, weighted=self.weighted)
+
+    def pagerank(self, damp=0.85, tol=1e-8, normalized=False, norm=1, max_iterations=2**64 - 1,
+                 nthreads=0, want_ranking=True):
+        lib = ref_lib()
+        z, n = self.z, self.n
+        scores = np.empty(z, np.float64)
+        iters = C.c_uint64(0)
+        mx = C.c_double(0.0)
+        secs = C.c_double(0.0)
+        ids = np.empty(n, np.uint64) if want_ranking else None
+        vals = np.empty(n, np.float64) if want_ranking else None
+        rc = lib.nkref_pagerank(self.h, damp, tol, int(bool(normalized)), int(norm),
+                                int(max_iterations), int(nthreads), _ptr(scores, _f64p),
+                                C.byref(iters), C.byref(mx), _ptr(ids, _u64p), _ptr(vals, _f64p),
+                                C.byref(secs))
+        if rc != 0:
+            raise RuntimeError(lib.nkref_last_error().decode())
+        return dict(scores=scores, iterations=int(iters.value), maximum=float(mx.value),
+                    ranking_ids=ids, ranking_vals=vals, seconds=float(secs.value))

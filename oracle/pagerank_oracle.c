@@ -1,0 +1,280 @@
+/* Test infrastructure only (the oracle): plain-C restatement of the reference
+ * PageRank path. Each function cites the reference lines it follows. It is
+ * the checker for the CUDA path; the product never links it.
+ *
+ * Parity pin: with distribute_sinks = 0, a uniform teleport and nthreads <= 1
+ * this follows PageRank.cpp:20-104 operation for operation, so its scores are
+ * bit-identical to the reference library built from the reference sources
+ * (oracle/_ref/libnkref.so) run on one OpenMP thread; tests/test_oracle.py
+ * checks that on every golden fixture. The distributeSinks term, the
+ * personalised teleport and the adjoint have no reference implementation
+ * (parity unpinned); they extend the same loop. */
+#include "pagerank_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+static int exists_at(const uint8_t *exists, uint64_t u) { return exists == NULL || exists[u] != 0; }
+
+/* Graph::parallelSumForNodes (Graph.hpp:2123-2134) of |a-b| or (a-b)^2. */
+static double residual_sum(uint64_t z, const uint8_t *exists, const double *a, const double *b,
+                           int l2, int nthreads) {
+    double sum = 0.0;
+    if (nthreads > 1) {
+#pragma omp parallel for reduction(+ : sum) num_threads(nthreads) schedule(static)
+        for (int64_t u = 0; u < (int64_t)z; ++u) {
+            if (exists_at(exists, (uint64_t)u)) {
+                const double d = a[u] - b[u];
+                sum += l2 ? d * d : fabs(d);
+            }
+        }
+    } else {
+        for (uint64_t u = 0; u < z; ++u) {
+            if (exists_at(exists, u)) {
+                const double d = a[u] - b[u];
+                sum += l2 ? d * d : fabs(d);
+            }
+        }
+    }
+    return sum;
+}
+
+static double sink_mass(uint64_t z, const uint8_t *exists, const uint32_t *outdeg,
+                        const double *x) {
+    double s = 0.0;
+    for (uint64_t u = 0; u < z; ++u)
+        if (exists_at(exists, u) && outdeg[u] == 0)
+            s += x[u];
+    return s;
+}
+
+int nko_pagerank(uint64_t z, const uint64_t *in_ptr, const uint32_t *in_col, const double *in_w,
+                 const double *wdeg, const uint32_t *outdeg, const uint8_t *exists,
+                 const double *teleport, const nko_params *p, double *scores, uint64_t *iterations,
+                 double *max_out, double *trace, uint64_t trace_cap) {
+    if (!in_ptr || !wdeg || !outdeg || !p || !scores || z == 0)
+        return -1;
+    uint64_t n = 0;
+    for (uint64_t u = 0; u < z; ++u)
+        n += exists_at(exists, u);
+    if (n == 0)
+        return -1;
+    const int nthreads = p->nthreads;
+    const double damp = p->damp;
+    /* PageRank.cpp:25-27 */
+    const double teleportProb = (1.0 - damp) / (double)n;
+    double *scoreData = scores;
+    for (uint64_t u = 0; u < z; ++u)
+        scoreData[u] = 1.0 / (double)n;
+    double *pr = (double *)malloc(z * sizeof(double));
+    if (!pr)
+        return -1;
+    memcpy(pr, scoreData, z * sizeof(double));
+    /* PageRank.cpp:29-30: deg[u] = weightedDegree(u) is the caller's wdeg. */
+    uint64_t iters = 0;
+    int converged = 0;
+    do {
+        /* Sink term (distributeSinks): the mass of dangling nodes of the
+         * previous iterate, spread like the teleport. */
+        double share = 0.0, S = 0.0;
+        if (p->distribute_sinks) {
+            S = sink_mass(z, exists, outdeg, scoreData);
+            share = S / (double)n;
+        }
+        /* PageRank.cpp:56-66 (balancedParallelForNodes + forInEdgesOf) */
+#pragma omp parallel for schedule(guided) num_threads(nthreads > 1 ? nthreads : 1)
+        for (int64_t ui = 0; ui < (int64_t)z; ++ui) {
+            const uint64_t u = (uint64_t)ui;
+            if (!exists_at(exists, u))
+                continue;
+            double acc = 0.0;
+            for (uint64_t e = in_ptr[u]; e < in_ptr[u + 1]; ++e) {
+                const uint32_t v = in_col[e];
+                const double w = in_w ? in_w[e] : 1.0;
+                acc += scoreData[v] * w / wdeg[v];
+            }
+            if (p->distribute_sinks)
+                acc += teleport ? S * teleport[u] : share;
+            acc *= damp;
+            acc += teleport ? (1.0 - damp) * teleport[u] : teleportProb;
+            pr[u] = acc;
+        }
+        ++iters;
+        /* PageRank.cpp:41-51 */
+        double res;
+        if (p->norm == 1)
+            res = sqrt(residual_sum(z, exists, scoreData, pr, 1, nthreads));
+        else
+            res = residual_sum(z, exists, scoreData, pr, 0, nthreads);
+        if (trace && iters <= trace_cap)
+            trace[iters - 1] = res;
+        converged = iters >= p->max_iterations || res <= p->tol;
+        /* PageRank.cpp:70: std::swap(pr, scoreData) */
+        double *t = pr;
+        pr = scoreData;
+        scoreData = t;
+    } while (!converged);
+
+    if (scoreData != scores) {
+        memcpy(scores, scoreData, z * sizeof(double));
+        pr = scoreData; /* the malloc'd buffer, freed below */
+    }
+    /* PageRank.cpp:75-92 */
+    if (!p->normalized) {
+        double sum = 0.0;
+        for (uint64_t u = 0; u < z; ++u)
+            if (exists_at(exists, u))
+                sum += scores[u];
+        for (uint64_t u = 0; u < z; ++u)
+            if (exists_at(exists, u))
+                scores[u] /= sum;
+    } else {
+        double sum = 0.0;
+        for (uint64_t u = 0; u < z; ++u)
+            if (exists_at(exists, u) && outdeg[u] == 0)
+                sum += scores[u];
+        const double normFactor = (1.0 / (double)n) * ((1 - damp) + (damp * sum));
+        for (uint64_t u = 0; u < z; ++u)
+            if (exists_at(exists, u))
+                scores[u] /= normFactor;
+    }
+    /* PageRank.cpp:95-102 */
+    if (max_out) {
+        if (!p->normalized) {
+            *max_out = 1.0;
+        } else {
+            double m = scores[0];
+            for (uint64_t u = 0; u < z; ++u)
+                if (exists_at(exists, u) && scores[u] > m)
+                    m = scores[u];
+            *max_out = m;
+        }
+    }
+    if (iterations)
+        *iterations = iters;
+    free(pr);
+    return 0;
+}
+
+typedef struct {
+    uint64_t id;
+    double val;
+} rank_pair;
+
+/* Centrality.cpp:34-38: score descending, ties by node id ascending. */
+static int rank_cmp(const void *a, const void *b) {
+    const rank_pair *x = (const rank_pair *)a, *y = (const rank_pair *)b;
+    if (x->val == y->val)
+        return x->id < y->id ? -1 : (x->id > y->id ? 1 : 0);
+    return x->val > y->val ? -1 : 1;
+}
+
+int nko_ranking(uint64_t z, const double *scores, const uint8_t *exists, uint64_t *ids,
+                double *vals) {
+    rank_pair *r = (rank_pair *)malloc((z ? z : 1) * sizeof(rank_pair));
+    if (!r)
+        return -1;
+    uint64_t n = 0;
+    for (uint64_t u = 0; u < z; ++u)
+        if (exists_at(exists, u)) {
+            r[n].id = u;
+            r[n].val = scores[u];
+            ++n;
+        }
+    qsort(r, n, sizeof(rank_pair), rank_cmp);
+    for (uint64_t i = 0; i < n; ++i) {
+        if (ids)
+            ids[i] = r[i].id;
+        if (vals)
+            vals[i] = r[i].val;
+    }
+    free(r);
+    return 0;
+}
+
+int64_t nko_pagerank_adjoint(uint64_t z, const uint64_t *in_ptr, const uint32_t *in_col,
+                             const double *in_w, const double *wdeg, const uint32_t *outdeg,
+                             const double *teleport, double damp, int distribute_sinks,
+                             const double *x, const double *g, double tol, uint64_t max_iter,
+                             double *lam, double *grad_w, double *grad_t) {
+    if (!in_ptr || !wdeg || !outdeg || !x || !g || !lam || z == 0)
+        return -1;
+    const double n = (double)z;
+    double sumx = 0.0, S = 0.0;
+    for (uint64_t u = 0; u < z; ++u) {
+        sumx += x[u];
+        if (outdeg[u] == 0)
+            S += x[u];
+    }
+    double gp = 0.0;
+    for (uint64_t u = 0; u < z; ++u)
+        gp += g[u] * (x[u] / sumx);
+    double *gbar = (double *)malloc(z * sizeof(double));
+    double *c = (double *)malloc(z * sizeof(double));
+    double *lam2 = (double *)malloc(z * sizeof(double));
+    if (!gbar || !c || !lam2) {
+        free(gbar);
+        free(c);
+        free(lam2);
+        return -1;
+    }
+    for (uint64_t u = 0; u < z; ++u) {
+        gbar[u] = (g[u] - gp) / sumx;
+        lam[u] = gbar[u];
+    }
+    int64_t sweeps = 0;
+    for (;;) {
+        /* c = A^T lam: scatter over the in-arcs (u <- v). */
+        memset(c, 0, z * sizeof(double));
+        for (uint64_t u = 0; u < z; ++u)
+            for (uint64_t e = in_ptr[u]; e < in_ptr[u + 1]; ++e) {
+                const uint32_t v = in_col[e];
+                const double w = in_w ? in_w[e] : 1.0;
+                c[v] += w / wdeg[v] * lam[u];
+            }
+        double tl = 0.0;
+        if (distribute_sinks)
+            for (uint64_t u = 0; u < z; ++u)
+                tl += (teleport ? teleport[u] : 1.0 / n) * lam[u];
+        double res = 0.0;
+        for (uint64_t v = 0; v < z; ++v) {
+            double s = c[v];
+            if (distribute_sinks && outdeg[v] == 0)
+                s += tl;
+            lam2[v] = gbar[v] + damp * s;
+            res += fabs(lam2[v] - lam[v]);
+        }
+        memcpy(lam, lam2, z * sizeof(double));
+        ++sweeps;
+        if (res <= tol || (uint64_t)sweeps >= max_iter)
+            break;
+    }
+    /* c for the final lam */
+    memset(c, 0, z * sizeof(double));
+    for (uint64_t u = 0; u < z; ++u)
+        for (uint64_t e = in_ptr[u]; e < in_ptr[u + 1]; ++e) {
+            const uint32_t v = in_col[e];
+            const double w = in_w ? in_w[e] : 1.0;
+            c[v] += w / wdeg[v] * lam[u];
+        }
+    if (grad_w)
+        for (uint64_t u = 0; u < z; ++u)
+            for (uint64_t e = in_ptr[u]; e < in_ptr[u + 1]; ++e) {
+                const uint32_t v = in_col[e];
+                grad_w[e] = damp * (x[v] / wdeg[v]) * (lam[u] - c[v]);
+            }
+    if (grad_t) {
+        const double f = (distribute_sinks ? damp * S : 0.0) + 1.0 - damp;
+        for (uint64_t u = 0; u < z; ++u)
+            grad_t[u] = f * lam[u];
+    }
+    free(gbar);
+    free(c);
+    free(lam2);
+    return sweeps;
+}

@@ -1,0 +1,74 @@
+/* Test infrastructure only (the oracle): a plain-C restatement of the
+ * reference PageRank path, used by the tests, the smoke check and the CPU
+ * baseline of bench.py as the checker. The product never links it.
+ *
+ * Graph input is the in-adjacency in CSR form, exactly what the reference's
+ * Graph::forInEdgesOf visits (include/networkit/graph/Graph.hpp:1917-1938):
+ * directed graphs -> inEdges[u], undirected graphs -> outEdges[u] (both
+ * directions stored, self-loops once, Graph.cpp:549-596), in storage order.
+ */
+#ifndef NK_PAGERANK_ORACLE_H
+#define NK_PAGERANK_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    double damp;             /* PageRank.hpp:70 */
+    double tol;              /* PageRank.hpp:71 */
+    int32_t norm;            /* 0 = L1Norm, 1 = L2Norm (PageRank.hpp:31,67) */
+    int32_t normalized;      /* PageRank.hpp:73 */
+    int32_t distribute_sinks;/* new: redistribute dangling mass every iteration */
+    int32_t nthreads;        /* <= 1: sequential sums in node order */
+    uint64_t max_iterations; /* PageRank.hpp:64 */
+} nko_params;
+
+/* PageRank::run() (PageRank.cpp:20-104) over the in-CSR.
+ *   z         upperNodeIdBound
+ *   in_ptr    z+1 row offsets; in_col the source of each in-arc
+ *   in_w      in-arc weights or NULL (unweighted: every weight is 1.0)
+ *   wdeg      weightedDegree(u) of every node (out-degree / out-weight sum)
+ *   outdeg    degree(u) (number of out-arcs) of every node, used by the
+ *             normalized branch (PageRank.cpp:84) and the sink set
+ *   exists    node-existence mask or NULL (all exist)
+ *   teleport  personalised teleport distribution (z entries summing to 1 over
+ *             existing nodes) or NULL for the uniform (1-damp)/n
+ *   scores    out: z entries; iterations, max_out: out
+ *   trace     optional per-iteration residual (before the sqrt for L2 it is
+ *             already the norm), up to trace_cap entries
+ * Returns 0, or -1 on invalid arguments. */
+int nko_pagerank(uint64_t z, const uint64_t *in_ptr, const uint32_t *in_col, const double *in_w,
+                 const double *wdeg, const uint32_t *outdeg, const uint8_t *exists,
+                 const double *teleport, const nko_params *p, double *scores, uint64_t *iterations,
+                 double *max_out, double *trace, uint64_t trace_cap);
+
+/* Centrality::ranking() (Centrality.cpp:29-41): existing nodes sorted by
+ * score descending, ties by node id ascending. ids/vals get n entries. */
+int nko_ranking(uint64_t z, const double *scores, const uint8_t *exists, uint64_t *ids,
+                double *vals);
+
+/* FP64 host adjoint for the differentiable form (no reference counterpart).
+ * Forward fixed point, with t the teleport distribution (uniform 1/n when
+ * teleport is NULL), m the sink mask and A[u,v] = w(v->u)/wdeg[v]:
+ *     x = d*(A x + [distribute_sinks] (m.x) t) + (1-d) t,   p = x / sum(x)
+ * (the final division is PageRank.cpp:75-80). For a loss L with g = dL/dp:
+ *     gbar = (g - (g.p) 1) / sum(x)
+ *     lam  = gbar + d*(A^T lam + [distribute_sinks] m (t.lam))   (Jacobi, L1 tol)
+ *     c    = A^T lam
+ *     dL/dw(v->u) = d * (x[v]/wdeg[v]) * (lam[u] - c[v])
+ *     dL/dt[u]    = (d*[distribute_sinks](m.x) + 1 - d) * lam[u]
+ * x is the converged, un-normalised vector. grad_w is indexed like in_col.
+ * Returns the number of Jacobi sweeps, or -1 on invalid arguments. */
+int64_t nko_pagerank_adjoint(uint64_t z, const uint64_t *in_ptr, const uint32_t *in_col,
+                             const double *in_w, const double *wdeg, const uint32_t *outdeg,
+                             const double *teleport, double damp, int distribute_sinks,
+                             const double *x, const double *g, double tol, uint64_t max_iter,
+                             double *lam, double *grad_w, double *grad_t);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,190 @@
+// Test infrastructure only (the oracle): a small extern "C" driver around the
+// reference's own PageRank, compiled together with the reference sources by
+// oracle/Makefile into oracle/_ref/libnkref.so. Nothing in the product path
+// links or loads this library; only the tests, the smoke check and the CPU
+// baseline of bench.py do.
+//
+// It builds a NetworKit::Graph through Graph::addEdge in the caller's edge
+// order (the in-edge order of each node is insertion order, Graph.cpp:549-596),
+// runs NetworKit::PageRank::run() (PageRank.cpp:20-104) and hands back scores,
+// the iteration count, maximum() and ranking() (Centrality.cpp:29-41).
+// The SNAP, METIS and GML readers are exported so that fixtures can be
+// produced with exactly the reference's node numbering and edge order.
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <omp.h>
+
+#include <networkit/centrality/PageRank.hpp>
+#include <networkit/graph/Graph.hpp>
+#include <networkit/io/GMLGraphReader.hpp>
+#include <networkit/io/METISGraphReader.hpp>
+#include <networkit/io/SNAPGraphReader.hpp>
+
+namespace {
+thread_local std::string g_err;
+
+struct RefGraph {
+    std::unique_ptr<NetworKit::Graph> G;
+};
+
+int fail(const std::exception &e) {
+    g_err = e.what();
+    return -1;
+}
+} // namespace
+
+extern "C" {
+
+const char *nkref_last_error(void) { return g_err.c_str(); }
+
+// Build a graph from an ordered edge list. exists (nullable, length n) marks
+// nodes to delete after insertion (deleted nodes must have no edges).
+int nkref_graph_create(void **out, uint64_t n, int weighted, int directed, uint64_t m,
+                       const uint32_t *src, const uint32_t *dst, const double *w,
+                       const uint8_t *exists) {
+    try {
+        auto *h = new RefGraph();
+        h->G.reset(new NetworKit::Graph(n, weighted != 0, directed != 0));
+        for (uint64_t e = 0; e < m; ++e) {
+            h->G->addEdge(src[e], dst[e], w ? w[e] : NetworKit::defaultEdgeWeight);
+        }
+        if (exists) {
+            for (uint64_t v = 0; v < n; ++v)
+                if (!exists[v])
+                    h->G->removeNode(v);
+        }
+        *out = h;
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+void nkref_graph_destroy(void *g) { delete static_cast<RefGraph *>(g); }
+
+uint64_t nkref_graph_num_nodes(void *g) { return static_cast<RefGraph *>(g)->G->numberOfNodes(); }
+uint64_t nkref_graph_upper_node_id(void *g) {
+    return static_cast<RefGraph *>(g)->G->upperNodeIdBound();
+}
+uint64_t nkref_graph_num_edges(void *g) { return static_cast<RefGraph *>(g)->G->numberOfEdges(); }
+
+// Run the reference PageRank. norm: 0 = L1Norm, 1 = L2Norm (PageRank.hpp:31).
+// scores_out has upperNodeIdBound() entries; ranking_* (nullable) have
+// numberOfNodes() entries. nthreads <= 0 keeps the OpenMP default.
+int nkref_pagerank(void *g, double damp, double tol, int normalized, int norm,
+                   uint64_t max_iterations, int nthreads, double *scores_out,
+                   uint64_t *iterations_out, double *max_out, uint64_t *ranking_ids_out,
+                   double *ranking_vals_out, double *run_seconds_out) {
+    try {
+        if (nthreads > 0)
+            omp_set_num_threads(nthreads);
+        auto &G = *static_cast<RefGraph *>(g)->G;
+        NetworKit::PageRank pr(G, damp, tol, normalized != 0);
+        pr.norm = norm == 0 ? NetworKit::PageRank::L1Norm : NetworKit::PageRank::L2Norm;
+        pr.maxIterations = max_iterations;
+        auto t0 = std::chrono::steady_clock::now();
+        pr.run();
+        auto t1 = std::chrono::steady_clock::now();
+        if (run_seconds_out)
+            *run_seconds_out = std::chrono::duration<double>(t1 - t0).count();
+        const auto &s = pr.scores();
+        std::memcpy(scores_out, s.data(), s.size() * sizeof(double));
+        if (iterations_out)
+            *iterations_out = pr.numberOfIterations();
+        if (max_out)
+            *max_out = pr.maximum();
+        if (ranking_ids_out || ranking_vals_out) {
+            auto r = pr.ranking();
+            for (size_t i = 0; i < r.size(); ++i) {
+                if (ranking_ids_out)
+                    ranking_ids_out[i] = r[i].first;
+                if (ranking_vals_out)
+                    ranking_vals_out[i] = r[i].second;
+            }
+        }
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// Read a file with the reference's SNAP (kind 0), METIS (kind 1) or GML
+// (kind 2) reader into a graph handle.
+int nkref_graph_read(void **out, const char *path, int kind, int directed) {
+    try {
+        auto *h = new RefGraph();
+        h->G.reset(new NetworKit::Graph(
+            kind == 0   ? NetworKit::SNAPGraphReader(directed != 0).read(path)
+            : kind == 1 ? NetworKit::METISGraphReader().read(path)
+                        : NetworKit::GMLGraphReader().read(path)));
+        *out = h;
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+int nkref_graph_is_directed(void *g) { return static_cast<RefGraph *>(g)->G->isDirected(); }
+int nkref_graph_is_weighted(void *g) { return static_cast<RefGraph *>(g)->G->isWeighted(); }
+
+// Number of stored out-arcs (undirected: both directions, self-loops once) and
+// in-arcs (directed only; 0 otherwise).
+void nkref_graph_arc_counts(void *g, uint64_t *out_arcs, uint64_t *in_arcs) {
+    auto &G = *static_cast<RefGraph *>(g)->G;
+    uint64_t o = 0, i = 0;
+    for (uint64_t u = 0; u < G.upperNodeIdBound(); ++u) {
+        o += G.degreeOut(u);
+        if (G.isDirected())
+            i += G.degreeIn(u);
+    }
+    *out_arcs = o;
+    *in_arcs = i;
+}
+
+// Export the adjacency in storage order: per node u its out-list outEdges[u]
+// (with weights when out_w is non-null) and, for directed graphs, its in-list
+// inEdges[u] (with weights when in_w is non-null). exists_out (nullable) gets
+// the node-existence mask. Buffers are sized with nkref_graph_arc_counts.
+int nkref_graph_export(void *g, uint64_t *out_ptr, uint32_t *out_adj, double *out_w,
+                       uint64_t *in_ptr, uint32_t *in_adj, double *in_w, uint8_t *exists_out) {
+    try {
+        auto &G = *static_cast<RefGraph *>(g)->G;
+        const uint64_t z = G.upperNodeIdBound();
+        uint64_t o = 0, i = 0;
+        out_ptr[0] = 0;
+        if (in_ptr)
+            in_ptr[0] = 0;
+        for (uint64_t u = 0; u < z; ++u) {
+            if (exists_out)
+                exists_out[u] = G.hasNode(u) ? 1 : 0;
+            G.forNeighborsOf(u, [&](NetworKit::node v, NetworKit::edgeweight ew) {
+                out_adj[o] = static_cast<uint32_t>(v);
+                if (out_w)
+                    out_w[o] = ew;
+                ++o;
+            });
+            out_ptr[u + 1] = o;
+            if (G.isDirected() && in_ptr) {
+                G.forInNeighborsOf(u, [&](NetworKit::node v, NetworKit::edgeweight ew) {
+                    in_adj[i] = static_cast<uint32_t>(v);
+                    if (in_w)
+                        in_w[i] = ew;
+                    ++i;
+                });
+                in_ptr[u + 1] = i;
+            }
+        }
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+} // extern "C"
