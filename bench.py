@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""PageRank benchmark: GTEPS per iteration and HBM roofline on R-MAT scale 24.
+
+Workload (one step): PageRank run to convergence on the directed R-MAT graph
+scale 24 / edgefactor 16 / (a, b, c, d) = (0.57, 0.19, 0.19, 0.05), duplicates
+and self-loops removed, unweighted; damp 0.85, tol 1e-10, L1 norm, FP64
+(the reference's arithmetic), reference sink semantics. The graph is resident
+in HBM before the timed region (value); the e2e figure repeats the same run
+through the C ABI from pinned host arrays, with the upload and the score
+read-back inside the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 (under torchrun) runs N replicas of the same workload, one per GPU: the
+plain single-graph path has no partitioned form here, so scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SCALE = 24
+EDGEFACTOR = 16
+RMAT = (0.57, 0.19, 0.19)
+SEED = 42
+DAMP = 0.85
+TOL = 1e-10
+NORM_L1 = 0
+METRIC = "PageRank GTEPS/iter (R-MAT scale 24, FP64)"
+UNIT = "GTEPS/iter"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=SCALE)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cache", default=os.path.join(tempfile.gettempdir(), "nk_b200_graphs"))
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def graph_path(cache, scale):
+    return os.path.join(cache, f"rmat{scale}_ef{EDGEFACTOR}_s{SEED}.npz")
+
+
+def make_graph(scale, cache, rank, barrier):
+    """Generate once (rank 0), cache on local disk, load everywhere."""
+    from networkit_b200 import generators
+    from networkit_b200.graph import InCSR
+
+    path = graph_path(cache, scale)
+    if rank == 0 and not os.path.exists(path):
+        csr = generators.rmat_directed(scale, EDGEFACTOR, *RMAT, seed=SEED)
+        os.makedirs(cache, exist_ok=True)
+        tmp = path + f".tmp{os.getpid()}.npz"
+        np.savez(tmp, in_ptr=csr.in_ptr, in_col=csr.in_col, outdeg=csr.outdeg)
+        os.replace(tmp, path)
+    barrier()
+    d = np.load(path)
+    outdeg = d["outdeg"]
+    z = outdeg.shape[0]
+    return InCSR(z, z, d["in_ptr"], d["in_col"], None, outdeg.astype(np.float64), outdeg, None,
+                 True)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[5 + i].strip().lower() == "active"})
+        load = [s for s in sm if smax and s >= 0.3 * max(smax)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel_tag):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/<kernel_tag>.txt, line 'traffic_bytes_per_launch: X')."""
+    p = os.path.join(ROOT, "profiles", kernel_tag + ".txt")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline_port(csr, nthreads, target_s=15.0):
+    """The oracle's C restatement on the host cores, over a bounded number of
+    iterations of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    t0 = time.perf_counter()
+    oracle.pagerank(csr, damp=DAMP, tol=TOL, norm=NORM_L1, max_iterations=1, nthreads=nthreads)
+    t1 = time.perf_counter() - t0
+    iters = int(max(2, min(20, target_s / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    r = oracle.pagerank(csr, damp=DAMP, tol=TOL, norm=NORM_L1, max_iterations=iters,
+                        nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return {"value": csr.arcs * r.iterations / dt / 1e9, "unit": UNIT, "cores": nthreads,
+            "kind": "port",
+            "sample": f"{r.iterations} iterations of the same R-MAT scale-{int(np.log2(csr.z))} "
+                      f"FP64 run (oracle C restatement, OpenMP rows), {dt:.1f} s"}
+
+
+def run_reference_arm(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libnkref.so (reference PageRank built from the "
+                          "reference sources) is not present"}))
+        return
+    cores = os.cpu_count() or 1
+    csr = make_graph(args.scale, args.cache, 0, lambda: None)
+    rows = np.repeat(np.arange(csr.z, dtype=np.uint32), np.diff(csr.in_ptr).astype(np.int64))
+    # Inserting the arcs row by row reproduces every in-list in the same
+    # order (unweighted graph: out-list order does not enter the result).
+    g = oracle.RefGraph.from_edges(csr.z, csr.in_col, rows, directed=True)
+    del rows
+    probe = g.pagerank(damp=DAMP, tol=TOL, norm=NORM_L1, max_iterations=1, nthreads=cores,
+                       want_ranking=False)
+    iters = int(max(2, min(20, 3.0 / max(probe["seconds"], 1e-3))))
+    times, its = [], []
+    for i in range(args.warmup + args.steps):
+        r = g.pagerank(damp=DAMP, tol=TOL, norm=NORM_L1, max_iterations=iters, nthreads=cores,
+                       want_ranking=False)
+        if i >= args.warmup:
+            times.append(r["seconds"])
+            its.append(r["iterations"])
+    total = sum(times)
+    value = csr.arcs * sum(its) / total / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"pagerank_rmat{args.scale}_fp64", "scale": args.scale,
+                   "edgefactor": EDGEFACTOR, "n": csr.z, "arcs": csr.arcs, "damp": DAMP,
+                   "tol": TOL, "norm": "L1", "iterations_per_step": iters},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{iters} iterations of NetworKit::PageRank::run() per step "
+                                   f"(maxIterations={iters}) on the same graph"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    rank, world, local = dist_env()
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+        def barrier():
+            dist.barrier()
+    else:
+        def barrier():
+            pass
+
+    from networkit_b200 import _capi
+
+    csr = make_graph(args.scale, args.cache, rank, barrier)
+    arcs, n = csr.arcs, csr.z
+    dg = _capi.DeviceGraph(csr, device=local)
+    info = dg.info()
+    p = dg.params(DAMP, TOL, NORM_L1, False, False, _capi.NKG_PREC_FP64, _capi.UINT64_MAX)
+    d_out = torch.empty(n, dtype=torch.float64, device=f"cuda:{local}")
+
+    for _ in range(max(args.warmup, 3)):
+        dg.run_device(p, d_out.data_ptr())
+
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dev_ms, iters, launches = [], [], 0
+        for _ in range(args.steps):
+            it, mx, st = dg.run_device(p, d_out.data_ptr())
+            dev_ms.append(st["ms_total"])
+            iters.append(it)
+            launches += st["kernel_launches"]
+        torch.cuda.synchronize()
+        barrier()
+        wall = time.perf_counter() - t0
+    clocks = clk.summary()
+
+    total_ms = float(sum(dev_ms))
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * arcs * sum(iters) / (total_ms / 1e3) / 1e9
+
+    # Roofline of the dominant kernel (the sweep), timed alone with events.
+    ms_kernel, ms_iter = dg.profile_sweeps(_capi.NKG_PREC_FP64, 20)
+    bytes_sweep = st["bytes_per_sweep_fp64"]
+    peak, peak_kind = measured_peak_hbm()
+    achieved = bytes_sweep / (ms_kernel / 1e3) / 1e9
+
+    # End to end through the C ABI: pinned host CSR -> create -> run -> scores.
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    from networkit_b200.graph import InCSR
+
+    hcsr = InCSR(csr.z, csr.n, pin(csr.in_ptr), pin(csr.in_col), None, pin(csr.wdeg),
+                 csr.outdeg, None, True)
+    e2e_t, e2e_it = [], []
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        g2 = _capi.DeviceGraph(hcsr, device=local)
+        sc, it2, _, _ = g2.run(p)
+        g2.close()
+        dt = time.perf_counter() - t1
+        if i > 0:  # first call warms the allocator and the module
+            e2e_t.append(dt)
+            e2e_it.append(it2)
+    e2e_value = world * arcs * sum(e2e_it) / sum(e2e_t) / 1e9
+    h2d = 8 * (n + 1) + 4 * arcs
+    d2h = 8 * n
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(csr, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"pagerank_rmat{args.scale}_fp64", "scale": args.scale,
+                       "edgefactor": EDGEFACTOR, "abcd": [*RMAT, round(1 - sum(RMAT), 6)],
+                       "n": n, "arcs": arcs, "sinks": info["sinks"], "damp": DAMP, "tol": TOL,
+                       "norm": "L1", "iterations": iters[0], "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (CSR 1.1 GB)",
+                       "wall_s": wall, "ms_create": info["ms_create"]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profiled_traffic(
+                             f"sweep_fp64_rmat{args.scale}"),
+                         "kernel": "sweep_kernel<double> (merge-path pull SpMV)",
+                         "bytes_per_launch": bytes_sweep, "ms_per_launch": ms_kernel,
+                         "ms_per_iteration": ms_iter, "peak_source": peak_kind},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * sum(e2e_t) / len(e2e_t)},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    dg.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,177 @@
+/*
+ * nkgpu.h - C ABI of the B200 PageRank library (libnkgpu.so).
+ *
+ * Drop-in boundary for NetworKit's PageRank path. The reference reaches its
+ * C++ through Cython (networkit/centrality.pyx:1989-2037 -> PageRank.hpp:28-75);
+ * a Cython class replacing it binds the functions below (INTEGRATION.md shows
+ * the binding). Plain pointers and sizes only; host arrays are caller-owned and
+ * copied; device buffers are owned by the opaque handle.
+ *
+ * Return codes: 0 on success, a negative NKG_ERR_* otherwise; the message of
+ * the last failure on the calling thread is nkg_last_error(). The Python layer
+ * raises RuntimeError(nkg_last_error()) like the reference's `except +`
+ * translation of std::runtime_error.
+ */
+#ifndef NKGPU_H
+#define NKGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NKG_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define NKG_API __attribute__((visibility("default")))
+#else
+#define NKG_API
+#endif
+
+enum {
+    NKG_OK = 0,
+    NKG_ERR_INVALID_ARG = -1, /* bad sizes, pointers, CSR contents */
+    NKG_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+    NKG_ERR_OOM = -3,         /* device allocation failed */
+    NKG_ERR_CANCELLED = -4,   /* nkg_cancel() was called during the run */
+    NKG_ERR_TIMEOUT = -5,     /* a bounded device-side wait gave up */
+    NKG_ERR_NOT_RUN = -6,     /* result requested before a run */
+    NKG_ERR_NO_DEVICE = -7    /* no usable CUDA device */
+};
+
+/* PageRank::Norm (PageRank.hpp:31): L1Norm = 0, L2Norm = 1. */
+enum { NKG_NORM_L1 = 0, NKG_NORM_L2 = 1 };
+
+/* Arithmetic of the iteration. FP64 keeps the reference's arithmetic
+ * (PageRank.cpp:56-66). FP32_REFINE runs the sweeps in FP32 and corrects the
+ * iterate with FP64 residual sweeps until the FP64 stopping test holds. */
+enum { NKG_PREC_FP64 = 0, NKG_PREC_FP32_REFINE = 1, NKG_PREC_FP32 = 2 };
+
+typedef struct nkg_graph nkg_graph;
+
+/* PageRank(G, damp, tol, normalized) (PageRank.hpp:40, centrality.pyx:2006)
+ * plus the public fields norm / maxIterations (PageRank.hpp:64,67) and the
+ * distributeSinks flag (redistribute the mass of out-degree-0 nodes uniformly
+ * every iteration; 0 keeps the reference's semantics). */
+typedef struct {
+    double damp;
+    double tol;
+    int32_t norm;
+    int32_t normalized;
+    int32_t distribute_sinks;
+    int32_t precision;
+    uint64_t max_iterations; /* UINT64_MAX = unbounded (the reference default) */
+} nkg_pr_params;
+
+/* Per-run statistics (device timings from CUDA events on the handle's stream). */
+typedef struct {
+    uint64_t iterations;       /* numberOfIterations() */
+    double residual;           /* last residual norm (L1 sum or L2 sqrt) */
+    double sink_mass;          /* sum of scores of out-degree-0 nodes, last iterate */
+    double ms_total;           /* device time of the whole run */
+    double ms_iterations;      /* device time of the iteration loop */
+    uint64_t kernel_launches;  /* kernels this library launched for the run */
+    uint64_t fp64_sweeps;      /* SpMV sweeps in FP64 */
+    uint64_t fp32_sweeps;      /* SpMV sweeps in FP32 */
+    uint64_t bytes_per_sweep_fp64; /* algorithmic bytes of one FP64 sweep */
+    uint64_t bytes_per_sweep_fp32; /* algorithmic bytes of one FP32 sweep */
+} nkg_stats;
+
+/* Graph shape after upload. */
+typedef struct {
+    uint64_t z;          /* upperNodeIdBound */
+    uint64_t n;          /* numberOfNodes */
+    uint64_t arcs;       /* in-arcs traversed per sweep */
+    uint64_t sinks;      /* existing nodes with out-degree 0 */
+    uint64_t tiles;      /* merge-path tiles of the sweep kernel */
+    int32_t weighted;
+    int32_t directed;
+    int32_t device;
+    int32_t reordered;
+    double ms_create;    /* device time of nkg_graph_create after the copies */
+} nkg_graph_info;
+
+/* Options of nkg_graph_create_ex. */
+typedef struct {
+    int32_t device;      /* CUDA device ordinal (-1: current device) */
+    int32_t reorder;     /* 1: relabel nodes by out-degree (default); 0: keep ids */
+} nkg_graph_options;
+
+/* Upload a graph given as its in-adjacency CSR.
+ * Replaces constructing NetworKit::Graph + the per-run deg[] setup
+ * (PageRank.cpp:29-30) on the GPU side; the in-adjacency is what
+ * Graph::forInEdgesOf visits (Graph.hpp:1917-1938): for directed graphs the
+ * in-lists, for undirected graphs the neighbour lists (self-loops once).
+ *   z           upperNodeIdBound (node ids 0..z-1), 1 <= z < 2^32
+ *   arcs        in_row_ptr[z], < 2^32
+ *   in_row_ptr  z+1 offsets, non-decreasing, in_row_ptr[0] = 0
+ *   in_col      source node of each in-arc, < z and existing
+ *   in_w        in-arc weights (NULL: unweighted, every weight 1.0)
+ *   out_wdeg    weightedDegree(u) (Graph.cpp:426-452); read only for weighted
+ *               graphs (for unweighted graphs it is the out-degree, which
+ *               the library counts itself). May be NULL when in_w is NULL.
+ *   exists      node-existence mask (NULL: all nodes exist); deleted nodes
+ *               must have no arcs
+ *   directed    informational (the CSR already encodes the direction) */
+NKG_API int nkg_graph_create(nkg_graph **out, uint64_t z, uint64_t arcs, const uint64_t *in_row_ptr,
+                     const uint32_t *in_col, const double *in_w, const double *out_wdeg,
+                     const uint8_t *exists, int directed);
+NKG_API int nkg_graph_create_ex(nkg_graph **out, uint64_t z, uint64_t arcs, const uint64_t *in_row_ptr,
+                        const uint32_t *in_col, const double *in_w, const double *out_wdeg,
+                        const uint8_t *exists, int directed, const nkg_graph_options *opts);
+NKG_API void nkg_graph_destroy(nkg_graph *g);
+NKG_API int nkg_graph_get_info(const nkg_graph *g, nkg_graph_info *info);
+
+/* PageRank::run() (PageRank.cpp:20-104) followed by scores()
+ * (Centrality.cpp:43-46) and maximum() (PageRank.cpp:106-108).
+ * scores_out: host array of z doubles (non-existent ids get 1/n, as the
+ * reference leaves them). Any of iterations_out, max_out, stats may be NULL.
+ * Blocks until the run has finished. */
+NKG_API int nkg_pagerank_run(nkg_graph *g, const nkg_pr_params *p, double *scores_out,
+                     uint64_t *iterations_out, double *max_out, nkg_stats *stats);
+
+/* Same as nkg_pagerank_run, but the z scores are written to DEVICE memory
+ * (d_scores_out, on the graph's device); nothing crosses PCIe but the
+ * iteration status. */
+NKG_API int nkg_pagerank_run_device(nkg_graph *g, const nkg_pr_params *p, double *d_scores_out,
+                            uint64_t *iterations_out, double *max_out, nkg_stats *stats);
+
+/* Personalised PageRank with an explicit teleport distribution t (host array
+ * of z doubles, summing to 1 over existing nodes): the uniform (1-damp)/n of
+ * PageRank.cpp:25,65 becomes (1-damp)*t[u] and, with distribute_sinks, the
+ * sink mass is spread along t. Otherwise identical to nkg_pagerank_run. */
+NKG_API int nkg_pagerank_run_teleport(nkg_graph *g, const nkg_pr_params *p, const double *teleport,
+                              double *scores_out, uint64_t *iterations_out, double *max_out,
+                              nkg_stats *stats);
+
+/* Centrality::ranking() (Centrality.cpp:29-41): existing nodes sorted by score
+ * descending, ties by node id ascending. scores: host array of z doubles (any
+ * scores, e.g. from nkg_pagerank_run); ids_out / vals_out: n entries each. */
+NKG_API int nkg_ranking(nkg_graph *g, const double *scores, uint64_t *ids_out, double *vals_out);
+
+/* Ask a running nkg_pagerank_run* on this handle to stop (the reference's
+ * SIGINT check, PageRank.cpp:55 / SignalHandling.cpp:62-66). Safe from any
+ * thread or a signal handler; the run returns NKG_ERR_CANCELLED. */
+NKG_API void nkg_cancel(nkg_graph *g);
+
+/* Diagnostic, no reference counterpart: run `sweeps` iterations (precision
+ * NKG_PREC_FP64 or NKG_PREC_FP32, the stopping test disabled) on the
+ * resident graph with CUDA events on the handle's stream around every
+ * launch of the sweep kernel. Reports the mean duration of one sweep-kernel
+ * launch and of one whole iteration (sweep + fix-up). bench.py derives the
+ * roofline figure from it. */
+NKG_API int nkg_profile_sweeps(nkg_graph *g, int precision, int sweeps, double *ms_sweep_kernel,
+                               double *ms_iteration);
+
+/* Message of the last failure on the calling thread ("" if none). */
+NKG_API const char *nkg_last_error(void);
+
+/* Library ABI version (NKG_ABI_VERSION). */
+NKG_API int nkg_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NKGPU_H */

@@ -1,0 +1,236 @@
+"""ctypes binding of libnkgpu.so (include/nkgpu.h).
+
+This plays the role of the Cython declarations a NetworKit build would use
+(``cdef extern from "nkgpu.h"``); INTEGRATION.md shows that Cython form. The
+library is loaded from the package's ``_lib`` directory; if it is missing the
+import fails loudly - there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libnkgpu.so")
+
+NKG_OK = 0
+NKG_ERR_INVALID_ARG = -1
+NKG_ERR_CUDA = -2
+NKG_ERR_OOM = -3
+NKG_ERR_CANCELLED = -4
+NKG_ERR_TIMEOUT = -5
+NKG_ERR_NOT_RUN = -6
+NKG_ERR_NO_DEVICE = -7
+
+NKG_PREC_FP64 = 0
+NKG_PREC_FP32_REFINE = 1
+NKG_PREC_FP32 = 2
+
+UINT64_MAX = 2**64 - 1
+
+
+class PRParams(C.Structure):
+    _fields_ = [
+        ("damp", C.c_double),
+        ("tol", C.c_double),
+        ("norm", C.c_int32),
+        ("normalized", C.c_int32),
+        ("distribute_sinks", C.c_int32),
+        ("precision", C.c_int32),
+        ("max_iterations", C.c_uint64),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_uint64),
+        ("residual", C.c_double),
+        ("sink_mass", C.c_double),
+        ("ms_total", C.c_double),
+        ("ms_iterations", C.c_double),
+        ("kernel_launches", C.c_uint64),
+        ("fp64_sweeps", C.c_uint64),
+        ("fp32_sweeps", C.c_uint64),
+        ("bytes_per_sweep_fp64", C.c_uint64),
+        ("bytes_per_sweep_fp32", C.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [
+        ("z", C.c_uint64),
+        ("n", C.c_uint64),
+        ("arcs", C.c_uint64),
+        ("sinks", C.c_uint64),
+        ("tiles", C.c_uint64),
+        ("weighted", C.c_int32),
+        ("directed", C.c_int32),
+        ("device", C.c_int32),
+        ("reordered", C.c_int32),
+        ("ms_create", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class GraphOptions(C.Structure):
+    _fields_ = [("device", C.c_int32), ("reorder", C.c_int32)]
+
+
+_u64p = C.POINTER(C.c_uint64)
+_u32p = C.POINTER(C.c_uint32)
+_u8p = C.POINTER(C.c_uint8)
+_f64p = C.POINTER(C.c_double)
+_vp = C.c_void_p
+
+# name -> (restype, argtypes); the exported surface of include/nkgpu.h
+SIGNATURES = {
+    "nkg_abi_version": (C.c_int, []),
+    "nkg_last_error": (C.c_char_p, []),
+    "nkg_graph_create": (C.c_int, [C.POINTER(_vp), C.c_uint64, C.c_uint64, _u64p, _u32p, _f64p,
+                                   _f64p, _u8p, C.c_int]),
+    "nkg_graph_create_ex": (C.c_int, [C.POINTER(_vp), C.c_uint64, C.c_uint64, _u64p, _u32p,
+                                      _f64p, _f64p, _u8p, C.c_int, C.POINTER(GraphOptions)]),
+    "nkg_graph_destroy": (None, [_vp]),
+    "nkg_graph_get_info": (C.c_int, [_vp, C.POINTER(GraphInfo)]),
+    "nkg_pagerank_run": (C.c_int, [_vp, C.POINTER(PRParams), _f64p, _u64p, _f64p,
+                                   C.POINTER(Stats)]),
+    "nkg_pagerank_run_device": (C.c_int, [_vp, C.POINTER(PRParams), _vp, _u64p, _f64p,
+                                          C.POINTER(Stats)]),
+    "nkg_pagerank_run_teleport": (C.c_int, [_vp, C.POINTER(PRParams), _f64p, _f64p, _u64p,
+                                            _f64p, C.POINTER(Stats)]),
+    "nkg_ranking": (C.c_int, [_vp, _f64p, _u64p, _f64p]),
+    "nkg_cancel": (None, [_vp]),
+    "nkg_profile_sweeps": (C.c_int, [_vp, C.c_int, C.c_int, _f64p, _f64p]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libnkgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m networkit_b200.build` "
+                "(the PageRank path has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class NkgError(RuntimeError):
+    """A failed libnkgpu call (RuntimeError, like the reference's `except +`)."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+def check(rc: int) -> None:
+    if rc != NKG_OK:
+        msg = lib().nkg_last_error().decode(errors="replace")
+        raise NkgError(rc, msg)
+
+
+def ptr(a, t):
+    if a is None:
+        return None
+    return a.ctypes.data_as(t)
+
+
+class DeviceGraph:
+    """Owning wrapper of an nkg_graph handle."""
+
+    def __init__(self, csr, device: int = -1, reorder: bool = True):
+        L = lib()
+        h = _vp()
+        in_ptr = np.ascontiguousarray(csr.in_ptr, np.uint64)
+        in_col = np.ascontiguousarray(csr.in_col, np.uint32)
+        in_w = None if csr.in_w is None else np.ascontiguousarray(csr.in_w, np.float64)
+        wdeg = np.ascontiguousarray(csr.wdeg, np.float64)
+        ex = None if csr.exists is None else np.ascontiguousarray(csr.exists, np.uint8)
+        opts = GraphOptions(int(device), 1 if reorder else 0)
+        check(L.nkg_graph_create_ex(C.byref(h), int(csr.z), int(in_col.shape[0]),
+                                    ptr(in_ptr, _u64p), ptr(in_col, _u32p), ptr(in_w, _f64p),
+                                    ptr(wdeg, _f64p), ptr(ex, _u8p), int(bool(csr.directed)),
+                                    C.byref(opts)))
+        self.h = h
+        self.z = int(csr.z)
+        self.n = int(csr.n)
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().nkg_graph_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        gi = GraphInfo()
+        check(lib().nkg_graph_get_info(self.h, C.byref(gi)))
+        return gi.as_dict()
+
+    @staticmethod
+    def params(damp, tol, norm, normalized, distribute_sinks, precision, max_iterations):
+        return PRParams(float(damp), float(tol), int(norm), int(bool(normalized)),
+                        int(bool(distribute_sinks)), int(precision), int(max_iterations))
+
+    def run(self, p: PRParams, teleport=None):
+        """Run to convergence; returns (scores[z], iterations, maximum, stats)."""
+        L = lib()
+        scores = np.empty(self.z, np.float64)
+        it = C.c_uint64(0)
+        mx = C.c_double(0.0)
+        st = Stats()
+        if teleport is None:
+            check(L.nkg_pagerank_run(self.h, C.byref(p), ptr(scores, _f64p), C.byref(it),
+                                     C.byref(mx), C.byref(st)))
+        else:
+            t = np.ascontiguousarray(teleport, np.float64)
+            if t.shape != (self.z,):
+                raise ValueError("teleport must have upperNodeIdBound() entries")
+            check(L.nkg_pagerank_run_teleport(self.h, C.byref(p), ptr(t, _f64p),
+                                              ptr(scores, _f64p), C.byref(it), C.byref(mx),
+                                              C.byref(st)))
+        return scores, int(it.value), float(mx.value), st.as_dict()
+
+    def run_device(self, p: PRParams, d_out_ptr: int):
+        """Run with the scores written to device memory at d_out_ptr."""
+        it = C.c_uint64(0)
+        mx = C.c_double(0.0)
+        st = Stats()
+        check(lib().nkg_pagerank_run_device(self.h, C.byref(p), _vp(d_out_ptr), C.byref(it),
+                                            C.byref(mx), C.byref(st)))
+        return int(it.value), float(mx.value), st.as_dict()
+
+    def ranking(self, scores):
+        s = np.ascontiguousarray(scores, np.float64)
+        ids = np.empty(self.n, np.uint64)
+        vals = np.empty(self.n, np.float64)
+        check(lib().nkg_ranking(self.h, ptr(s, _f64p), ptr(ids, _u64p), ptr(vals, _f64p)))
+        return ids, vals
+
+    def cancel(self):
+        lib().nkg_cancel(self.h)
+
+    def profile_sweeps(self, precision: int, sweeps: int):
+        """(ms per sweep-kernel launch, ms per iteration) from CUDA events."""
+        a, b = C.c_double(0.0), C.c_double(0.0)
+        check(lib().nkg_profile_sweeps(self.h, int(precision), int(sweeps), C.byref(a),
+                                       C.byref(b)))
+        return float(a.value), float(b.value)

@@ -1,0 +1,85 @@
+"""Build recipe of the native libraries (in-tree, so they travel with the repo).
+
+* ``_lib/libnkgpu.so``  - the CUDA PageRank library behind include/nkgpu.h,
+  compiled for sm_100a only.
+* ``_lib/libnkgen.so``  - host-side synthetic graph generators (C++/OpenMP),
+  used by the benchmarks and tests to make their inputs.
+
+``python -m networkit_b200.build`` rebuilds whatever is out of date.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIBDIR = os.path.join(PKG, "_lib")
+INCLUDE = os.path.join(ROOT, "include")
+
+GPU_LIB = os.path.join(LIBDIR, "libnkgpu.so")
+GEN_LIB = os.path.join(LIBDIR, "libnkgen.so")
+
+GPU_SOURCES = ["nkgpu.cu"]
+GPU_HEADERS = ["common.cuh", "sweep.cuh", "graph.hpp"]
+GEN_SOURCES = ["graphgen.cpp"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    cand = os.environ.get("NVCC") or shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    return cand
+
+
+def _host_cxx() -> str:
+    # The system g++ ships libgomp; an inherited CXX may not.
+    return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
+
+
+def _stale(target, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_gpu(force: bool = False, verbose: bool = False) -> str:
+    srcs = [os.path.join(CSRC, s) for s in GPU_SOURCES]
+    deps = srcs + [os.path.join(CSRC, h) for h in GPU_HEADERS] + [os.path.join(INCLUDE, "nkgpu.h"),
+                                                                  __file__]
+    if not force and not _stale(GPU_LIB, deps):
+        return GPU_LIB
+    os.makedirs(LIBDIR, exist_ok=True)
+    cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
+           "-Xcompiler", "-fvisibility=hidden", "-ccbin", _host_cxx(),
+           "-I" + INCLUDE, "-I" + CSRC, "-o", GPU_LIB + ".tmp", *srcs]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    subprocess.run(cmd, check=True)
+    os.replace(GPU_LIB + ".tmp", GPU_LIB)
+    return GPU_LIB
+
+
+def build_gen(force: bool = False) -> str:
+    srcs = [os.path.join(CSRC, s) for s in GEN_SOURCES]
+    if not force and not _stale(GEN_LIB, srcs + [__file__]):
+        return GEN_LIB
+    os.makedirs(LIBDIR, exist_ok=True)
+    cmd = [_host_cxx(), "-std=c++17", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared",
+           "-o", GEN_LIB + ".tmp", *srcs]
+    subprocess.run(cmd, check=True)
+    os.replace(GEN_LIB + ".tmp", GEN_LIB)
+    return GEN_LIB
+
+
+def build_all(force: bool = False, verbose: bool = False) -> None:
+    build_gen(force)
+    build_gpu(force, verbose)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv, verbose="-v" in sys.argv)

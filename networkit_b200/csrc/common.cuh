@@ -1,0 +1,181 @@
+// Shared host/device helpers of libnkgpu: error plumbing, RAII device
+// buffers, warp/block reductions with a fixed combination order.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+#include "nkgpu.h"
+
+namespace nkg {
+
+// Internal failure carrying an NKG_ERR_* code; the C-ABI wrappers turn it into
+// a return code plus the thread-local message.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string &m);
+
+inline void cuda_check(cudaError_t e, const char *what, const char *file, int line) {
+    if (e == cudaSuccess)
+        return;
+    const int code = (e == cudaErrorMemoryAllocation) ? NKG_ERR_OOM
+                     : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+                         ? NKG_ERR_NO_DEVICE
+                         : NKG_ERR_CUDA;
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    throw Error(code, buf);
+}
+
+#define NKG_CUDA(call) ::nkg::cuda_check((call), #call, __FILE__, __LINE__)
+
+inline void require(bool ok, const std::string &msg) {
+    if (!ok)
+        throw Error(NKG_ERR_INVALID_ARG, msg);
+}
+
+// Owning device allocation (cudaMalloc/cudaFree). Sizes are in elements; the
+// allocation is padded by `pad` elements so that vectorised or bulk copies
+// that round an end offset up stay inside it.
+template <typename T>
+class DeviceArray {
+  public:
+    DeviceArray() = default;
+    explicit DeviceArray(size_t n, size_t pad = 0) { alloc(n, pad); }
+    DeviceArray(const DeviceArray &) = delete;
+    DeviceArray &operator=(const DeviceArray &) = delete;
+    DeviceArray(DeviceArray &&o) noexcept : p_(o.p_), n_(o.n_) {
+        o.p_ = nullptr;
+        o.n_ = 0;
+    }
+    DeviceArray &operator=(DeviceArray &&o) noexcept {
+        if (this != &o) {
+            reset();
+            p_ = o.p_;
+            n_ = o.n_;
+            o.p_ = nullptr;
+            o.n_ = 0;
+        }
+        return *this;
+    }
+    ~DeviceArray() { reset(); }
+
+    void alloc(size_t n, size_t pad = 0) {
+        reset();
+        const size_t bytes = (n + pad) * sizeof(T);
+        if (bytes) {
+            NKG_CUDA(cudaMalloc(reinterpret_cast<void **>(&p_), bytes));
+        }
+        n_ = n;
+    }
+    void reset() {
+        if (p_)
+            cudaFree(p_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    T *get() const { return p_; }
+    size_t size() const { return n_; }
+    explicit operator bool() const { return p_ != nullptr; }
+
+  private:
+    T *p_ = nullptr;
+    size_t n_ = 0;
+};
+
+// Pinned host buffer (cudaHostAlloc) for status read-back.
+template <typename T>
+class PinnedHost {
+  public:
+    PinnedHost() = default;
+    explicit PinnedHost(size_t n) { alloc(n); }
+    void alloc(size_t n) {
+        if (p_)
+            cudaFreeHost(p_);
+        p_ = nullptr;
+        NKG_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&p_), n * sizeof(T), cudaHostAllocDefault));
+    }
+    PinnedHost(const PinnedHost &) = delete;
+    PinnedHost &operator=(const PinnedHost &) = delete;
+    ~PinnedHost() {
+        if (p_)
+            cudaFreeHost(p_);
+    }
+    T *get() const { return p_; }
+
+  private:
+    T *p_ = nullptr;
+};
+
+constexpr uint32_t kNone = 0xffffffffu;
+
+inline unsigned ceil_div(uint64_t a, uint64_t b) { return static_cast<unsigned>((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// Device helpers
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide sum with a fixed tree (deterministic for a fixed block size).
+// Result valid in thread 0. `scratch` holds >= 32 doubles. Ends with a barrier
+// so the scratch can be reused right away.
+template <int THREADS>
+__device__ __forceinline__ double block_sum(double v, double *scratch) {
+    static_assert(THREADS % 32 == 0 && THREADS <= 1024, "block size");
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    v = warp_sum(v);
+    if (lane == 0)
+        scratch[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (wid == 0) {
+        r = lane < THREADS / 32 ? scratch[lane] : 0.0;
+        r = warp_sum(r);
+    }
+    __syncthreads();
+    return r;
+}
+
+template <int THREADS>
+__device__ __forceinline__ double block_max(double v, double *scratch) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    v = warp_max(v);
+    if (lane == 0)
+        scratch[wid] = v;
+    __syncthreads();
+    double r = -1.0 / 0.0;
+    if (wid == 0) {
+        r = lane < THREADS / 32 ? scratch[lane] : -1.0 / 0.0;
+        r = warp_max(r);
+    }
+    __syncthreads();
+    return r;
+}
+
+// Streaming (evict-first) read-only loads for data touched once per sweep, so
+// that the L2 keeps the gathered score vector instead.
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t *p) { return __ldcs(p); }
+__device__ __forceinline__ float ld_stream(const float *p) { return __ldcs(p); }
+__device__ __forceinline__ double ld_stream(const double *p) { return __ldcs(p); }
+
+} // namespace nkg

@@ -1,0 +1,990 @@
+// libnkgpu: B200 PageRank behind the C ABI of include/nkgpu.h.
+//
+// Graph upload (nkg_graph_create*) relabels the nodes by out-degree (stable,
+// descending) so that the hot part of the gathered score vector is dense in
+// memory and in L2, and so that all sinks form a suffix of the id range; the
+// per-row arc order (the reference's summation order) is kept. Results are
+// mapped back to the caller's ids on the way out.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "graph.hpp"
+
+using namespace nkg;
+
+namespace nkg {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string &m) { g_last_error = m; }
+
+// ---------------------------------------------------------------------------
+// Graph build kernels
+
+// Checks the caller's CSR: monotone offsets, columns in range and pointing at
+// existing nodes, deleted nodes without arcs. Sets *err on the first problem
+// (1: offsets, 2: column range, 3: column to deleted node, 4: deleted node
+// with in-arcs) and counts out-degrees.
+__global__ void validate_and_count(const uint64_t *__restrict__ in_ptr,
+                                   const uint32_t *__restrict__ in_col,
+                                   const uint8_t *__restrict__ exists, uint64_t z, uint64_t arcs,
+                                   uint32_t *__restrict__ outdeg, int *__restrict__ err) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < z;
+         i += stride) {
+        const uint64_t a = in_ptr[i], b = in_ptr[i + 1];
+        if (b < a || b > arcs)
+            atomicCAS(err, 0, 1);
+        else if (exists && !exists[i] && b != a)
+            atomicCAS(err, 0, 4);
+    }
+    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < arcs;
+         e += stride) {
+        const uint32_t v = in_col[e];
+        if (v >= z) {
+            atomicCAS(err, 0, 2);
+            continue;
+        }
+        if (exists && !exists[v]) {
+            atomicCAS(err, 0, 3);
+            continue;
+        }
+        atomicAdd(outdeg + v, 1u);
+    }
+}
+
+// Sort key per original id: deleted nodes 0 (sorted last), then either the
+// out-degree + 1 (reorder) or just "has out-arcs" (stable partition only).
+__global__ void make_keys(const uint32_t *__restrict__ outdeg, const uint8_t *__restrict__ exists,
+                          uint64_t z, int reorder, uint32_t *__restrict__ keys,
+                          uint32_t *__restrict__ ids, unsigned long long *__restrict__ counts) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    bool nonsink = false;
+    if (i < z) {
+        const bool ex = exists == nullptr || exists[i];
+        const uint32_t d = outdeg[i];
+        uint32_t k = 0;
+        if (ex)
+            k = reorder ? (d >= 0xfffffffeu ? 0xffffffffu : d + 1u) : (d > 0 ? 2u : 1u);
+        keys[i] = k;
+        ids[i] = static_cast<uint32_t>(i);
+        nonsink = ex && d > 0;
+    }
+    const int c = __syncthreads_count(nonsink);
+    if (threadIdx.x == 0 && c)
+        atomicAdd(counts, static_cast<unsigned long long>(c));
+}
+
+// Ranking input: deleted ids get -inf so that they sort behind every score.
+__global__ void ranking_prepare_kernel(double *__restrict__ keys, uint32_t *__restrict__ ids,
+                                       const uint32_t *__restrict__ inv, uint64_t z) {
+    const uint64_t o = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (o >= z)
+        return;
+    if (inv[o] == kNone)
+        keys[o] = -1.0 / 0.0;
+    ids[o] = static_cast<uint32_t>(o);
+}
+
+static void ranking_prepare(double *keys, uint32_t *ids, const uint32_t *inv, uint64_t z,
+                            cudaStream_t s) {
+    ranking_prepare_kernel<<<ceil_div(z, 256), 256, 0, s>>>(keys, ids, inv, z);
+    NKG_CUDA(cudaGetLastError());
+}
+
+__global__ void build_perm(const uint32_t *__restrict__ sorted_ids, uint64_t n,
+                           const uint64_t *__restrict__ in_ptr, uint32_t *__restrict__ perm,
+                           uint32_t *__restrict__ inv, uint32_t *__restrict__ rowlen,
+                           const uint32_t *__restrict__ outdeg, uint32_t *__restrict__ degc,
+                           const double *__restrict__ wdeg, double *__restrict__ degw) {
+    const uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (r >= n)
+        return;
+    const uint32_t o = sorted_ids[r];
+    perm[r] = o;
+    inv[o] = static_cast<uint32_t>(r);
+    rowlen[r] = static_cast<uint32_t>(in_ptr[o + 1] - in_ptr[o]);
+    degc[r] = outdeg[o];
+    if (degw)
+        degw[r] = wdeg[o];
+}
+
+// Copy every row into its new place, mapping column ids; one warp per row.
+__global__ void relabel_rows(const uint32_t *__restrict__ perm, const uint64_t *__restrict__ in_ptr,
+                             const uint32_t *__restrict__ in_col, const double *__restrict__ in_w,
+                             const uint32_t *__restrict__ inv, const uint32_t *__restrict__ row_ptr,
+                             uint64_t n, uint32_t *__restrict__ col, double *__restrict__ w) {
+    const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (uint64_t r = warp; r < n; r += nwarps) {
+        const uint64_t src = in_ptr[perm[r]];
+        const uint32_t dst = row_ptr[r];
+        const uint32_t len = row_ptr[r + 1] - dst;
+        for (uint32_t j = lane; j < len; j += 32) {
+            col[dst + j] = inv[in_col[src + j]];
+            if (w)
+                w[dst + j] = in_w[src + j];
+        }
+    }
+}
+
+// Merge-path coordinates of every tile boundary (row ends vs arcs).
+__global__ void tile_coords(const uint32_t *__restrict__ row_ptr, uint32_t n, uint32_t arcs,
+                            uint32_t ntiles, uint32_t tile, uint32_t *__restrict__ tile_row,
+                            uint32_t *__restrict__ tile_arc) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > ntiles)
+        return;
+    const uint64_t total = static_cast<uint64_t>(n) + arcs;
+    const uint64_t d64 = static_cast<uint64_t>(t) * tile;
+    const int64_t diag = static_cast<int64_t>(d64 < total ? d64 : total);
+    const int64_t lo0 = diag - static_cast<int64_t>(arcs);
+    int64_t lo = lo0 > 0 ? lo0 : 0;
+    int64_t hi = diag < static_cast<int64_t>(n) ? diag : static_cast<int64_t>(n);
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (static_cast<int64_t>(row_ptr[mid + 1]) <= diag - mid - 1)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    tile_row[t] = static_cast<uint32_t>(lo);
+    tile_arc[t] = static_cast<uint32_t>(diag - lo);
+}
+
+template <typename T>
+__global__ void convert_array(const double *__restrict__ in, T *__restrict__ out, uint64_t m) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < m; i += stride)
+        out[i] = static_cast<T>(in[i]);
+}
+
+// ---------------------------------------------------------------------------
+// Per-run kernels
+
+// PageRank.cpp:26: x = 1/n, stored in gather form.
+template <typename T, bool WEIGHTED>
+__global__ void init_iterate(T *__restrict__ y, const uint32_t *__restrict__ degc,
+                             const T *__restrict__ degw, uint32_t n, uint32_t n_nonsink,
+                             double x0) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n)
+        return;
+    const T x = static_cast<T>(x0);
+    if (r >= n_nonsink)
+        y[r] = x;
+    else
+        y[r] = x / (WEIGHTED ? degw[r] : static_cast<T>(degc[r]));
+}
+
+// Personalised teleport into the relabelled order.
+template <typename T>
+__global__ void permute_teleport(const double *__restrict__ t_orig, const uint32_t *__restrict__ perm,
+                                 uint32_t n, T *__restrict__ t_new) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n)
+        t_new[r] = static_cast<T>(t_orig[perm[r]]);
+}
+
+template <typename T, bool WEIGHTED>
+__device__ __forceinline__ double final_x(const T *y, const uint32_t *degc, const T *degw,
+                                          uint32_t r, uint32_t n_nonsink) {
+    const T yv = y[r];
+    if (r >= n_nonsink)
+        return static_cast<double>(yv);
+    const T d = WEIGHTED ? degw[r] : static_cast<T>(degc[r]);
+    return static_cast<double>(t_mul(yv, d));
+}
+
+constexpr int kRedThreads = 256;
+
+// Sum of x, sum of x over sinks and max x (PageRank.cpp:76,83-87,95-102), two
+// levels with a fixed order. red[0..2] receive the totals.
+template <typename T, bool WEIGHTED>
+__global__ void __launch_bounds__(kRedThreads)
+    final_reduce(const T *__restrict__ y, const uint32_t *__restrict__ degc,
+                 const T *__restrict__ degw, uint32_t n, uint32_t n_nonsink,
+                 double *__restrict__ part, double *__restrict__ red,
+                 unsigned int *__restrict__ ticket) {
+    __shared__ double s_red[32];
+    __shared__ bool s_last;
+    double s = 0.0, ss = 0.0, mx = -1.0 / 0.0;
+    for (uint32_t r = blockIdx.x * kRedThreads + threadIdx.x; r < n; r += gridDim.x * kRedThreads) {
+        const double x = final_x<T, WEIGHTED>(y, degc, degw, r, n_nonsink);
+        s += x;
+        if (r >= n_nonsink)
+            ss += x;
+        mx = fmax(mx, x);
+    }
+    s = block_sum<kRedThreads>(s, s_red);
+    ss = block_sum<kRedThreads>(ss, s_red);
+    mx = block_max<kRedThreads>(mx, s_red);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x + 0] = s;
+        part[3 * blockIdx.x + 1] = ss;
+        part[3 * blockIdx.x + 2] = mx;
+        __threadfence();
+        s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last)
+        return;
+    __threadfence();
+    s = 0.0;
+    ss = 0.0;
+    mx = -1.0 / 0.0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += kRedThreads) {
+        s += ((volatile double *)part)[3 * i + 0];
+        ss += ((volatile double *)part)[3 * i + 1];
+        mx = fmax(mx, ((volatile double *)part)[3 * i + 2]);
+    }
+    s = block_sum<kRedThreads>(s, s_red);
+    ss = block_sum<kRedThreads>(ss, s_red);
+    mx = block_max<kRedThreads>(mx, s_red);
+    if (threadIdx.x == 0) {
+        red[0] = s;
+        red[1] = ss;
+        red[2] = mx;
+        *ticket = 0;
+    }
+}
+
+// PageRank.cpp:75-92 scaling, written in the caller's id order; non-existent
+// ids keep 1/n. red[3] receives maximum() for the normalised form.
+template <typename T, bool WEIGHTED>
+__global__ void final_scale(const T *__restrict__ y, const uint32_t *__restrict__ degc,
+                            const T *__restrict__ degw, const uint32_t *__restrict__ inv,
+                            uint64_t z, uint32_t n, uint32_t n_nonsink, double damp,
+                            int normalized, double *__restrict__ red, double *__restrict__ out) {
+    const uint64_t o = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (o >= z)
+        return;
+    const double inv_n_val = 1.0 / static_cast<double>(n);
+    const double factor =
+        normalized ? (1.0 / static_cast<double>(n)) * ((1 - damp) + (damp * red[1])) : red[0];
+    const uint32_t r = inv[o];
+    double v;
+    if (r == kNone) {
+        v = inv_n_val;
+    } else {
+        v = final_x<T, WEIGHTED>(y, degc, degw, r, n_nonsink) / factor;
+    }
+    out[o] = v;
+    if (o == 0)
+        red[3] = normalized ? fmax(v, red[2] / factor) : 1.0;
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        NKG_CUDA(cudaGetDevice(&prev));
+        if (prev != dev)
+            NKG_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0)
+            cudaSetDevice(prev);
+    }
+};
+
+static unsigned num_sms(int dev) {
+    int v = 0;
+    NKG_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+    return static_cast<unsigned>(v);
+}
+
+static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr,
+                               const uint32_t *in_col, const double *in_w, const double *wdeg,
+                               const uint8_t *exists, int directed, const nkg_graph_options *opt) {
+    require(z >= 1, "graph must have at least one node id (z >= 1)");
+    require(z < 0xffffffffull, "node ids must fit in 32 bits (z < 2^32 - 1)");
+    require(arcs < 0xffffffffull, "graphs with 2^32 or more arcs are not supported");
+    require(in_ptr != nullptr, "in_row_ptr is NULL");
+    require(arcs == 0 || in_col != nullptr, "in_col is NULL");
+    require(in_w == nullptr || wdeg != nullptr, "weighted graph needs out_wdeg");
+    require(in_ptr[0] == 0 && in_ptr[z] == arcs, "in_row_ptr must start at 0 and end at arcs");
+
+    int dev = opt && opt->device >= 0 ? opt->device : -1;
+    if (dev < 0)
+        NKG_CUDA(cudaGetDevice(&dev));
+    DeviceGuard guard(dev);
+    std::unique_ptr<nkg_graph> g(new nkg_graph());
+    g->device = dev;
+    g->z = z;
+    g->arcs = arcs;
+    g->weighted = in_w != nullptr;
+    g->directed = directed != 0;
+    g->reordered = !(opt && opt->reorder == 0);
+    NKG_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    NKG_CUDA(cudaEventCreate(&g->ev0));
+    NKG_CUDA(cudaEventCreate(&g->ev1));
+    NKG_CUDA(cudaEventCreate(&g->ev2));
+    cudaStream_t s = g->stream;
+
+    // Upload.
+    DeviceArray<uint64_t> d_ptr(z + 1);
+    DeviceArray<uint32_t> d_col(arcs);
+    DeviceArray<double> d_w, d_wdeg;
+    DeviceArray<uint8_t> d_ex;
+    NKG_CUDA(cudaMemcpyAsync(d_ptr.get(), in_ptr, (z + 1) * sizeof(uint64_t),
+                             cudaMemcpyHostToDevice, s));
+    if (arcs)
+        NKG_CUDA(cudaMemcpyAsync(d_col.get(), in_col, arcs * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, s));
+    if (in_w) {
+        d_w.alloc(arcs);
+        d_wdeg.alloc(z);
+        if (arcs)
+            NKG_CUDA(cudaMemcpyAsync(d_w.get(), in_w, arcs * sizeof(double),
+                                     cudaMemcpyHostToDevice, s));
+        NKG_CUDA(cudaMemcpyAsync(d_wdeg.get(), wdeg, z * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    if (exists) {
+        d_ex.alloc(z);
+        NKG_CUDA(cudaMemcpyAsync(d_ex.get(), exists, z, cudaMemcpyHostToDevice, s));
+    }
+    NKG_CUDA(cudaEventRecord(g->ev0, s));
+
+    // Validate + out-degree count.
+    DeviceArray<uint32_t> outdeg(z);
+    DeviceArray<int> err(1);
+    DeviceArray<unsigned long long> cnt(1);
+    NKG_CUDA(cudaMemsetAsync(outdeg.get(), 0, z * sizeof(uint32_t), s));
+    NKG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
+    NKG_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(unsigned long long), s));
+    const unsigned sms = num_sms(dev);
+    validate_and_count<<<sms * 8, 256, 0, s>>>(d_ptr.get(), d_col.get(), d_ex.get(), z, arcs,
+                                              outdeg.get(), err.get());
+    NKG_CUDA(cudaGetLastError());
+    int h_err = 0;
+    NKG_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    NKG_CUDA(cudaStreamSynchronize(s));
+    switch (h_err) {
+    case 0: break;
+    case 1: throw Error(NKG_ERR_INVALID_ARG, "in_row_ptr is not non-decreasing within [0, arcs]");
+    case 2: throw Error(NKG_ERR_INVALID_ARG, "in_col holds a node id >= z");
+    case 3: throw Error(NKG_ERR_INVALID_ARG, "in_col refers to a non-existent node");
+    default: throw Error(NKG_ERR_INVALID_ARG, "a non-existent node has in-arcs");
+    }
+
+    // Relabelling order.
+    DeviceArray<uint32_t> keys(z), ids(z), keys_s(z), ids_s(z);
+    make_keys<<<ceil_div(z, 256), 256, 0, s>>>(outdeg.get(), d_ex.get(), z, g->reordered ? 1 : 0,
+                                               keys.get(), ids.get(), cnt.get());
+    NKG_CUDA(cudaGetLastError());
+    size_t tmp_bytes = 0;
+    NKG_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, keys.get(), keys_s.get(),
+                                                       ids.get(), ids_s.get(), static_cast<int64_t>(z),
+                                                       0, 32, s));
+    DeviceArray<unsigned char> tmp(tmp_bytes);
+    NKG_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.get(), tmp_bytes, keys.get(), keys_s.get(),
+                                                       ids.get(), ids_s.get(), static_cast<int64_t>(z),
+                                                       0, 32, s));
+    uint64_t n = z;
+    if (exists) {
+        n = 0;
+        for (uint64_t i = 0; i < z; ++i)
+            n += exists[i] != 0;
+    }
+    require(n >= 1, "graph has no existing node");
+    unsigned long long h_cnt = 0;
+    NKG_CUDA(cudaMemcpyAsync(&h_cnt, cnt.get(), sizeof(h_cnt), cudaMemcpyDeviceToHost, s));
+    g->n = n;
+
+    g->perm.alloc(n);
+    g->inv.alloc(z);
+    g->degc.alloc(n);
+    g->row_ptr.alloc(n + 1, 4);
+    DeviceArray<uint32_t> rowlen(n);
+    if (g->weighted)
+        g->degw64src.alloc(n);
+    NKG_CUDA(cudaMemsetAsync(g->inv.get(), 0xff, z * sizeof(uint32_t), s));
+    build_perm<<<ceil_div(n, 256), 256, 0, s>>>(ids_s.get(), n, d_ptr.get(), g->perm.get(),
+                                                g->inv.get(), rowlen.get(), outdeg.get(),
+                                                g->degc.get(), d_wdeg.get(), g->degw64src.get());
+    NKG_CUDA(cudaGetLastError());
+    NKG_CUDA(cudaMemsetAsync(g->row_ptr.get(), 0, sizeof(uint32_t), s));
+    tmp_bytes = 0;
+    NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, rowlen.get(), g->row_ptr.get() + 1,
+                                           static_cast<int64_t>(n), s));
+    tmp.alloc(tmp_bytes);
+    NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tmp_bytes, rowlen.get(), g->row_ptr.get() + 1,
+                                           static_cast<int64_t>(n), s));
+    g->col.alloc(arcs, 4);
+    if (g->weighted)
+        g->w64src.alloc(arcs, 4);
+    if (arcs)
+        relabel_rows<<<sms * 16, 256, 0, s>>>(g->perm.get(), d_ptr.get(), d_col.get(), d_w.get(),
+                                              g->inv.get(), g->row_ptr.get(), n, g->col.get(),
+                                              g->w64src.get());
+    NKG_CUDA(cudaGetLastError());
+
+    g->ntiles = std::max<uint64_t>(1, (n + arcs + kTile - 1) / kTile);
+    require(g->ntiles < 0xffffffffull, "too many tiles");
+    g->tile_row.alloc(g->ntiles + 1);
+    g->tile_arc.alloc(g->ntiles + 1);
+    tile_coords<<<ceil_div(g->ntiles + 1, 256), 256, 0, s>>>(
+        g->row_ptr.get(), static_cast<uint32_t>(n), static_cast<uint32_t>(arcs),
+        static_cast<uint32_t>(g->ntiles), kTile, g->tile_row.get(), g->tile_arc.get());
+    NKG_CUDA(cudaGetLastError());
+    NKG_CUDA(cudaEventRecord(g->ev1, s));
+    NKG_CUDA(cudaStreamSynchronize(s));
+    g->n_nonsink = h_cnt;
+    float ms = 0.f;
+    NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    g->ms_create = ms;
+
+    // Per-run bookkeeping buffers. The partial-sum arrays are sized for the
+    // largest grid any sweep variant can use (32 resident CTAs per SM), so
+    // they are never reallocated under a captured graph.
+    g->cta_res.alloc(static_cast<size_t>(sms) * 32);
+    g->cta_sink.alloc(static_cast<size_t>(sms) * 32);
+    g->fix_res.alloc(ceil_div(g->ntiles, kFixThreads));
+    g->fix_sink.alloc(ceil_div(g->ntiles, kFixThreads));
+    g->rp.alloc(1);
+    g->st.alloc(1);
+    g->red.alloc(4 + 3 * 4096);
+    g->red_ticket.alloc(1);
+    NKG_CUDA(cudaMemsetAsync(g->red_ticket.get(), 0, sizeof(unsigned int), s));
+    g->st_host.alloc(1);
+    g->scalars_host.alloc(8);
+    NKG_CUDA(cudaStreamSynchronize(s));
+    return g.release();
+}
+
+static void destroy_plane_graphs(nkg_graph *g) {
+    for (int i = 0; i < 2; ++i) {
+        if (g->p64.exec[i])
+            cudaGraphExecDestroy(g->p64.exec[i]);
+        if (g->p32.exec[i])
+            cudaGraphExecDestroy(g->p32.exec[i]);
+        g->p64.exec[i] = g->p32.exec[i] = nullptr;
+    }
+}
+
+template <typename T>
+Plane<T> &plane(nkg_graph *g);
+template <>
+Plane<double> &plane<double>(nkg_graph *g) { return g->p64; }
+template <>
+Plane<float> &plane<float>(nkg_graph *g) { return g->p32; }
+
+template <typename T, bool WEIGHTED>
+static void sweep_setup(nkg_graph *g) {
+    Plane<T> &P = plane<T>(g);
+    if (P.y[0])
+        return;
+    cudaStream_t s = g->stream;
+    const uint64_t n = g->n;
+    P.y[0].alloc(n, 4);
+    P.y[1].alloc(n, 4);
+    P.head.alloc(g->ntiles);
+    P.tail.alloc(g->ntiles);
+    if (WEIGHTED) {
+        if (std::is_same<T, double>::value) {
+            // FP64 plane reads the FP64 source arrays directly.
+        } else {
+            P.w.alloc(g->arcs, 4);
+            P.degw.alloc(n);
+            if (g->arcs)
+                convert_array<T><<<num_sms(g->device) * 8, 256, 0, s>>>(g->w64src.get(), P.w.get(),
+                                                                         g->arcs);
+            convert_array<T><<<num_sms(g->device) * 8, 256, 0, s>>>(g->degw64src.get(),
+                                                                     P.degw.get(), n);
+            NKG_CUDA(cudaGetLastError());
+        }
+    }
+    constexpr size_t smem = SweepSmem<T, WEIGHTED, kSweepThreads, kSweepIPT>::bytes;
+    auto kfn = sweep_kernel<T, WEIGHTED, kSweepThreads, kSweepIPT>;
+    NKG_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem)));
+    int occ = 0;
+    NKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kSweepThreads, smem));
+    occ = std::max(occ, 1);
+    P.sweep_ctas = static_cast<unsigned>(std::min<uint64_t>(
+        static_cast<uint64_t>(occ) * num_sms(g->device), g->ntiles));
+    P.fix_ctas = ceil_div(g->ntiles, kFixThreads);
+    require(P.sweep_ctas <= g->cta_res.size() && P.fix_ctas <= g->fix_res.size(),
+            "partial-sum buffers too small");
+}
+
+template <typename T, bool WEIGHTED>
+static SweepArgs<T> sweep_args(nkg_graph *g, int in_buf) {
+    Plane<T> &P = plane<T>(g);
+    SweepArgs<T> a{};
+    a.row_ptr = g->row_ptr.get();
+    a.col = g->col.get();
+    if (std::is_same<T, double>::value) {
+        a.w = reinterpret_cast<const T *>(g->w64src.get());
+        a.degw = reinterpret_cast<const T *>(g->degw64src.get());
+    } else {
+        a.w = P.w.get();
+        a.degw = P.degw.get();
+    }
+    a.degc = g->degc.get();
+    a.tele = P.tele.get();
+    a.y_in = P.y[in_buf].get();
+    a.y_out = P.y[in_buf ^ 1].get();
+    a.tile_row = g->tile_row.get();
+    a.tile_arc = g->tile_arc.get();
+    a.head_val = P.head.get();
+    a.tail_val = P.tail.get();
+    a.cta_res = g->cta_res.get();
+    a.cta_sink = g->cta_sink.get();
+    a.fix_res = g->fix_res.get();
+    a.fix_sink = g->fix_sink.get();
+    a.rp = g->rp.get();
+    a.st = g->st.get();
+    a.ntiles = static_cast<uint32_t>(g->ntiles);
+    a.n = static_cast<uint32_t>(g->n);
+    a.n_nonsink = static_cast<uint32_t>(g->n_nonsink);
+    a.sweep_ctas = P.sweep_ctas;
+    return a;
+}
+
+template <typename T, bool WEIGHTED>
+static void launch_sweep(nkg_graph *g, int in_buf, cudaStream_t s) {
+    Plane<T> &P = plane<T>(g);
+    const SweepArgs<T> a = sweep_args<T, WEIGHTED>(g, in_buf);
+    constexpr size_t smem = SweepSmem<T, WEIGHTED, kSweepThreads, kSweepIPT>::bytes;
+    sweep_kernel<T, WEIGHTED, kSweepThreads, kSweepIPT><<<P.sweep_ctas, kSweepThreads, smem, s>>>(a);
+    fixup_kernel<T, WEIGHTED, kFixThreads><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
+}
+
+// Capture kSweepsPerGraph sweeps (sweep + fix-up each) as one CUDA graph.
+template <typename T, bool WEIGHTED>
+static cudaGraphExec_t sweep_graph(nkg_graph *g, int personal) {
+    Plane<T> &P = plane<T>(g);
+    cudaGraphExec_t &exec = P.exec[personal];
+    if (exec)
+        return exec;
+    cudaStream_t s = g->stream;
+    cudaGraph_t graph = nullptr;
+    NKG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < kSweepsPerGraph; ++i)
+        launch_sweep<T, WEIGHTED>(g, i & 1, s);
+    cudaError_t e = cudaStreamEndCapture(s, &graph);
+    NKG_CUDA(e);
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    NKG_CUDA(e);
+    return exec;
+}
+
+struct RunResult {
+    uint64_t iterations = 0;
+    double residual = 0.0, sink_mass = 0.0, maximum = 1.0;
+    double ms_total = 0.0, ms_iter = 0.0;
+    uint64_t launches = 0;
+};
+
+static uint64_t bytes_per_sweep(const nkg_graph *g, int elem) {
+    // Algorithmic bytes of one sweep: column ids, row offsets, gathered
+    // iterate (each value once), previous iterate, new iterate, degree
+    // (+ weights and a weighted degree of `elem` bytes for weighted graphs).
+    uint64_t b = 4 * g->arcs + 4 * (g->n + 1) + 3ull * elem * g->n;
+    if (g->weighted)
+        b += static_cast<uint64_t>(elem) * g->arcs + static_cast<uint64_t>(elem) * g->n;
+    else
+        b += 4 * g->n;
+    return b;
+}
+
+template <typename T, bool WEIGHTED>
+static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *teleport_host,
+                           double *d_out) {
+    cudaStream_t s = g->stream;
+    sweep_setup<T, WEIGHTED>(g);
+    Plane<T> &P = plane<T>(g);
+    const int personal = teleport_host ? 1 : 0;
+    const uint32_t n = static_cast<uint32_t>(g->n);
+    RunResult R;
+
+    RunParams *rp = reinterpret_cast<RunParams *>(g->scalars_host.get());
+    // scalars_host holds 8 doubles = 64 bytes >= sizeof(RunParams)
+    static_assert(sizeof(RunParams) <= 8 * sizeof(double), "RunParams fits the pinned buffer");
+    rp->damp = p.damp;
+    rp->tele_uniform = (1.0 - p.damp) / static_cast<double>(n);
+    rp->one_minus_damp = 1.0 - p.damp;
+    rp->inv_n = 1.0 / static_cast<double>(n);
+    rp->distribute = p.distribute_sinks ? 1 : 0;
+    rp->personal = personal;
+    rp->l2 = p.norm == NKG_NORM_L2 ? 1 : 0;
+    rp->tol = p.tol;
+    rp->max_iterations = p.max_iterations;
+
+    DeviceArray<double> d_tele_orig;
+    NKG_CUDA(cudaEventRecord(g->ev0, s));
+    NKG_CUDA(cudaMemcpyAsync(g->rp.get(), rp, sizeof(RunParams), cudaMemcpyHostToDevice, s));
+    const double x0 = 1.0 / static_cast<double>(n);
+    double S0 = 0.0;
+    if (personal) {
+        if (!P.tele)
+            P.tele.alloc(n);
+        d_tele_orig.alloc(g->z);
+        NKG_CUDA(cudaMemcpyAsync(d_tele_orig.get(), teleport_host, g->z * sizeof(double),
+                                 cudaMemcpyHostToDevice, s));
+        permute_teleport<T><<<ceil_div(n, 256), 256, 0, s>>>(d_tele_orig.get(), g->perm.get(), n,
+                                                             P.tele.get());
+        R.launches++;
+    }
+    S0 = static_cast<double>(g->n - g->n_nonsink) * x0;
+    IterState *sh = g->st_host.get();
+    std::memset(sh, 0, sizeof(IterState));
+    sh->sink_coef = p.distribute_sinks ? (personal ? S0 : S0 / static_cast<double>(n)) : 0.0;
+    sh->sink_mass = S0;
+    NKG_CUDA(cudaMemcpyAsync(g->st.get(), sh, sizeof(IterState), cudaMemcpyHostToDevice, s));
+    init_iterate<T, WEIGHTED><<<ceil_div(n, 256), 256, 0, s>>>(
+        P.y[0].get(), g->degc.get(), WEIGHTED ? sweep_args<T, WEIGHTED>(g, 0).degw : nullptr, n,
+        static_cast<uint32_t>(g->n_nonsink), x0);
+    NKG_CUDA(cudaGetLastError());
+    R.launches++;
+
+    cudaGraphExec_t exec = sweep_graph<T, WEIGHTED>(g, personal);
+    int batch = 1;
+    for (;;) {
+        for (int b = 0; b < batch; ++b)
+            NKG_CUDA(cudaGraphLaunch(exec, s));
+        R.launches += static_cast<uint64_t>(batch) * 2 * kSweepsPerGraph;
+        NKG_CUDA(cudaMemcpyAsync(sh, g->st.get(), sizeof(IterState), cudaMemcpyDeviceToHost, s));
+        NKG_CUDA(cudaStreamSynchronize(s));
+        if (sh->done)
+            break;
+        if (g->cancel.load()) {
+            g->cancel.store(0);
+            throw Error(NKG_ERR_CANCELLED, "PageRank run cancelled");
+        }
+        batch = std::min(batch * 2, 8);
+    }
+    NKG_CUDA(cudaEventRecord(g->ev1, s));
+    R.iterations = sh->iteration;
+    R.residual = sh->residual;
+    R.sink_mass = sh->sink_mass;
+    const int fin = static_cast<int>(R.iterations & 1ull);
+    const T *yfin = P.y[fin].get();
+    const T *degw = WEIGHTED ? sweep_args<T, WEIGHTED>(g, 0).degw : nullptr;
+    const unsigned rblocks = std::min<unsigned>(num_sms(g->device) * 2, 4096);
+    final_reduce<T, WEIGHTED><<<rblocks, kRedThreads, 0, s>>>(yfin, g->degc.get(), degw, n,
+                                                              static_cast<uint32_t>(g->n_nonsink),
+                                                              g->red.get() + 4, g->red.get(),
+                                                              g->red_ticket.get());
+    final_scale<T, WEIGHTED><<<ceil_div(g->z, 256), 256, 0, s>>>(
+        yfin, g->degc.get(), degw, g->inv.get(), g->z, n, static_cast<uint32_t>(g->n_nonsink),
+        p.damp, p.normalized ? 1 : 0, g->red.get(), d_out);
+    NKG_CUDA(cudaGetLastError());
+    R.launches += 2;
+    NKG_CUDA(cudaEventRecord(g->ev2, s));
+    double *hs = g->scalars_host.get();
+    NKG_CUDA(cudaMemcpyAsync(hs, g->red.get(), 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    NKG_CUDA(cudaStreamSynchronize(s));
+    R.maximum = hs[3];
+    float ms = 0.f;
+    NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev2));
+    R.ms_total = ms;
+    NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    R.ms_iter = ms;
+    return R;
+}
+
+static void check_params(const nkg_pr_params *p) {
+    require(p != nullptr, "params is NULL");
+    require(p->norm == NKG_NORM_L1 || p->norm == NKG_NORM_L2, "norm must be L1 (0) or L2 (1)");
+    require(p->precision >= NKG_PREC_FP64 && p->precision <= NKG_PREC_FP32,
+            "unknown precision");
+    require(std::isfinite(p->damp), "damp must be finite");
+    require(!std::isnan(p->tol), "tol must not be NaN");
+}
+
+static RunResult run_dispatch(nkg_graph *g, const nkg_pr_params *p, const double *teleport,
+                              double *d_out) {
+    check_params(p);
+    DeviceGuard guard(g->device);
+    g->cancel.store(0);
+    RunResult R;
+    if (p->precision == NKG_PREC_FP64) {
+        R = g->weighted ? run_power<double, true>(g, *p, teleport, d_out)
+                        : run_power<double, false>(g, *p, teleport, d_out);
+    } else if (p->precision == NKG_PREC_FP32) {
+        R = g->weighted ? run_power<float, true>(g, *p, teleport, d_out)
+                        : run_power<float, false>(g, *p, teleport, d_out);
+    } else {
+        throw Error(NKG_ERR_INVALID_ARG, "FP32 refinement is not available in this build");
+    }
+    g->has_run = true;
+    return R;
+}
+
+static void fill_stats(const nkg_graph *g, const RunResult &R, int precision, nkg_stats *st) {
+    if (!st)
+        return;
+    std::memset(st, 0, sizeof(*st));
+    st->iterations = R.iterations;
+    st->residual = R.residual;
+    st->sink_mass = R.sink_mass;
+    st->ms_total = R.ms_total;
+    st->ms_iterations = R.ms_iter;
+    st->kernel_launches = R.launches;
+    if (precision == NKG_PREC_FP64)
+        st->fp64_sweeps = R.iterations;
+    else
+        st->fp32_sweeps = R.iterations;
+    st->bytes_per_sweep_fp64 = bytes_per_sweep(g, 8);
+    st->bytes_per_sweep_fp32 = bytes_per_sweep(g, 4);
+}
+
+// Time `sweeps` sweeps with events around every sweep-kernel launch; the
+// stopping test is disabled (tol < 0, no iteration cap).
+template <typename T, bool WEIGHTED>
+static void profile_sweeps(nkg_graph *g, int sweeps, double *ms_kernel, double *ms_iter) {
+    cudaStream_t s = g->stream;
+    sweep_setup<T, WEIGHTED>(g);
+    Plane<T> &P = plane<T>(g);
+    const uint32_t n = static_cast<uint32_t>(g->n);
+    RunParams *rp = reinterpret_cast<RunParams *>(g->scalars_host.get());
+    std::memset(rp, 0, sizeof(RunParams));
+    rp->damp = 0.85;
+    rp->tele_uniform = 0.15 / static_cast<double>(n);
+    rp->one_minus_damp = 0.15;
+    rp->inv_n = 1.0 / static_cast<double>(n);
+    rp->tol = -1.0;
+    rp->max_iterations = ~0ull;
+    IterState *sh = g->st_host.get();
+    std::memset(sh, 0, sizeof(IterState));
+    NKG_CUDA(cudaMemcpyAsync(g->rp.get(), rp, sizeof(RunParams), cudaMemcpyHostToDevice, s));
+    NKG_CUDA(cudaMemcpyAsync(g->st.get(), sh, sizeof(IterState), cudaMemcpyHostToDevice, s));
+    init_iterate<T, WEIGHTED><<<ceil_div(n, 256), 256, 0, s>>>(
+        P.y[0].get(), g->degc.get(), sweep_args<T, WEIGHTED>(g, 0).degw, n,
+        static_cast<uint32_t>(g->n_nonsink), 1.0 / static_cast<double>(n));
+    NKG_CUDA(cudaGetLastError());
+    std::vector<cudaEvent_t> ev(2 * static_cast<size_t>(sweeps), nullptr);
+    for (auto &e : ev)
+        NKG_CUDA(cudaEventCreate(&e));
+    constexpr size_t smem = SweepSmem<T, WEIGHTED, kSweepThreads, kSweepIPT>::bytes;
+    for (int i = 0; i < sweeps; ++i) {
+        const SweepArgs<T> a = sweep_args<T, WEIGHTED>(g, i & 1);
+        NKG_CUDA(cudaEventRecord(ev[2 * i], s));
+        sweep_kernel<T, WEIGHTED, kSweepThreads, kSweepIPT><<<P.sweep_ctas, kSweepThreads, smem, s>>>(a);
+        NKG_CUDA(cudaEventRecord(ev[2 * i + 1], s));
+        fixup_kernel<T, WEIGHTED, kFixThreads><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
+    }
+    NKG_CUDA(cudaGetLastError());
+    NKG_CUDA(cudaStreamSynchronize(s));
+    double sum = 0.0;
+    for (int i = 0; i < sweeps; ++i) {
+        float ms = 0.f;
+        NKG_CUDA(cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]));
+        sum += ms;
+    }
+    float total = 0.f;
+    // first sweep start -> last sweep end, plus one fix-up per sweep: use the
+    // span from the first sweep to the start of the last one over sweeps-1
+    if (sweeps > 1)
+        NKG_CUDA(cudaEventElapsedTime(&total, ev[0], ev[2 * (sweeps - 1)]));
+    for (auto &e : ev)
+        cudaEventDestroy(e);
+    *ms_kernel = sum / sweeps;
+    *ms_iter = sweeps > 1 ? total / (sweeps - 1) : sum;
+}
+
+template <typename F>
+static int guarded(F &&f) {
+    try {
+        f();
+        return NKG_OK;
+    } catch (const Error &e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_last_error("host allocation failed");
+        return NKG_ERR_OOM;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return NKG_ERR_CUDA;
+    }
+}
+
+static int run_to(nkg_graph *g, const nkg_pr_params *p, const double *teleport, double *out,
+                  bool out_is_host, uint64_t *iters, double *max_out, nkg_stats *stats) {
+    return guarded([&] {
+        require(g != nullptr, "graph handle is NULL");
+        require(out != nullptr, "scores_out is NULL");
+        DeviceGuard guard(g->device);
+        double *d_out = out;
+        if (out_is_host) {
+            if (!g->out_buf)
+                g->out_buf.alloc(g->z);
+            d_out = g->out_buf.get();
+        }
+        RunResult R = run_dispatch(g, p, teleport, d_out);
+        if (out_is_host) {
+            NKG_CUDA(cudaMemcpyAsync(out, d_out, g->z * sizeof(double), cudaMemcpyDeviceToHost,
+                                     g->stream));
+            NKG_CUDA(cudaStreamSynchronize(g->stream));
+        }
+        if (iters)
+            *iters = R.iterations;
+        if (max_out)
+            *max_out = R.maximum;
+        fill_stats(g, R, p->precision, stats);
+    });
+}
+
+} // namespace nkg
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+extern "C" {
+
+const char *nkg_last_error(void) { return nkg::g_last_error.c_str(); }
+
+int nkg_abi_version(void) { return NKG_ABI_VERSION; }
+
+int nkg_graph_create_ex(nkg_graph **out, uint64_t z, uint64_t arcs, const uint64_t *in_row_ptr,
+                        const uint32_t *in_col, const double *in_w, const double *out_wdeg,
+                        const uint8_t *exists, int directed, const nkg_graph_options *opts) {
+    return guarded([&] {
+        require(out != nullptr, "out is NULL");
+        *out = nullptr;
+        *out = create_graph(z, arcs, in_row_ptr, in_col, in_w, out_wdeg, exists, directed, opts);
+    });
+}
+
+int nkg_graph_create(nkg_graph **out, uint64_t z, uint64_t arcs, const uint64_t *in_row_ptr,
+                     const uint32_t *in_col, const double *in_w, const double *out_wdeg,
+                     const uint8_t *exists, int directed) {
+    return nkg_graph_create_ex(out, z, arcs, in_row_ptr, in_col, in_w, out_wdeg, exists, directed,
+                               nullptr);
+}
+
+void nkg_graph_destroy(nkg_graph *g) {
+    if (!g)
+        return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(g->device);
+    cudaStreamSynchronize(g->stream);
+    destroy_plane_graphs(g);
+    if (g->ev0)
+        cudaEventDestroy(g->ev0);
+    if (g->ev1)
+        cudaEventDestroy(g->ev1);
+    if (g->ev2)
+        cudaEventDestroy(g->ev2);
+    cudaStream_t s = g->stream;
+    delete g;
+    if (s)
+        cudaStreamDestroy(s);
+    if (prev >= 0)
+        cudaSetDevice(prev);
+}
+
+int nkg_graph_get_info(const nkg_graph *g, nkg_graph_info *info) {
+    return guarded([&] {
+        require(g != nullptr && info != nullptr, "NULL argument");
+        std::memset(info, 0, sizeof(*info));
+        info->z = g->z;
+        info->n = g->n;
+        info->arcs = g->arcs;
+        info->sinks = g->n - g->n_nonsink;
+        info->tiles = g->ntiles;
+        info->weighted = g->weighted;
+        info->directed = g->directed;
+        info->device = g->device;
+        info->reordered = g->reordered;
+        info->ms_create = g->ms_create;
+    });
+}
+
+int nkg_pagerank_run(nkg_graph *g, const nkg_pr_params *p, double *scores_out,
+                     uint64_t *iterations_out, double *max_out, nkg_stats *stats) {
+    return run_to(g, p, nullptr, scores_out, true, iterations_out, max_out, stats);
+}
+
+int nkg_pagerank_run_device(nkg_graph *g, const nkg_pr_params *p, double *d_scores_out,
+                            uint64_t *iterations_out, double *max_out, nkg_stats *stats) {
+    return run_to(g, p, nullptr, d_scores_out, false, iterations_out, max_out, stats);
+}
+
+int nkg_pagerank_run_teleport(nkg_graph *g, const nkg_pr_params *p, const double *teleport,
+                              double *scores_out, uint64_t *iterations_out, double *max_out,
+                              nkg_stats *stats) {
+    if (!teleport) {
+        nkg::set_last_error("teleport is NULL");
+        return NKG_ERR_INVALID_ARG;
+    }
+    return run_to(g, p, teleport, scores_out, true, iterations_out, max_out, stats);
+}
+
+int nkg_ranking(nkg_graph *g, const double *scores, uint64_t *ids_out, double *vals_out) {
+    return guarded([&] {
+        require(g != nullptr && scores != nullptr, "NULL argument");
+        DeviceGuard guard(g->device);
+        cudaStream_t s = g->stream;
+        const uint64_t z = g->z;
+        DeviceArray<double> keys(z), keys_s(z);
+        DeviceArray<uint32_t> ids(z), ids_s(z);
+        NKG_CUDA(cudaMemcpyAsync(keys.get(), scores, z * sizeof(double), cudaMemcpyHostToDevice, s));
+        ranking_prepare(keys.get(), ids.get(), g->inv.get(), z, s);
+        size_t tmp_bytes = 0;
+        NKG_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, keys.get(),
+                                                           keys_s.get(), ids.get(), ids_s.get(),
+                                                           static_cast<int64_t>(z), 0, 64, s));
+        DeviceArray<unsigned char> tmp(tmp_bytes);
+        NKG_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.get(), tmp_bytes, keys.get(),
+                                                           keys_s.get(), ids.get(), ids_s.get(),
+                                                           static_cast<int64_t>(z), 0, 64, s));
+        const uint64_t n = g->n;
+        std::vector<uint32_t> hid(n);
+        if (vals_out)
+            NKG_CUDA(cudaMemcpyAsync(vals_out, keys_s.get(), n * sizeof(double),
+                                     cudaMemcpyDeviceToHost, s));
+        NKG_CUDA(cudaMemcpyAsync(hid.data(), ids_s.get(), n * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, s));
+        NKG_CUDA(cudaStreamSynchronize(s));
+        if (ids_out)
+            for (uint64_t i = 0; i < n; ++i)
+                ids_out[i] = hid[i];
+    });
+}
+
+void nkg_cancel(nkg_graph *g) {
+    if (g)
+        g->cancel.store(1);
+}
+
+int nkg_profile_sweeps(nkg_graph *g, int precision, int sweeps, double *ms_sweep_kernel,
+                       double *ms_iteration) {
+    return guarded([&] {
+        require(g != nullptr && ms_sweep_kernel != nullptr && ms_iteration != nullptr,
+                "NULL argument");
+        require(sweeps >= 1 && sweeps <= 100000, "sweeps must be in [1, 100000]");
+        require(precision == NKG_PREC_FP64 || precision == NKG_PREC_FP32,
+                "precision must be FP64 or FP32");
+        DeviceGuard guard(g->device);
+        if (precision == NKG_PREC_FP64) {
+            if (g->weighted)
+                profile_sweeps<double, true>(g, sweeps, ms_sweep_kernel, ms_iteration);
+            else
+                profile_sweeps<double, false>(g, sweeps, ms_sweep_kernel, ms_iteration);
+        } else {
+            if (g->weighted)
+                profile_sweeps<float, true>(g, sweeps, ms_sweep_kernel, ms_iteration);
+            else
+                profile_sweeps<float, false>(g, sweeps, ms_sweep_kernel, ms_iteration);
+        }
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,134 @@
+"""The oracle (C restatement) pinned against the reference's own results.
+
+CPU only. The golden fixtures hold the reference's PageRank run on one OpenMP
+thread (tests/golden/make_golden.py); the restatement must reproduce them bit
+for bit, and they must satisfy the reference's own asserts
+(CentralityGTest.cpp:484-539,582-664)."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_NAMES, load_golden
+
+
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
+@pytest.mark.parametrize("norm", [0, 1])
+@pytest.mark.parametrize("normalized", [False, True])
+def test_oracle_bit_exact_vs_reference(oracle_mod, name, norm, normalized):
+    csr, ref = load_golden(name)
+    key = f"n{norm}_z{int(normalized)}"
+    r = oracle_mod.pagerank(csr, norm=norm, normalized=normalized)
+    assert r.iterations == int(ref[key + "_iterations"])
+    np.testing.assert_array_equal(r.scores, ref[key + "_scores"])
+    assert r.maximum == float(ref[key + "_maximum"])
+    ids, _ = oracle_mod.ranking(r.scores, csr.exists)
+    np.testing.assert_array_equal(ids.astype(np.uint32), ref[key + "_rank_ids"])
+    r2 = oracle_mod.pagerank(csr, norm=norm, normalized=normalized, max_iterations=2)
+    assert r2.iterations == int(ref[key + "_max2_iterations"]) <= 2
+    if key + "_max2_scores" in ref:
+        np.testing.assert_array_equal(r2.scores, ref[key + "_max2_scores"])
+
+
+def test_reference_golden_values(oracle_mod):
+    """The asserts of CentralityGTest testPageRank / testNormalizedPageRank."""
+    for name, top, val, nval in (("wikivote_directed", 326, 0.00460, 57.6657),
+                                 ("wikivote_undirected", 699, 0.00432, 205.7324)):
+        csr, _ = load_golden(name)
+        for norm in (0, 1):
+            r = oracle_mod.pagerank(csr, norm=norm)
+            ids, vals = oracle_mod.ranking(r.scores)
+            assert ids[0] == top and abs(vals[0] - val) <= 1e-3
+            rn = oracle_mod.pagerank(csr, norm=norm, normalized=True)
+            ids, vals = oracle_mod.ranking(rn.scores)
+            assert ids[0] == top and abs(vals[0] - nval) <= 1e-4
+
+
+def test_matlab_vectors(oracle_mod):
+    """testPageRankCentrality / testNormalizedPageRankCentrality (±1e-4)."""
+    csr, _ = load_golden("matlab8")
+    r = oracle_mod.pagerank(csr)
+    np.testing.assert_allclose(r.scores, [0.0753, 0.0565, 0.2552, 0.1319, 0.0942, 0.2552,
+                                          0.0753, 0.0565], atol=1e-4)
+    r = oracle_mod.pagerank(csr, normalized=True)
+    np.testing.assert_allclose(r.scores, [4.0175, 3.0117, 13.6083, 7.0350, 5.0233, 13.6083,
+                                          4.0175, 3.0117], atol=1e-4)
+
+
+def test_oracle_matches_reference_library_when_built(oracle_mod):
+    """Where the reference library was built here, compare on an R-MAT graph."""
+    if not oracle_mod.ref_available():
+        pytest.skip("oracle/_ref not built")
+    from networkit_b200 import generators
+    csr = generators.rmat_directed(12, 8, seed=7)
+    out_ptr, out_col, _ = csr.out_csr()
+    src = np.repeat(np.arange(csr.z, dtype=np.uint32), np.diff(out_ptr).astype(np.int64))
+    g = oracle_mod.RefGraph.from_edges(csr.z, src, out_col, directed=True)
+    ref = g.pagerank(tol=1e-10, norm=0, nthreads=1)
+    r = oracle_mod.pagerank(csr, tol=1e-10, norm=0)
+    assert r.iterations == ref["iterations"]
+    np.testing.assert_array_equal(r.scores, ref["scores"])
+
+
+def test_distribute_sinks_vs_dense_solve(oracle_mod):
+    """distributeSinks has no reference implementation: pin the restatement to
+    the exact solution of (I - d(A + t m^T)) x = (1-d) t on a small graph."""
+    from networkit_b200 import generators
+    csr = generators.rmat_directed(8, 4, seed=3)
+    z = csr.z
+    A = np.zeros((z, z))
+    rows = np.repeat(np.arange(z), np.diff(csr.in_ptr).astype(np.int64))
+    for u, v in zip(rows, csr.in_col):
+        A[u, v] += 1.0 / csr.wdeg[v]
+    m = (csr.outdeg == 0).astype(np.float64)
+    t = np.full(z, 1.0 / z)
+    M = A + np.outer(t, m)
+    x = np.linalg.solve(np.eye(z) - 0.85 * M, 0.15 * t)
+    r = oracle_mod.pagerank(csr, tol=1e-14, norm=0, distribute_sinks=True)
+    np.testing.assert_allclose(r.scores, x / x.sum(), rtol=0, atol=1e-13)
+    # personalised teleport, too
+    rng = np.random.default_rng(0)
+    t = rng.random(z)
+    t /= t.sum()
+    M = A + np.outer(t, m)
+    x = np.linalg.solve(np.eye(z) - 0.85 * M, 0.15 * t)
+    r = oracle_mod.pagerank(csr, tol=1e-14, norm=0, distribute_sinks=True, teleport=t)
+    np.testing.assert_allclose(r.scores, x / x.sum(), rtol=0, atol=1e-13)
+
+
+def test_adjoint_vs_finite_differences(oracle_mod):
+    """The FP64 host adjoint against central differences of the oracle."""
+    from networkit_b200 import generators
+    csr = generators.with_uniform_weights(generators.rmat_directed(7, 4, seed=5), seed=6)
+    rng = np.random.default_rng(1)
+    g = rng.standard_normal(csr.z)
+
+    def loss(c, tele=None):
+        r = oracle_mod.pagerank(c, tol=1e-15, norm=0, distribute_sinks=True, teleport=tele)
+        return float(g @ r.scores), r
+
+    L0, r0 = loss(csr)
+    # un-normalised fixed point: rerun without the final division is not
+    # exposed, but with distributeSinks the iterate sums to 1 already
+    lam, gw, gt, sweeps = oracle_mod.adjoint(csr, r0.scores, g, distribute_sinks=True)
+    assert sweeps > 10
+    h = 1e-5
+    for e in rng.choice(csr.arcs, 12, replace=False):
+        w = csr.in_w.copy()
+        w[e] += h
+        cp = generators.InCSR(csr.z, csr.n, csr.in_ptr, csr.in_col, w,
+                              np.bincount(csr.in_col, weights=w, minlength=csr.z), csr.outdeg,
+                              None, True)
+        w2 = csr.in_w.copy()
+        w2[e] -= h
+        cm = generators.InCSR(csr.z, csr.n, csr.in_ptr, csr.in_col, w2,
+                              np.bincount(csr.in_col, weights=w2, minlength=csr.z), csr.outdeg,
+                              None, True)
+        fd = (loss(cp)[0] - loss(cm)[0]) / (2 * h)
+        assert abs(fd - gw[e]) <= 1e-7 + 1e-5 * abs(fd)
+    t0 = np.full(csr.z, 1.0 / csr.z)
+    for u in rng.choice(csr.z, 6, replace=False):
+        tp = t0.copy()
+        tp[u] += h
+        tm = t0.copy()
+        tm[u] -= h
+        fd = (loss(csr, tp)[0] - loss(csr, tm)[0]) / (2 * h)
+        assert abs(fd - gt[u]) <= 1e-7 + 1e-5 * abs(fd)

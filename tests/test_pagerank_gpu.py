@@ -1,0 +1,209 @@
+"""Parity of the CUDA PageRank path (through the C ABI) with the oracle.
+
+Bar (plain FP64): L1(scores - oracle) <= 1e-10, |iterations - oracle| <= 1,
+ranking identical apart from (near-)exact ties. FP32: 1e-5 L1 at tol 1e-8."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_NAMES, load_golden
+from networkit_b200 import Graph, _capi, centrality, generators
+from networkit_b200.graph import InCSR
+
+pytestmark = pytest.mark.gpu
+
+L1_FP64 = 1e-10
+
+
+def gpu_run(csr, damp=0.85, tol=1e-8, norm=1, normalized=False, distribute=False,
+            precision=_capi.NKG_PREC_FP64, max_iterations=_capi.UINT64_MAX, teleport=None,
+            reorder=True):
+    dg = _capi.DeviceGraph(csr, reorder=reorder)
+    p = dg.params(damp, tol, norm, normalized, distribute, precision, max_iterations)
+    scores, it, mx, st = dg.run(p, teleport)
+    return dg, scores, it, mx, st
+
+
+def assert_ranking_equal(ids_gpu, ids_ref, scores, rel=1e-12):
+    """Identical except where the two orders swap nodes whose scores tie to
+    within rounding."""
+    ids_gpu = np.asarray(ids_gpu, np.int64)
+    ids_ref = np.asarray(ids_ref, np.int64)
+    assert ids_gpu.shape == ids_ref.shape
+    diff = np.flatnonzero(ids_gpu != ids_ref)
+    for i in diff:
+        a, b = scores[ids_gpu[i]], scores[ids_ref[i]]
+        assert abs(a - b) <= rel * max(abs(a), abs(b)), (i, ids_gpu[i], ids_ref[i], a, b)
+
+
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
+@pytest.mark.parametrize("norm", [0, 1])
+@pytest.mark.parametrize("normalized", [False, True])
+def test_fp64_matches_reference_fixtures(name, norm, normalized):
+    csr, ref = load_golden(name)
+    key = f"n{norm}_z{int(normalized)}"
+    dg, s, it, mx, st = gpu_run(csr, norm=norm, normalized=normalized)
+    ref_s = ref[key + "_scores"]
+    scale = 1.0 if not normalized else float(np.abs(ref_s).sum())
+    assert np.abs(s - ref_s).sum() <= L1_FP64 * scale
+    assert abs(it - int(ref[key + "_iterations"])) <= 1
+    assert abs(mx - float(ref[key + "_maximum"])) <= 1e-10 * max(1.0, abs(mx))
+    ids, vals = dg.ranking(s)
+    assert_ranking_equal(ids, ref[key + "_rank_ids"], s)
+    np.testing.assert_array_equal(vals, s[ids.astype(np.int64)])
+    assert st["kernel_launches"] > 0 and st["fp64_sweeps"] == it
+
+
+@pytest.mark.parametrize("name", ["wikivote_directed", "celegans"])
+def test_max_iterations_two(name):
+    csr, ref = load_golden(name)
+    dg, s, it, mx, st = gpu_run(csr, norm=1, max_iterations=2)
+    assert it == int(ref["n1_z0_max2_iterations"]) == 2
+    assert np.abs(s - ref["n1_z0_max2_scores"]).sum() <= L1_FP64
+
+
+@pytest.mark.parametrize("distribute", [False, True])
+@pytest.mark.parametrize("reorder", [True, False])
+def test_rmat_parity_l1(oracle_mod, distribute, reorder):
+    csr = generators.rmat_directed(16, 16, seed=42)
+    o = oracle_mod.pagerank(csr, tol=1e-10, norm=0, distribute_sinks=distribute)
+    dg, s, it, mx, st = gpu_run(csr, tol=1e-10, norm=0, distribute=distribute, reorder=reorder)
+    assert np.abs(s - o.scores).sum() <= L1_FP64
+    assert abs(it - o.iterations) <= 1
+    ids_o, _ = oracle_mod.ranking(o.scores)
+    ids, _ = dg.ranking(s)
+    assert_ranking_equal(ids, ids_o, o.scores)
+
+
+def test_er_config_parity(oracle_mod):
+    """G(n=1e5, avg degree 10) undirected, L2 1e-8, distributeSinks."""
+    csr = generators.erdos_renyi(100000, 10 / 99999, seed=42)
+    for distribute in (False, True):
+        o = oracle_mod.pagerank(csr, tol=1e-8, norm=1, distribute_sinks=distribute)
+        dg, s, it, mx, st = gpu_run(csr, tol=1e-8, norm=1, distribute=distribute)
+        assert np.abs(s - o.scores).sum() <= L1_FP64
+        assert abs(it - o.iterations) <= 1
+
+
+def test_weighted_parity(oracle_mod):
+    csr = generators.with_uniform_weights(generators.rmat_directed(14, 16, seed=9), seed=43)
+    for normalized in (False, True):
+        o = oracle_mod.pagerank(csr, tol=1e-10, norm=0, normalized=normalized)
+        dg, s, it, mx, st = gpu_run(csr, tol=1e-10, norm=0, normalized=normalized)
+        scale = 1.0 if not normalized else float(np.abs(o.scores).sum())
+        assert np.abs(s - o.scores).sum() <= L1_FP64 * scale
+        assert abs(it - o.iterations) <= 1
+        assert abs(mx - o.maximum) <= 1e-10 * max(1.0, o.maximum)
+
+
+def test_personalised_teleport(oracle_mod):
+    csr = generators.rmat_directed(13, 8, seed=11)
+    rng = np.random.default_rng(3)
+    t = rng.random(csr.z)
+    t /= t.sum()
+    for distribute in (False, True):
+        o = oracle_mod.pagerank(csr, tol=1e-12, norm=0, distribute_sinks=distribute, teleport=t)
+        dg, s, it, mx, st = gpu_run(csr, tol=1e-12, norm=0, distribute=distribute, teleport=t)
+        assert np.abs(s - o.scores).sum() <= L1_FP64
+        assert abs(it - o.iterations) <= 1
+
+
+def test_hub_rows_span_many_tiles(oracle_mod):
+    """Star-like graph: one row of 50k in-arcs crosses ~25 tiles, plus empty
+    and tiny rows around it."""
+    n = 60000
+    src = np.arange(1, 50001, dtype=np.int64)
+    dst = np.zeros(50000, np.int64)
+    extra_s = np.arange(50001, n - 1, dtype=np.int64)
+    extra_d = extra_s + 1
+    s_all = np.concatenate([src, extra_s, [0]])
+    d_all = np.concatenate([dst, extra_d, [7]])
+    G = Graph(n, directed=True)
+    G.addEdges(s_all, d_all)
+    csr = G.inCSR()
+    o = oracle_mod.pagerank(csr, tol=1e-12, norm=0)
+    dg, s, it, mx, st = gpu_run(csr, tol=1e-12, norm=0)
+    assert np.abs(s - o.scores).sum() <= L1_FP64
+    assert abs(it - o.iterations) <= 1
+
+
+def test_deleted_nodes_keep_one_over_n(oracle_mod):
+    G = Graph(10, directed=True)
+    for u, v in [(0, 1), (1, 2), (2, 0), (3, 0), (5, 6), (6, 5), (9, 0)]:
+        G.addEdge(u, v)
+    G.removeNode(4)
+    G.removeNode(8)
+    csr = G.inCSR()
+    o = oracle_mod.pagerank(csr, tol=1e-12, norm=0)
+    pr = centrality.PageRank(G, 0.85, 1e-12)
+    pr.norm = centrality.Norm.l1norm
+    pr.run()
+    s = np.array(pr.scores())
+    assert np.abs(s - o.scores).sum() <= L1_FP64
+    assert s[4] == 1.0 / 8 and s[8] == 1.0 / 8
+    r = pr.ranking()
+    assert len(r) == 8 and 4 not in [u for u, _ in r]
+
+
+@pytest.mark.parametrize("n,edges", [(1, []), (2, []), (3, [(0, 1), (1, 2), (2, 0)]),
+                                     (5, [(0, 0), (1, 1)])])
+def test_tiny_and_degenerate_graphs(oracle_mod, n, edges):
+    for directed in (True, False):
+        G = Graph(n, directed=directed)
+        for u, v in edges:
+            G.addEdge(u, v)
+        csr = G.inCSR()
+        o = oracle_mod.pagerank(csr, norm=1)
+        dg, s, it, mx, st = gpu_run(csr, norm=1)
+        assert np.abs(s - o.scores).sum() <= L1_FP64
+        assert abs(it - o.iterations) <= 1
+
+
+def test_python_api_end_to_end_matches_golden():
+    csr, ref = load_golden("wikivote_directed")
+    G = Graph.fromInCSR(csr)
+    pr = centrality.PageRank(G)
+    assert pr.run() is pr
+    assert pr.hasFinished()
+    s = np.array(pr.scores())
+    assert np.abs(s - ref["n1_z0_scores"]).sum() <= L1_FP64
+    top = pr.ranking()[0]
+    assert top[0] == 326 and abs(top[1] - 0.00460) <= 1e-3
+    assert abs(pr.score(326) - top[1]) == 0.0
+    assert pr.maximum() == 1.0
+    assert abs(pr.numberOfIterations() - int(ref["n1_z0_iterations"])) <= 1
+    assert 0.0 <= pr.centralization() <= 1.0
+
+
+def test_fp32_close_to_fp64(oracle_mod):
+    csr = generators.rmat_directed(15, 16, seed=5)
+    o = oracle_mod.pagerank(csr, tol=1e-8, norm=0)
+    dg, s, it, mx, st = gpu_run(csr, tol=1e-8, norm=0, precision=_capi.NKG_PREC_FP32)
+    assert np.abs(s - o.scores).sum() <= 1e-5
+    assert st["fp32_sweeps"] == it
+
+
+def test_invalid_arguments_raise():
+    csr = generators.rmat_directed(8, 4, seed=1)
+    bad = InCSR(csr.z, csr.n, csr.in_ptr, csr.in_col.copy(), None, csr.wdeg, csr.outdeg, None,
+                True)
+    bad.in_col[3] = csr.z + 5
+    with pytest.raises(_capi.NkgError, match="node id >= z"):
+        _capi.DeviceGraph(bad)
+    bad2 = InCSR(csr.z, csr.n, csr.in_ptr.copy(), csr.in_col, None, csr.wdeg, csr.outdeg, None,
+                 True)
+    bad2.in_ptr[5] = bad2.in_ptr[6] + 1
+    with pytest.raises(_capi.NkgError):
+        _capi.DeviceGraph(bad2)
+    dg = _capi.DeviceGraph(csr)
+    with pytest.raises(_capi.NkgError, match="norm"):
+        dg.run(dg.params(0.85, 1e-8, 7, False, False, 0, 100))
+
+
+def test_repeated_runs_are_bit_identical():
+    csr = generators.rmat_directed(14, 16, seed=2)
+    dg = _capi.DeviceGraph(csr)
+    p = dg.params(0.85, 1e-10, 0, False, True, 0, _capi.UINT64_MAX)
+    a = dg.run(p)
+    b = dg.run(p)
+    np.testing.assert_array_equal(a[0], b[0])
+    assert a[1] == b[1]
