@@ -50,6 +50,11 @@ def parse_args():
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-only", type=int, default=0, metavar="SWEEPS",
+                    help="only upload the graph and run SWEEPS individually launched sweeps "
+                         "(the small, fixed launch sequence used for ncu captures)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="precision of the --profile-only sweeps")
     ap.add_argument("--cache", default=os.path.join(tempfile.gettempdir(), "nk_b200_graphs"))
     return ap.parse_args()
 
@@ -255,6 +260,14 @@ def main():
     arcs, n = csr.arcs, csr.z
     dg = _capi.DeviceGraph(csr, device=local)
     info = dg.info()
+    if args.profile_only:
+        prec = _capi.NKG_PREC_FP64 if args.precision == "fp64" else _capi.NKG_PREC_FP32
+        ms_k, ms_i = dg.profile_sweeps(prec, args.profile_only)
+        print(json.dumps({"profile_only": args.profile_only, "precision": args.precision,
+                          "scale": args.scale, "n": n, "arcs": arcs,
+                          "ms_sweep_kernel": ms_k, "ms_iteration": ms_i}))
+        dg.close()
+        return
     p = dg.params(DAMP, TOL, NORM_L1, False, False, _capi.NKG_PREC_FP64, _capi.UINT64_MAX)
     d_out = torch.empty(n, dtype=torch.float64, device=f"cuda:{local}")
 
@@ -298,7 +311,7 @@ def main():
     hcsr = InCSR(csr.z, csr.n, pin(csr.in_ptr), pin(csr.in_col), None, pin(csr.wdeg),
                  csr.outdeg, None, True)
     e2e_t, e2e_it = [], []
-    for i in range(args.e2e_steps + 1):
+    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         g2 = _capi.DeviceGraph(hcsr, device=local)
@@ -308,7 +321,7 @@ def main():
         if i > 0:  # first call warms the allocator and the module
             e2e_t.append(dt)
             e2e_it.append(it2)
-    e2e_value = world * arcs * sum(e2e_it) / sum(e2e_t) / 1e9
+    e2e_value = world * arcs * sum(e2e_it) / sum(e2e_t) / 1e9 if e2e_t else None
     h2d = 8 * (n + 1) + 4 * arcs
     d2h = 8 * n
 
@@ -335,7 +348,8 @@ def main():
                          "bytes_per_launch": bytes_sweep, "ms_per_launch": ms_kernel,
                          "ms_per_iteration": ms_iter, "peak_source": peak_kind},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * sum(e2e_t) / len(e2e_t)},
+                    "d2h_bytes_per_step": d2h,
+                    "ms_per_step": 1e3 * sum(e2e_t) / len(e2e_t) if e2e_t else None},
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,

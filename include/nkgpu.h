@@ -85,18 +85,19 @@ typedef struct {
     uint64_t n;          /* numberOfNodes */
     uint64_t arcs;       /* in-arcs traversed per sweep */
     uint64_t sinks;      /* existing nodes with out-degree 0 */
-    uint64_t tiles;      /* merge-path tiles of the sweep kernel */
+    uint64_t slots;      /* arc slots of the sliced layout (arcs + padding) */
+    uint64_t split_rows; /* rows longer than one chunk, summed in pieces */
     int32_t weighted;
     int32_t directed;
     int32_t device;
-    int32_t reordered;
+    int32_t reserved;
     double ms_create;    /* device time of nkg_graph_create after the copies */
 } nkg_graph_info;
 
 /* Options of nkg_graph_create_ex. */
 typedef struct {
     int32_t device;      /* CUDA device ordinal (-1: current device) */
-    int32_t reorder;     /* 1: relabel nodes by out-degree (default); 0: keep ids */
+    int32_t reserved[3]; /* must be 0 */
 } nkg_graph_options;
 
 /* Upload a graph given as its in-adjacency CSR.

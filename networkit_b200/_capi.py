@@ -66,11 +66,12 @@ class GraphInfo(C.Structure):
         ("n", C.c_uint64),
         ("arcs", C.c_uint64),
         ("sinks", C.c_uint64),
-        ("tiles", C.c_uint64),
+        ("slots", C.c_uint64),
+        ("split_rows", C.c_uint64),
         ("weighted", C.c_int32),
         ("directed", C.c_int32),
         ("device", C.c_int32),
-        ("reordered", C.c_int32),
+        ("reserved", C.c_int32),
         ("ms_create", C.c_double),
     ]
 
@@ -79,7 +80,7 @@ class GraphInfo(C.Structure):
 
 
 class GraphOptions(C.Structure):
-    _fields_ = [("device", C.c_int32), ("reorder", C.c_int32)]
+    _fields_ = [("device", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 _u64p = C.POINTER(C.c_uint64)
@@ -152,7 +153,7 @@ def ptr(a, t):
 class DeviceGraph:
     """Owning wrapper of an nkg_graph handle."""
 
-    def __init__(self, csr, device: int = -1, reorder: bool = True):
+    def __init__(self, csr, device: int = -1):
         L = lib()
         h = _vp()
         in_ptr = np.ascontiguousarray(csr.in_ptr, np.uint64)
@@ -160,7 +161,8 @@ class DeviceGraph:
         in_w = None if csr.in_w is None else np.ascontiguousarray(csr.in_w, np.float64)
         wdeg = np.ascontiguousarray(csr.wdeg, np.float64)
         ex = None if csr.exists is None else np.ascontiguousarray(csr.exists, np.uint8)
-        opts = GraphOptions(int(device), 1 if reorder else 0)
+        opts = GraphOptions()
+        opts.device = int(device)
         check(L.nkg_graph_create_ex(C.byref(h), int(csr.z), int(in_col.shape[0]),
                                     ptr(in_ptr, _u64p), ptr(in_col, _u32p), ptr(in_w, _f64p),
                                     ptr(wdeg, _f64p), ptr(ex, _u8p), int(bool(csr.directed)),

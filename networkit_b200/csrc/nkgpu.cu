@@ -1,10 +1,9 @@
 // libnkgpu: B200 PageRank behind the C ABI of include/nkgpu.h.
 //
-// Graph upload (nkg_graph_create*) relabels the nodes by out-degree (stable,
-// descending) so that the hot part of the gathered score vector is dense in
-// memory and in L2, and so that all sinks form a suffix of the id range; the
-// per-row arc order (the reference's summation order) is kept. Results are
-// mapped back to the caller's ids on the way out.
+// Graph upload (nkg_graph_create*) relabels the nodes by in-degree,
+// descending (stable), and builds the sliced layout of sweep.cuh; the arc
+// order inside every row (the reference's summation order) is kept. Results
+// are mapped back to the caller's ids on the way out.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -59,26 +58,24 @@ __global__ void validate_and_count(const uint64_t *__restrict__ in_ptr,
     }
 }
 
-// Sort key per original id: deleted nodes 0 (sorted last), then either the
-// out-degree + 1 (reorder) or just "has out-arcs" (stable partition only).
-__global__ void make_keys(const uint32_t *__restrict__ outdeg, const uint8_t *__restrict__ exists,
-                          uint64_t z, int reorder, uint32_t *__restrict__ keys,
-                          uint32_t *__restrict__ ids, unsigned long long *__restrict__ counts) {
+// Sort key per original id: deleted nodes 0 (sorted last), existing nodes
+// in-degree + 1. Counts sinks (existing, out-degree 0).
+__global__ void make_keys(const uint64_t *__restrict__ in_ptr, const uint32_t *__restrict__ outdeg,
+                          const uint8_t *__restrict__ exists, uint64_t z,
+                          uint32_t *__restrict__ keys, uint32_t *__restrict__ ids,
+                          unsigned long long *__restrict__ sinks) {
     const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    bool nonsink = false;
+    bool sink = false;
     if (i < z) {
         const bool ex = exists == nullptr || exists[i];
-        const uint32_t d = outdeg[i];
-        uint32_t k = 0;
-        if (ex)
-            k = reorder ? (d >= 0xfffffffeu ? 0xffffffffu : d + 1u) : (d > 0 ? 2u : 1u);
-        keys[i] = k;
+        const uint64_t d = in_ptr[i + 1] - in_ptr[i];
+        keys[i] = ex ? static_cast<uint32_t>(d + 1) : 0u;
         ids[i] = static_cast<uint32_t>(i);
-        nonsink = ex && d > 0;
+        sink = ex && outdeg[i] == 0;
     }
-    const int c = __syncthreads_count(nonsink);
+    const int c = __syncthreads_count(sink);
     if (threadIdx.x == 0 && c)
-        atomicAdd(counts, static_cast<unsigned long long>(c));
+        atomicAdd(sinks, static_cast<unsigned long long>(c));
 }
 
 // Ranking input: deleted ids get -inf so that they sort behind every score.
@@ -90,12 +87,6 @@ __global__ void ranking_prepare_kernel(double *__restrict__ keys, uint32_t *__re
     if (inv[o] == kNone)
         keys[o] = -1.0 / 0.0;
     ids[o] = static_cast<uint32_t>(o);
-}
-
-static void ranking_prepare(double *keys, uint32_t *ids, const uint32_t *inv, uint64_t z,
-                            cudaStream_t s) {
-    ranking_prepare_kernel<<<ceil_div(z, 256), 256, 0, s>>>(keys, ids, inv, z);
-    NKG_CUDA(cudaGetLastError());
 }
 
 __global__ void build_perm(const uint32_t *__restrict__ sorted_ids, uint64_t n,
@@ -135,28 +126,148 @@ __global__ void relabel_rows(const uint32_t *__restrict__ perm, const uint64_t *
     }
 }
 
-// Merge-path coordinates of every tile boundary (row ends vs arcs).
-__global__ void tile_coords(const uint32_t *__restrict__ row_ptr, uint32_t n, uint32_t arcs,
-                            uint32_t ntiles, uint32_t tile, uint32_t *__restrict__ tile_row,
-                            uint32_t *__restrict__ tile_arc) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t > ntiles)
+// Rows longer than kChunk (a prefix, the rows are sorted by length) and, of
+// those, rows with more than kShortChunks chunks.
+__global__ void count_long(const uint32_t *__restrict__ rowlen, uint64_t n,
+                           unsigned long long *__restrict__ cnt) {
+    const uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    const bool lg = r < n && rowlen[r] > kChunk;
+    const bool vl = r < n && rowlen[r] > kChunk * kShortChunks;
+    const int a = __syncthreads_count(lg);
+    const int b = __syncthreads_count(vl);
+    if (threadIdx.x == 0) {
+        if (a)
+            atomicAdd(cnt, static_cast<unsigned long long>(a));
+        if (b)
+            atomicAdd(cnt + 1, static_cast<unsigned long long>(b));
+    }
+}
+
+__global__ void chunk_counts(const uint32_t *__restrict__ rowlen, uint32_t n_long,
+                             uint32_t *__restrict__ nch) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n_long)
+        nch[r] = (rowlen[r] + kChunk - 1) / kChunk;
+}
+
+// chunk_row[k] = split row of chunk k, chunk_idx[k] = its index in that row.
+__global__ void expand_chunks(const uint32_t *__restrict__ chunk_begin, uint32_t n_long,
+                              uint32_t *__restrict__ chunk_row, uint32_t *__restrict__ chunk_idx) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t r = warp; r < n_long; r += nwarps) {
+        const uint32_t b = chunk_begin[r], e = chunk_begin[r + 1];
+        for (uint32_t k = b + lane; k < e; k += 32) {
+            chunk_row[k] = r;
+            chunk_idx[k] = k - b;
+        }
+    }
+}
+
+// Virtual row v of slice s / lane: its first arc and its length.
+struct VRow {
+    uint32_t start;
+    uint32_t len;
+};
+
+__device__ __forceinline__ VRow vrow_of(uint32_t s, int lane, uint32_t s_chunk, uint32_t n_chunks,
+                                        uint32_t n_long, uint32_t n,
+                                        const uint32_t *__restrict__ chunk_row,
+                                        const uint32_t *__restrict__ chunk_idx,
+                                        const uint32_t *__restrict__ row_ptr) {
+    VRow v{0, 0};
+    if (s < s_chunk) {
+        const uint32_t k = s * 32 + lane;
+        if (k < n_chunks) {
+            const uint32_t r = chunk_row[k], c = chunk_idx[k];
+            const uint32_t rs = row_ptr[r], re = row_ptr[r + 1];
+            v.start = rs + c * kChunk;
+            v.len = min(kChunk, re - v.start);
+        }
+    } else {
+        const uint32_t r = n_long + (s - s_chunk) * 32 + lane;
+        if (r < n) {
+            v.start = row_ptr[r];
+            v.len = row_ptr[r + 1] - v.start;
+        }
+    }
+    return v;
+}
+
+// Slice length = longest of its 32 virtual rows (one warp per slice).
+__global__ void slice_lengths(uint32_t slices, uint32_t s_chunk, uint32_t n_chunks,
+                              uint32_t n_long, uint32_t n, const uint32_t *__restrict__ chunk_row,
+                              const uint32_t *__restrict__ chunk_idx,
+                              const uint32_t *__restrict__ row_ptr, uint32_t *__restrict__ slen,
+                              uint64_t *__restrict__ scost) {
+    const uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (s >= slices)
         return;
-    const uint64_t total = static_cast<uint64_t>(n) + arcs;
-    const uint64_t d64 = static_cast<uint64_t>(t) * tile;
-    const int64_t diag = static_cast<int64_t>(d64 < total ? d64 : total);
-    const int64_t lo0 = diag - static_cast<int64_t>(arcs);
-    int64_t lo = lo0 > 0 ? lo0 : 0;
-    int64_t hi = diag < static_cast<int64_t>(n) ? diag : static_cast<int64_t>(n);
+    const VRow v = vrow_of(s, lane, s_chunk, n_chunks, n_long, n, chunk_row, chunk_idx, row_ptr);
+    uint32_t m = v.len;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) {
+        slen[s] = m;
+        scost[s] = static_cast<uint64_t>(m) + kSliceOverhead;
+    }
+}
+
+// Fill the column-major slices; padding slots point at the zero entry n.
+__global__ void fill_slices(uint32_t slices, uint32_t s_chunk, uint32_t n_chunks, uint32_t n_long,
+                            uint32_t n, const uint32_t *__restrict__ chunk_row,
+                            const uint32_t *__restrict__ chunk_idx,
+                            const uint32_t *__restrict__ row_ptr, const uint32_t *__restrict__ col,
+                            const double *__restrict__ w, const uint32_t *__restrict__ slice_off,
+                            uint32_t *__restrict__ col_sell, double *__restrict__ w_sell) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t s = warp; s < slices; s += nwarps) {
+        const VRow v =
+            vrow_of(s, lane, s_chunk, n_chunks, n_long, n, chunk_row, chunk_idx, row_ptr);
+        const uint32_t off = slice_off[s], len = slice_off[s + 1] - off;
+        for (uint32_t j = 0; j < len; ++j) {
+            const size_t slot = (static_cast<size_t>(off) + j) * 32 + lane;
+            const bool real = j < v.len;
+            col_sell[slot] = real ? col[v.start + j] : n;
+            if (w_sell)
+                w_sell[slot] = real ? w[v.start + j] : 0.0;
+        }
+    }
+}
+
+// Unit u covers slices [unit_start[u], unit_start[u+1]): the boundaries cut
+// the inclusive cost prefix into `units` equal parts.
+__global__ void unit_bounds(const uint64_t *__restrict__ cost_incl, uint32_t slices,
+                            uint32_t units, uint32_t *__restrict__ unit_start) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u > units)
+        return;
+    if (u == units) {
+        unit_start[u] = slices;
+        return;
+    }
+    if (u == 0) {
+        unit_start[0] = 0;
+        return;
+    }
+    const uint64_t total = slices ? cost_incl[slices - 1] : 0;
+    const uint64_t target = total * u / units;
+    // First slice s whose exclusive prefix cost_incl[s-1] >= target, i.e.
+    // one past the first index with an inclusive prefix >= target.
+    uint32_t lo = 0, hi = slices;
     while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (static_cast<int64_t>(row_ptr[mid + 1]) <= diag - mid - 1)
+        const uint32_t mid = (lo + hi) >> 1;
+        if (cost_incl[mid] < target)
             lo = mid + 1;
         else
             hi = mid;
     }
-    tile_row[t] = static_cast<uint32_t>(lo);
-    tile_arc[t] = static_cast<uint32_t>(diag - lo);
+    unit_start[u] = lo + 1 < slices ? lo + 1 : slices;
 }
 
 template <typename T>
@@ -172,16 +283,16 @@ __global__ void convert_array(const double *__restrict__ in, T *__restrict__ out
 // PageRank.cpp:26: x = 1/n, stored in gather form.
 template <typename T, bool WEIGHTED>
 __global__ void init_iterate(T *__restrict__ y, const uint32_t *__restrict__ degc,
-                             const T *__restrict__ degw, uint32_t n, uint32_t n_nonsink,
-                             double x0) {
+                             const T *__restrict__ degw, uint32_t n, double x0) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n)
         return;
     const T x = static_cast<T>(x0);
-    if (r >= n_nonsink)
+    const uint32_t dc = degc[r];
+    if (dc == 0)
         y[r] = x;
     else
-        y[r] = x / (WEIGHTED ? degw[r] : static_cast<T>(degc[r]));
+        y[r] = x / (WEIGHTED ? degw[r] : static_cast<T>(dc));
 }
 
 // Personalised teleport into the relabelled order.
@@ -195,11 +306,12 @@ __global__ void permute_teleport(const double *__restrict__ t_orig, const uint32
 
 template <typename T, bool WEIGHTED>
 __device__ __forceinline__ double final_x(const T *y, const uint32_t *degc, const T *degw,
-                                          uint32_t r, uint32_t n_nonsink) {
+                                          uint32_t r) {
     const T yv = y[r];
-    if (r >= n_nonsink)
+    const uint32_t dc = degc[r];
+    if (dc == 0)
         return static_cast<double>(yv);
-    const T d = WEIGHTED ? degw[r] : static_cast<T>(degc[r]);
+    const T d = WEIGHTED ? degw[r] : static_cast<T>(dc);
     return static_cast<double>(t_mul(yv, d));
 }
 
@@ -210,16 +322,15 @@ constexpr int kRedThreads = 256;
 template <typename T, bool WEIGHTED>
 __global__ void __launch_bounds__(kRedThreads)
     final_reduce(const T *__restrict__ y, const uint32_t *__restrict__ degc,
-                 const T *__restrict__ degw, uint32_t n, uint32_t n_nonsink,
-                 double *__restrict__ part, double *__restrict__ red,
-                 unsigned int *__restrict__ ticket) {
+                 const T *__restrict__ degw, uint32_t n, double *__restrict__ part,
+                 double *__restrict__ red, unsigned int *__restrict__ ticket) {
     __shared__ double s_red[32];
     __shared__ bool s_last;
     double s = 0.0, ss = 0.0, mx = -1.0 / 0.0;
     for (uint32_t r = blockIdx.x * kRedThreads + threadIdx.x; r < n; r += gridDim.x * kRedThreads) {
-        const double x = final_x<T, WEIGHTED>(y, degc, degw, r, n_nonsink);
+        const double x = final_x<T, WEIGHTED>(y, degc, degw, r);
         s += x;
-        if (r >= n_nonsink)
+        if (degc[r] == 0)
             ss += x;
         mx = fmax(mx, x);
     }
@@ -261,21 +372,19 @@ __global__ void __launch_bounds__(kRedThreads)
 template <typename T, bool WEIGHTED>
 __global__ void final_scale(const T *__restrict__ y, const uint32_t *__restrict__ degc,
                             const T *__restrict__ degw, const uint32_t *__restrict__ inv,
-                            uint64_t z, uint32_t n, uint32_t n_nonsink, double damp,
-                            int normalized, double *__restrict__ red, double *__restrict__ out) {
+                            uint64_t z, uint32_t n, double damp, int normalized,
+                            double *__restrict__ red, double *__restrict__ out) {
     const uint64_t o = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (o >= z)
         return;
-    const double inv_n_val = 1.0 / static_cast<double>(n);
     const double factor =
         normalized ? (1.0 / static_cast<double>(n)) * ((1 - damp) + (damp * red[1])) : red[0];
     const uint32_t r = inv[o];
     double v;
-    if (r == kNone) {
-        v = inv_n_val;
-    } else {
-        v = final_x<T, WEIGHTED>(y, degc, degw, r, n_nonsink) / factor;
-    }
+    if (r == kNone)
+        v = 1.0 / static_cast<double>(n);
+    else
+        v = final_x<T, WEIGHTED>(y, degc, degw, r) / factor;
     out[o] = v;
     if (o == 0)
         red[3] = normalized ? fmax(v, red[2] / factor) : 1.0;
@@ -304,12 +413,100 @@ static unsigned num_sms(int dev) {
     return static_cast<unsigned>(v);
 }
 
+template <typename T>
+static T read_scalar(const T *d, cudaStream_t s) {
+    T h{};
+    NKG_CUDA(cudaMemcpyAsync(&h, d, sizeof(T), cudaMemcpyDeviceToHost, s));
+    NKG_CUDA(cudaStreamSynchronize(s));
+    return h;
+}
+
+// Build the sliced layout from the relabelled in-CSR (row_ptr, col, w64src).
+static void build_slices(nkg_graph *g, const uint32_t *rowlen, cudaStream_t s) {
+    const uint32_t n = static_cast<uint32_t>(g->n);
+    const unsigned sms = num_sms(g->device);
+    DeviceArray<unsigned long long> cnt(2);
+    NKG_CUDA(cudaMemsetAsync(cnt.get(), 0, 2 * sizeof(unsigned long long), s));
+    count_long<<<ceil_div(n, 256), 256, 0, s>>>(rowlen, n, cnt.get());
+    NKG_CUDA(cudaGetLastError());
+    unsigned long long h_cnt[2];
+    NKG_CUDA(cudaMemcpyAsync(h_cnt, cnt.get(), sizeof(h_cnt), cudaMemcpyDeviceToHost, s));
+    NKG_CUDA(cudaStreamSynchronize(s));
+    g->n_long = static_cast<uint32_t>(h_cnt[0]);
+    g->n_vlong = static_cast<uint32_t>(h_cnt[1]);
+
+    g->chunk_begin.alloc(static_cast<size_t>(g->n_long) + 1);
+    NKG_CUDA(cudaMemsetAsync(g->chunk_begin.get(), 0, sizeof(uint32_t), s));
+    DeviceArray<uint32_t> chunk_row, chunk_idx;
+    if (g->n_long) {
+        DeviceArray<uint32_t> nch(g->n_long);
+        chunk_counts<<<ceil_div(g->n_long, 256), 256, 0, s>>>(rowlen, g->n_long, nch.get());
+        size_t tb = 0;
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, nch.get(), g->chunk_begin.get() + 1,
+                                               static_cast<int64_t>(g->n_long), s));
+        DeviceArray<unsigned char> tmp(tb);
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb, nch.get(), g->chunk_begin.get() + 1,
+                                               static_cast<int64_t>(g->n_long), s));
+        g->n_chunks = read_scalar(g->chunk_begin.get() + g->n_long, s);
+        chunk_row.alloc(g->n_chunks);
+        chunk_idx.alloc(g->n_chunks);
+        expand_chunks<<<sms * 4, 256, 0, s>>>(g->chunk_begin.get(), g->n_long, chunk_row.get(),
+                                              chunk_idx.get());
+        NKG_CUDA(cudaGetLastError());
+    } else {
+        g->n_chunks = 0;
+    }
+    g->s_chunk = (g->n_chunks + 31) / 32;
+    const uint64_t s_rows = (static_cast<uint64_t>(n - g->n_long) + 31) / 32;
+    const uint64_t slices = g->s_chunk + s_rows;
+    require(slices < 0xffffffffull, "too many slices");
+    g->slices = static_cast<uint32_t>(slices);
+
+    DeviceArray<uint32_t> slen(g->slices);
+    DeviceArray<uint64_t> scost(g->slices);
+    g->slice_cost.alloc(g->slices);
+    g->slice_off.alloc(static_cast<size_t>(g->slices) + 1);
+    if (g->slices) {
+        slice_lengths<<<ceil_div(static_cast<uint64_t>(g->slices) * 32, 256), 256, 0, s>>>(
+            g->slices, g->s_chunk, g->n_chunks, g->n_long, n, chunk_row.get(), chunk_idx.get(),
+            g->row_ptr.get(), slen.get(), scost.get());
+        NKG_CUDA(cudaGetLastError());
+    }
+    NKG_CUDA(cudaMemsetAsync(g->slice_off.get(), 0, sizeof(uint32_t), s));
+    if (g->slices) {
+        size_t tb = 0;
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, slen.get(), g->slice_off.get() + 1,
+                                               static_cast<int64_t>(g->slices), s));
+        size_t tb2 = 0;
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb2, scost.get(), g->slice_cost.get(),
+                                               static_cast<int64_t>(g->slices), s));
+        DeviceArray<unsigned char> tmp(std::max(tb, tb2));
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb, slen.get(), g->slice_off.get() + 1,
+                                               static_cast<int64_t>(g->slices), s));
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb2, scost.get(), g->slice_cost.get(),
+                                               static_cast<int64_t>(g->slices), s));
+    }
+    const uint32_t cols = read_scalar(g->slice_off.get() + g->slices, s);
+    g->slots = static_cast<uint64_t>(cols) * 32;
+    g->col_sell.alloc(g->slots, 4);
+    if (g->weighted)
+        g->w_sell64.alloc(g->slots, 4);
+    if (g->slices) {
+        fill_slices<<<sms * 16, 256, 0, s>>>(g->slices, g->s_chunk, g->n_chunks, g->n_long, n,
+                                             chunk_row.get(), chunk_idx.get(), g->row_ptr.get(),
+                                             g->col.get(), g->w64src.get(), g->slice_off.get(),
+                                             g->col_sell.get(), g->w_sell64.get());
+        NKG_CUDA(cudaGetLastError());
+    }
+    NKG_CUDA(cudaStreamSynchronize(s));
+}
+
 static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr,
                                const uint32_t *in_col, const double *in_w, const double *wdeg,
                                const uint8_t *exists, int directed, const nkg_graph_options *opt) {
     require(z >= 1, "graph must have at least one node id (z >= 1)");
     require(z < 0xffffffffull, "node ids must fit in 32 bits (z < 2^32 - 1)");
-    require(arcs < 0xffffffffull, "graphs with 2^32 or more arcs are not supported");
+    require(arcs < 0xfffffff0ull, "graphs with 2^32 or more arcs are not supported");
     require(in_ptr != nullptr, "in_row_ptr is NULL");
     require(arcs == 0 || in_col != nullptr, "in_col is NULL");
     require(in_w == nullptr || wdeg != nullptr, "weighted graph needs out_wdeg");
@@ -325,7 +522,6 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
     g->arcs = arcs;
     g->weighted = in_w != nullptr;
     g->directed = directed != 0;
-    g->reordered = !(opt && opt->reorder == 0);
     NKG_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
     NKG_CUDA(cudaEventCreate(&g->ev0));
     NKG_CUDA(cudaEventCreate(&g->ev1));
@@ -367,9 +563,7 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
     validate_and_count<<<sms * 8, 256, 0, s>>>(d_ptr.get(), d_col.get(), d_ex.get(), z, arcs,
                                               outdeg.get(), err.get());
     NKG_CUDA(cudaGetLastError());
-    int h_err = 0;
-    NKG_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-    NKG_CUDA(cudaStreamSynchronize(s));
+    const int h_err = read_scalar(err.get(), s);
     switch (h_err) {
     case 0: break;
     case 1: throw Error(NKG_ERR_INVALID_ARG, "in_row_ptr is not non-decreasing within [0, arcs]");
@@ -378,10 +572,10 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
     default: throw Error(NKG_ERR_INVALID_ARG, "a non-existent node has in-arcs");
     }
 
-    // Relabelling order.
+    // Relabelling order: in-degree descending, ties by id.
     DeviceArray<uint32_t> keys(z), ids(z), keys_s(z), ids_s(z);
-    make_keys<<<ceil_div(z, 256), 256, 0, s>>>(outdeg.get(), d_ex.get(), z, g->reordered ? 1 : 0,
-                                               keys.get(), ids.get(), cnt.get());
+    make_keys<<<ceil_div(z, 256), 256, 0, s>>>(d_ptr.get(), outdeg.get(), d_ex.get(), z, keys.get(),
+                                               ids.get(), cnt.get());
     NKG_CUDA(cudaGetLastError());
     size_t tmp_bytes = 0;
     NKG_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, keys.get(), keys_s.get(),
@@ -398,9 +592,8 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
             n += exists[i] != 0;
     }
     require(n >= 1, "graph has no existing node");
-    unsigned long long h_cnt = 0;
-    NKG_CUDA(cudaMemcpyAsync(&h_cnt, cnt.get(), sizeof(h_cnt), cudaMemcpyDeviceToHost, s));
     g->n = n;
+    g->sinks = read_scalar(cnt.get(), s);
 
     g->perm.alloc(n);
     g->inv.alloc(z);
@@ -429,29 +622,21 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
                                               g->inv.get(), g->row_ptr.get(), n, g->col.get(),
                                               g->w64src.get());
     NKG_CUDA(cudaGetLastError());
-
-    g->ntiles = std::max<uint64_t>(1, (n + arcs + kTile - 1) / kTile);
-    require(g->ntiles < 0xffffffffull, "too many tiles");
-    g->tile_row.alloc(g->ntiles + 1);
-    g->tile_arc.alloc(g->ntiles + 1);
-    tile_coords<<<ceil_div(g->ntiles + 1, 256), 256, 0, s>>>(
-        g->row_ptr.get(), static_cast<uint32_t>(n), static_cast<uint32_t>(arcs),
-        static_cast<uint32_t>(g->ntiles), kTile, g->tile_row.get(), g->tile_arc.get());
-    NKG_CUDA(cudaGetLastError());
+    build_slices(g.get(), rowlen.get(), s);
     NKG_CUDA(cudaEventRecord(g->ev1, s));
     NKG_CUDA(cudaStreamSynchronize(s));
-    g->n_nonsink = h_cnt;
     float ms = 0.f;
     NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
     g->ms_create = ms;
 
     // Per-run bookkeeping buffers. The partial-sum arrays are sized for the
-    // largest grid any sweep variant can use (32 resident CTAs per SM), so
+    // largest grid any sweep launch can use (32 resident CTAs per SM), so
     // they are never reallocated under a captured graph.
     g->cta_res.alloc(static_cast<size_t>(sms) * 32);
     g->cta_sink.alloc(static_cast<size_t>(sms) * 32);
-    g->fix_res.alloc(ceil_div(g->ntiles, kFixThreads));
-    g->fix_sink.alloc(ceil_div(g->ntiles, kFixThreads));
+    const size_t fix = static_cast<size_t>(g->n_vlong) + ceil_div(g->n_long, kFixThreads) + 1;
+    g->fix_res.alloc(fix);
+    g->fix_sink.alloc(fix);
     g->rp.alloc(1);
     g->st.alloc(1);
     g->red.alloc(4 + 3 * 4096);
@@ -487,68 +672,71 @@ static void sweep_setup(nkg_graph *g) {
         return;
     cudaStream_t s = g->stream;
     const uint64_t n = g->n;
-    P.y[0].alloc(n, 4);
-    P.y[1].alloc(n, 4);
-    P.head.alloc(g->ntiles);
-    P.tail.alloc(g->ntiles);
-    if (WEIGHTED) {
-        if (std::is_same<T, double>::value) {
-            // FP64 plane reads the FP64 source arrays directly.
-        } else {
-            P.w.alloc(g->arcs, 4);
-            P.degw.alloc(n);
-            if (g->arcs)
-                convert_array<T><<<num_sms(g->device) * 8, 256, 0, s>>>(g->w64src.get(), P.w.get(),
-                                                                         g->arcs);
-            convert_array<T><<<num_sms(g->device) * 8, 256, 0, s>>>(g->degw64src.get(),
-                                                                     P.degw.get(), n);
-            NKG_CUDA(cudaGetLastError());
-        }
+    const unsigned sms = num_sms(g->device);
+    for (int b = 0; b < 2; ++b) {
+        P.y[b].alloc(n + 1, 4);
+        NKG_CUDA(cudaMemsetAsync(P.y[b].get(), 0, (n + 1 + 4) * sizeof(T), s));
     }
-    constexpr size_t smem = SweepSmem<T, WEIGHTED, kSweepThreads, kSweepIPT>::bytes;
-    auto kfn = sweep_kernel<T, WEIGHTED, kSweepThreads, kSweepIPT>;
-    NKG_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(smem)));
+    P.chunk_val.alloc(static_cast<size_t>(g->s_chunk) * 32 + 1);
+    if (WEIGHTED && !std::is_same<T, double>::value) {
+        P.w_sell.alloc(g->slots, 4);
+        P.degw.alloc(n);
+        if (g->slots)
+            convert_array<T><<<sms * 8, 256, 0, s>>>(g->w_sell64.get(), P.w_sell.get(), g->slots);
+        convert_array<T><<<sms * 8, 256, 0, s>>>(g->degw64src.get(), P.degw.get(), n);
+        NKG_CUDA(cudaGetLastError());
+    }
     int occ = 0;
-    NKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kSweepThreads, smem));
+    NKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sweep_kernel<T, WEIGHTED>,
+                                                           kSweepThreads, 0));
     occ = std::max(occ, 1);
-    P.sweep_ctas = static_cast<unsigned>(std::min<uint64_t>(
-        static_cast<uint64_t>(occ) * num_sms(g->device), g->ntiles));
-    P.fix_ctas = ceil_div(g->ntiles, kFixThreads);
+    P.sweep_ctas = static_cast<unsigned>(std::max<uint64_t>(
+        1, std::min<uint64_t>(static_cast<uint64_t>(occ) * sms,
+                              (static_cast<uint64_t>(g->slices) + 7) / 8)));
+    const uint64_t warps = static_cast<uint64_t>(P.sweep_ctas) * (kSweepThreads / 32);
+    P.units = static_cast<uint32_t>(
+        std::max<uint64_t>(1, std::min<uint64_t>(warps * kUnitsPerWarp, g->slices)));
+    P.unit_start.alloc(static_cast<size_t>(P.units) + 1);
+    unit_bounds<<<ceil_div(static_cast<uint64_t>(P.units) + 1, 256), 256, 0, s>>>(
+        g->slice_cost.get(), g->slices, P.units, P.unit_start.get());
+    NKG_CUDA(cudaGetLastError());
+    P.fix_ctas = g->n_vlong + ceil_div(std::max<uint32_t>(g->n_long - g->n_vlong, 1), kFixThreads);
     require(P.sweep_ctas <= g->cta_res.size() && P.fix_ctas <= g->fix_res.size(),
             "partial-sum buffers too small");
+    NKG_CUDA(cudaStreamSynchronize(s));
 }
 
 template <typename T, bool WEIGHTED>
 static SweepArgs<T> sweep_args(nkg_graph *g, int in_buf) {
     Plane<T> &P = plane<T>(g);
     SweepArgs<T> a{};
-    a.row_ptr = g->row_ptr.get();
-    a.col = g->col.get();
+    a.col_sell = g->col_sell.get();
     if (std::is_same<T, double>::value) {
-        a.w = reinterpret_cast<const T *>(g->w64src.get());
+        a.w_sell = reinterpret_cast<const T *>(g->w_sell64.get());
         a.degw = reinterpret_cast<const T *>(g->degw64src.get());
     } else {
-        a.w = P.w.get();
+        a.w_sell = P.w_sell.get();
         a.degw = P.degw.get();
     }
+    a.slice_off = g->slice_off.get();
+    a.unit_start = P.unit_start.get();
+    a.chunk_begin = g->chunk_begin.get();
     a.degc = g->degc.get();
     a.tele = P.tele.get();
     a.y_in = P.y[in_buf].get();
     a.y_out = P.y[in_buf ^ 1].get();
-    a.tile_row = g->tile_row.get();
-    a.tile_arc = g->tile_arc.get();
-    a.head_val = P.head.get();
-    a.tail_val = P.tail.get();
+    a.chunk_val = P.chunk_val.get();
     a.cta_res = g->cta_res.get();
     a.cta_sink = g->cta_sink.get();
     a.fix_res = g->fix_res.get();
     a.fix_sink = g->fix_sink.get();
     a.rp = g->rp.get();
     a.st = g->st.get();
-    a.ntiles = static_cast<uint32_t>(g->ntiles);
     a.n = static_cast<uint32_t>(g->n);
-    a.n_nonsink = static_cast<uint32_t>(g->n_nonsink);
+    a.n_long = g->n_long;
+    a.n_vlong = g->n_vlong;
+    a.s_chunk = g->s_chunk;
+    a.units = P.units;
     a.sweep_ctas = P.sweep_ctas;
     return a;
 }
@@ -557,9 +745,8 @@ template <typename T, bool WEIGHTED>
 static void launch_sweep(nkg_graph *g, int in_buf, cudaStream_t s) {
     Plane<T> &P = plane<T>(g);
     const SweepArgs<T> a = sweep_args<T, WEIGHTED>(g, in_buf);
-    constexpr size_t smem = SweepSmem<T, WEIGHTED, kSweepThreads, kSweepIPT>::bytes;
-    sweep_kernel<T, WEIGHTED, kSweepThreads, kSweepIPT><<<P.sweep_ctas, kSweepThreads, smem, s>>>(a);
-    fixup_kernel<T, WEIGHTED, kFixThreads><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
+    sweep_kernel<T, WEIGHTED><<<P.sweep_ctas, kSweepThreads, 0, s>>>(a);
+    fixup_kernel<T, WEIGHTED><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
 }
 
 // Capture kSweepsPerGraph sweeps (sweep + fix-up each) as one CUDA graph.
@@ -602,18 +789,14 @@ static uint64_t bytes_per_sweep(const nkg_graph *g, int elem) {
 }
 
 template <typename T, bool WEIGHTED>
-static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *teleport_host,
-                           double *d_out) {
+static void upload_run_state(nkg_graph *g, const nkg_pr_params &p, int personal,
+                             const double *teleport_host, DeviceArray<double> &d_tele_orig) {
     cudaStream_t s = g->stream;
-    sweep_setup<T, WEIGHTED>(g);
     Plane<T> &P = plane<T>(g);
-    const int personal = teleport_host ? 1 : 0;
     const uint32_t n = static_cast<uint32_t>(g->n);
-    RunResult R;
-
     RunParams *rp = reinterpret_cast<RunParams *>(g->scalars_host.get());
-    // scalars_host holds 8 doubles = 64 bytes >= sizeof(RunParams)
     static_assert(sizeof(RunParams) <= 8 * sizeof(double), "RunParams fits the pinned buffer");
+    std::memset(rp, 0, sizeof(RunParams));
     rp->damp = p.damp;
     rp->tele_uniform = (1.0 - p.damp) / static_cast<double>(n);
     rp->one_minus_damp = 1.0 - p.damp;
@@ -623,12 +806,8 @@ static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *t
     rp->l2 = p.norm == NKG_NORM_L2 ? 1 : 0;
     rp->tol = p.tol;
     rp->max_iterations = p.max_iterations;
-
-    DeviceArray<double> d_tele_orig;
-    NKG_CUDA(cudaEventRecord(g->ev0, s));
     NKG_CUDA(cudaMemcpyAsync(g->rp.get(), rp, sizeof(RunParams), cudaMemcpyHostToDevice, s));
     const double x0 = 1.0 / static_cast<double>(n);
-    double S0 = 0.0;
     if (personal) {
         if (!P.tele)
             P.tele.alloc(n);
@@ -637,21 +816,35 @@ static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *t
                                  cudaMemcpyHostToDevice, s));
         permute_teleport<T><<<ceil_div(n, 256), 256, 0, s>>>(d_tele_orig.get(), g->perm.get(), n,
                                                              P.tele.get());
-        R.launches++;
     }
-    S0 = static_cast<double>(g->n - g->n_nonsink) * x0;
+    const double S0 = static_cast<double>(g->sinks) * x0;
     IterState *sh = g->st_host.get();
     std::memset(sh, 0, sizeof(IterState));
     sh->sink_coef = p.distribute_sinks ? (personal ? S0 : S0 / static_cast<double>(n)) : 0.0;
     sh->sink_mass = S0;
     NKG_CUDA(cudaMemcpyAsync(g->st.get(), sh, sizeof(IterState), cudaMemcpyHostToDevice, s));
     init_iterate<T, WEIGHTED><<<ceil_div(n, 256), 256, 0, s>>>(
-        P.y[0].get(), g->degc.get(), WEIGHTED ? sweep_args<T, WEIGHTED>(g, 0).degw : nullptr, n,
-        static_cast<uint32_t>(g->n_nonsink), x0);
+        P.y[0].get(), g->degc.get(), sweep_args<T, WEIGHTED>(g, 0).degw, n, x0);
     NKG_CUDA(cudaGetLastError());
-    R.launches++;
+}
+
+template <typename T, bool WEIGHTED>
+static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *teleport_host,
+                           double *d_out) {
+    cudaStream_t s = g->stream;
+    sweep_setup<T, WEIGHTED>(g);
+    Plane<T> &P = plane<T>(g);
+    const int personal = teleport_host ? 1 : 0;
+    const uint32_t n = static_cast<uint32_t>(g->n);
+    RunResult R;
+
+    DeviceArray<double> d_tele_orig;
+    NKG_CUDA(cudaEventRecord(g->ev0, s));
+    upload_run_state<T, WEIGHTED>(g, p, personal, teleport_host, d_tele_orig);
+    R.launches += 1 + personal;
 
     cudaGraphExec_t exec = sweep_graph<T, WEIGHTED>(g, personal);
+    IterState *sh = g->st_host.get();
     int batch = 1;
     for (;;) {
         for (int b = 0; b < batch; ++b)
@@ -673,15 +866,13 @@ static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *t
     R.sink_mass = sh->sink_mass;
     const int fin = static_cast<int>(R.iterations & 1ull);
     const T *yfin = P.y[fin].get();
-    const T *degw = WEIGHTED ? sweep_args<T, WEIGHTED>(g, 0).degw : nullptr;
+    const T *degw = sweep_args<T, WEIGHTED>(g, 0).degw;
     const unsigned rblocks = std::min<unsigned>(num_sms(g->device) * 2, 4096);
-    final_reduce<T, WEIGHTED><<<rblocks, kRedThreads, 0, s>>>(yfin, g->degc.get(), degw, n,
-                                                              static_cast<uint32_t>(g->n_nonsink),
-                                                              g->red.get() + 4, g->red.get(),
-                                                              g->red_ticket.get());
+    final_reduce<T, WEIGHTED><<<rblocks, kRedThreads, 0, s>>>(
+        yfin, g->degc.get(), degw, n, g->red.get() + 4, g->red.get(), g->red_ticket.get());
     final_scale<T, WEIGHTED><<<ceil_div(g->z, 256), 256, 0, s>>>(
-        yfin, g->degc.get(), degw, g->inv.get(), g->z, n, static_cast<uint32_t>(g->n_nonsink),
-        p.damp, p.normalized ? 1 : 0, g->red.get(), d_out);
+        yfin, g->degc.get(), degw, g->inv.get(), g->z, n, p.damp, p.normalized ? 1 : 0,
+        g->red.get(), d_out);
     NKG_CUDA(cudaGetLastError());
     R.launches += 2;
     NKG_CUDA(cudaEventRecord(g->ev2, s));
@@ -750,33 +941,22 @@ static void profile_sweeps(nkg_graph *g, int sweeps, double *ms_kernel, double *
     cudaStream_t s = g->stream;
     sweep_setup<T, WEIGHTED>(g);
     Plane<T> &P = plane<T>(g);
-    const uint32_t n = static_cast<uint32_t>(g->n);
-    RunParams *rp = reinterpret_cast<RunParams *>(g->scalars_host.get());
-    std::memset(rp, 0, sizeof(RunParams));
-    rp->damp = 0.85;
-    rp->tele_uniform = 0.15 / static_cast<double>(n);
-    rp->one_minus_damp = 0.15;
-    rp->inv_n = 1.0 / static_cast<double>(n);
-    rp->tol = -1.0;
-    rp->max_iterations = ~0ull;
-    IterState *sh = g->st_host.get();
-    std::memset(sh, 0, sizeof(IterState));
-    NKG_CUDA(cudaMemcpyAsync(g->rp.get(), rp, sizeof(RunParams), cudaMemcpyHostToDevice, s));
-    NKG_CUDA(cudaMemcpyAsync(g->st.get(), sh, sizeof(IterState), cudaMemcpyHostToDevice, s));
-    init_iterate<T, WEIGHTED><<<ceil_div(n, 256), 256, 0, s>>>(
-        P.y[0].get(), g->degc.get(), sweep_args<T, WEIGHTED>(g, 0).degw, n,
-        static_cast<uint32_t>(g->n_nonsink), 1.0 / static_cast<double>(n));
-    NKG_CUDA(cudaGetLastError());
+    nkg_pr_params p{};
+    p.damp = 0.85;
+    p.tol = -1.0;
+    p.norm = NKG_NORM_L1;
+    p.max_iterations = ~0ull;
+    DeviceArray<double> unused;
+    upload_run_state<T, WEIGHTED>(g, p, 0, nullptr, unused);
     std::vector<cudaEvent_t> ev(2 * static_cast<size_t>(sweeps), nullptr);
     for (auto &e : ev)
         NKG_CUDA(cudaEventCreate(&e));
-    constexpr size_t smem = SweepSmem<T, WEIGHTED, kSweepThreads, kSweepIPT>::bytes;
     for (int i = 0; i < sweeps; ++i) {
         const SweepArgs<T> a = sweep_args<T, WEIGHTED>(g, i & 1);
         NKG_CUDA(cudaEventRecord(ev[2 * i], s));
-        sweep_kernel<T, WEIGHTED, kSweepThreads, kSweepIPT><<<P.sweep_ctas, kSweepThreads, smem, s>>>(a);
+        sweep_kernel<T, WEIGHTED><<<P.sweep_ctas, kSweepThreads, 0, s>>>(a);
         NKG_CUDA(cudaEventRecord(ev[2 * i + 1], s));
-        fixup_kernel<T, WEIGHTED, kFixThreads><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
+        fixup_kernel<T, WEIGHTED><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
     }
     NKG_CUDA(cudaGetLastError());
     NKG_CUDA(cudaStreamSynchronize(s));
@@ -787,8 +967,6 @@ static void profile_sweeps(nkg_graph *g, int sweeps, double *ms_kernel, double *
         sum += ms;
     }
     float total = 0.f;
-    // first sweep start -> last sweep end, plus one fix-up per sweep: use the
-    // span from the first sweep to the start of the last one over sweeps-1
     if (sweeps > 1)
         NKG_CUDA(cudaEventElapsedTime(&total, ev[0], ev[2 * (sweeps - 1)]));
     for (auto &e : ev)
@@ -838,6 +1016,12 @@ static int run_to(nkg_graph *g, const nkg_pr_params *p, const double *teleport, 
             *max_out = R.maximum;
         fill_stats(g, R, p->precision, stats);
     });
+}
+
+static void ranking_prepare(double *keys, uint32_t *ids, const uint32_t *inv, uint64_t z,
+                            cudaStream_t s) {
+    ranking_prepare_kernel<<<ceil_div(z, 256), 256, 0, s>>>(keys, ids, inv, z);
+    NKG_CUDA(cudaGetLastError());
 }
 
 } // namespace nkg
@@ -897,12 +1081,12 @@ int nkg_graph_get_info(const nkg_graph *g, nkg_graph_info *info) {
         info->z = g->z;
         info->n = g->n;
         info->arcs = g->arcs;
-        info->sinks = g->n - g->n_nonsink;
-        info->tiles = g->ntiles;
+        info->sinks = g->sinks;
+        info->slots = g->slots;
+        info->split_rows = g->n_long;
         info->weighted = g->weighted;
         info->directed = g->directed;
         info->device = g->device;
-        info->reordered = g->reordered;
         info->ms_create = g->ms_create;
     });
 }

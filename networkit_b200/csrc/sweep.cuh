@@ -1,25 +1,35 @@
-// One Jacobi sweep of PageRank (PageRank.cpp:56-70) as a merge-path pull SpMV
-// over the in-CSR plus a fix-up kernel that finishes rows cut by tile
-// boundaries and closes the iteration (residual, sink mass, convergence).
+// One Jacobi sweep of PageRank (PageRank.cpp:56-70) as a sliced-ELLPACK pull
+// SpMV over the in-adjacency, plus a fix-up kernel that finishes the rows that
+// were split into chunks and closes the iteration (residual, sink mass,
+// convergence test).
 //
-// Storage: the iterate is kept in "gather form" y[r] = x[r] / deg[r] for nodes
-// with out-arcs and y[r] = x[r] for sinks, so that a sweep gathers exactly the
-// per-arc term x[v]*w/deg[v] of PageRank.cpp:62 (bit-identical for unweighted
-// graphs, where w = 1). The previous x[r] needed by the stopping test
-// (PageRank.cpp:41-51) is recovered as y[r]*deg[r].
+// Storage of the iterate: "gather form" y[r] = x[r] / deg[r] for nodes with
+// out-arcs and y[r] = x[r] for sinks, so a sweep gathers exactly the per-arc
+// term x[v]*w/deg[v] of PageRank.cpp:62 (bit-identical for unweighted graphs,
+// where w = 1). The previous x[r] for the stopping test (PageRank.cpp:41-51)
+// is recovered as y[r]*deg[r]. y has one extra zero entry at index n, the
+// target of padding slots.
 //
-// Work split (Merrill & Garland, "Merge-based Parallel Sparse Matrix-Vector
-// Multiplication", SC'16): the sequence of n row-ends and `arcs` arcs is cut
-// into tiles of TILE = THREADS*IPT items; a persistent CTA walks tiles
-// blockIdx.x, blockIdx.x+gridDim.x, ... Every thread consumes IPT consecutive
-// items, so power-law rows cost the same per item as short ones. Rows that
-// straddle a tile boundary leave a head/tail partial for the fix-up kernel.
-// All sums use fixed trees, so a run is bit-reproducible.
+// Layout (SELL-C-sigma, Kreutzer et al., SIAM J. Sci. Comput. 36(5), 2014, with
+// C = 32 and sigma = n): nodes are relabelled by in-degree, descending, so 32
+// consecutive rows have nearly equal length. Rows longer than kChunk arcs are
+// cut into chunks of kChunk arcs ("virtual rows", placed first). Slice s holds
+// 32 virtual rows column-major: slot (j, lane) at col_sell[(off[s] + j) * 32 +
+// lane], so a warp loads 128 contiguous bytes per step and every lane sums its
+// own row sequentially, in the reference's arc order. No shared memory and no
+// barriers are needed: the whole L1 is left to cache the hot part of y.
+// Warps walk contiguous, cost-balanced ranges of slices ("units", fixed at
+// set-up), so every sum has a fixed order and a run is bit-reproducible.
 #pragma once
 
 #include "common.cuh"
 
 namespace nkg {
+
+// Arcs per chunk of a split row; also the longest sequential loop of a lane.
+constexpr uint32_t kChunk = 256;
+// A split row with more chunks than this is summed by a whole CTA.
+constexpr uint32_t kShortChunks = 16;
 
 // Constant per run, read from device memory so that captured CUDA graphs
 // stay valid across runs with different parameters.
@@ -44,32 +54,34 @@ struct IterState {
     double sink_coef;              // sink term applied by the next sweep
     int done;                      // converged / max reached
     unsigned int ticket;           // last-block detection in the fix-up
-    int pad[2];
+    int error;
+    int pad;
 };
 
 template <typename T>
 struct SweepArgs {
-    const uint32_t *__restrict__ row_ptr;  // n+1
-    const uint32_t *__restrict__ col;      // arcs (node ids after relabelling)
-    const T *__restrict__ w;               // arc weights (weighted graphs)
-    const uint32_t *__restrict__ degc;     // out-degree count (unweighted)
-    const T *__restrict__ degw;            // weighted out-degree (weighted)
-    const T *__restrict__ tele;            // personalised teleport (n) or null
-    const T *__restrict__ y_in;
+    const uint32_t *__restrict__ col_sell;   // slices, column-major, padded with n
+    const T *__restrict__ w_sell;            // matching weights (weighted graphs)
+    const uint32_t *__restrict__ slice_off;  // S+1, in units of 32 slots
+    const uint32_t *__restrict__ unit_start; // U+1 slice indices
+    const uint32_t *__restrict__ chunk_begin;// n_long+1: chunks of split row r
+    const uint32_t *__restrict__ degc;       // out-degree count (sink test)
+    const T *__restrict__ degw;              // weighted out-degree (weighted graphs)
+    const T *__restrict__ tele;              // personalised teleport (n) or null
+    const T *__restrict__ y_in;              // n+1 (y_in[n] = 0)
     T *__restrict__ y_out;
-    const uint32_t *__restrict__ tile_row; // ntiles+1 merge-path coordinates
-    const uint32_t *__restrict__ tile_arc;
-    T *__restrict__ head_val;              // per tile: partial of its first row
-    T *__restrict__ tail_val;              // per tile: partial of its last row
-    double *__restrict__ cta_res;          // per sweep CTA
+    T *__restrict__ chunk_val;               // per chunk slot: partial row sum
+    double *__restrict__ cta_res;            // per sweep CTA
     double *__restrict__ cta_sink;
-    double *__restrict__ fix_res;          // per fix-up CTA
+    double *__restrict__ fix_res;            // per fix-up CTA
     double *__restrict__ fix_sink;
     const RunParams *__restrict__ rp;
     IterState *st;
-    uint32_t ntiles;
     uint32_t n;
-    uint32_t n_nonsink;  // rows [n_nonsink, n) are sinks (out-degree 0)
+    uint32_t n_long;        // rows [0, n_long) are split into chunks
+    uint32_t n_vlong;       // rows [0, n_vlong) have more than kShortChunks chunks
+    uint32_t s_chunk;       // slices [0, s_chunk) hold chunks, the rest rows
+    uint32_t units;
     uint32_t sweep_ctas;
 };
 
@@ -93,18 +105,15 @@ __device__ __forceinline__ float t_add<float>(float a, float b) { return __fadd_
 template <typename T, bool WEIGHTED>
 __device__ __forceinline__ void finish_row(const SweepArgs<T> &a, const RunParams &rp, T sink_coef,
                                            uint32_t r, T acc, double &res, double &sink) {
+    const uint32_t dc = ld_stream(a.degc + r);
+    const T deg = WEIGHTED ? ld_stream(a.degw + r) : static_cast<T>(dc);
+    const T yo = a.y_in[r];
     if (rp.distribute)
         acc = t_add(acc, rp.personal ? t_mul(sink_coef, a.tele[r]) : sink_coef);
     T x = t_mul(acc, static_cast<T>(rp.damp));
     x = t_add(x, rp.personal ? t_mul(static_cast<T>(rp.one_minus_damp), a.tele[r])
                              : static_cast<T>(rp.tele_uniform));
-    const bool is_sink = r >= a.n_nonsink;
-    const T yo = a.y_in[r];
-    T deg;
-    if (WEIGHTED)
-        deg = ld_stream(a.degw + r);
-    else
-        deg = static_cast<T>(ld_stream(a.degc + r));
+    const bool is_sink = dc == 0;
     const T xo = is_sink ? yo : t_mul(yo, deg);
     const double d = static_cast<double>(xo) - static_cast<double>(x);
     res += rp.l2 ? __dmul_rn(d, d) : fabs(d);
@@ -116,178 +125,81 @@ __device__ __forceinline__ void finish_row(const SweepArgs<T> &a, const RunParam
     }
 }
 
-// Segmented inclusive scan of (row, value) pairs over the block in thread
-// order: (r1,v1) + (r2,v2) = (r2, r1 == r2 ? v1 + v2 : v2). Rows are
-// non-decreasing in thread order, which makes the operator associative.
-// Returns the exclusive prefix in (ex_row, ex_val) (ex_row = kNone for thread
-// 0) and the inclusive value in inc_val.
-template <typename T, int THREADS>
-__device__ __forceinline__ void seg_scan(uint32_t row, T val, uint32_t &ex_row, T &ex_val,
-                                         T &inc_val, uint32_t *s_wrow, T *s_wval) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    T v = val;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const T vu = __shfl_up_sync(0xffffffffu, v, o);
-        const uint32_t ru = __shfl_up_sync(0xffffffffu, row, o);
-        if (lane >= o && ru == row)
-            v = vu + v;
-    }
-    if (lane == 31) {
-        s_wrow[wid] = row;
-        s_wval[wid] = v;
-    }
-    __syncthreads();
-    uint32_t pr = kNone;
-    T pv = T(0);
-    for (int j = 0; j < wid; ++j) {
-        const uint32_t rj = s_wrow[j];
-        const T vj = s_wval[j];
-        pv = (pr == rj) ? pv + vj : vj;
-        pr = rj;
-    }
-    if (wid > 0 && pr == row)
-        v = pv + v;
-    inc_val = v;
-    const T vprev = __shfl_up_sync(0xffffffffu, v, 1);
-    const uint32_t rprev = __shfl_up_sync(0xffffffffu, row, 1);
-    if (lane > 0) {
-        ex_row = rprev;
-        ex_val = vprev;
-    } else {
-        ex_row = wid > 0 ? pr : kNone;
-        ex_val = pv;
-    }
-}
+constexpr int kSweepThreads = 256;
+constexpr int kUnroll = 8;
 
-template <typename T, bool WEIGHTED, int THREADS, int IPT>
-struct SweepSmem {
-    static constexpr int TILE = THREADS * IPT;
-    static constexpr size_t bytes = sizeof(T) * TILE * 2 + sizeof(uint32_t) * TILE;
-};
-
-template <typename T, bool WEIGHTED, int THREADS, int IPT>
-__global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs<T> a) {
-    constexpr int TILE = THREADS * IPT;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *s_val = reinterpret_cast<T *>(smem_raw);
-    T *s_rowsum = s_val + TILE;
-    uint32_t *s_rowend = reinterpret_cast<uint32_t *>(s_rowsum + TILE);
-    __shared__ uint32_t s_wrow[THREADS / 32];
-    __shared__ T s_wval[THREADS / 32];
+// The sweep: each warp walks its units; each lane accumulates one virtual
+// row of a slice. Chunk slices store partial sums; row slices finish rows.
+template <typename T, bool WEIGHTED>
+__global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepArgs<T> a) {
     __shared__ double s_red[32];
-    __shared__ int s_head;
-
     if (*(volatile int *)&a.st->done)
         return;
     const RunParams rp = *a.rp;
     const T sink_coef = static_cast<T>(a.st->sink_coef);
+    const int lane = threadIdx.x & 31;
+    const uint32_t wpc = kSweepThreads / 32;
+    const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);
+    const uint32_t nw = gridDim.x * wpc;
     double res = 0.0, sink = 0.0;
-
-    for (uint32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const uint32_t row0 = a.tile_row[t], row1 = a.tile_row[t + 1];
-        const uint32_t arc0 = a.tile_arc[t], arc1 = a.tile_arc[t + 1];
-        const int nr = static_cast<int>(row1 - row0);
-        const int na = static_cast<int>(arc1 - arc0);
-        __syncthreads();  // smem of the previous tile is no longer read
-        for (int i = threadIdx.x; i < nr; i += THREADS)
-            s_rowend[i] = ld_stream(a.row_ptr + row0 + i + 1) - arc0;
-        if (threadIdx.x == 0)
-            s_head = (nr > 0 && a.row_ptr[row0] < arc0) ? 1 : 0;
-        // Gather phase: all column loads first, then all gathers, so every
-        // thread keeps IPT independent loads in flight.
-        uint32_t c[IPT];
+    for (uint32_t u = gw; u < a.units; u += nw) {
+        const uint32_t s_end = a.unit_start[u + 1];
+        for (uint32_t s = a.unit_start[u]; s < s_end; ++s) {
+            const uint32_t off = a.slice_off[s];
+            const uint32_t len = a.slice_off[s + 1] - off;
+            const size_t base = static_cast<size_t>(off) * 32 + lane;
+            const uint32_t *cp = a.col_sell + base;
+            T acc = T(0);
+            uint32_t j = 0;
+            for (; j + kUnroll <= len; j += kUnroll) {
+                uint32_t c[kUnroll];
 #pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            const int i = k * THREADS + threadIdx.x;
-            c[k] = i < na ? ld_stream(a.col + arc0 + i) : kNone;
-        }
-        T v[IPT];
+                for (int k = 0; k < kUnroll; ++k)
+                    c[k] = ld_stream(cp + static_cast<size_t>(j + k) * 32);
+                T v[kUnroll];
 #pragma unroll
-        for (int k = 0; k < IPT; ++k)
-            v[k] = c[k] != kNone ? __ldg(a.y_in + c[k]) : T(0);
-        if (WEIGHTED) {
+                for (int k = 0; k < kUnroll; ++k)
+                    v[k] = __ldg(a.y_in + c[k]);
+                if (WEIGHTED) {
 #pragma unroll
-            for (int k = 0; k < IPT; ++k) {
-                const int i = k * THREADS + threadIdx.x;
-                if (i < na)
-                    v[k] = t_mul(v[k], ld_stream(a.w + arc0 + i));
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            const int i = k * THREADS + threadIdx.x;
-            if (i < na)
-                s_val[i] = v[k];
-        }
-        __syncthreads();
-
-        // Merge-path split of this thread's IPT items.
-        const int total = nr + na;
-        const int diag = min(static_cast<int>(threadIdx.x) * IPT, total);
-        const int diag_end = min(diag + IPT, total);
-        int lo = max(diag - na, 0), hi = min(diag, nr);
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (static_cast<int>(s_rowend[mid]) <= diag - mid - 1)
-                lo = mid + 1;
-            else
-                hi = mid;
-        }
-        int ri = lo, ai = diag - lo;
-        T acc = T(0), first_val = T(0);
-        int first_row = -1;
-        for (int k = diag; k < diag_end; ++k) {
-            if (ri < nr && ai >= static_cast<int>(s_rowend[ri])) {
-                if (first_row < 0) {
-                    first_row = ri;
-                    first_val = acc;
-                } else {
-                    s_rowsum[ri] = acc;
+                    for (int k = 0; k < kUnroll; ++k)
+                        v[k] = t_mul(v[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
                 }
-                acc = T(0);
-                ++ri;
+#pragma unroll
+                for (int k = 0; k < kUnroll; ++k)
+                    acc += v[k];
+            }
+            for (; j < len; ++j) {
+                T v = __ldg(a.y_in + ld_stream(cp + static_cast<size_t>(j) * 32));
+                if (WEIGHTED)
+                    v = t_mul(v, ld_stream(a.w_sell + base + static_cast<size_t>(j) * 32));
+                acc += v;
+            }
+            if (s < a.s_chunk) {
+                a.chunk_val[static_cast<size_t>(s) * 32 + lane] = acc;
             } else {
-                acc += s_val[ai];
-                ++ai;
+                const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
+                if (r < a.n)
+                    finish_row<T, WEIGHTED>(a, rp, sink_coef, r, acc, res, sink);
             }
-        }
-        // Rows cut between threads: add the partial sums of earlier threads.
-        uint32_t ex_row;
-        T ex_val, inc_val;
-        seg_scan<T, THREADS>(static_cast<uint32_t>(ri), acc, ex_row, ex_val, inc_val, s_wrow,
-                             s_wval);
-        if (first_row >= 0)
-            s_rowsum[first_row] =
-                (ex_row == static_cast<uint32_t>(first_row)) ? ex_val + first_val : first_val;
-        // The last row has arcs past the last row end: hand its partial on.
-        if (threadIdx.x == THREADS - 1) {
-            const bool tail = na > 0 && (nr == 0 || static_cast<int>(s_rowend[nr - 1]) < na);
-            if (tail)
-                a.tail_val[t] = inc_val;
-        }
-        __syncthreads();
-        const int head = s_head;
-        for (int i = threadIdx.x; i < nr; i += THREADS) {
-            if (i == 0 && head) {
-                a.head_val[t] = s_rowsum[0];
-                continue;
-            }
-            finish_row<T, WEIGHTED>(a, rp, sink_coef, row0 + i, s_rowsum[i], res, sink);
         }
     }
-    const double bres = block_sum<THREADS>(res, s_red);
-    const double bsink = block_sum<THREADS>(sink, s_red);
+    const double bres = block_sum<kSweepThreads>(res, s_red);
+    const double bsink = block_sum<kSweepThreads>(sink, s_red);
     if (threadIdx.x == 0) {
         a.cta_res[blockIdx.x] = bres;
         a.cta_sink[blockIdx.x] = bsink;
     }
 }
 
-// Finish the rows that start in an earlier tile, then (last CTA) reduce all
-// partial sums in index order and close the iteration (PageRank.cpp:68-70).
-template <typename T, bool WEIGHTED, int THREADS>
-__global__ void __launch_bounds__(THREADS) fixup_kernel(SweepArgs<T> a) {
+// Fix-up: finish the split rows from their chunk sums (in chunk order), then
+// (last CTA) reduce all partial sums in index order and close the iteration
+// (PageRank.cpp:68-70). CTAs [0, n_vlong) each finish one row with many
+// chunks; the others take one split row per thread.
+constexpr int kFixThreads = 256;
+
+template <typename T, bool WEIGHTED>
+__global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
     __shared__ double s_red[32];
     __shared__ bool s_last;
     if (*(volatile int *)&a.st->done)
@@ -295,24 +207,32 @@ __global__ void __launch_bounds__(THREADS) fixup_kernel(SweepArgs<T> a) {
     const RunParams rp = *a.rp;
     const T sink_coef = static_cast<T>(a.st->sink_coef);
     double res = 0.0, sink = 0.0;
-    const uint32_t t = blockIdx.x * THREADS + threadIdx.x;
-    if (t < a.ntiles) {
-        const uint32_t row0 = a.tile_row[t];
-        const uint32_t rs = a.row_ptr[row0];
-        if (a.tile_row[t + 1] > row0 && a.tile_arc[t] > rs) {
-            // Tiles t0..t-1 end inside row0; sum their tails in order.
-            uint32_t t0 = t - 1;
-            while (t0 > 0 && a.tile_row[t0] == row0 && a.tile_arc[t0] > rs)
-                --t0;
+    if (blockIdx.x < a.n_vlong) {
+        const uint32_t r = blockIdx.x;
+        const uint32_t cb = a.chunk_begin[r], ce = a.chunk_begin[r + 1];
+        T part = T(0);
+        for (uint32_t k = cb + threadIdx.x; k < ce; k += kFixThreads)
+            part += a.chunk_val[k];
+        const double tot = block_sum<kFixThreads>(static_cast<double>(part), s_red);
+        if (threadIdx.x == 0)
+            finish_row<T, WEIGHTED>(a, rp, sink_coef, r, static_cast<T>(tot), res, sink);
+    } else {
+        const uint32_t r = a.n_vlong + (blockIdx.x - a.n_vlong) * kFixThreads + threadIdx.x;
+        if (r < a.n_long) {
+            const uint32_t cb = a.chunk_begin[r], ce = a.chunk_begin[r + 1];
+            T parts[kShortChunks];
+#pragma unroll
+            for (uint32_t k = 0; k < kShortChunks; ++k)
+                parts[k] = cb + k < ce ? a.chunk_val[cb + k] : T(0);
             T sum = T(0);
-            for (uint32_t k = t0; k < t; ++k)
-                sum += a.tail_val[k];
-            sum += a.head_val[t];
-            finish_row<T, WEIGHTED>(a, rp, sink_coef, row0, sum, res, sink);
+#pragma unroll
+            for (uint32_t k = 0; k < kShortChunks; ++k)
+                sum += parts[k];
+            finish_row<T, WEIGHTED>(a, rp, sink_coef, r, sum, res, sink);
         }
     }
-    const double bres = block_sum<THREADS>(res, s_red);
-    const double bsink = block_sum<THREADS>(sink, s_red);
+    const double bres = block_sum<kFixThreads>(res, s_red);
+    const double bsink = block_sum<kFixThreads>(sink, s_red);
     if (threadIdx.x == 0) {
         a.fix_res[blockIdx.x] = bres;
         a.fix_sink[blockIdx.x] = bsink;
@@ -326,16 +246,16 @@ __global__ void __launch_bounds__(THREADS) fixup_kernel(SweepArgs<T> a) {
     __threadfence();
     // Fixed-order reduction of sweep-CTA and fix-up-CTA partials.
     double r = 0.0, s = 0.0;
-    for (uint32_t i = threadIdx.x; i < a.sweep_ctas; i += THREADS) {
+    for (uint32_t i = threadIdx.x; i < a.sweep_ctas; i += kFixThreads) {
         r += ((volatile double *)a.cta_res)[i];
         s += ((volatile double *)a.cta_sink)[i];
     }
-    for (uint32_t i = threadIdx.x; i < gridDim.x; i += THREADS) {
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += kFixThreads) {
         r += ((volatile double *)a.fix_res)[i];
         s += ((volatile double *)a.fix_sink)[i];
     }
-    r = block_sum<THREADS>(r, s_red);
-    s = block_sum<THREADS>(s, s_red);
+    r = block_sum<kFixThreads>(r, s_red);
+    s = block_sum<kFixThreads>(s, s_red);
     if (threadIdx.x == 0) {
         IterState *st = a.st;
         const unsigned long long it = st->iteration + 1;
