@@ -55,6 +55,10 @@ def parse_args():
                          "(the small, fixed launch sequence used for ncu captures)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
                     help="precision of the --profile-only sweeps")
+    ap.add_argument("--shape", type=int, default=-1,
+                    help="sweep launch shape (nkg_graph_options.sweep_shape; -1 default)")
+    ap.add_argument("--arc-order", type=int, default=0, choices=[0, 1],
+                    help="nkg_graph_options.arc_order (0 keep the reference order, 1 sorted)")
     ap.add_argument("--cache", default=os.path.join(tempfile.gettempdir(), "nk_b200_graphs"))
     return ap.parse_args()
 
@@ -258,13 +262,15 @@ def main():
 
     csr = make_graph(args.scale, args.cache, rank, barrier)
     arcs, n = csr.arcs, csr.z
-    dg = _capi.DeviceGraph(csr, device=local)
+    dg = _capi.DeviceGraph(csr, device=local, sweep_shape=args.shape, arc_order=args.arc_order)
     info = dg.info()
     if args.profile_only:
         prec = _capi.NKG_PREC_FP64 if args.precision == "fp64" else _capi.NKG_PREC_FP32
         ms_k, ms_i = dg.profile_sweeps(prec, args.profile_only)
         print(json.dumps({"profile_only": args.profile_only, "precision": args.precision,
+                          "shape": args.shape, "arc_order": args.arc_order,
                           "scale": args.scale, "n": n, "arcs": arcs,
+                          "slots": info["slots"], "split_rows": info["split_rows"],
                           "ms_sweep_kernel": ms_k, "ms_iteration": ms_i}))
         dg.close()
         return

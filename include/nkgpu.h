@@ -97,7 +97,14 @@ typedef struct {
 /* Options of nkg_graph_create_ex. */
 typedef struct {
     int32_t device;      /* CUDA device ordinal (-1: current device) */
-    int32_t reserved[3]; /* must be 0 */
+    int32_t sweep_shape; /* launch shape of the sweep kernel (-1 default; 0: 256
+                            threads, L1-cached gathers; 1: 256 threads, L2-only
+                            gathers; 2: 512 threads; 3: 128 threads) */
+    int32_t arc_order;   /* 0 (default): keep every in-row in the caller's order,
+                            which is the reference's summation order; 1: sort
+                            each in-row by source after relabelling (faster
+                            gathers, sums rounded in a different order) */
+    int32_t reserved;    /* must be 0 */
 } nkg_graph_options;
 
 /* Upload a graph given as its in-adjacency CSR.

@@ -80,7 +80,8 @@ class GraphInfo(C.Structure):
 
 
 class GraphOptions(C.Structure):
-    _fields_ = [("device", C.c_int32), ("reserved", C.c_int32 * 3)]
+    _fields_ = [("device", C.c_int32), ("sweep_shape", C.c_int32), ("arc_order", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 _u64p = C.POINTER(C.c_uint64)
@@ -153,7 +154,7 @@ def ptr(a, t):
 class DeviceGraph:
     """Owning wrapper of an nkg_graph handle."""
 
-    def __init__(self, csr, device: int = -1):
+    def __init__(self, csr, device: int = -1, sweep_shape: int = -1, arc_order: int = 0):
         L = lib()
         h = _vp()
         in_ptr = np.ascontiguousarray(csr.in_ptr, np.uint64)
@@ -163,6 +164,8 @@ class DeviceGraph:
         ex = None if csr.exists is None else np.ascontiguousarray(csr.exists, np.uint8)
         opts = GraphOptions()
         opts.device = int(device)
+        opts.sweep_shape = int(sweep_shape)
+        opts.arc_order = int(arc_order)
         check(L.nkg_graph_create_ex(C.byref(h), int(csr.z), int(in_col.shape[0]),
                                     ptr(in_ptr, _u64p), ptr(in_col, _u32p), ptr(in_w, _f64p),
                                     ptr(wdeg, _f64p), ptr(ex, _u8p), int(bool(csr.directed)),

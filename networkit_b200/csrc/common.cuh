@@ -172,10 +172,34 @@ __device__ __forceinline__ double block_max(double v, double *scratch) {
     return r;
 }
 
-// Streaming (evict-first) read-only loads for data touched once per sweep, so
-// that the L2 keeps the gathered score vector instead.
-__device__ __forceinline__ uint32_t ld_stream(const uint32_t *p) { return __ldcs(p); }
-__device__ __forceinline__ float ld_stream(const float *p) { return __ldcs(p); }
-__device__ __forceinline__ double ld_stream(const double *p) { return __ldcs(p); }
+// Streaming read-only loads for data touched once per sweep: no L1
+// allocation and an evict-first L2 policy, so both caches keep the gathered
+// scores.
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
+        : "=r"(v)
+        : "l"(p), "l"(l2_evict_first_policy()));
+    return v;
+}
+__device__ __forceinline__ float ld_stream(const float *p) {
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;"
+        : "=f"(v)
+        : "l"(p), "l"(l2_evict_first_policy()));
+    return v;
+}
+__device__ __forceinline__ double ld_stream(const double *p) {
+    double v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;"
+        : "=d"(v)
+        : "l"(p), "l"(l2_evict_first_policy()));
+    return v;
+}
 
 } // namespace nkg

@@ -12,7 +12,7 @@ namespace nkg {
 // Sweeps per captured CUDA graph (even, so every graph starts on buffer 0).
 constexpr int kSweepsPerGraph = 8;
 // Work units per resident warp of the sweep kernel.
-constexpr uint32_t kUnitsPerWarp = 4;
+constexpr uint32_t kUnitsPerWarp = 8;
 // Cost of a slice in units of one slot step, besides its length (the
 // epilogue of its 32 rows).
 constexpr uint32_t kSliceOverhead = 3;
@@ -51,6 +51,8 @@ struct nkg_graph {
 
     // Sliced layout of the sweep.
     uint32_t n_long = 0, n_vlong = 0, n_chunks = 0, s_chunk = 0, slices = 0;
+    int sweep_shape = 0;
+    bool arc_sorted = false;
     uint64_t slots = 0;
     nkg::DeviceArray<uint32_t> chunk_begin;  // n_long+1
     nkg::DeviceArray<uint32_t> slice_off;    // slices+1

@@ -421,6 +421,37 @@ static T read_scalar(const T *d, cudaStream_t s) {
     return h;
 }
 
+// Sort every in-row by source id (relabelled), weights alongside.
+static void sort_rows(nkg_graph *g, cudaStream_t s) {
+    const int items = static_cast<int>(g->arcs);
+    const int segs = static_cast<int>(g->n);
+    DeviceArray<uint32_t> col2(g->arcs, 4);
+    size_t tb = 0;
+    if (g->weighted) {
+        DeviceArray<double> w2(g->arcs, 4);
+        NKG_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, tb, g->col.get(), col2.get(),
+                                                     g->w64src.get(), w2.get(), items, segs,
+                                                     g->row_ptr.get(), g->row_ptr.get() + 1, s));
+        DeviceArray<unsigned char> tmp(tb);
+        NKG_CUDA(cub::DeviceSegmentedSort::SortPairs(tmp.get(), tb, g->col.get(), col2.get(),
+                                                     g->w64src.get(), w2.get(), items, segs,
+                                                     g->row_ptr.get(), g->row_ptr.get() + 1, s));
+        NKG_CUDA(cudaStreamSynchronize(s));
+        g->w64src = std::move(w2);
+    } else {
+        NKG_CUDA(cub::DeviceSegmentedSort::SortKeys(nullptr, tb, g->col.get(), col2.get(), items,
+                                                    segs, g->row_ptr.get(), g->row_ptr.get() + 1,
+                                                    s));
+        DeviceArray<unsigned char> tmp(tb);
+        NKG_CUDA(cub::DeviceSegmentedSort::SortKeys(tmp.get(), tb, g->col.get(), col2.get(), items,
+                                                    segs, g->row_ptr.get(), g->row_ptr.get() + 1,
+                                                    s));
+        NKG_CUDA(cudaStreamSynchronize(s));
+    }
+    g->col = std::move(col2);
+    g->arc_sorted = true;
+}
+
 // Build the sliced layout from the relabelled in-CSR (row_ptr, col, w64src).
 static void build_slices(nkg_graph *g, const uint32_t *rowlen, cudaStream_t s) {
     const uint32_t n = static_cast<uint32_t>(g->n);
@@ -622,6 +653,16 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
                                               g->inv.get(), g->row_ptr.get(), n, g->col.get(),
                                               g->w64src.get());
     NKG_CUDA(cudaGetLastError());
+    if (opt) {
+        require(opt->reserved == 0, "reserved options must be 0");
+        require(opt->sweep_shape >= -1 && opt->sweep_shape < kNumSweepShapes,
+                "unknown sweep shape");
+        require(opt->arc_order == 0 || opt->arc_order == 1, "arc_order must be 0 or 1");
+        if (opt->sweep_shape >= 0)
+            g->sweep_shape = opt->sweep_shape;
+        if (opt->arc_order == 1 && arcs > 1 && arcs < 0x7fffffffull)
+            sort_rows(g.get(), s);
+    }
     build_slices(g.get(), rowlen.get(), s);
     NKG_CUDA(cudaEventRecord(g->ev1, s));
     NKG_CUDA(cudaStreamSynchronize(s));
@@ -686,14 +727,20 @@ static void sweep_setup(nkg_graph *g) {
         convert_array<T><<<sms * 8, 256, 0, s>>>(g->degw64src.get(), P.degw.get(), n);
         NKG_CUDA(cudaGetLastError());
     }
-    int occ = 0;
-    NKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sweep_kernel<T, WEIGHTED>,
-                                                           kSweepThreads, 0));
-    occ = std::max(occ, 1);
+    int occ = 0, threads = 0;
+    with_sweep_shape(g->sweep_shape, [&](auto S) {
+        using Sh = decltype(S);
+        auto kfn = sweep_kernel<T, WEIGHTED, Sh::threads, Sh::unroll>;
+        // The kernel needs almost no shared memory: give the L1 the most room.
+        NKG_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, 0));
+        NKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, Sh::threads, 0));
+        threads = Sh::threads;
+    });
+    require(occ >= 1, "sweep kernel does not fit on an SM");
     P.sweep_ctas = static_cast<unsigned>(std::max<uint64_t>(
         1, std::min<uint64_t>(static_cast<uint64_t>(occ) * sms,
-                              (static_cast<uint64_t>(g->slices) + 7) / 8)));
-    const uint64_t warps = static_cast<uint64_t>(P.sweep_ctas) * (kSweepThreads / 32);
+                              (static_cast<uint64_t>(g->slices) * 32 + threads - 1) / threads)));
+    const uint64_t warps = static_cast<uint64_t>(P.sweep_ctas) * (threads / 32);
     P.units = static_cast<uint32_t>(
         std::max<uint64_t>(1, std::min<uint64_t>(warps * kUnitsPerWarp, g->slices)));
     P.unit_start.alloc(static_cast<size_t>(P.units) + 1);
@@ -742,10 +789,19 @@ static SweepArgs<T> sweep_args(nkg_graph *g, int in_buf) {
 }
 
 template <typename T, bool WEIGHTED>
+static void launch_sweep_kernel(nkg_graph *g, const SweepArgs<T> &a, cudaStream_t s) {
+    Plane<T> &P = plane<T>(g);
+    with_sweep_shape(g->sweep_shape, [&](auto S) {
+        using Sh = decltype(S);
+        sweep_kernel<T, WEIGHTED, Sh::threads, Sh::unroll><<<P.sweep_ctas, Sh::threads, 0, s>>>(a);
+    });
+}
+
+template <typename T, bool WEIGHTED>
 static void launch_sweep(nkg_graph *g, int in_buf, cudaStream_t s) {
     Plane<T> &P = plane<T>(g);
     const SweepArgs<T> a = sweep_args<T, WEIGHTED>(g, in_buf);
-    sweep_kernel<T, WEIGHTED><<<P.sweep_ctas, kSweepThreads, 0, s>>>(a);
+    launch_sweep_kernel<T, WEIGHTED>(g, a, s);
     fixup_kernel<T, WEIGHTED><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
 }
 
@@ -954,7 +1010,7 @@ static void profile_sweeps(nkg_graph *g, int sweeps, double *ms_kernel, double *
     for (int i = 0; i < sweeps; ++i) {
         const SweepArgs<T> a = sweep_args<T, WEIGHTED>(g, i & 1);
         NKG_CUDA(cudaEventRecord(ev[2 * i], s));
-        sweep_kernel<T, WEIGHTED><<<P.sweep_ctas, kSweepThreads, 0, s>>>(a);
+        launch_sweep_kernel<T, WEIGHTED>(g, a, s);
         NKG_CUDA(cudaEventRecord(ev[2 * i + 1], s));
         fixup_kernel<T, WEIGHTED><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
     }

@@ -125,20 +125,45 @@ __device__ __forceinline__ void finish_row(const SweepArgs<T> &a, const RunParam
     }
 }
 
-constexpr int kSweepThreads = 256;
-constexpr int kUnroll = 8;
+
+// Gathers go through L1 with the default policy (__ldg); the kernel uses no
+// shared memory, so the whole L1 caches the hot scores. The sweep is bound by
+// L1 miss requests to L2 (one sector per scattered lane). Measured
+// alternatives that were slower on B200: L2-only loads; holding the hottest
+// scores in shared memory (random 8-byte loads hit bank conflicts and
+// throttle the MIO queue); per-lane L1 evict-last / no-allocate hints (the
+// predicated loads raise register use and cut occupancy).
+
+// Launch shapes of the sweep kernel: threads per CTA and slot steps per batch
+// of independent gathers.
+template <int TH, int UNROLL_>
+struct SweepShape {
+    static constexpr int threads = TH, unroll = UNROLL_;
+};
+constexpr int kNumSweepShapes = 4;
+
+template <typename F>
+inline void with_sweep_shape(int v, F &&f) {
+    switch (v) {
+    case 1: f(SweepShape<256, 8>{}); break;
+    case 2: f(SweepShape<256, 4>{}); break;
+    case 3: f(SweepShape<256, 16>{}); break;
+    default: f(SweepShape<512, 8>{}); break;
+    }
+}
 
 // The sweep: each warp walks its units; each lane accumulates one virtual
-// row of a slice. Chunk slices store partial sums; row slices finish rows.
-template <typename T, bool WEIGHTED>
-__global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepArgs<T> a) {
+// row of a slice in arc order. Chunk slices store partial sums; row slices
+// finish rows.
+template <typename T, bool WEIGHTED, int THREADS, int UNROLL>
+__global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs<T> a) {
     __shared__ double s_red[32];
     if (*(volatile int *)&a.st->done)
         return;
     const RunParams rp = *a.rp;
     const T sink_coef = static_cast<T>(a.st->sink_coef);
     const int lane = threadIdx.x & 31;
-    const uint32_t wpc = kSweepThreads / 32;
+    const uint32_t wpc = THREADS / 32;
     const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);
     const uint32_t nw = gridDim.x * wpc;
     double res = 0.0, sink = 0.0;
@@ -151,26 +176,27 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepArgs<T> a) {
             const uint32_t *cp = a.col_sell + base;
             T acc = T(0);
             uint32_t j = 0;
-            for (; j + kUnroll <= len; j += kUnroll) {
-                uint32_t c[kUnroll];
+            for (; j + UNROLL <= len; j += UNROLL) {
+                uint32_t c[UNROLL];
 #pragma unroll
-                for (int k = 0; k < kUnroll; ++k)
+                for (int k = 0; k < UNROLL; ++k)
                     c[k] = ld_stream(cp + static_cast<size_t>(j + k) * 32);
-                T v[kUnroll];
+                T v[UNROLL];
 #pragma unroll
-                for (int k = 0; k < kUnroll; ++k)
+                for (int k = 0; k < UNROLL; ++k)
                     v[k] = __ldg(a.y_in + c[k]);
                 if (WEIGHTED) {
 #pragma unroll
-                    for (int k = 0; k < kUnroll; ++k)
+                    for (int k = 0; k < UNROLL; ++k)
                         v[k] = t_mul(v[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
                 }
 #pragma unroll
-                for (int k = 0; k < kUnroll; ++k)
+                for (int k = 0; k < UNROLL; ++k)
                     acc += v[k];
             }
             for (; j < len; ++j) {
-                T v = __ldg(a.y_in + ld_stream(cp + static_cast<size_t>(j) * 32));
+                const uint32_t c = ld_stream(cp + static_cast<size_t>(j) * 32);
+                T v = __ldg(a.y_in + c);
                 if (WEIGHTED)
                     v = t_mul(v, ld_stream(a.w_sell + base + static_cast<size_t>(j) * 32));
                 acc += v;
@@ -184,8 +210,8 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepArgs<T> a) {
             }
         }
     }
-    const double bres = block_sum<kSweepThreads>(res, s_red);
-    const double bsink = block_sum<kSweepThreads>(sink, s_red);
+    const double bres = block_sum<THREADS>(res, s_red);
+    const double bsink = block_sum<THREADS>(sink, s_red);
     if (threadIdx.x == 0) {
         a.cta_res[blockIdx.x] = bres;
         a.cta_sink[blockIdx.x] = bsink;

@@ -62,10 +62,13 @@ def test_max_iterations_two(name):
 
 @pytest.mark.parametrize("distribute", [False, True])
 @pytest.mark.parametrize("scale", [10, 16])
-def test_rmat_parity_l1(oracle_mod, distribute, scale):
+@pytest.mark.parametrize("arc_order", [0, 1])
+@pytest.mark.parametrize("shape", [-1, 1, 2, 3])
+def test_rmat_parity_l1(oracle_mod, distribute, scale, arc_order, shape):
     csr = generators.rmat_directed(scale, 16, seed=42)
     o = oracle_mod.pagerank(csr, tol=1e-10, norm=0, distribute_sinks=distribute)
-    dg, s, it, mx, st = gpu_run(csr, tol=1e-10, norm=0, distribute=distribute)
+    dg = _capi.DeviceGraph(csr, sweep_shape=shape, arc_order=arc_order)
+    s, it, mx, st = dg.run(dg.params(0.85, 1e-10, 0, False, distribute, 0, _capi.UINT64_MAX))
     info = dg.info()
     assert info["slots"] >= csr.arcs and info["n"] == csr.z
     assert np.abs(s - o.scores).sum() <= L1_FP64
