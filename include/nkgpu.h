@@ -173,6 +173,28 @@ NKG_API void nkg_cancel(nkg_graph *g);
 NKG_API int nkg_profile_sweeps(nkg_graph *g, int precision, int sweeps, double *ms_sweep_kernel,
                                double *ms_iteration);
 
+/* PageRank without any device allocation; no counterpart in the reference.
+ * For callers that cannot allocate device memory when they call in: a
+ * framework whose caching allocator owns the device memory, a service with
+ * a memory budget fixed at start-up, a latency-critical loop in which
+ * cudaMalloc/cudaFree would synchronise the device. The caller passes the
+ * graph and the output in device memory:
+ *   d_in_row_ptr  n+1 in-CSR offsets (device), d_in_col  arcs sources (device)
+ *   d_scores_out  n doubles (device)
+ * FP64 only, n <= 524288 nodes; larger graphs are rejected with
+ * NKG_ERR_INVALID_ARG. All working storage is one 12.1 MB file-scope
+ * __device__ array of the library, held by every GPU that loads the library
+ * until the process exits. The first call on a device looks up that array's
+ * address (cudaGetSymbolAddress, with the device current); make that first
+ * call before any stream capture. Calls share the array: calls that overlap
+ * on the GPU (other threads, other streams) race and must be serialised by
+ * the caller. Work runs on `stream` (a cudaStream_t; NULL = default stream)
+ * and the call returns when it has finished. */
+NKG_API int nkg_pagerank_csr_noalloc(uint64_t n, uint64_t arcs, const uint64_t *d_in_row_ptr,
+                                     const uint32_t *d_in_col, const nkg_pr_params *p,
+                                     double *d_scores_out, uint64_t *iterations_out,
+                                     void *stream);
+
 /* Message of the last failure on the calling thread ("" if none). */
 NKG_API const char *nkg_last_error(void);
 

@@ -109,6 +109,8 @@ SIGNATURES = {
     "nkg_ranking": (C.c_int, [_vp, _f64p, _u64p, _f64p]),
     "nkg_cancel": (None, [_vp]),
     "nkg_profile_sweeps": (C.c_int, [_vp, C.c_int, C.c_int, _f64p, _f64p]),
+    "nkg_pagerank_csr_noalloc": (C.c_int, [C.c_uint64, C.c_uint64, _vp, _vp, C.POINTER(PRParams),
+                                           _vp, _u64p, _vp]),
 }
 
 _lib = None

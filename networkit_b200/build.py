@@ -23,7 +23,7 @@ INCLUDE = os.path.join(ROOT, "include")
 GPU_LIB = os.path.join(LIBDIR, "libnkgpu.so")
 GEN_LIB = os.path.join(LIBDIR, "libnkgen.so")
 
-GPU_SOURCES = ["nkgpu.cu"]
+GPU_SOURCES = ["nkgpu.cu", "noalloc.cu"]
 GPU_HEADERS = ["common.cuh", "sweep.cuh", "graph.hpp"]
 GEN_SOURCES = ["graphgen.cpp"]
 
