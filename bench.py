@@ -59,6 +59,8 @@ def parse_args():
                     help="sweep launch shape (nkg_graph_options.sweep_shape; -1 default)")
     ap.add_argument("--arc-order", type=int, default=0, choices=[0, 1],
                     help="nkg_graph_options.arc_order (0 keep the reference order, 1 sorted)")
+    ap.add_argument("--form", default="", choices=["", "ppr"],
+                    help="run only one companion form and print its figures")
     ap.add_argument("--cache", default=os.path.join(tempfile.gettempdir(), "nk_b200_graphs"))
     return ap.parse_args()
 
@@ -188,6 +190,38 @@ def cpu_baseline_port(csr, nthreads, target_s=15.0):
                       f"FP64 run (oracle C restatement, OpenMP rows), {dt:.1f} s"}
 
 
+def form_ppr(local, n=4_000_000, m=8, k=256, steps=2):
+    """Batched personalised PageRank: Barabasi-Albert n=4M, m=8 (undirected),
+    256 one-hot seeds (uniform, seed 42), one FP32 SpMM with k = 256 columns,
+    FP64 residual per column, damp 0.85, tol 1e-7 (L1)."""
+    import torch
+
+    from networkit_b200 import _capi, generators
+
+    csr = generators.barabasi_albert(m, n, seed=42)
+    seeds = np.random.default_rng(42).choice(csr.z, k, replace=False).astype(np.uint32)
+    dg = _capi.DeviceGraph(csr, device=local)
+    p = dg.params(0.85, 1e-7, NORM_L1, False, False, _capi.NKG_PREC_FP32, 1000)
+    out = torch.empty((k, csr.z), dtype=torch.float32, device=f"cuda:{local}")
+    dg.ppr(seeds, p, out.data_ptr())  # warm-up
+    ms, sweeps, launches = 0.0, 0, 0
+    for _ in range(steps):
+        _, its, st = dg.ppr(seeds, p, out.data_ptr())
+        ms += st["ms_total"]
+        sweeps += st["fp32_sweeps"]
+        launches += st["kernel_launches"]
+        col_sweeps = int(its.sum())
+    bytes_sweep = st["bytes_per_sweep_fp32"]
+    per_sweep_ms = ms / sweeps
+    dg.close()
+    return {"workload": f"ppr_ba{n}_m{m}_k{k}_fp32", "n": csr.z, "arcs": csr.arcs, "k": k,
+            "sweeps": sweeps // steps, "column_sweeps": col_sweeps, "ms_per_run": ms / steps,
+            "ms_per_sweep": per_sweep_ms,
+            "gteps_per_iter": csr.arcs * k / (per_sweep_ms / 1e3) / 1e9,
+            "alg_bytes_per_sweep": bytes_sweep,
+            "alg_gbs": bytes_sweep / (per_sweep_ms / 1e3) / 1e9, "gpu_launches": launches}
+
+
 def run_reference_arm(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -244,6 +278,9 @@ def main():
     import torch
 
     torch.cuda.set_device(local)
+    if args.form == "ppr":
+        print(json.dumps(form_ppr(local)))
+        return
     if world > 1:
         import datetime
 

@@ -154,6 +154,21 @@ NKG_API int nkg_pagerank_run_teleport(nkg_graph *g, const nkg_pr_params *p, cons
                               double *scores_out, uint64_t *iterations_out, double *max_out,
                               nkg_stats *stats);
 
+/* Batched personalised PageRank, no reference counterpart: k <= 256 columns,
+ * column j with the teleport t_j = e_{seeds[j]} (seeds are node ids of the
+ * caller), solved together as one FP32 SpMM over the shared graph (each
+ * column is PageRank.cpp:56-70 with the uniform teleport replaced by t_j;
+ * with distribute_sinks the sink mass of column j goes to seeds[j]). Every
+ * column starts at 1/n, keeps its own FP64 residual and stops (its values
+ * freeze) once that residual is <= tol or max_iterations sweeps are done.
+ * Output: column-major k x z floats, column j at scores_out + j*z, in the
+ * caller's ids, each column normalised like PageRank.cpp:75-92.
+ * scores_out is host memory (out_on_device = 0) or device memory (1).
+ * iterations_out (nullable): k sweep counts. Unweighted graphs only. */
+NKG_API int nkg_ppr_run(nkg_graph *g, const nkg_pr_params *p, uint32_t k, const uint32_t *seeds,
+                        float *scores_out, int out_on_device, uint64_t *iterations_out,
+                        nkg_stats *stats);
+
 /* Centrality::ranking() (Centrality.cpp:29-41): existing nodes sorted by score
  * descending, ties by node id ascending. scores: host array of z doubles (any
  * scores, e.g. from nkg_pagerank_run); ids_out / vals_out: n entries each. */

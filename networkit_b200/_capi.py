@@ -111,6 +111,8 @@ SIGNATURES = {
     "nkg_profile_sweeps": (C.c_int, [_vp, C.c_int, C.c_int, _f64p, _f64p]),
     "nkg_pagerank_csr_noalloc": (C.c_int, [C.c_uint64, C.c_uint64, _vp, _vp, C.POINTER(PRParams),
                                            _vp, _u64p, _vp]),
+    "nkg_ppr_run": (C.c_int, [_vp, C.POINTER(PRParams), C.c_uint32, _u32p, _vp, C.c_int, _u64p,
+                              C.POINTER(Stats)]),
 }
 
 _lib = None
@@ -224,6 +226,23 @@ class DeviceGraph:
         check(lib().nkg_pagerank_run_device(self.h, C.byref(p), _vp(d_out_ptr), C.byref(it),
                                             C.byref(mx), C.byref(st)))
         return int(it.value), float(mx.value), st.as_dict()
+
+    def ppr(self, seeds, p: PRParams, d_out_ptr: int = 0):
+        """Batched personalised PageRank (one column per seed). Returns
+        (scores float32[k, z] or None when written to d_out_ptr on the device,
+        iterations uint64[k], stats)."""
+        s = np.ascontiguousarray(seeds, np.uint32)
+        k = int(s.shape[0])
+        it = np.zeros(k, np.uint64)
+        st = Stats()
+        if d_out_ptr:
+            check(lib().nkg_ppr_run(self.h, C.byref(p), k, ptr(s, _u32p), _vp(d_out_ptr), 1,
+                                    ptr(it, _u64p), C.byref(st)))
+            return None, it, st.as_dict()
+        out = np.empty((k, self.z), np.float32)
+        check(lib().nkg_ppr_run(self.h, C.byref(p), k, ptr(s, _u32p),
+                                _vp(out.ctypes.data), 0, ptr(it, _u64p), C.byref(st)))
+        return out, it, st.as_dict()
 
     def ranking(self, scores):
         s = np.ascontiguousarray(scores, np.float64)

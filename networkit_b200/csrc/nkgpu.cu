@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "graph.hpp"
+#include "host.hpp"
 
 using namespace nkg;
 
@@ -392,34 +393,6 @@ __global__ void final_scale(const T *__restrict__ y, const uint32_t *__restrict_
 
 // ---------------------------------------------------------------------------
 // Host side
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        NKG_CUDA(cudaGetDevice(&prev));
-        if (prev != dev)
-            NKG_CUDA(cudaSetDevice(dev));
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0)
-            cudaSetDevice(prev);
-    }
-};
-
-static unsigned num_sms(int dev) {
-    int v = 0;
-    NKG_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
-    return static_cast<unsigned>(v);
-}
-
-template <typename T>
-static T read_scalar(const T *d, cudaStream_t s) {
-    T h{};
-    NKG_CUDA(cudaMemcpyAsync(&h, d, sizeof(T), cudaMemcpyDeviceToHost, s));
-    NKG_CUDA(cudaStreamSynchronize(s));
-    return h;
-}
 
 // Sort every in-row by source id (relabelled), weights alongside.
 static void sort_rows(nkg_graph *g, cudaStream_t s) {
@@ -1029,23 +1002,6 @@ static void profile_sweeps(nkg_graph *g, int sweeps, double *ms_kernel, double *
         cudaEventDestroy(e);
     *ms_kernel = sum / sweeps;
     *ms_iter = sweeps > 1 ? total / (sweeps - 1) : sum;
-}
-
-template <typename F>
-static int guarded(F &&f) {
-    try {
-        f();
-        return NKG_OK;
-    } catch (const Error &e) {
-        set_last_error(e.what());
-        return e.code;
-    } catch (const std::bad_alloc &) {
-        set_last_error("host allocation failed");
-        return NKG_ERR_OOM;
-    } catch (const std::exception &e) {
-        set_last_error(e.what());
-        return NKG_ERR_CUDA;
-    }
 }
 
 static int run_to(nkg_graph *g, const nkg_pr_params *p, const double *teleport, double *out,
