@@ -59,7 +59,7 @@ def parse_args():
                     help="sweep launch shape (nkg_graph_options.sweep_shape; -1 default)")
     ap.add_argument("--arc-order", type=int, default=0, choices=[0, 1],
                     help="nkg_graph_options.arc_order (0 keep the reference order, 1 sorted)")
-    ap.add_argument("--form", default="", choices=["", "ppr"],
+    ap.add_argument("--form", default="", choices=["", "ppr", "refine"],
                     help="run only one companion form and print its figures")
     ap.add_argument("--cache", default=os.path.join(tempfile.gettempdir(), "nk_b200_graphs"))
     return ap.parse_args()
@@ -222,6 +222,44 @@ def form_ppr(local, n=4_000_000, m=8, k=256, steps=2):
             "alg_gbs": bytes_sweep / (per_sweep_ms / 1e3) / 1e9, "gpu_launches": launches}
 
 
+def form_refine(local, csr, steps=2):
+    """Plain FP64 vs FP32+FP64-refinement on the R-MAT scale-24 graph: time to
+    the FP64 stopping test at tol 1e-10 (L1), and at tol 1.5e-7, the point
+    where both reach ~1e-6 L1 error. Errors are against an FP64 solve to tol
+    1e-14 on the same GPU (the FP64 path is parity-tested against the oracle)."""
+    import torch
+
+    from networkit_b200 import _capi
+
+    dg = _capi.DeviceGraph(csr, device=local)
+    n = csr.z
+    d_ref = torch.empty(n, dtype=torch.float64, device=f"cuda:{local}")
+    dg.run_device(dg.params(DAMP, 1e-14, NORM_L1, False, False, _capi.NKG_PREC_FP64, 2000),
+                  d_ref.data_ptr())
+    ref = d_ref.cpu().numpy()
+    out = torch.empty(n, dtype=torch.float64, device=f"cuda:{local}")
+    res = {}
+    for tol in (1e-10, 1.5e-7):
+        for name, prec in (("fp64", _capi.NKG_PREC_FP64), ("fp32_refine", _capi.NKG_PREC_FP32_REFINE)):
+            p = dg.params(DAMP, tol, NORM_L1, False, False, prec, _capi.UINT64_MAX)
+            dg.run_device(p, out.data_ptr())  # warm-up
+            ms, st = 0.0, None
+            for _ in range(steps):
+                it, mx, st = dg.run_device(p, out.data_ptr())
+                ms += st["ms_total"]
+            s = out.cpu().numpy()
+            diff = np.abs(s - ref)
+            res[f"{name}_tol{tol:g}"] = {
+                "ms": ms / steps, "fp64_sweeps": st["fp64_sweeps"], "fp32_sweeps": st["fp32_sweeps"],
+                "l1_err": float(diff.sum()),
+                "max_rel_err": float((diff / np.maximum(np.abs(ref), 1e-300)).max()),
+                "gpu_launches": st["kernel_launches"]}
+    dg.close()
+    for tol in ("1e-10", "1.5e-07"):
+        res[f"speedup_tol{tol}"] = res[f"fp64_tol{tol}"]["ms"] / res[f"fp32_refine_tol{tol}"]["ms"]
+    return res
+
+
 def run_reference_arm(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -298,6 +336,9 @@ def main():
     from networkit_b200 import _capi
 
     csr = make_graph(args.scale, args.cache, rank, barrier)
+    if args.form == "refine":
+        print(json.dumps(form_refine(local, csr)))
+        return
     arcs, n = csr.arcs, csr.z
     dg = _capi.DeviceGraph(csr, device=local, sweep_shape=args.shape, arc_order=args.arc_order)
     info = dg.info()
@@ -387,7 +428,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic(
                              f"sweep_fp64_rmat{args.scale}"),
-                         "kernel": "sweep_kernel<double> (merge-path pull SpMV)",
+                         "kernel": "sweep_kernel<double> (SELL-32 pull SpMV)",
                          "bytes_per_launch": bytes_sweep, "ms_per_launch": ms_kernel,
                          "ms_per_iteration": ms_iter, "peak_source": peak_kind},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,

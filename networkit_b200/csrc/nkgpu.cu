@@ -16,6 +16,7 @@
 
 #include "graph.hpp"
 #include "host.hpp"
+#include "refine.cuh"
 
 using namespace nkg;
 
@@ -657,7 +658,7 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
     g->red_ticket.alloc(1);
     NKG_CUDA(cudaMemsetAsync(g->red_ticket.get(), 0, sizeof(unsigned int), s));
     g->st_host.alloc(1);
-    g->scalars_host.alloc(8);
+    g->scalars_host.alloc(16);
     NKG_CUDA(cudaStreamSynchronize(s));
     return g.release();
 }
@@ -803,7 +804,36 @@ struct RunResult {
     double residual = 0.0, sink_mass = 0.0, maximum = 1.0;
     double ms_total = 0.0, ms_iter = 0.0;
     uint64_t launches = 0;
+    uint64_t fp64_sweeps = 0, fp32_sweeps = 0;
 };
+
+// PageRank.cpp:75-102 on the final iterate yfin (gather form, this plane's
+// precision), written to d_out in the caller's id order; fills the timings.
+template <typename T, bool WEIGHTED>
+static void finalize(nkg_graph *g, const nkg_pr_params &p, const T *yfin, double *d_out,
+                     RunResult &R) {
+    cudaStream_t s = g->stream;
+    const uint32_t n = static_cast<uint32_t>(g->n);
+    const T *degw = sweep_args<T, WEIGHTED>(g, 0).degw;
+    const unsigned rblocks = std::min<unsigned>(num_sms(g->device) * 2, 4096);
+    final_reduce<T, WEIGHTED><<<rblocks, kRedThreads, 0, s>>>(
+        yfin, g->degc.get(), degw, n, g->red.get() + 4, g->red.get(), g->red_ticket.get());
+    final_scale<T, WEIGHTED><<<ceil_div(g->z, 256), 256, 0, s>>>(
+        yfin, g->degc.get(), degw, g->inv.get(), g->z, n, p.damp, p.normalized ? 1 : 0,
+        g->red.get(), d_out);
+    NKG_CUDA(cudaGetLastError());
+    R.launches += 2;
+    NKG_CUDA(cudaEventRecord(g->ev2, s));
+    double *hs = g->scalars_host.get();
+    NKG_CUDA(cudaMemcpyAsync(hs, g->red.get(), 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    NKG_CUDA(cudaStreamSynchronize(s));
+    R.maximum = hs[3];
+    float ms = 0.f;
+    NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev2));
+    R.ms_total = ms;
+    NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    R.ms_iter = ms;
+}
 
 static uint64_t bytes_per_sweep(const nkg_graph *g, int elem) {
     // Algorithmic bytes of one sweep: column ids, row offsets, gathered
@@ -864,7 +894,6 @@ static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *t
     sweep_setup<T, WEIGHTED>(g);
     Plane<T> &P = plane<T>(g);
     const int personal = teleport_host ? 1 : 0;
-    const uint32_t n = static_cast<uint32_t>(g->n);
     RunResult R;
 
     DeviceArray<double> d_tele_orig;
@@ -894,26 +923,149 @@ static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *t
     R.residual = sh->residual;
     R.sink_mass = sh->sink_mass;
     const int fin = static_cast<int>(R.iterations & 1ull);
-    const T *yfin = P.y[fin].get();
-    const T *degw = sweep_args<T, WEIGHTED>(g, 0).degw;
-    const unsigned rblocks = std::min<unsigned>(num_sms(g->device) * 2, 4096);
-    final_reduce<T, WEIGHTED><<<rblocks, kRedThreads, 0, s>>>(
-        yfin, g->degc.get(), degw, n, g->red.get() + 4, g->red.get(), g->red_ticket.get());
-    final_scale<T, WEIGHTED><<<ceil_div(g->z, 256), 256, 0, s>>>(
-        yfin, g->degc.get(), degw, g->inv.get(), g->z, n, p.damp, p.normalized ? 1 : 0,
-        g->red.get(), d_out);
-    NKG_CUDA(cudaGetLastError());
-    R.launches += 2;
-    NKG_CUDA(cudaEventRecord(g->ev2, s));
-    double *hs = g->scalars_host.get();
-    NKG_CUDA(cudaMemcpyAsync(hs, g->red.get(), 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
-    NKG_CUDA(cudaStreamSynchronize(s));
-    R.maximum = hs[3];
-    float ms = 0.f;
-    NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev2));
-    R.ms_total = ms;
-    NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
-    R.ms_iter = ms;
+    finalize<T, WEIGHTED>(g, p, P.y[fin].get(), d_out, R);
+    return R;
+}
+
+// FP32 BiCGSTAB bulk solve + FP64 Jacobi residual / correction rounds
+// (refine.cuh). The stopping test is the reference's, applied to the FP64
+// sweep: the returned scores are that sweep's iterate, like PageRank.cpp:70.
+template <bool WEIGHTED>
+static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *teleport_host,
+                            double *d_out) {
+    cudaStream_t s = g->stream;
+    sweep_setup<float, WEIGHTED>(g);
+    sweep_setup<double, WEIGHTED>(g);
+    Plane<float> &P32 = g->p32;
+    Plane<double> &P64 = g->p64;
+    const int personal = teleport_host ? 1 : 0;
+    const uint32_t n = static_cast<uint32_t>(g->n);
+    const unsigned sms = num_sms(g->device);
+    RunResult R;
+    NKG_CUDA(cudaEventRecord(g->ev0, s));
+    nkg_pr_params p1 = p;
+    p1.max_iterations = 1;  // every FP64 launch is exactly one Jacobi sweep
+    DeviceArray<double> d_tele_orig;
+    upload_run_state<double, WEIGHTED>(g, p1, personal, teleport_host, d_tele_orig);
+    if (personal) {
+        if (!P32.tele)
+            P32.tele.alloc(n);
+        permute_teleport<float><<<ceil_div(n, 256), 256, 0, s>>>(d_tele_orig.get(), g->perm.get(),
+                                                                 n, P32.tele.get());
+    }
+    DeviceArray<float> bx(n), br(n), brhat(n), bp(n), bv(n), bs(n), bt(n), bg(n + 1, 4);
+    DeviceArray<double> x64(n);
+    const unsigned vec_ctas = std::max<unsigned>(1, std::min<unsigned>(sms * 4, ceil_div(n, kBiThreads)));
+    const unsigned fix_ctas = std::max<unsigned>(1, ceil_div(g->n_long, kBiThreads));
+    DeviceArray<double> part(2 * static_cast<size_t>(std::max<unsigned>(P32.sweep_ctas, vec_ctas)));
+    DeviceArray<double> fix_part(2 * static_cast<size_t>(fix_ctas));
+    DeviceArray<BiScalars> sc(1);
+    NKG_CUDA(cudaMemsetAsync(sc.get(), 0, sizeof(BiScalars), s));
+    NKG_CUDA(cudaMemsetAsync(bg.get(), 0, (n + 1 + 4) * sizeof(float), s));
+    BiArgs a{};
+    a.col_sell = g->col_sell.get();
+    a.w_sell = P32.w_sell.get();
+    a.slice_off = g->slice_off.get();
+    a.unit_start = P32.unit_start.get();
+    a.chunk_begin = g->chunk_begin.get();
+    a.degc = g->degc.get();
+    a.degw = P32.degw.get();
+    a.tele = P32.tele.get();
+    a.chunk_val = P32.chunk_val.get();
+    a.x = bx.get();
+    a.r = br.get();
+    a.rhat = brhat.get();
+    a.p = bp.get();
+    a.v = bv.get();
+    a.s = bs.get();
+    a.t = bt.get();
+    a.g = bg.get();
+    a.part = part.get();
+    a.fix_part = fix_part.get();
+    a.sc = sc.get();
+    a.damp = p.damp;
+    a.inv_n = 1.0 / static_cast<double>(n);
+    a.n = n;
+    a.n_long = g->n_long;
+    a.n_vlong = g->n_vlong;
+    a.s_chunk = g->s_chunk;
+    a.units = P32.units;
+    a.sweep_ctas = P32.sweep_ctas;
+    a.distribute = p.distribute_sinks ? 1 : 0;
+    a.personal = personal;
+    a.l2 = p.norm == NKG_NORM_L2;
+    BiScalars *hsc = reinterpret_cast<BiScalars *>(g->scalars_host.get());
+    static_assert(sizeof(BiScalars) <= 16 * sizeof(double), "BiScalars fits the pinned buffer");
+    uint64_t matvecs = 0;
+
+    // Solve (I - dM) x = r (r holds the right-hand side) to `inner_tol`.
+    auto solve = [&](double rel) {
+        bi_start<<<vec_ctas, kBiThreads, 0, s>>>(a);
+        NKG_CUDA(cudaMemcpyAsync(hsc, sc.get(), sizeof(BiScalars), cudaMemcpyDeviceToHost, s));
+        NKG_CUDA(cudaStreamSynchronize(s));
+        const double inner_tol = std::max(hsc->res * rel, 0.25 * p.tol);
+        R.launches += 1;
+        for (int it = 0; it < 400 && !hsc->breakdown && hsc->res > inner_tol; it += 4) {
+            for (int k = 0; k < 4; ++k) {
+                bi_vec_p<WEIGHTED><<<vec_ctas, kBiThreads, 0, s>>>(a);
+                with_sweep_shape(g->sweep_shape, [&](auto S) {
+                    using Sh = decltype(S);
+                    bi_mv<WEIGHTED, 0, Sh::threads, Sh::unroll><<<P32.sweep_ctas, Sh::threads, 0, s>>>(a);
+                });
+                bi_mv_fix<WEIGHTED, 0><<<fix_ctas, kBiThreads, 0, s>>>(a);
+                bi_vec_s<WEIGHTED><<<vec_ctas, kBiThreads, 0, s>>>(a);
+                with_sweep_shape(g->sweep_shape, [&](auto S) {
+                    using Sh = decltype(S);
+                    bi_mv<WEIGHTED, 1, Sh::threads, Sh::unroll><<<P32.sweep_ctas, Sh::threads, 0, s>>>(a);
+                });
+                bi_mv_fix<WEIGHTED, 1><<<fix_ctas, kBiThreads, 0, s>>>(a);
+                bi_vec_x<<<vec_ctas, kBiThreads, 0, s>>>(a);
+            }
+            NKG_CUDA(cudaGetLastError());
+            R.launches += 28;
+            matvecs += 8;
+            NKG_CUDA(cudaMemcpyAsync(hsc, sc.get(), sizeof(BiScalars), cudaMemcpyDeviceToHost, s));
+            NKG_CUDA(cudaStreamSynchronize(s));
+            if (g->cancel.load()) {
+                g->cancel.store(0);
+                throw Error(NKG_ERR_CANCELLED, "PageRank run cancelled");
+            }
+        }
+    };
+
+    cudaGraphExec_t exec = sweep_graph<double, WEIGHTED>(g, personal);
+    IterState *sh = g->st_host.get();
+    const double *degw64 = g->degw64src.get();
+    bi_rhs_teleport<<<ceil_div(n, 256), 256, 0, s>>>(a);
+    solve(1e-6);
+    int add = 0;
+    uint64_t fp64 = 0;
+    for (int round = 0;; ++round) {
+        require(round < 40, "FP32 refinement did not reach the tolerance in 40 rounds");
+        std::memset(sh, 0, sizeof(IterState));
+        NKG_CUDA(cudaMemcpyAsync(g->st.get(), sh, sizeof(IterState), cudaMemcpyHostToDevice, s));
+        bi_to_fp64<WEIGHTED><<<vec_ctas, kBiThreads, 0, s>>>(
+            bx.get(), x64.get(), P64.y[0].get(), g->degc.get(), degw64, n, add, part.get(),
+            g->st.get(), &sc.get()->ticket, a.distribute, personal);
+        NKG_CUDA(cudaGraphLaunch(exec, s));
+        R.launches += 1 + 2 * kSweepsPerGraph;
+        ++fp64;
+        NKG_CUDA(cudaMemcpyAsync(sh, g->st.get(), sizeof(IterState), cudaMemcpyDeviceToHost, s));
+        NKG_CUDA(cudaStreamSynchronize(s));
+        if (sh->residual <= p.tol)
+            break;
+        bi_residual_rhs<WEIGHTED><<<ceil_div(n, 256), 256, 0, s>>>(
+            P64.y[1].get(), x64.get(), g->degc.get(), degw64, n, br.get());
+        solve(1e-5);
+        add = 1;
+    }
+    NKG_CUDA(cudaEventRecord(g->ev1, s));
+    R.iterations = fp64 + matvecs;
+    R.residual = sh->residual;
+    R.sink_mass = sh->sink_mass;
+    R.fp64_sweeps = fp64;
+    R.fp32_sweeps = matvecs;
+    finalize<double, WEIGHTED>(g, p, P64.y[1].get(), d_out, R);
     return R;
 }
 
@@ -939,7 +1091,8 @@ static RunResult run_dispatch(nkg_graph *g, const nkg_pr_params *p, const double
         R = g->weighted ? run_power<float, true>(g, *p, teleport, d_out)
                         : run_power<float, false>(g, *p, teleport, d_out);
     } else {
-        throw Error(NKG_ERR_INVALID_ARG, "FP32 refinement is not available in this build");
+        R = g->weighted ? run_refine<true>(g, *p, teleport, d_out)
+                        : run_refine<false>(g, *p, teleport, d_out);
     }
     g->has_run = true;
     return R;
@@ -955,10 +1108,14 @@ static void fill_stats(const nkg_graph *g, const RunResult &R, int precision, nk
     st->ms_total = R.ms_total;
     st->ms_iterations = R.ms_iter;
     st->kernel_launches = R.launches;
-    if (precision == NKG_PREC_FP64)
+    if (precision == NKG_PREC_FP64) {
         st->fp64_sweeps = R.iterations;
-    else
+    } else if (precision == NKG_PREC_FP32) {
         st->fp32_sweeps = R.iterations;
+    } else {
+        st->fp64_sweeps = R.fp64_sweeps;
+        st->fp32_sweeps = R.fp32_sweeps;
+    }
     st->bytes_per_sweep_fp64 = bytes_per_sweep(g, 8);
     st->bytes_per_sweep_fp32 = bytes_per_sweep(g, 4);
 }

@@ -1,0 +1,427 @@
+// FP32 bulk solve with FP64 refinement (the FP32_REFINE precision). The
+// PageRank fixed point is the linear system (I - d M) x = b with
+// M = A + [distributeSinks] t m^T, A[u,v] = w(v->u)/wdeg[v], m the sink mask
+// and b = (1-d) t. The bulk work is an FP32 BiCGSTAB solve of that system
+// (van der Vorst, SIAM J. Sci. Stat. Comput. 13(2), 1992; applied to
+// PageRank by Gleich, Zhukov and Berkhin, 2005) whose matrix-vector product is
+// the sliced-ELLPACK SpMV of sweep.cuh in FP32 with FP32 accumulation. Dot
+// products, norms and sink masses are FP64 with fixed-order reductions; the
+// scalars stay on the device. The FP64 part is the reference's own Jacobi
+// step (the FP64 sweep), which gives the residual x' - x; while its norm is
+// above tol the residual is solved for a correction in FP32 again.
+#pragma once
+
+#include "sweep.cuh"
+
+namespace nkg {
+
+// Device-side scalars of one BiCGSTAB solve (FP64).
+struct BiScalars {
+    double rho, rho_prev, alpha, omega;
+    double vdot;      // (rhat, v)
+    double ts, tt;    // (t, s), (t, t)
+    double res;       // norm of the current residual r
+    double sink_vec;  // m . (vector entering the next product)
+    int breakdown;
+    unsigned int ticket;
+};
+
+struct BiArgs {
+    // SELL structure of the graph (FP32 plane).
+    const uint32_t *__restrict__ col_sell;
+    const float *__restrict__ w_sell;
+    const uint32_t *__restrict__ slice_off;
+    const uint32_t *__restrict__ unit_start;
+    const uint32_t *__restrict__ chunk_begin;
+    const uint32_t *__restrict__ degc;
+    const float *__restrict__ degw;
+    const float *__restrict__ tele;   // personalised teleport (n) or null
+    float *__restrict__ chunk_val;
+    // vectors (x-form, n entries; g is the gather form, n+1 with g[n] = 0)
+    float *x, *r, *rhat, *p, *v, *s, *t, *g;
+    double *__restrict__ part;        // per-CTA partial sums (3 per CTA)
+    double *__restrict__ fix_part;
+    BiScalars *sc;
+    double damp, inv_n;
+    uint32_t n, n_long, n_vlong, s_chunk, units, sweep_ctas;
+    int distribute, personal, l2;
+};
+
+__device__ __forceinline__ float bi_tel(const BiArgs &a, uint32_t r) {
+    return a.personal ? a.tele[r] : static_cast<float>(a.inv_n);
+}
+
+template <bool WEIGHTED>
+__device__ __forceinline__ float bi_deg(const BiArgs &a, uint32_t r, uint32_t &dc) {
+    dc = a.degc[r];
+    return WEIGHTED ? a.degw[r] : static_cast<float>(dc);
+}
+
+// Last-CTA detection; every thread of the winning CTA returns true.
+__device__ __forceinline__ bool bi_last_block(unsigned int *ticket, bool *s_flag) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        *s_flag = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (*s_flag)
+        __threadfence();
+    return *s_flag;
+}
+
+constexpr int kBiThreads = 256;
+
+// out = in - d (A in + (m.in) tel): the product with (I - d M). `in` is given
+// in gather form g (in/deg, sinks in) and x-form px. MODE 0 accumulates
+// (rhat, out); MODE 1 accumulates (out, s) and (out, out).
+template <bool WEIGHTED, int MODE>
+__device__ __forceinline__ void bi_mv_row(const BiArgs &a, uint32_t r, float acc, const float *px,
+                                          float *out, double &d1, double &d2) {
+    const float sv = static_cast<float>(a.sc->sink_vec);
+    float q = acc;
+    if (a.distribute)
+        q = __fadd_rn(q, __fmul_rn(sv, bi_tel(a, r)));
+    q = __fsub_rn(px[r], __fmul_rn(static_cast<float>(a.damp), q));
+    out[r] = q;
+    if (MODE == 0) {
+        d1 += static_cast<double>(a.rhat[r]) * static_cast<double>(q);
+    } else {
+        d1 += static_cast<double>(q) * static_cast<double>(a.s[r]);
+        d2 += static_cast<double>(q) * static_cast<double>(q);
+    }
+}
+
+// The SpMV of one slice per warp (the loop of sweep_kernel in FP32).
+template <bool WEIGHTED, int MODE, int THREADS, int UNROLL>
+__global__ void __launch_bounds__(THREADS) bi_mv(BiArgs a) {
+    __shared__ double s_red[32];
+    if (a.sc->breakdown)
+        return;
+    const float *px = MODE == 0 ? a.p : a.s;
+    float *out = MODE == 0 ? a.v : a.t;
+    const int lane = threadIdx.x & 31;
+    const uint32_t wpc = THREADS / 32;
+    const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);
+    const uint32_t nw = gridDim.x * wpc;
+    double d1 = 0.0, d2 = 0.0;
+    for (uint32_t u = gw; u < a.units; u += nw) {
+        const uint32_t s_end = a.unit_start[u + 1];
+        for (uint32_t s = a.unit_start[u]; s < s_end; ++s) {
+            const uint32_t off = a.slice_off[s];
+            const uint32_t len = a.slice_off[s + 1] - off;
+            const size_t base = static_cast<size_t>(off) * 32 + lane;
+            const uint32_t *cp = a.col_sell + base;
+            float acc = 0.f;
+            uint32_t j = 0;
+            for (; j + UNROLL <= len; j += UNROLL) {
+                uint32_t c[UNROLL];
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    c[k] = ld_stream(cp + static_cast<size_t>(j + k) * 32);
+                float vv[UNROLL];
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    vv[k] = __ldg(a.g + c[k]);
+                if (WEIGHTED) {
+#pragma unroll
+                    for (int k = 0; k < UNROLL; ++k)
+                        vv[k] = __fmul_rn(vv[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
+                }
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    acc += vv[k];
+            }
+            for (; j < len; ++j) {
+                float vv = __ldg(a.g + ld_stream(cp + static_cast<size_t>(j) * 32));
+                if (WEIGHTED)
+                    vv = __fmul_rn(vv, ld_stream(a.w_sell + base + static_cast<size_t>(j) * 32));
+                acc += vv;
+            }
+            if (s < a.s_chunk) {
+                a.chunk_val[static_cast<size_t>(s) * 32 + lane] = acc;
+            } else {
+                const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
+                if (r < a.n)
+                    bi_mv_row<WEIGHTED, MODE>(a, r, acc, px, out, d1, d2);
+            }
+        }
+    }
+    d1 = block_sum<THREADS>(d1, s_red);
+    d2 = block_sum<THREADS>(d2, s_red);
+    if (threadIdx.x == 0) {
+        a.part[2 * blockIdx.x] = d1;
+        a.part[2 * blockIdx.x + 1] = d2;
+    }
+}
+
+// Split rows of the product, then (last CTA) the scalar that follows it:
+// MODE 0: alpha = rho / (rhat, v); MODE 1: omega = (t, s) / (t, t).
+template <bool WEIGHTED, int MODE>
+__global__ void __launch_bounds__(kBiThreads) bi_mv_fix(BiArgs a) {
+    __shared__ double s_red[32];
+    __shared__ bool s_last;
+    if (a.sc->breakdown)
+        return;
+    const float *px = MODE == 0 ? a.p : a.s;
+    float *out = MODE == 0 ? a.v : a.t;
+    double d1 = 0.0, d2 = 0.0;
+    const uint32_t r = blockIdx.x * kBiThreads + threadIdx.x;
+    if (r < a.n_long) {
+        float acc = 0.f;
+        for (uint32_t k = a.chunk_begin[r]; k < a.chunk_begin[r + 1]; ++k)
+            acc += a.chunk_val[k];
+        bi_mv_row<WEIGHTED, MODE>(a, r, acc, px, out, d1, d2);
+    }
+    d1 = block_sum<kBiThreads>(d1, s_red);
+    d2 = block_sum<kBiThreads>(d2, s_red);
+    if (threadIdx.x == 0) {
+        a.fix_part[2 * blockIdx.x] = d1;
+        a.fix_part[2 * blockIdx.x + 1] = d2;
+    }
+    if (!bi_last_block(&a.sc->ticket, &s_last))
+        return;
+    double t1 = 0.0, t2 = 0.0;
+    for (uint32_t i = threadIdx.x; i < a.sweep_ctas; i += kBiThreads) {
+        t1 += ((volatile double *)a.part)[2 * i];
+        t2 += ((volatile double *)a.part)[2 * i + 1];
+    }
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += kBiThreads) {
+        t1 += ((volatile double *)a.fix_part)[2 * i];
+        t2 += ((volatile double *)a.fix_part)[2 * i + 1];
+    }
+    t1 = block_sum<kBiThreads>(t1, s_red);
+    t2 = block_sum<kBiThreads>(t2, s_red);
+    if (threadIdx.x == 0) {
+        BiScalars *sc = a.sc;
+        if (MODE == 0) {
+            sc->vdot = t1;
+            if (!(fabs(t1) > 1e-300) || !isfinite(t1))
+                sc->breakdown = 1;
+            else
+                sc->alpha = sc->rho / t1;
+        } else {
+            sc->ts = t1;
+            sc->tt = t2;
+            sc->omega = t2 > 0.0 ? t1 / t2 : 0.0;
+            if (!(t2 > 0.0))
+                sc->breakdown = 1;
+        }
+        sc->ticket = 0;
+    }
+}
+
+// Vector step 1: p = r + beta (p - omega v), beta = (rho/rho_prev)(alpha/omega);
+// g = p in gather form; sink_vec = m.p.
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(kBiThreads) bi_vec_p(BiArgs a) {
+    __shared__ double s_red[32];
+    __shared__ bool s_last;
+    BiScalars *sc = a.sc;
+    if (sc->breakdown)
+        return;
+    const double beta = (sc->rho / sc->rho_prev) * (sc->alpha / sc->omega);
+    const float b = static_cast<float>(beta), om = static_cast<float>(sc->omega);
+    double sk = 0.0;
+    for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < a.n; i += gridDim.x * kBiThreads) {
+        const float pv = __fadd_rn(a.r[i], __fmul_rn(b, __fsub_rn(a.p[i], __fmul_rn(om, a.v[i]))));
+        a.p[i] = pv;
+        uint32_t dc;
+        const float d = bi_deg<WEIGHTED>(a, i, dc);
+        a.g[i] = dc ? pv / d : pv;
+        if (!dc)
+            sk += pv;
+    }
+    sk = block_sum<kBiThreads>(sk, s_red);
+    if (threadIdx.x == 0)
+        a.part[blockIdx.x] = sk;
+    if (!bi_last_block(&sc->ticket, &s_last))
+        return;
+    double t = 0.0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += kBiThreads)
+        t += ((volatile double *)a.part)[i];
+    t = block_sum<kBiThreads>(t, s_red);
+    if (threadIdx.x == 0) {
+        sc->sink_vec = t;
+        sc->rho_prev = sc->rho;
+        sc->ticket = 0;
+    }
+}
+
+// Vector step 2: s = r - alpha v; g = s in gather form; sink_vec = m.s.
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(kBiThreads) bi_vec_s(BiArgs a) {
+    __shared__ double s_red[32];
+    __shared__ bool s_last;
+    BiScalars *sc = a.sc;
+    if (sc->breakdown)
+        return;
+    const float al = static_cast<float>(sc->alpha);
+    double sk = 0.0;
+    for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < a.n; i += gridDim.x * kBiThreads) {
+        const float sv = __fsub_rn(a.r[i], __fmul_rn(al, a.v[i]));
+        a.s[i] = sv;
+        uint32_t dc;
+        const float d = bi_deg<WEIGHTED>(a, i, dc);
+        a.g[i] = dc ? sv / d : sv;
+        if (!dc)
+            sk += sv;
+    }
+    sk = block_sum<kBiThreads>(sk, s_red);
+    if (threadIdx.x == 0)
+        a.part[blockIdx.x] = sk;
+    if (!bi_last_block(&sc->ticket, &s_last))
+        return;
+    double t = 0.0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += kBiThreads)
+        t += ((volatile double *)a.part)[i];
+    t = block_sum<kBiThreads>(t, s_red);
+    if (threadIdx.x == 0) {
+        sc->sink_vec = t;
+        sc->ticket = 0;
+    }
+}
+
+// Vector step 3: x += alpha p + omega s; r = s - omega t; res = |r|; rho = (rhat, r).
+__global__ void __launch_bounds__(kBiThreads) bi_vec_x(BiArgs a) {
+    __shared__ double s_red[32];
+    __shared__ bool s_last;
+    BiScalars *sc = a.sc;
+    if (sc->breakdown)
+        return;
+    const float al = static_cast<float>(sc->alpha), om = static_cast<float>(sc->omega);
+    double nr = 0.0, rr = 0.0;
+    for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < a.n; i += gridDim.x * kBiThreads) {
+        a.x[i] = __fadd_rn(a.x[i], __fadd_rn(__fmul_rn(al, a.p[i]), __fmul_rn(om, a.s[i])));
+        const float rv = __fsub_rn(a.s[i], __fmul_rn(om, a.t[i]));
+        a.r[i] = rv;
+        const double d = rv;
+        nr += a.l2 ? d * d : fabs(d);
+        rr += static_cast<double>(a.rhat[i]) * d;
+    }
+    nr = block_sum<kBiThreads>(nr, s_red);
+    rr = block_sum<kBiThreads>(rr, s_red);
+    if (threadIdx.x == 0) {
+        a.part[2 * blockIdx.x] = nr;
+        a.part[2 * blockIdx.x + 1] = rr;
+    }
+    if (!bi_last_block(&sc->ticket, &s_last))
+        return;
+    double t1 = 0.0, t2 = 0.0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += kBiThreads) {
+        t1 += ((volatile double *)a.part)[2 * i];
+        t2 += ((volatile double *)a.part)[2 * i + 1];
+    }
+    t1 = block_sum<kBiThreads>(t1, s_red);
+    t2 = block_sum<kBiThreads>(t2, s_red);
+    if (threadIdx.x == 0) {
+        sc->res = a.l2 ? sqrt(t1) : t1;
+        sc->rho = t2;
+        if (!(fabs(t2) > 1e-300) || !isfinite(t2))
+            sc->breakdown = 1;
+        sc->ticket = 0;
+    }
+}
+
+// Start of a solve from x = 0: r = rhat = b (x-form, given in r), p = v = 0;
+// rho = (b, b), res = |b|; rho_prev = alpha = omega = 1.
+__global__ void __launch_bounds__(kBiThreads) bi_start(BiArgs a) {
+    __shared__ double s_red[32];
+    __shared__ bool s_last;
+    BiScalars *sc = a.sc;
+    double nr = 0.0, rr = 0.0;
+    for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < a.n; i += gridDim.x * kBiThreads) {
+        const float b = a.r[i];
+        a.rhat[i] = b;
+        a.x[i] = 0.f;
+        a.p[i] = 0.f;
+        a.v[i] = 0.f;
+        const double d = b;
+        nr += a.l2 ? d * d : fabs(d);
+        rr += d * d;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        a.g[a.n] = 0.f;
+    nr = block_sum<kBiThreads>(nr, s_red);
+    rr = block_sum<kBiThreads>(rr, s_red);
+    if (threadIdx.x == 0) {
+        a.part[2 * blockIdx.x] = nr;
+        a.part[2 * blockIdx.x + 1] = rr;
+    }
+    if (!bi_last_block(&sc->ticket, &s_last))
+        return;
+    double t1 = 0.0, t2 = 0.0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += kBiThreads) {
+        t1 += ((volatile double *)a.part)[2 * i];
+        t2 += ((volatile double *)a.part)[2 * i + 1];
+    }
+    t1 = block_sum<kBiThreads>(t1, s_red);
+    t2 = block_sum<kBiThreads>(t2, s_red);
+    if (threadIdx.x == 0) {
+        sc->res = a.l2 ? sqrt(t1) : t1;
+        sc->rho = t2;
+        sc->rho_prev = 1.0;
+        sc->alpha = 1.0;
+        sc->omega = 1.0;
+        sc->breakdown = t2 > 0.0 ? 0 : 1;
+        sc->ticket = 0;
+    }
+}
+
+// Right-hand side of the first solve: b = (1-d) t.
+__global__ void bi_rhs_teleport(BiArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.n)
+        a.r[i] = static_cast<float>(1.0 - a.damp) * bi_tel(a, i);
+}
+
+// FP64 iterate from the FP32 solution (x64 = x32), or add a correction
+// (x64 += x32); write its gather form y64 and the sink term of the FP64 sweep.
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(kBiThreads)
+    bi_to_fp64(const float *__restrict__ x32, double *__restrict__ x64, double *__restrict__ y64,
+               const uint32_t *__restrict__ degc, const double *__restrict__ degw, uint32_t n,
+               int add, double *part, IterState *st, unsigned int *ticket, int distribute,
+               int personal) {
+    __shared__ double s_red[32];
+    __shared__ bool s_last;
+    double sk = 0.0;
+    for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < n; i += gridDim.x * kBiThreads) {
+        const double x = add ? x64[i] + static_cast<double>(x32[i]) : static_cast<double>(x32[i]);
+        x64[i] = x;
+        const uint32_t dc = degc[i];
+        const double d = WEIGHTED ? degw[i] : static_cast<double>(dc);
+        y64[i] = dc ? x / d : x;
+        if (!dc)
+            sk += x;
+    }
+    sk = block_sum<kBiThreads>(sk, s_red);
+    if (threadIdx.x == 0)
+        part[blockIdx.x] = sk;
+    if (!bi_last_block(ticket, &s_last))
+        return;
+    double t = 0.0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += kBiThreads)
+        t += ((volatile double *)part)[i];
+    t = block_sum<kBiThreads>(t, s_red);
+    if (threadIdx.x == 0) {
+        st->sink_mass = t;
+        st->sink_coef = distribute ? (personal ? t : t / static_cast<double>(n)) : 0.0;
+        *ticket = 0;
+    }
+}
+
+// Right-hand side of a correction solve: r32 = x' - x from the FP64 sweep.
+template <bool WEIGHTED>
+__global__ void bi_residual_rhs(const double *__restrict__ y64_new, const double *__restrict__ x64,
+                                const uint32_t *__restrict__ degc, const double *__restrict__ degw,
+                                uint32_t n, float *__restrict__ r32) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint32_t dc = degc[i];
+    const double d = WEIGHTED ? degw[i] : static_cast<double>(dc);
+    const double xn = dc ? __dmul_rn(y64_new[i], d) : y64_new[i];
+    r32[i] = static_cast<float>(xn - x64[i]);
+}
+
+} // namespace nkg

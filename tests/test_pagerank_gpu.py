@@ -186,6 +186,41 @@ def test_fp32_close_to_fp64(oracle_mod):
     assert st["fp32_sweeps"] == it
 
 
+@pytest.mark.parametrize("case", ["rmat", "rmat_distribute", "er_l2", "weighted", "personal",
+                                  "normalized"])
+def test_fp32_refine_reaches_fp64_accuracy(oracle_mod, case):
+    """FP32 BiCGSTAB bulk solve + FP64 residual/correction rounds: the FP64
+    stopping test holds at tol, so the result is as close to the oracle as
+    the FP64 path (the bar: 1e-8 L1 at tol 1e-10; the reference's own answer
+    is within ~tol/(1-d) of the fixed point)."""
+    if case == "er_l2":
+        csr, norm, tol = generators.erdos_renyi(50000, 10 / 49999, seed=42), 1, 1e-8
+    elif case == "weighted":
+        csr = generators.with_uniform_weights(generators.rmat_directed(14, 16, seed=9), seed=43)
+        norm, tol = 0, 1e-10
+    else:
+        csr, norm, tol = generators.rmat_directed(15, 16, seed=4), 0, 1e-10
+    distribute = case == "rmat_distribute"
+    normalized = case == "normalized"
+    tele = None
+    if case == "personal":
+        rng = np.random.default_rng(2)
+        tele = rng.random(csr.z)
+        tele /= tele.sum()
+    o = oracle_mod.pagerank(csr, tol=tol, norm=norm, distribute_sinks=distribute,
+                            normalized=normalized, teleport=tele)
+    dg = _capi.DeviceGraph(csr)
+    p = dg.params(0.85, tol, norm, normalized, distribute, _capi.NKG_PREC_FP32_REFINE,
+                  _capi.UINT64_MAX)
+    s, it, mx, st = dg.run(p, tele)
+    scale = 1.0 if not normalized else float(np.abs(o.scores).sum())
+    err = np.abs(s - o.scores).sum() / scale
+    assert err <= (1e-8 if norm == 0 else 1e-6), err
+    assert 1 <= st["fp64_sweeps"] <= 6 and st["fp32_sweeps"] >= 2
+    assert st["residual"] <= tol
+    assert it == st["fp64_sweeps"] + st["fp32_sweeps"]
+
+
 def test_invalid_arguments_raise():
     csr = generators.rmat_directed(8, 4, seed=1)
     bad = InCSR(csr.z, csr.n, csr.in_ptr, csr.in_col.copy(), None, csr.wdeg, csr.outdeg, None,
