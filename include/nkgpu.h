@@ -51,6 +51,11 @@ enum { NKG_PREC_FP64 = 0, NKG_PREC_FP32_REFINE = 1, NKG_PREC_FP32 = 2 };
 
 typedef struct nkg_graph nkg_graph;
 
+/* Flag of nkg_pagerank_run_ex, nkg_graph_set_weights and nkg_pagerank_adjoint:
+ * every array argument is DEVICE memory on the graph's device (without it,
+ * host memory). */
+#define NKG_DEVICE_PTRS 1
+
 /* PageRank(G, damp, tol, normalized) (PageRank.hpp:40, centrality.pyx:2006)
  * plus the public fields norm / maxIterations (PageRank.hpp:64,67) and the
  * distributeSinks flag (redistribute the mass of out-degree-0 nodes uniformly
@@ -153,6 +158,42 @@ NKG_API int nkg_pagerank_run_device(nkg_graph *g, const nkg_pr_params *p, double
 NKG_API int nkg_pagerank_run_teleport(nkg_graph *g, const nkg_pr_params *p, const double *teleport,
                               double *scores_out, uint64_t *iterations_out, double *max_out,
                               nkg_stats *stats);
+
+/* nkg_pagerank_run / nkg_pagerank_run_teleport with the array arguments in
+ * host or device memory (flags: 0 or NKG_DEVICE_PTRS): teleport (z doubles,
+ * NULL for the uniform teleport) and scores_out (z doubles). */
+NKG_API int nkg_pagerank_run_ex(nkg_graph *g, const nkg_pr_params *p, const double *teleport,
+                                double *scores_out, int flags, uint64_t *iterations_out,
+                                double *max_out, nkg_stats *stats);
+
+/* Differentiable form, no reference counterpart.
+ *
+ * nkg_graph_set_weights: replace the arc weights of a graph created weighted
+ * (with arc_order 0): in_w holds `arcs` weights in the order of the in_col
+ * given to nkg_graph_create; out_wdeg (z doubles) the new weighted degrees,
+ * or NULL to have them summed on the device (over each node's out-arcs, in
+ * the order those arcs appear in the in-CSR). The graph keeps its layout and
+ * buffers; what differs is the weights only, as if the graph had been created
+ * with them.
+ *
+ * nkg_pagerank_adjoint: the backward pass of PageRank (normalized = 0) for a
+ * loss L(scores). Inputs: the parameters and teleport (NULL: uniform) of the
+ * forward run, its scores (z doubles, the converged output of
+ * nkg_pagerank_run*), and grad_scores = dL/dscores (z doubles). Outputs
+ * (each may be NULL): grad_w_out = dL/dw for every arc (`arcs` doubles, the
+ * order of in_col; for unweighted graphs the derivative at w = 1), and
+ * grad_t_out = dL/dteleport (z doubles; 0 at deleted ids). The adjoint
+ * system (I - damp M^T) lam = grad - (grad.scores) 1 is solved to
+ * |residual|_1 <= tol * |right-hand side|_1: p->precision FP64 by Jacobi
+ * sweeps, FP32_REFINE by FP32 BiCGSTAB with FP64 residual sweeps, FP32 by
+ * FP32 BiCGSTAB alone (to max(tol, 3e-7)). iterations_out / stats count the
+ * sweeps (fp64_sweeps, fp32_sweeps). flags: 0 or NKG_DEVICE_PTRS. */
+NKG_API int nkg_graph_set_weights(nkg_graph *g, const double *in_w, const double *out_wdeg,
+                                  int flags);
+NKG_API int nkg_pagerank_adjoint(nkg_graph *g, const nkg_pr_params *p, const double *teleport,
+                                 const double *scores, const double *grad_scores,
+                                 double *grad_w_out, double *grad_t_out, int flags,
+                                 uint64_t *iterations_out, nkg_stats *stats);
 
 /* Batched personalised PageRank, no reference counterpart: k <= 256 columns,
  * column j with the teleport t_j = e_{seeds[j]} (seeds are node ids of the

@@ -28,6 +28,7 @@ NKG_PREC_FP32_REFINE = 1
 NKG_PREC_FP32 = 2
 
 UINT64_MAX = 2**64 - 1
+NKG_DEVICE_PTRS = 1
 
 
 class PRParams(C.Structure):
@@ -113,6 +114,11 @@ SIGNATURES = {
                                            _vp, _u64p, _vp]),
     "nkg_ppr_run": (C.c_int, [_vp, C.POINTER(PRParams), C.c_uint32, _u32p, _vp, C.c_int, _u64p,
                               C.POINTER(Stats)]),
+    "nkg_pagerank_run_ex": (C.c_int, [_vp, C.POINTER(PRParams), _vp, _vp, C.c_int, _u64p, _f64p,
+                                      C.POINTER(Stats)]),
+    "nkg_graph_set_weights": (C.c_int, [_vp, _vp, _vp, C.c_int]),
+    "nkg_pagerank_adjoint": (C.c_int, [_vp, C.POINTER(PRParams), _vp, _vp, _vp, _vp, _vp, C.c_int,
+                                       _u64p, C.POINTER(Stats)]),
 }
 
 _lib = None
@@ -226,6 +232,58 @@ class DeviceGraph:
         check(lib().nkg_pagerank_run_device(self.h, C.byref(p), _vp(d_out_ptr), C.byref(it),
                                             C.byref(mx), C.byref(st)))
         return int(it.value), float(mx.value), st.as_dict()
+
+    def run_ex(self, p: PRParams, teleport_ptr: int, out_ptr: int, on_device: bool):
+        """nkg_pagerank_run_ex on raw pointers (host or device, per on_device);
+        teleport_ptr 0 = uniform. Returns (iterations, maximum, stats)."""
+        it = C.c_uint64(0)
+        mx = C.c_double(0.0)
+        st = Stats()
+        check(lib().nkg_pagerank_run_ex(self.h, C.byref(p), _vp(teleport_ptr or None),
+                                        _vp(out_ptr), NKG_DEVICE_PTRS if on_device else 0,
+                                        C.byref(it), C.byref(mx), C.byref(st)))
+        return int(it.value), float(mx.value), st.as_dict()
+
+    def set_weights(self, in_w, out_wdeg=None):
+        """New arc weights (numpy, in in_col order); out_wdeg None = summed on
+        the device."""
+        w = np.ascontiguousarray(in_w, np.float64)
+        d = None if out_wdeg is None else np.ascontiguousarray(out_wdeg, np.float64)
+        check(lib().nkg_graph_set_weights(self.h, _vp(w.ctypes.data),
+                                          None if d is None else _vp(d.ctypes.data), 0))
+
+    def set_weights_device(self, w_ptr: int, wdeg_ptr: int = 0):
+        check(lib().nkg_graph_set_weights(self.h, _vp(w_ptr), _vp(wdeg_ptr or None),
+                                          NKG_DEVICE_PTRS))
+
+    def adjoint(self, p: PRParams, scores, grad, teleport=None, arcs=None):
+        """Backward pass on host arrays: returns (grad_w[arcs], grad_t[z],
+        sweeps, stats)."""
+        s = np.ascontiguousarray(scores, np.float64)
+        g = np.ascontiguousarray(grad, np.float64)
+        t = None if teleport is None else np.ascontiguousarray(teleport, np.float64)
+        m = int(self.info()["arcs"] if arcs is None else arcs)
+        gw = np.empty(max(m, 1), np.float64)
+        gt = np.empty(self.z, np.float64)
+        it = C.c_uint64(0)
+        st = Stats()
+        check(lib().nkg_pagerank_adjoint(self.h, C.byref(p),
+                                         None if t is None else _vp(t.ctypes.data),
+                                         _vp(s.ctypes.data), _vp(g.ctypes.data),
+                                         _vp(gw.ctypes.data), _vp(gt.ctypes.data), 0,
+                                         C.byref(it), C.byref(st)))
+        return gw[:m], gt, int(it.value), st.as_dict()
+
+    def adjoint_device(self, p: PRParams, scores_ptr: int, grad_ptr: int, gw_ptr: int,
+                       gt_ptr: int, teleport_ptr: int = 0):
+        """Backward pass on device pointers (0 = NULL); returns (sweeps, stats)."""
+        it = C.c_uint64(0)
+        st = Stats()
+        check(lib().nkg_pagerank_adjoint(self.h, C.byref(p), _vp(teleport_ptr or None),
+                                         _vp(scores_ptr), _vp(grad_ptr), _vp(gw_ptr or None),
+                                         _vp(gt_ptr or None), NKG_DEVICE_PTRS, C.byref(it),
+                                         C.byref(st)))
+        return int(it.value), st.as_dict()
 
     def ppr(self, seeds, p: PRParams, d_out_ptr: int = 0):
         """Batched personalised PageRank (one column per seed). Returns

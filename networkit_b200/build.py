@@ -23,8 +23,8 @@ INCLUDE = os.path.join(ROOT, "include")
 GPU_LIB = os.path.join(LIBDIR, "libnkgpu.so")
 GEN_LIB = os.path.join(LIBDIR, "libnkgen.so")
 
-GPU_SOURCES = ["nkgpu.cu", "noalloc.cu", "ppr.cu"]
-GPU_HEADERS = ["common.cuh", "sweep.cuh", "graph.hpp", "host.hpp"]
+GPU_SOURCES = ["nkgpu.cu", "noalloc.cu", "ppr.cu", "adjoint.cu"]
+GPU_HEADERS = ["common.cuh", "sweep.cuh", "refine.cuh", "graph.hpp", "host.hpp"]
 GEN_SOURCES = ["graphgen.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -17,6 +17,38 @@ constexpr uint32_t kUnitsPerWarp = 8;
 // epilogue of its 32 rows).
 constexpr uint32_t kSliceOverhead = 3;
 
+// Sliced layout (SELL-32 with chunked long rows, see sweep.cuh) of one
+// adjacency: the in-adjacency for the forward sweeps, the out-adjacency for
+// the adjoint.
+struct SellLayout {
+    uint32_t n_long = 0, n_vlong = 0, n_chunks = 0, s_chunk = 0, slices = 0;
+    uint64_t slots = 0;
+    DeviceArray<uint32_t> chunk_begin;  // n_long+1
+    DeviceArray<uint32_t> slice_off;    // slices+1
+    DeviceArray<uint64_t> slice_cost;   // slices, inclusive prefix of slice costs
+    DeviceArray<uint32_t> col_sell;     // slots
+    DeviceArray<double> w_sell64;       // slots (weighted)
+};
+
+// Build the sliced layout of a CSR whose n rows are sorted by length,
+// descending; the weight of entry k is w[w_index[k]] (w[k] without an index,
+// no weights when w is null).
+void build_sell(SellLayout &L, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                const double *w, const uint32_t *w_index, const uint32_t *rowlen, int device,
+                cudaStream_t s);
+// Rewrite the FP64 slot weights of a layout built by build_sell.
+void refill_sell_weights(SellLayout &L, uint32_t n, const uint32_t *row_ptr, const double *w,
+                         const uint32_t *w_index, int device, cudaStream_t s);
+// Cost-balanced unit boundaries over the slices of L (units+1 entries).
+void sell_units(const SellLayout &L, uint32_t units, uint32_t *unit_start, cudaStream_t s);
+void convert_to_float(const double *in, float *out, uint64_t m, int device, cudaStream_t s);
+
+struct AdjointState;
+void destroy_adjoint(AdjointState *a);
+struct AdjointDeleter {
+    void operator()(AdjointState *a) const { destroy_adjoint(a); }
+};
+
 // Per-precision work buffers and the captured sweep graph.
 template <typename T>
 struct Plane {
@@ -49,16 +81,15 @@ struct nkg_graph {
     nkg::DeviceArray<double> w64src;     // CSR arc weights (FP64, relabelled order)
     nkg::DeviceArray<double> degw64src;  // weighted degree (FP64)
 
-    // Sliced layout of the sweep.
-    uint32_t n_long = 0, n_vlong = 0, n_chunks = 0, s_chunk = 0, slices = 0;
+    nkg::DeviceArray<uint64_t> row_src; // n: offset of new row r in the caller's in-CSR
+
+    // Sliced layout of the sweep (the in-adjacency).
+    nkg::SellLayout fw;
     int sweep_shape = 0;
     bool arc_sorted = false;
-    uint64_t slots = 0;
-    nkg::DeviceArray<uint32_t> chunk_begin;  // n_long+1
-    nkg::DeviceArray<uint32_t> slice_off;    // slices+1
-    nkg::DeviceArray<uint64_t> slice_cost;   // slices, inclusive prefix of slice costs
-    nkg::DeviceArray<uint32_t> col_sell;     // slots
-    nkg::DeviceArray<double> w_sell64;       // slots (weighted)
+
+    // Out-adjacency layout and buffers of the adjoint (built on first use).
+    std::unique_ptr<nkg::AdjointState, nkg::AdjointDeleter> adj;
 
     nkg::Plane<double> p64;
     nkg::Plane<float> p32;
@@ -76,3 +107,13 @@ struct nkg_graph {
     std::atomic<int> cancel{0};
     bool has_run = false;
 };
+
+namespace nkg {
+// The out-adjacency layout of the adjoint (adjoint.cu), built on first use.
+AdjointState &adjoint_ensure(nkg_graph *g);
+// Refresh the adjoint's copies of the arc weights after w64src changed.
+void adjoint_refresh_weights(nkg_graph *g);
+// Weighted out-degree of every node (relabelled order) summed over its
+// out-arcs in the order they appear in the in-CSR.
+void adjoint_out_wdeg(nkg_graph *g, double *degw);
+} // namespace nkg

@@ -95,12 +95,14 @@ __global__ void build_perm(const uint32_t *__restrict__ sorted_ids, uint64_t n,
                            const uint64_t *__restrict__ in_ptr, uint32_t *__restrict__ perm,
                            uint32_t *__restrict__ inv, uint32_t *__restrict__ rowlen,
                            const uint32_t *__restrict__ outdeg, uint32_t *__restrict__ degc,
-                           const double *__restrict__ wdeg, double *__restrict__ degw) {
+                           const double *__restrict__ wdeg, double *__restrict__ degw,
+                           uint64_t *__restrict__ row_src) {
     const uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (r >= n)
         return;
     const uint32_t o = sorted_ids[r];
     perm[r] = o;
+    row_src[r] = in_ptr[o];
     inv[o] = static_cast<uint32_t>(r);
     rowlen[r] = static_cast<uint32_t>(in_ptr[o + 1] - in_ptr[o]);
     degc[r] = outdeg[o];
@@ -218,12 +220,15 @@ __global__ void slice_lengths(uint32_t slices, uint32_t s_chunk, uint32_t n_chun
     }
 }
 
-// Fill the column-major slices; padding slots point at the zero entry n.
+// Fill the column-major slices; padding slots point at the zero entry n. The
+// weight of CSR entry k is w[w_index[k]] (w[k] without an index); a null
+// col_sell refreshes the weights only.
 __global__ void fill_slices(uint32_t slices, uint32_t s_chunk, uint32_t n_chunks, uint32_t n_long,
                             uint32_t n, const uint32_t *__restrict__ chunk_row,
                             const uint32_t *__restrict__ chunk_idx,
                             const uint32_t *__restrict__ row_ptr, const uint32_t *__restrict__ col,
-                            const double *__restrict__ w, const uint32_t *__restrict__ slice_off,
+                            const double *__restrict__ w, const uint32_t *__restrict__ w_index,
+                            const uint32_t *__restrict__ slice_off,
                             uint32_t *__restrict__ col_sell, double *__restrict__ w_sell) {
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -235,9 +240,10 @@ __global__ void fill_slices(uint32_t slices, uint32_t s_chunk, uint32_t n_chunks
         for (uint32_t j = 0; j < len; ++j) {
             const size_t slot = (static_cast<size_t>(off) + j) * 32 + lane;
             const bool real = j < v.len;
-            col_sell[slot] = real ? col[v.start + j] : n;
+            if (col_sell)
+                col_sell[slot] = real ? col[v.start + j] : n;
             if (w_sell)
-                w_sell[slot] = real ? w[v.start + j] : 0.0;
+                w_sell[slot] = real ? w[w_index ? w_index[v.start + j] : v.start + j] : 0.0;
         }
     }
 }
@@ -426,10 +432,12 @@ static void sort_rows(nkg_graph *g, cudaStream_t s) {
     g->arc_sorted = true;
 }
 
-// Build the sliced layout from the relabelled in-CSR (row_ptr, col, w64src).
-static void build_slices(nkg_graph *g, const uint32_t *rowlen, cudaStream_t s) {
-    const uint32_t n = static_cast<uint32_t>(g->n);
-    const unsigned sms = num_sms(g->device);
+// Build the sliced layout L of a CSR whose n rows are sorted by length,
+// descending (row_ptr, col, optional weights w through w_index, rowlen).
+void build_sell(SellLayout &L, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
+                const double *w, const uint32_t *w_index, const uint32_t *rowlen, int device,
+                cudaStream_t s) {
+    const unsigned sms = num_sms(device);
     DeviceArray<unsigned long long> cnt(2);
     NKG_CUDA(cudaMemsetAsync(cnt.get(), 0, 2 * sizeof(unsigned long long), s));
     count_long<<<ceil_div(n, 256), 256, 0, s>>>(rowlen, n, cnt.get());
@@ -437,73 +445,105 @@ static void build_slices(nkg_graph *g, const uint32_t *rowlen, cudaStream_t s) {
     unsigned long long h_cnt[2];
     NKG_CUDA(cudaMemcpyAsync(h_cnt, cnt.get(), sizeof(h_cnt), cudaMemcpyDeviceToHost, s));
     NKG_CUDA(cudaStreamSynchronize(s));
-    g->n_long = static_cast<uint32_t>(h_cnt[0]);
-    g->n_vlong = static_cast<uint32_t>(h_cnt[1]);
+    L.n_long = static_cast<uint32_t>(h_cnt[0]);
+    L.n_vlong = static_cast<uint32_t>(h_cnt[1]);
 
-    g->chunk_begin.alloc(static_cast<size_t>(g->n_long) + 1);
-    NKG_CUDA(cudaMemsetAsync(g->chunk_begin.get(), 0, sizeof(uint32_t), s));
+    L.chunk_begin.alloc(static_cast<size_t>(L.n_long) + 1);
+    NKG_CUDA(cudaMemsetAsync(L.chunk_begin.get(), 0, sizeof(uint32_t), s));
     DeviceArray<uint32_t> chunk_row, chunk_idx;
-    if (g->n_long) {
-        DeviceArray<uint32_t> nch(g->n_long);
-        chunk_counts<<<ceil_div(g->n_long, 256), 256, 0, s>>>(rowlen, g->n_long, nch.get());
+    if (L.n_long) {
+        DeviceArray<uint32_t> nch(L.n_long);
+        chunk_counts<<<ceil_div(L.n_long, 256), 256, 0, s>>>(rowlen, L.n_long, nch.get());
         size_t tb = 0;
-        NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, nch.get(), g->chunk_begin.get() + 1,
-                                               static_cast<int64_t>(g->n_long), s));
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, nch.get(), L.chunk_begin.get() + 1,
+                                               static_cast<int64_t>(L.n_long), s));
         DeviceArray<unsigned char> tmp(tb);
-        NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb, nch.get(), g->chunk_begin.get() + 1,
-                                               static_cast<int64_t>(g->n_long), s));
-        g->n_chunks = read_scalar(g->chunk_begin.get() + g->n_long, s);
-        chunk_row.alloc(g->n_chunks);
-        chunk_idx.alloc(g->n_chunks);
-        expand_chunks<<<sms * 4, 256, 0, s>>>(g->chunk_begin.get(), g->n_long, chunk_row.get(),
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb, nch.get(), L.chunk_begin.get() + 1,
+                                               static_cast<int64_t>(L.n_long), s));
+        L.n_chunks = read_scalar(L.chunk_begin.get() + L.n_long, s);
+        chunk_row.alloc(L.n_chunks);
+        chunk_idx.alloc(L.n_chunks);
+        expand_chunks<<<sms * 4, 256, 0, s>>>(L.chunk_begin.get(), L.n_long, chunk_row.get(),
                                               chunk_idx.get());
         NKG_CUDA(cudaGetLastError());
     } else {
-        g->n_chunks = 0;
+        L.n_chunks = 0;
     }
-    g->s_chunk = (g->n_chunks + 31) / 32;
-    const uint64_t s_rows = (static_cast<uint64_t>(n - g->n_long) + 31) / 32;
-    const uint64_t slices = g->s_chunk + s_rows;
+    L.s_chunk = (L.n_chunks + 31) / 32;
+    const uint64_t s_rows = (static_cast<uint64_t>(n - L.n_long) + 31) / 32;
+    const uint64_t slices = L.s_chunk + s_rows;
     require(slices < 0xffffffffull, "too many slices");
-    g->slices = static_cast<uint32_t>(slices);
+    L.slices = static_cast<uint32_t>(slices);
 
-    DeviceArray<uint32_t> slen(g->slices);
-    DeviceArray<uint64_t> scost(g->slices);
-    g->slice_cost.alloc(g->slices);
-    g->slice_off.alloc(static_cast<size_t>(g->slices) + 1);
-    if (g->slices) {
-        slice_lengths<<<ceil_div(static_cast<uint64_t>(g->slices) * 32, 256), 256, 0, s>>>(
-            g->slices, g->s_chunk, g->n_chunks, g->n_long, n, chunk_row.get(), chunk_idx.get(),
-            g->row_ptr.get(), slen.get(), scost.get());
+    DeviceArray<uint32_t> slen(L.slices);
+    DeviceArray<uint64_t> scost(L.slices);
+    L.slice_cost.alloc(L.slices);
+    L.slice_off.alloc(static_cast<size_t>(L.slices) + 1);
+    if (L.slices) {
+        slice_lengths<<<ceil_div(static_cast<uint64_t>(L.slices) * 32, 256), 256, 0, s>>>(
+            L.slices, L.s_chunk, L.n_chunks, L.n_long, n, chunk_row.get(), chunk_idx.get(),
+            row_ptr, slen.get(), scost.get());
         NKG_CUDA(cudaGetLastError());
     }
-    NKG_CUDA(cudaMemsetAsync(g->slice_off.get(), 0, sizeof(uint32_t), s));
-    if (g->slices) {
+    NKG_CUDA(cudaMemsetAsync(L.slice_off.get(), 0, sizeof(uint32_t), s));
+    if (L.slices) {
         size_t tb = 0;
-        NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, slen.get(), g->slice_off.get() + 1,
-                                               static_cast<int64_t>(g->slices), s));
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, slen.get(), L.slice_off.get() + 1,
+                                               static_cast<int64_t>(L.slices), s));
         size_t tb2 = 0;
-        NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb2, scost.get(), g->slice_cost.get(),
-                                               static_cast<int64_t>(g->slices), s));
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb2, scost.get(), L.slice_cost.get(),
+                                               static_cast<int64_t>(L.slices), s));
         DeviceArray<unsigned char> tmp(std::max(tb, tb2));
-        NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb, slen.get(), g->slice_off.get() + 1,
-                                               static_cast<int64_t>(g->slices), s));
-        NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb2, scost.get(), g->slice_cost.get(),
-                                               static_cast<int64_t>(g->slices), s));
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb, slen.get(), L.slice_off.get() + 1,
+                                               static_cast<int64_t>(L.slices), s));
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb2, scost.get(), L.slice_cost.get(),
+                                               static_cast<int64_t>(L.slices), s));
     }
-    const uint32_t cols = read_scalar(g->slice_off.get() + g->slices, s);
-    g->slots = static_cast<uint64_t>(cols) * 32;
-    g->col_sell.alloc(g->slots, 4);
-    if (g->weighted)
-        g->w_sell64.alloc(g->slots, 4);
-    if (g->slices) {
-        fill_slices<<<sms * 16, 256, 0, s>>>(g->slices, g->s_chunk, g->n_chunks, g->n_long, n,
-                                             chunk_row.get(), chunk_idx.get(), g->row_ptr.get(),
-                                             g->col.get(), g->w64src.get(), g->slice_off.get(),
-                                             g->col_sell.get(), g->w_sell64.get());
+    const uint32_t cols = read_scalar(L.slice_off.get() + L.slices, s);
+    L.slots = static_cast<uint64_t>(cols) * 32;
+    L.col_sell.alloc(L.slots, 4);
+    if (w)
+        L.w_sell64.alloc(L.slots, 4);
+    if (L.slices) {
+        fill_slices<<<sms * 16, 256, 0, s>>>(L.slices, L.s_chunk, L.n_chunks, L.n_long, n,
+                                             chunk_row.get(), chunk_idx.get(), row_ptr, col, w,
+                                             w_index, L.slice_off.get(), L.col_sell.get(),
+                                             L.w_sell64.get());
         NKG_CUDA(cudaGetLastError());
     }
     NKG_CUDA(cudaStreamSynchronize(s));
+}
+
+// Rewrite the FP64 slot weights of L from new CSR weights (same structure).
+void refill_sell_weights(SellLayout &L, uint32_t n, const uint32_t *row_ptr, const double *w,
+                         const uint32_t *w_index, int device, cudaStream_t s) {
+    if (!L.slices)
+        return;
+    const unsigned sms = num_sms(device);
+    DeviceArray<uint32_t> chunk_row(std::max<uint32_t>(L.n_chunks, 1)),
+        chunk_idx(std::max<uint32_t>(L.n_chunks, 1));
+    if (L.n_long)
+        expand_chunks<<<sms * 4, 256, 0, s>>>(L.chunk_begin.get(), L.n_long, chunk_row.get(),
+                                              chunk_idx.get());
+    fill_slices<<<sms * 16, 256, 0, s>>>(L.slices, L.s_chunk, L.n_chunks, L.n_long, n,
+                                         chunk_row.get(), chunk_idx.get(), row_ptr, nullptr, w,
+                                         w_index, L.slice_off.get(), nullptr, L.w_sell64.get());
+    NKG_CUDA(cudaGetLastError());
+    NKG_CUDA(cudaStreamSynchronize(s));
+}
+
+// Cut the slices of L into `units` cost-balanced ranges (unit_start, units+1).
+void sell_units(const SellLayout &L, uint32_t units, uint32_t *unit_start, cudaStream_t s) {
+    unit_bounds<<<ceil_div(static_cast<uint64_t>(units) + 1, 256), 256, 0, s>>>(
+        L.slice_cost.get(), L.slices, units, unit_start);
+    NKG_CUDA(cudaGetLastError());
+}
+
+void convert_to_float(const double *in, float *out, uint64_t m, int device, cudaStream_t s) {
+    if (!m)
+        return;
+    convert_array<float><<<num_sms(device) * 8, 256, 0, s>>>(in, out, m);
+    NKG_CUDA(cudaGetLastError());
 }
 
 static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr,
@@ -603,6 +643,7 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
     g->perm.alloc(n);
     g->inv.alloc(z);
     g->degc.alloc(n);
+    g->row_src.alloc(n);
     g->row_ptr.alloc(n + 1, 4);
     DeviceArray<uint32_t> rowlen(n);
     if (g->weighted)
@@ -610,7 +651,8 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
     NKG_CUDA(cudaMemsetAsync(g->inv.get(), 0xff, z * sizeof(uint32_t), s));
     build_perm<<<ceil_div(n, 256), 256, 0, s>>>(ids_s.get(), n, d_ptr.get(), g->perm.get(),
                                                 g->inv.get(), rowlen.get(), outdeg.get(),
-                                                g->degc.get(), d_wdeg.get(), g->degw64src.get());
+                                                g->degc.get(), d_wdeg.get(), g->degw64src.get(),
+                                                g->row_src.get());
     NKG_CUDA(cudaGetLastError());
     NKG_CUDA(cudaMemsetAsync(g->row_ptr.get(), 0, sizeof(uint32_t), s));
     tmp_bytes = 0;
@@ -637,7 +679,8 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
         if (opt->arc_order == 1 && arcs > 1 && arcs < 0x7fffffffull)
             sort_rows(g.get(), s);
     }
-    build_slices(g.get(), rowlen.get(), s);
+    build_sell(g->fw, static_cast<uint32_t>(n), g->row_ptr.get(), g->col.get(), g->w64src.get(),
+               nullptr, rowlen.get(), dev, s);
     NKG_CUDA(cudaEventRecord(g->ev1, s));
     NKG_CUDA(cudaStreamSynchronize(s));
     float ms = 0.f;
@@ -649,7 +692,7 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
     // they are never reallocated under a captured graph.
     g->cta_res.alloc(static_cast<size_t>(sms) * 32);
     g->cta_sink.alloc(static_cast<size_t>(sms) * 32);
-    const size_t fix = static_cast<size_t>(g->n_vlong) + ceil_div(g->n_long, kFixThreads) + 1;
+    const size_t fix = static_cast<size_t>(g->fw.n_vlong) + ceil_div(g->fw.n_long, kFixThreads) + 1;
     g->fix_res.alloc(fix);
     g->fix_sink.alloc(fix);
     g->rp.alloc(1);
@@ -692,12 +735,12 @@ static void sweep_setup(nkg_graph *g) {
         P.y[b].alloc(n + 1, 4);
         NKG_CUDA(cudaMemsetAsync(P.y[b].get(), 0, (n + 1 + 4) * sizeof(T), s));
     }
-    P.chunk_val.alloc(static_cast<size_t>(g->s_chunk) * 32 + 1);
+    P.chunk_val.alloc(static_cast<size_t>(g->fw.s_chunk) * 32 + 1);
     if (WEIGHTED && !std::is_same<T, double>::value) {
-        P.w_sell.alloc(g->slots, 4);
+        P.w_sell.alloc(g->fw.slots, 4);
         P.degw.alloc(n);
-        if (g->slots)
-            convert_array<T><<<sms * 8, 256, 0, s>>>(g->w_sell64.get(), P.w_sell.get(), g->slots);
+        if (g->fw.slots)
+            convert_array<T><<<sms * 8, 256, 0, s>>>(g->fw.w_sell64.get(), P.w_sell.get(), g->fw.slots);
         convert_array<T><<<sms * 8, 256, 0, s>>>(g->degw64src.get(), P.degw.get(), n);
         NKG_CUDA(cudaGetLastError());
     }
@@ -713,15 +756,15 @@ static void sweep_setup(nkg_graph *g) {
     require(occ >= 1, "sweep kernel does not fit on an SM");
     P.sweep_ctas = static_cast<unsigned>(std::max<uint64_t>(
         1, std::min<uint64_t>(static_cast<uint64_t>(occ) * sms,
-                              (static_cast<uint64_t>(g->slices) * 32 + threads - 1) / threads)));
+                              (static_cast<uint64_t>(g->fw.slices) * 32 + threads - 1) / threads)));
     const uint64_t warps = static_cast<uint64_t>(P.sweep_ctas) * (threads / 32);
     P.units = static_cast<uint32_t>(
-        std::max<uint64_t>(1, std::min<uint64_t>(warps * kUnitsPerWarp, g->slices)));
+        std::max<uint64_t>(1, std::min<uint64_t>(warps * kUnitsPerWarp, g->fw.slices)));
     P.unit_start.alloc(static_cast<size_t>(P.units) + 1);
     unit_bounds<<<ceil_div(static_cast<uint64_t>(P.units) + 1, 256), 256, 0, s>>>(
-        g->slice_cost.get(), g->slices, P.units, P.unit_start.get());
+        g->fw.slice_cost.get(), g->fw.slices, P.units, P.unit_start.get());
     NKG_CUDA(cudaGetLastError());
-    P.fix_ctas = g->n_vlong + ceil_div(std::max<uint32_t>(g->n_long - g->n_vlong, 1), kFixThreads);
+    P.fix_ctas = g->fw.n_vlong + ceil_div(std::max<uint32_t>(g->fw.n_long - g->fw.n_vlong, 1), kFixThreads);
     require(P.sweep_ctas <= g->cta_res.size() && P.fix_ctas <= g->fix_res.size(),
             "partial-sum buffers too small");
     NKG_CUDA(cudaStreamSynchronize(s));
@@ -731,17 +774,17 @@ template <typename T, bool WEIGHTED>
 static SweepArgs<T> sweep_args(nkg_graph *g, int in_buf) {
     Plane<T> &P = plane<T>(g);
     SweepArgs<T> a{};
-    a.col_sell = g->col_sell.get();
+    a.col_sell = g->fw.col_sell.get();
     if (std::is_same<T, double>::value) {
-        a.w_sell = reinterpret_cast<const T *>(g->w_sell64.get());
+        a.w_sell = reinterpret_cast<const T *>(g->fw.w_sell64.get());
         a.degw = reinterpret_cast<const T *>(g->degw64src.get());
     } else {
         a.w_sell = P.w_sell.get();
         a.degw = P.degw.get();
     }
-    a.slice_off = g->slice_off.get();
+    a.slice_off = g->fw.slice_off.get();
     a.unit_start = P.unit_start.get();
-    a.chunk_begin = g->chunk_begin.get();
+    a.chunk_begin = g->fw.chunk_begin.get();
     a.degc = g->degc.get();
     a.tele = P.tele.get();
     a.y_in = P.y[in_buf].get();
@@ -754,9 +797,9 @@ static SweepArgs<T> sweep_args(nkg_graph *g, int in_buf) {
     a.rp = g->rp.get();
     a.st = g->st.get();
     a.n = static_cast<uint32_t>(g->n);
-    a.n_long = g->n_long;
-    a.n_vlong = g->n_vlong;
-    a.s_chunk = g->s_chunk;
+    a.n_long = g->fw.n_long;
+    a.n_vlong = g->fw.n_vlong;
+    a.s_chunk = g->fw.s_chunk;
     a.units = P.units;
     a.sweep_ctas = P.sweep_ctas;
     return a;
@@ -849,7 +892,7 @@ static uint64_t bytes_per_sweep(const nkg_graph *g, int elem) {
 
 template <typename T, bool WEIGHTED>
 static void upload_run_state(nkg_graph *g, const nkg_pr_params &p, int personal,
-                             const double *teleport_host, DeviceArray<double> &d_tele_orig) {
+                             const double *d_tele) {
     cudaStream_t s = g->stream;
     Plane<T> &P = plane<T>(g);
     const uint32_t n = static_cast<uint32_t>(g->n);
@@ -870,10 +913,7 @@ static void upload_run_state(nkg_graph *g, const nkg_pr_params &p, int personal,
     if (personal) {
         if (!P.tele)
             P.tele.alloc(n);
-        d_tele_orig.alloc(g->z);
-        NKG_CUDA(cudaMemcpyAsync(d_tele_orig.get(), teleport_host, g->z * sizeof(double),
-                                 cudaMemcpyHostToDevice, s));
-        permute_teleport<T><<<ceil_div(n, 256), 256, 0, s>>>(d_tele_orig.get(), g->perm.get(), n,
+        permute_teleport<T><<<ceil_div(n, 256), 256, 0, s>>>(d_tele, g->perm.get(), n,
                                                              P.tele.get());
     }
     const double S0 = static_cast<double>(g->sinks) * x0;
@@ -888,17 +928,16 @@ static void upload_run_state(nkg_graph *g, const nkg_pr_params &p, int personal,
 }
 
 template <typename T, bool WEIGHTED>
-static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *teleport_host,
+static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *d_tele,
                            double *d_out) {
     cudaStream_t s = g->stream;
     sweep_setup<T, WEIGHTED>(g);
     Plane<T> &P = plane<T>(g);
-    const int personal = teleport_host ? 1 : 0;
+    const int personal = d_tele ? 1 : 0;
     RunResult R;
 
-    DeviceArray<double> d_tele_orig;
     NKG_CUDA(cudaEventRecord(g->ev0, s));
-    upload_run_state<T, WEIGHTED>(g, p, personal, teleport_host, d_tele_orig);
+    upload_run_state<T, WEIGHTED>(g, p, personal, d_tele);
     R.launches += 1 + personal;
 
     cudaGraphExec_t exec = sweep_graph<T, WEIGHTED>(g, personal);
@@ -931,43 +970,42 @@ static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *t
 // (refine.cuh). The stopping test is the reference's, applied to the FP64
 // sweep: the returned scores are that sweep's iterate, like PageRank.cpp:70.
 template <bool WEIGHTED>
-static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *teleport_host,
+static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *d_tele,
                             double *d_out) {
     cudaStream_t s = g->stream;
     sweep_setup<float, WEIGHTED>(g);
     sweep_setup<double, WEIGHTED>(g);
     Plane<float> &P32 = g->p32;
     Plane<double> &P64 = g->p64;
-    const int personal = teleport_host ? 1 : 0;
+    const int personal = d_tele ? 1 : 0;
     const uint32_t n = static_cast<uint32_t>(g->n);
     const unsigned sms = num_sms(g->device);
     RunResult R;
     NKG_CUDA(cudaEventRecord(g->ev0, s));
     nkg_pr_params p1 = p;
     p1.max_iterations = 1;  // every FP64 launch is exactly one Jacobi sweep
-    DeviceArray<double> d_tele_orig;
-    upload_run_state<double, WEIGHTED>(g, p1, personal, teleport_host, d_tele_orig);
+    upload_run_state<double, WEIGHTED>(g, p1, personal, d_tele);
     if (personal) {
         if (!P32.tele)
             P32.tele.alloc(n);
-        permute_teleport<float><<<ceil_div(n, 256), 256, 0, s>>>(d_tele_orig.get(), g->perm.get(),
+        permute_teleport<float><<<ceil_div(n, 256), 256, 0, s>>>(d_tele, g->perm.get(),
                                                                  n, P32.tele.get());
     }
     DeviceArray<float> bx(n), br(n), brhat(n), bp(n), bv(n), bs(n), bt(n), bg(n + 1, 4);
     DeviceArray<double> x64(n);
     const unsigned vec_ctas = std::max<unsigned>(1, std::min<unsigned>(sms * 4, ceil_div(n, kBiThreads)));
-    const unsigned fix_ctas = std::max<unsigned>(1, ceil_div(g->n_long, kBiThreads));
+    const unsigned fix_ctas = std::max<unsigned>(1, ceil_div(g->fw.n_long, kBiThreads));
     DeviceArray<double> part(2 * static_cast<size_t>(std::max<unsigned>(P32.sweep_ctas, vec_ctas)));
     DeviceArray<double> fix_part(2 * static_cast<size_t>(fix_ctas));
     DeviceArray<BiScalars> sc(1);
     NKG_CUDA(cudaMemsetAsync(sc.get(), 0, sizeof(BiScalars), s));
     NKG_CUDA(cudaMemsetAsync(bg.get(), 0, (n + 1 + 4) * sizeof(float), s));
     BiArgs a{};
-    a.col_sell = g->col_sell.get();
+    a.col_sell = g->fw.col_sell.get();
     a.w_sell = P32.w_sell.get();
-    a.slice_off = g->slice_off.get();
+    a.slice_off = g->fw.slice_off.get();
     a.unit_start = P32.unit_start.get();
-    a.chunk_begin = g->chunk_begin.get();
+    a.chunk_begin = g->fw.chunk_begin.get();
     a.degc = g->degc.get();
     a.degw = P32.degw.get();
     a.tele = P32.tele.get();
@@ -986,9 +1024,9 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
     a.damp = p.damp;
     a.inv_n = 1.0 / static_cast<double>(n);
     a.n = n;
-    a.n_long = g->n_long;
-    a.n_vlong = g->n_vlong;
-    a.s_chunk = g->s_chunk;
+    a.n_long = g->fw.n_long;
+    a.n_vlong = g->fw.n_vlong;
+    a.s_chunk = g->fw.s_chunk;
     a.units = P32.units;
     a.sweep_ctas = P32.sweep_ctas;
     a.distribute = p.distribute_sinks ? 1 : 0;
@@ -996,42 +1034,18 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
     a.l2 = p.norm == NKG_NORM_L2;
     BiScalars *hsc = reinterpret_cast<BiScalars *>(g->scalars_host.get());
     static_assert(sizeof(BiScalars) <= 16 * sizeof(double), "BiScalars fits the pinned buffer");
-    uint64_t matvecs = 0;
 
-    // Solve (I - dM) x = r (r holds the right-hand side) to `inner_tol`.
-    auto solve = [&](double rel) {
-        bi_start<<<vec_ctas, kBiThreads, 0, s>>>(a);
-        NKG_CUDA(cudaMemcpyAsync(hsc, sc.get(), sizeof(BiScalars), cudaMemcpyDeviceToHost, s));
-        NKG_CUDA(cudaStreamSynchronize(s));
-        const double inner_tol = std::max(hsc->res * rel, 0.25 * p.tol);
-        R.launches += 1;
-        for (int it = 0; it < 400 && !hsc->breakdown && hsc->res > inner_tol; it += 4) {
-            for (int k = 0; k < 4; ++k) {
-                bi_vec_p<WEIGHTED><<<vec_ctas, kBiThreads, 0, s>>>(a);
-                with_sweep_shape(g->sweep_shape, [&](auto S) {
-                    using Sh = decltype(S);
-                    bi_mv<WEIGHTED, 0, Sh::threads, Sh::unroll><<<P32.sweep_ctas, Sh::threads, 0, s>>>(a);
-                });
-                bi_mv_fix<WEIGHTED, 0><<<fix_ctas, kBiThreads, 0, s>>>(a);
-                bi_vec_s<WEIGHTED><<<vec_ctas, kBiThreads, 0, s>>>(a);
-                with_sweep_shape(g->sweep_shape, [&](auto S) {
-                    using Sh = decltype(S);
-                    bi_mv<WEIGHTED, 1, Sh::threads, Sh::unroll><<<P32.sweep_ctas, Sh::threads, 0, s>>>(a);
-                });
-                bi_mv_fix<WEIGHTED, 1><<<fix_ctas, kBiThreads, 0, s>>>(a);
-                bi_vec_x<<<vec_ctas, kBiThreads, 0, s>>>(a);
-            }
-            NKG_CUDA(cudaGetLastError());
-            R.launches += 28;
-            matvecs += 8;
-            NKG_CUDA(cudaMemcpyAsync(hsc, sc.get(), sizeof(BiScalars), cudaMemcpyDeviceToHost, s));
-            NKG_CUDA(cudaStreamSynchronize(s));
-            if (g->cancel.load()) {
-                g->cancel.store(0);
-                throw Error(NKG_ERR_CANCELLED, "PageRank run cancelled");
-            }
-        }
-    };
+    BiLaunch bl;
+    bl.stream = s;
+    bl.sweep_shape = g->sweep_shape;
+    bl.sweep_ctas = P32.sweep_ctas;
+    bl.vec_ctas = vec_ctas;
+    bl.fix_ctas = fix_ctas;
+    bl.d_sc = sc.get();
+    bl.h_sc = hsc;
+    bl.cancel = &g->cancel;
+    // Solve (I - dM) x = r (r holds the right-hand side).
+    auto solve = [&](double rel) { bi_solve<WEIGHTED, 0>(a, bl, rel, 0.25 * p.tol); };
 
     cudaGraphExec_t exec = sweep_graph<double, WEIGHTED>(g, personal);
     IterState *sh = g->st_host.get();
@@ -1060,11 +1074,12 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
         add = 1;
     }
     NKG_CUDA(cudaEventRecord(g->ev1, s));
-    R.iterations = fp64 + matvecs;
+    R.iterations = fp64 + bl.matvecs;
     R.residual = sh->residual;
     R.sink_mass = sh->sink_mass;
     R.fp64_sweeps = fp64;
-    R.fp32_sweeps = matvecs;
+    R.fp32_sweeps = bl.matvecs;
+    R.launches += bl.launches;
     finalize<double, WEIGHTED>(g, p, P64.y[1].get(), d_out, R);
     return R;
 }
@@ -1132,8 +1147,7 @@ static void profile_sweeps(nkg_graph *g, int sweeps, double *ms_kernel, double *
     p.tol = -1.0;
     p.norm = NKG_NORM_L1;
     p.max_iterations = ~0ull;
-    DeviceArray<double> unused;
-    upload_run_state<T, WEIGHTED>(g, p, 0, nullptr, unused);
+    upload_run_state<T, WEIGHTED>(g, p, 0, nullptr);
     std::vector<cudaEvent_t> ev(2 * static_cast<size_t>(sweeps), nullptr);
     for (auto &e : ev)
         NKG_CUDA(cudaEventCreate(&e));
@@ -1161,12 +1175,20 @@ static void profile_sweeps(nkg_graph *g, int sweeps, double *ms_kernel, double *
     *ms_iter = sweeps > 1 ? total / (sweeps - 1) : sum;
 }
 
-static int run_to(nkg_graph *g, const nkg_pr_params *p, const double *teleport, double *out,
-                  bool out_is_host, uint64_t *iters, double *max_out, nkg_stats *stats) {
+static int run_to(nkg_graph *g, const nkg_pr_params *p, const double *teleport, bool tele_is_host,
+                  double *out, bool out_is_host, uint64_t *iters, double *max_out,
+                  nkg_stats *stats) {
     return guarded([&] {
         require(g != nullptr, "graph handle is NULL");
         require(out != nullptr, "scores_out is NULL");
         DeviceGuard guard(g->device);
+        DeviceArray<double> d_tele_tmp;
+        if (teleport && tele_is_host) {
+            d_tele_tmp.alloc(g->z);
+            NKG_CUDA(cudaMemcpyAsync(d_tele_tmp.get(), teleport, g->z * sizeof(double),
+                                     cudaMemcpyHostToDevice, g->stream));
+            teleport = d_tele_tmp.get();
+        }
         double *d_out = out;
         if (out_is_host) {
             if (!g->out_buf)
@@ -1185,6 +1207,69 @@ static int run_to(nkg_graph *g, const nkg_pr_params *p, const double *teleport, 
             *max_out = R.maximum;
         fill_stats(g, R, p->precision, stats);
     });
+}
+
+// New arc weights (caller's in-CSR order) into the relabelled CSR; one warp
+// per row.
+__global__ void scatter_weights(const uint32_t *__restrict__ row_ptr,
+                                const uint64_t *__restrict__ row_src, const double *__restrict__ w_in,
+                                uint64_t n, double *__restrict__ w) {
+    const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (uint64_t r = warp; r < n; r += nwarps) {
+        const uint32_t b = row_ptr[r], e = row_ptr[r + 1];
+        const uint64_t src = row_src[r];
+        for (uint32_t k = b + lane; k < e; k += 32)
+            w[k] = w_in[src + (k - b)];
+    }
+}
+
+__global__ void permute_wdeg(const double *__restrict__ wdeg_orig, const uint32_t *__restrict__ perm,
+                             uint64_t n, double *__restrict__ degw) {
+    const uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (r < n)
+        degw[r] = wdeg_orig[perm[r]];
+}
+
+// Replace the arc weights (and weighted degrees) of a weighted graph in place:
+// every buffer keeps its address, so captured sweep graphs stay valid.
+static void set_weights(nkg_graph *g, const double *in_w, const double *out_wdeg, bool on_device) {
+    cudaStream_t s = g->stream;
+    const uint32_t n = static_cast<uint32_t>(g->n);
+    const unsigned sms = num_sms(g->device);
+    DeviceArray<double> w_tmp, d_tmp;
+    const double *d_w = in_w, *d_wdeg = out_wdeg;
+    if (!on_device) {
+        w_tmp.alloc(std::max<uint64_t>(g->arcs, 1));
+        if (g->arcs)
+            NKG_CUDA(cudaMemcpyAsync(w_tmp.get(), in_w, g->arcs * sizeof(double),
+                                     cudaMemcpyHostToDevice, s));
+        d_w = w_tmp.get();
+        if (out_wdeg) {
+            d_tmp.alloc(g->z);
+            NKG_CUDA(cudaMemcpyAsync(d_tmp.get(), out_wdeg, g->z * sizeof(double),
+                                     cudaMemcpyHostToDevice, s));
+            d_wdeg = d_tmp.get();
+        }
+    }
+    if (g->arcs)
+        scatter_weights<<<sms * 16, 256, 0, s>>>(g->row_ptr.get(), g->row_src.get(), d_w, n,
+                                                 g->w64src.get());
+    NKG_CUDA(cudaGetLastError());
+    if (d_wdeg)
+        permute_wdeg<<<ceil_div(n, 256), 256, 0, s>>>(d_wdeg, g->perm.get(), n,
+                                                     g->degw64src.get());
+    else
+        adjoint_out_wdeg(g, g->degw64src.get());
+    NKG_CUDA(cudaGetLastError());
+    refill_sell_weights(g->fw, n, g->row_ptr.get(), g->w64src.get(), nullptr, g->device, s);
+    if (g->p32.w_sell) {
+        convert_to_float(g->fw.w_sell64.get(), g->p32.w_sell.get(), g->fw.slots, g->device, s);
+        convert_to_float(g->degw64src.get(), g->p32.degw.get(), n, g->device, s);
+    }
+    adjoint_refresh_weights(g);
+    NKG_CUDA(cudaStreamSynchronize(s));
 }
 
 static void ranking_prepare(double *keys, uint32_t *ids, const uint32_t *inv, uint64_t z,
@@ -1251,8 +1336,8 @@ int nkg_graph_get_info(const nkg_graph *g, nkg_graph_info *info) {
         info->n = g->n;
         info->arcs = g->arcs;
         info->sinks = g->sinks;
-        info->slots = g->slots;
-        info->split_rows = g->n_long;
+        info->slots = g->fw.slots;
+        info->split_rows = g->fw.n_long;
         info->weighted = g->weighted;
         info->directed = g->directed;
         info->device = g->device;
@@ -1262,12 +1347,12 @@ int nkg_graph_get_info(const nkg_graph *g, nkg_graph_info *info) {
 
 int nkg_pagerank_run(nkg_graph *g, const nkg_pr_params *p, double *scores_out,
                      uint64_t *iterations_out, double *max_out, nkg_stats *stats) {
-    return run_to(g, p, nullptr, scores_out, true, iterations_out, max_out, stats);
+    return run_to(g, p, nullptr, true, scores_out, true, iterations_out, max_out, stats);
 }
 
 int nkg_pagerank_run_device(nkg_graph *g, const nkg_pr_params *p, double *d_scores_out,
                             uint64_t *iterations_out, double *max_out, nkg_stats *stats) {
-    return run_to(g, p, nullptr, d_scores_out, false, iterations_out, max_out, stats);
+    return run_to(g, p, nullptr, true, d_scores_out, false, iterations_out, max_out, stats);
 }
 
 int nkg_pagerank_run_teleport(nkg_graph *g, const nkg_pr_params *p, const double *teleport,
@@ -1277,7 +1362,29 @@ int nkg_pagerank_run_teleport(nkg_graph *g, const nkg_pr_params *p, const double
         nkg::set_last_error("teleport is NULL");
         return NKG_ERR_INVALID_ARG;
     }
-    return run_to(g, p, teleport, scores_out, true, iterations_out, max_out, stats);
+    return run_to(g, p, teleport, true, scores_out, true, iterations_out, max_out, stats);
+}
+
+int nkg_pagerank_run_ex(nkg_graph *g, const nkg_pr_params *p, const double *teleport,
+                        double *scores_out, int flags, uint64_t *iterations_out, double *max_out,
+                        nkg_stats *stats) {
+    if (flags & ~NKG_DEVICE_PTRS) {
+        nkg::set_last_error("unknown flags");
+        return NKG_ERR_INVALID_ARG;
+    }
+    const bool host = (flags & NKG_DEVICE_PTRS) == 0;
+    return run_to(g, p, teleport, host, scores_out, host, iterations_out, max_out, stats);
+}
+
+int nkg_graph_set_weights(nkg_graph *g, const double *in_w, const double *out_wdeg, int flags) {
+    return guarded([&] {
+        require(g != nullptr && in_w != nullptr, "NULL argument");
+        require((flags & ~NKG_DEVICE_PTRS) == 0, "unknown flags");
+        require(g->weighted, "the graph was created unweighted (in_w NULL)");
+        require(!g->arc_sorted, "new weights need the in-rows in the caller's order (arc_order 0)");
+        DeviceGuard guard(g->device);
+        set_weights(g, in_w, out_wdeg, (flags & NKG_DEVICE_PTRS) != 0);
+    });
 }
 
 int nkg_ranking(nkg_graph *g, const double *scores, uint64_t *ids_out, double *vals_out) {

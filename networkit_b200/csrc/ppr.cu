@@ -482,10 +482,10 @@ void run_ppr(nkg_graph *g, const nkg_pr_params &p, uint32_t k, const uint32_t *s
     NKG_CUDA(cudaEventRecord(g->ev0, s));
 
     // Virtual rows and their cost-balanced units.
-    const uint32_t nv = g->n_chunks + (n - g->n_long);
-    DeviceArray<uint32_t> chunk_row(std::max<uint32_t>(g->n_chunks, 1));
-    if (g->n_long)
-        ppr_chunk_rows<<<sms * 4, 256, 0, s>>>(g->chunk_begin.get(), g->n_long, chunk_row.get());
+    const uint32_t nv = g->fw.n_chunks + (n - g->fw.n_long);
+    DeviceArray<uint32_t> chunk_row(std::max<uint32_t>(g->fw.n_chunks, 1));
+    if (g->fw.n_long)
+        ppr_chunk_rows<<<sms * 4, 256, 0, s>>>(g->fw.chunk_begin.get(), g->fw.n_long, chunk_row.get());
     int occ = 0;
     const size_t smem_sweep = static_cast<size_t>(kPprWarps) * kp * sizeof(double);
     NKG_CUDA(cudaFuncSetAttribute(ppr_sweep<CPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -505,8 +505,8 @@ void run_ppr(nkg_graph *g, const nkg_pr_params &p, uint32_t k, const uint32_t *s
     DeviceArray<uint64_t> cost(std::max<uint32_t>(nv, 1)), cost_incl(std::max<uint32_t>(nv, 1));
     DeviceArray<uint32_t> unit_start(units + 1);
     if (nv) {
-        ppr_vrow_cost<<<ceil_div(nv, 256), 256, 0, s>>>(g->row_ptr.get(), g->chunk_begin.get(),
-                                                        chunk_row.get(), g->n_chunks, g->n_long,
+        ppr_vrow_cost<<<ceil_div(nv, 256), 256, 0, s>>>(g->row_ptr.get(), g->fw.chunk_begin.get(),
+                                                        chunk_row.get(), g->fw.n_chunks, g->fw.n_long,
                                                         n, cost.get());
         size_t tb = 0;
         NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, cost.get(), cost_incl.get(),
@@ -518,11 +518,11 @@ void run_ppr(nkg_graph *g, const nkg_pr_params &p, uint32_t k, const uint32_t *s
     ppr_unit_bounds<<<ceil_div(units + 1, 256), 256, 0, s>>>(cost_incl.get(), nv, units,
                                                              unit_start.get());
     const uint32_t fix_ctas = std::max<uint32_t>(
-        1, std::min<uint32_t>(sms * 2, (g->n_long + kPprWarps - 1) / kPprWarps));
+        1, std::min<uint32_t>(sms * 2, (g->fw.n_long + kPprWarps - 1) / kPprWarps));
 
     // Per-call buffers.
     DeviceArray<float> y0(static_cast<size_t>(n) * kp), y1(static_cast<size_t>(n) * kp);
-    DeviceArray<float> chunk_val(static_cast<size_t>(std::max<uint32_t>(g->n_chunks, 1)) * kp);
+    DeviceArray<float> chunk_val(static_cast<size_t>(std::max<uint32_t>(g->fw.n_chunks, 1)) * kp);
     DeviceArray<uint32_t> d_seeds_orig(k), seed(kp);
     DeviceArray<int> active(kp), bad(1);
     DeviceArray<float> sink_coef(kp);
@@ -552,7 +552,7 @@ void run_ppr(nkg_graph *g, const nkg_pr_params &p, uint32_t k, const uint32_t *s
     a.row_ptr = g->row_ptr.get();
     a.col = g->col.get();
     a.degc = g->degc.get();
-    a.chunk_begin = g->chunk_begin.get();
+    a.chunk_begin = g->fw.chunk_begin.get();
     a.chunk_row = chunk_row.get();
     a.unit_start = unit_start.get();
     a.seed = seed.get();
@@ -568,8 +568,8 @@ void run_ppr(nkg_graph *g, const nkg_pr_params &p, uint32_t k, const uint32_t *s
     a.tol = p.tol;
     a.max_iterations = p.max_iterations;
     a.n = n;
-    a.n_long = g->n_long;
-    a.n_chunks = g->n_chunks;
+    a.n_long = g->fw.n_long;
+    a.n_chunks = g->fw.n_chunks;
     a.units = units;
     a.kp = kp;
     a.sweep_ctas = sweep_ctas;

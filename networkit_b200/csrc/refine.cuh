@@ -9,7 +9,15 @@
 // scalars stay on the device. The FP64 part is the reference's own Jacobi
 // step (the FP64 sweep), which gives the residual x' - x; while its norm is
 // above tol the residual is solved for a correction in FP32 again.
+//
+// The same kernels solve the adjoint system (I - d M^T) lam = gbar of the
+// differentiable form (OP = 1): the product then runs over the sliced
+// out-adjacency, M^T q = A^T q + [distributeSinks] m (t.q) with
+// (A^T q)[v] = sum_{v->u} w q[u] / wdeg[v]: the vector is gathered as it is
+// (no degree scaling) and every row is scaled after its sum.
 #pragma once
+
+#include <atomic>
 
 #include "sweep.cuh"
 
@@ -21,7 +29,7 @@ struct BiScalars {
     double vdot;      // (rhat, v)
     double ts, tt;    // (t, s), (t, t)
     double res;       // norm of the current residual r
-    double sink_vec;  // m . (vector entering the next product)
+    double sink_vec;  // m.q (OP 0) or tel.q (OP 1), q the next product's input
     int breakdown;
     unsigned int ticket;
 };
@@ -36,8 +44,10 @@ struct BiArgs {
     const uint32_t *__restrict__ degc;
     const float *__restrict__ degw;
     const float *__restrict__ tele;   // personalised teleport (n) or null
+    const uint32_t *__restrict__ row_label;  // OP 1: node of each out-adjacency row
     float *__restrict__ chunk_val;
-    // vectors (x-form, n entries; g is the gather form, n+1 with g[n] = 0)
+    // vectors (x-form, n entries; g is the gather form, n+1 with g[n] = 0;
+    // for OP 1, p and s have n+1 entries with p[n] = s[n] = 0 and g is unused)
     float *x, *r, *rhat, *p, *v, *s, *t, *g;
     double *__restrict__ part;        // per-CTA partial sums (3 per CTA)
     double *__restrict__ fix_part;
@@ -71,16 +81,24 @@ __device__ __forceinline__ bool bi_last_block(unsigned int *ticket, bool *s_flag
 
 constexpr int kBiThreads = 256;
 
-// out = in - d (A in + (m.in) tel): the product with (I - d M). `in` is given
-// in gather form g (in/deg, sinks in) and x-form px. MODE 0 accumulates
-// (rhat, out); MODE 1 accumulates (out, s) and (out, out).
-template <bool WEIGHTED, int MODE>
+// OP 0: out = in - d (A in + (m.in) tel), the product with (I - d M); `in`
+// is given in gather form g (in/deg, sinks in) and x-form px.
+// OP 1: out = in - d (A^T in + m (tel.in)), the product with (I - d M^T);
+// acc is the weighted sum of `in` over the out-arcs of node r.
+// MODE 0 accumulates (rhat, out); MODE 1 accumulates (out, s) and (out, out).
+template <bool WEIGHTED, int MODE, int OP>
 __device__ __forceinline__ void bi_mv_row(const BiArgs &a, uint32_t r, float acc, const float *px,
                                           float *out, double &d1, double &d2) {
     const float sv = static_cast<float>(a.sc->sink_vec);
     float q = acc;
-    if (a.distribute)
-        q = __fadd_rn(q, __fmul_rn(sv, bi_tel(a, r)));
+    if (OP == 0) {
+        if (a.distribute)
+            q = __fadd_rn(q, __fmul_rn(sv, bi_tel(a, r)));
+    } else {
+        uint32_t dc;
+        const float deg = bi_deg<WEIGHTED>(a, r, dc);
+        q = dc ? __fdiv_rn(acc, deg) : (a.distribute ? sv : 0.f);
+    }
     q = __fsub_rn(px[r], __fmul_rn(static_cast<float>(a.damp), q));
     out[r] = q;
     if (MODE == 0) {
@@ -92,13 +110,14 @@ __device__ __forceinline__ void bi_mv_row(const BiArgs &a, uint32_t r, float acc
 }
 
 // The SpMV of one slice per warp (the loop of sweep_kernel in FP32).
-template <bool WEIGHTED, int MODE, int THREADS, int UNROLL>
+template <bool WEIGHTED, int MODE, int OP, int THREADS, int UNROLL>
 __global__ void __launch_bounds__(THREADS) bi_mv(BiArgs a) {
     __shared__ double s_red[32];
     if (a.sc->breakdown)
         return;
     const float *px = MODE == 0 ? a.p : a.s;
     float *out = MODE == 0 ? a.v : a.t;
+    const float *gsrc = OP == 0 ? a.g : px;
     const int lane = threadIdx.x & 31;
     const uint32_t wpc = THREADS / 32;
     const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);
@@ -121,7 +140,7 @@ __global__ void __launch_bounds__(THREADS) bi_mv(BiArgs a) {
                 float vv[UNROLL];
 #pragma unroll
                 for (int k = 0; k < UNROLL; ++k)
-                    vv[k] = __ldg(a.g + c[k]);
+                    vv[k] = __ldg(gsrc + c[k]);
                 if (WEIGHTED) {
 #pragma unroll
                     for (int k = 0; k < UNROLL; ++k)
@@ -132,7 +151,7 @@ __global__ void __launch_bounds__(THREADS) bi_mv(BiArgs a) {
                     acc += vv[k];
             }
             for (; j < len; ++j) {
-                float vv = __ldg(a.g + ld_stream(cp + static_cast<size_t>(j) * 32));
+                float vv = __ldg(gsrc + ld_stream(cp + static_cast<size_t>(j) * 32));
                 if (WEIGHTED)
                     vv = __fmul_rn(vv, ld_stream(a.w_sell + base + static_cast<size_t>(j) * 32));
                 acc += vv;
@@ -142,7 +161,8 @@ __global__ void __launch_bounds__(THREADS) bi_mv(BiArgs a) {
             } else {
                 const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
                 if (r < a.n)
-                    bi_mv_row<WEIGHTED, MODE>(a, r, acc, px, out, d1, d2);
+                    bi_mv_row<WEIGHTED, MODE, OP>(a, OP ? a.row_label[r] : r, acc, px, out, d1,
+                                                  d2);
             }
         }
     }
@@ -156,7 +176,7 @@ __global__ void __launch_bounds__(THREADS) bi_mv(BiArgs a) {
 
 // Split rows of the product, then (last CTA) the scalar that follows it:
 // MODE 0: alpha = rho / (rhat, v); MODE 1: omega = (t, s) / (t, t).
-template <bool WEIGHTED, int MODE>
+template <bool WEIGHTED, int MODE, int OP>
 __global__ void __launch_bounds__(kBiThreads) bi_mv_fix(BiArgs a) {
     __shared__ double s_red[32];
     __shared__ bool s_last;
@@ -170,7 +190,7 @@ __global__ void __launch_bounds__(kBiThreads) bi_mv_fix(BiArgs a) {
         float acc = 0.f;
         for (uint32_t k = a.chunk_begin[r]; k < a.chunk_begin[r + 1]; ++k)
             acc += a.chunk_val[k];
-        bi_mv_row<WEIGHTED, MODE>(a, r, acc, px, out, d1, d2);
+        bi_mv_row<WEIGHTED, MODE, OP>(a, OP ? a.row_label[r] : r, acc, px, out, d1, d2);
     }
     d1 = block_sum<kBiThreads>(d1, s_red);
     d2 = block_sum<kBiThreads>(d2, s_red);
@@ -210,9 +230,31 @@ __global__ void __launch_bounds__(kBiThreads) bi_mv_fix(BiArgs a) {
     }
 }
 
+// Contribution of entry i with value vv to sink_vec: m.vec (OP 0, which also
+// writes the gather form g) or tel.vec (OP 1; a uniform 1/n is applied once
+// to the total).
+template <bool WEIGHTED, int OP>
+__device__ __forceinline__ void bi_vec_entry(const BiArgs &a, uint32_t i, float vv, double &sk) {
+    if (OP == 0) {
+        uint32_t dc;
+        const float d = bi_deg<WEIGHTED>(a, i, dc);
+        a.g[i] = dc ? vv / d : vv;
+        if (!dc)
+            sk += vv;
+    } else {
+        sk += a.personal ? static_cast<double>(a.tele[i]) * static_cast<double>(vv)
+                         : static_cast<double>(vv);
+    }
+}
+
+template <int OP>
+__device__ __forceinline__ double bi_sink_total(const BiArgs &a, double t) {
+    return OP == 1 && !a.personal ? t * a.inv_n : t;
+}
+
 // Vector step 1: p = r + beta (p - omega v), beta = (rho/rho_prev)(alpha/omega);
-// g = p in gather form; sink_vec = m.p.
-template <bool WEIGHTED>
+// g = p in gather form; sink_vec = m.p (OP 0) or tel.p (OP 1).
+template <bool WEIGHTED, int OP>
 __global__ void __launch_bounds__(kBiThreads) bi_vec_p(BiArgs a) {
     __shared__ double s_red[32];
     __shared__ bool s_last;
@@ -225,11 +267,7 @@ __global__ void __launch_bounds__(kBiThreads) bi_vec_p(BiArgs a) {
     for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < a.n; i += gridDim.x * kBiThreads) {
         const float pv = __fadd_rn(a.r[i], __fmul_rn(b, __fsub_rn(a.p[i], __fmul_rn(om, a.v[i]))));
         a.p[i] = pv;
-        uint32_t dc;
-        const float d = bi_deg<WEIGHTED>(a, i, dc);
-        a.g[i] = dc ? pv / d : pv;
-        if (!dc)
-            sk += pv;
+        bi_vec_entry<WEIGHTED, OP>(a, i, pv, sk);
     }
     sk = block_sum<kBiThreads>(sk, s_red);
     if (threadIdx.x == 0)
@@ -241,14 +279,15 @@ __global__ void __launch_bounds__(kBiThreads) bi_vec_p(BiArgs a) {
         t += ((volatile double *)a.part)[i];
     t = block_sum<kBiThreads>(t, s_red);
     if (threadIdx.x == 0) {
-        sc->sink_vec = t;
+        sc->sink_vec = bi_sink_total<OP>(a, t);
         sc->rho_prev = sc->rho;
         sc->ticket = 0;
     }
 }
 
-// Vector step 2: s = r - alpha v; g = s in gather form; sink_vec = m.s.
-template <bool WEIGHTED>
+// Vector step 2: s = r - alpha v; g = s in gather form; sink_vec = m.s (OP 0)
+// or tel.s (OP 1).
+template <bool WEIGHTED, int OP>
 __global__ void __launch_bounds__(kBiThreads) bi_vec_s(BiArgs a) {
     __shared__ double s_red[32];
     __shared__ bool s_last;
@@ -260,11 +299,7 @@ __global__ void __launch_bounds__(kBiThreads) bi_vec_s(BiArgs a) {
     for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < a.n; i += gridDim.x * kBiThreads) {
         const float sv = __fsub_rn(a.r[i], __fmul_rn(al, a.v[i]));
         a.s[i] = sv;
-        uint32_t dc;
-        const float d = bi_deg<WEIGHTED>(a, i, dc);
-        a.g[i] = dc ? sv / d : sv;
-        if (!dc)
-            sk += sv;
+        bi_vec_entry<WEIGHTED, OP>(a, i, sv, sk);
     }
     sk = block_sum<kBiThreads>(sk, s_red);
     if (threadIdx.x == 0)
@@ -276,13 +311,13 @@ __global__ void __launch_bounds__(kBiThreads) bi_vec_s(BiArgs a) {
         t += ((volatile double *)a.part)[i];
     t = block_sum<kBiThreads>(t, s_red);
     if (threadIdx.x == 0) {
-        sc->sink_vec = t;
+        sc->sink_vec = bi_sink_total<OP>(a, t);
         sc->ticket = 0;
     }
 }
 
 // Vector step 3: x += alpha p + omega s; r = s - omega t; res = |r|; rho = (rhat, r).
-__global__ void __launch_bounds__(kBiThreads) bi_vec_x(BiArgs a) {
+static __global__ void __launch_bounds__(kBiThreads) bi_vec_x(BiArgs a) {
     __shared__ double s_red[32];
     __shared__ bool s_last;
     BiScalars *sc = a.sc;
@@ -324,7 +359,7 @@ __global__ void __launch_bounds__(kBiThreads) bi_vec_x(BiArgs a) {
 
 // Start of a solve from x = 0: r = rhat = b (x-form, given in r), p = v = 0;
 // rho = (b, b), res = |b|; rho_prev = alpha = omega = 1.
-__global__ void __launch_bounds__(kBiThreads) bi_start(BiArgs a) {
+static __global__ void __launch_bounds__(kBiThreads) bi_start(BiArgs a) {
     __shared__ double s_red[32];
     __shared__ bool s_last;
     BiScalars *sc = a.sc;
@@ -339,7 +374,7 @@ __global__ void __launch_bounds__(kBiThreads) bi_start(BiArgs a) {
         nr += a.l2 ? d * d : fabs(d);
         rr += d * d;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0)
+    if (a.g && blockIdx.x == 0 && threadIdx.x == 0)
         a.g[a.n] = 0.f;
     nr = block_sum<kBiThreads>(nr, s_red);
     rr = block_sum<kBiThreads>(rr, s_red);
@@ -368,7 +403,7 @@ __global__ void __launch_bounds__(kBiThreads) bi_start(BiArgs a) {
 }
 
 // Right-hand side of the first solve: b = (1-d) t.
-__global__ void bi_rhs_teleport(BiArgs a) {
+static __global__ void bi_rhs_teleport(BiArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < a.n)
         a.r[i] = static_cast<float>(1.0 - a.damp) * bi_tel(a, i);
@@ -422,6 +457,58 @@ __global__ void bi_residual_rhs(const double *__restrict__ y64_new, const double
     const double d = WEIGHTED ? degw[i] : static_cast<double>(dc);
     const double xn = dc ? __dmul_rn(y64_new[i], d) : y64_new[i];
     r32[i] = static_cast<float>(xn - x64[i]);
+}
+
+// ---------------------------------------------------------------------------
+// Host driver of one BiCGSTAB solve
+
+struct BiLaunch {
+    cudaStream_t stream = nullptr;
+    int sweep_shape = 0;
+    unsigned sweep_ctas = 0, vec_ctas = 0, fix_ctas = 0;
+    BiScalars *d_sc = nullptr;    // device scalars
+    BiScalars *h_sc = nullptr;    // pinned host copy
+    std::atomic<int> *cancel = nullptr;
+    uint64_t launches = 0, matvecs = 0;
+};
+
+// Solve (I - d M) x = r (OP 0) or (I - d M^T) x = r (OP 1) from x = 0, with
+// the right-hand side in a.r, until |r| <= max(rel * |r0|, floor). Four
+// BiCGSTAB steps (28 launches) go out between status read-backs.
+template <bool WEIGHTED, int OP>
+void bi_solve(const BiArgs &a, BiLaunch &L, double rel, double floor) {
+    cudaStream_t s = L.stream;
+    bi_start<<<L.vec_ctas, kBiThreads, 0, s>>>(a);
+    NKG_CUDA(cudaMemcpyAsync(L.h_sc, L.d_sc, sizeof(BiScalars), cudaMemcpyDeviceToHost, s));
+    NKG_CUDA(cudaStreamSynchronize(s));
+    const double inner_tol = L.h_sc->res * rel > floor ? L.h_sc->res * rel : floor;
+    L.launches += 1;
+    for (int it = 0; it < 400 && !L.h_sc->breakdown && L.h_sc->res > inner_tol; it += 4) {
+        for (int k = 0; k < 4; ++k) {
+            bi_vec_p<WEIGHTED, OP><<<L.vec_ctas, kBiThreads, 0, s>>>(a);
+            with_sweep_shape(L.sweep_shape, [&](auto S) {
+                using Sh = decltype(S);
+                bi_mv<WEIGHTED, 0, OP, Sh::threads, Sh::unroll><<<L.sweep_ctas, Sh::threads, 0, s>>>(a);
+            });
+            bi_mv_fix<WEIGHTED, 0, OP><<<L.fix_ctas, kBiThreads, 0, s>>>(a);
+            bi_vec_s<WEIGHTED, OP><<<L.vec_ctas, kBiThreads, 0, s>>>(a);
+            with_sweep_shape(L.sweep_shape, [&](auto S) {
+                using Sh = decltype(S);
+                bi_mv<WEIGHTED, 1, OP, Sh::threads, Sh::unroll><<<L.sweep_ctas, Sh::threads, 0, s>>>(a);
+            });
+            bi_mv_fix<WEIGHTED, 1, OP><<<L.fix_ctas, kBiThreads, 0, s>>>(a);
+            bi_vec_x<<<L.vec_ctas, kBiThreads, 0, s>>>(a);
+        }
+        NKG_CUDA(cudaGetLastError());
+        L.launches += 28;
+        L.matvecs += 8;
+        NKG_CUDA(cudaMemcpyAsync(L.h_sc, L.d_sc, sizeof(BiScalars), cudaMemcpyDeviceToHost, s));
+        NKG_CUDA(cudaStreamSynchronize(s));
+        if (L.cancel && L.cancel->load()) {
+            L.cancel->store(0);
+            throw Error(NKG_ERR_CANCELLED, "PageRank run cancelled");
+        }
+    }
 }
 
 } // namespace nkg
