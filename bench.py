@@ -59,8 +59,12 @@ def parse_args():
                     help="sweep launch shape (nkg_graph_options.sweep_shape; -1 default)")
     ap.add_argument("--arc-order", type=int, default=0, choices=[0, 1],
                     help="nkg_graph_options.arc_order (0 keep the reference order, 1 sorted)")
-    ap.add_argument("--form", default="", choices=["", "ppr", "refine"],
+    ap.add_argument("--form", default="", choices=["", "ppr", "refine", "adjoint"],
                     help="run only one companion form and print its figures")
+    ap.add_argument("--fd-edges", type=int, default=64,
+                    help="arcs checked by finite differences in --form adjoint")
+    ap.add_argument("--adjoint-step-only", action="store_true",
+                    help="--form adjoint: only the reference solves and one timed breakdown")
     ap.add_argument("--cache", default=os.path.join(tempfile.gettempdir(), "nk_b200_graphs"))
     return ap.parse_args()
 
@@ -260,6 +264,126 @@ def form_refine(local, csr, steps=2):
     return res
 
 
+def form_adjoint(local, scale=22, steps=3, fd_edges=64, only_step=False):
+    """Differentiable weighted PageRank: directed R-MAT scale 22, edgefactor
+    16, weights uniform in (0.1, 1] (seed 43), loss L = sum_v g_v p_v with
+    g ~ N(0, 1) (seed 42), damp 0.85, reference sink semantics. One step is
+    forward + backward through networkit_b200.autograd (weights copied in,
+    scores out, dL/dw and dL/dt out, all on the device), timed with CUDA
+    events around the whole call; against it the plain FP64 forward alone.
+    Errors are against the GPU FP64 forward to tol 1e-14 and FP64 adjoint to
+    1e-13 (both parity-tested against the oracle); the FP64 gradient is also
+    checked by central differences (h = 1e-4) of the FP64 forward on
+    `fd_edges` random arcs. only_step: the reference solves and the
+    time breakdown only (a short launch sequence for profiling)."""
+    import torch
+
+    from networkit_b200 import _capi, autograd, generators
+
+    dev = torch.device("cuda", local)
+    csr = generators.with_uniform_weights(generators.rmat_directed(scale, EDGEFACTOR, *RMAT,
+                                                                   seed=SEED), seed=43)
+    g_np = np.random.default_rng(42).standard_normal(csr.z)
+    G = autograd.DifferentiableGraph(csr, device=local)
+    dg = G.graph
+    w = torch.from_numpy(csr.in_w).to(dev)
+    g = torch.from_numpy(g_np).to(dev)
+    out = torch.empty(csr.z, dtype=torch.float64, device=dev)
+    gw_ref = torch.empty(csr.arcs, dtype=torch.float64, device=dev)
+    gt_ref = torch.empty(csr.z, dtype=torch.float64, device=dev)
+    dg.set_weights_device(w.data_ptr())
+    dg.run_ex(dg.params(DAMP, 1e-14, NORM_L1, False, False, _capi.NKG_PREC_FP64, 3000), 0,
+              out.data_ptr(), True)
+    p_ref = out.clone()
+    torch.cuda.synchronize()
+    dg.adjoint_device(dg.params(DAMP, 1e-13, NORM_L1, False, False, _capi.NKG_PREC_FP64, 5000),
+                      p_ref.data_ptr(), g.data_ptr(), gw_ref.data_ptr(), gt_ref.data_ptr())
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn):
+        fn()  # warm-up
+        ms = []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            ev[0].record()
+            r = fn()
+            ev[1].record()
+            torch.cuda.synchronize()
+            ms.append(ev[0].elapsed_time(ev[1]))
+        return statistics.median(ms), r
+
+    def plain(tol):
+        p = dg.params(DAMP, tol, NORM_L1, False, False, _capi.NKG_PREC_FP64, _capi.UINT64_MAX)
+        return lambda: (dg.run_ex(p, 0, out.data_ptr(), True), out.clone())[1]
+
+    def fwd_bwd(prec, tol, btol):
+        def f():
+            wp = w.clone().requires_grad_(True)
+            s = autograd.pagerank(G, wp, None, DAMP, tol, False, prec, prec, btol)
+            (s * g).sum().backward()
+            return s.detach(), wp.grad
+        return f
+
+    res = {"workload": f"adjoint_rmat{scale}_weighted", "n": csr.z, "arcs": csr.arcs}
+    # Where a forward + backward step spends its time (library device timers).
+    gw_b = torch.empty(csr.arcs, dtype=torch.float64, device=dev)
+    bd = {}
+    for _ in range(2):
+        torch.cuda.synchronize()
+        ev[0].record()
+        dg.set_weights_device(w.data_ptr())
+        ev[1].record()
+        torch.cuda.synchronize()
+        bd["set_weights_ms"] = ev[0].elapsed_time(ev[1])
+        pr = dg.params(DAMP, 1e-10, NORM_L1, False, False, _capi.NKG_PREC_FP32_REFINE,
+                       _capi.UINT64_MAX)
+        _, _, st = dg.run_ex(pr, 0, out.data_ptr(), True)
+        bd["fwd"] = {k: st[k] for k in ("ms_total", "fp32_sweeps", "fp64_sweeps",
+                                          "kernel_launches")}
+        _, st = dg.adjoint_device(pr, out.data_ptr(), g.data_ptr(), gw_b.data_ptr(), 0)
+        bd["bwd"] = {k: st[k] for k in ("ms_total", "fp32_sweeps", "fp64_sweeps",
+                                          "kernel_launches")}
+    res["breakdown_fp32_refine_tol1e-10"] = bd
+    if only_step:
+        G.graph.close()
+        return res
+    gwn = float(gw_ref.abs().max())
+    for tol, btol in ((1e-10, 1e-10), (1.5e-7, 1e-6)):
+        ms_p, s_p = timed(plain(tol))
+        row = {"plain_fp64_fwd_ms": ms_p, "plain_l1_err": float((s_p - p_ref).abs().sum())}
+        for prec in ("fp32_refine", "fp64"):
+            ms, (s, gw) = timed(fwd_bwd(prec, tol, btol))
+            row[f"{prec}_fwd_bwd_ms"] = ms
+            row[f"{prec}_l1_err"] = float((s - p_ref).abs().sum())
+            row[f"{prec}_max_rel_err"] = float(((s - p_ref).abs() / p_ref.abs()).max())
+            row[f"{prec}_grad_w_err"] = float((gw - gw_ref).abs().max()) / gwn
+        row["fwd_bwd_vs_plain_fwd"] = ms_p / row["fp32_refine_fwd_bwd_ms"]
+        res[f"tol{tol:g}"] = row
+    if fd_edges:
+        fwd = dg.params(DAMP, 0.0, NORM_L1, False, False, _capi.NKG_PREC_FP64, 400)
+        rng = np.random.default_rng(7)
+        edges = rng.choice(csr.arcs, fd_edges, replace=False)
+        h = 1e-4
+        fds = []
+        for e in edges:
+            vals = []
+            for sgn in (1.0, -1.0):
+                w2 = w.clone()
+                w2[int(e)] += sgn * h
+                torch.cuda.synchronize()
+                dg.set_weights_device(w2.data_ptr())
+                dg.run_ex(fwd, 0, out.data_ptr(), True)
+                vals.append(float((out * g).sum()))
+            fds.append((vals[0] - vals[1]) / (2 * h))
+        gsel = gw_ref[torch.from_numpy(edges).to(dev)].cpu().numpy()
+        res["fd_check"] = {"edges": fd_edges, "h": h,
+                           "max_abs_err_over_max_grad": float(np.abs(np.array(fds) - gsel).max()
+                                                              / np.abs(gsel).max())}
+        dg.set_weights_device(w.data_ptr())
+    G.graph.close()
+    return res
+
+
 def run_reference_arm(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -318,6 +442,10 @@ def main():
     torch.cuda.set_device(local)
     if args.form == "ppr":
         print(json.dumps(form_ppr(local)))
+        return
+    if args.form == "adjoint":
+        print(json.dumps(form_adjoint(local, fd_edges=args.fd_edges,
+                                      only_step=args.adjoint_step_only)))
         return
     if world > 1:
         import datetime

@@ -33,13 +33,19 @@ class DifferentiableGraph:
         self.device = torch.device("cuda", device)
         self.z = int(csr.z)
         self.arcs = int(csr.in_col.shape[0])
+        self.loaded_by = None  # the forward call whose weights the graph holds
 
-    def load_weights(self, w: torch.Tensor) -> None:
-        """Copy `w` into the graph (every call: a tensor can change in place
-        without a new version, e.g. through .data)."""
+    def load_weights(self, w: torch.Tensor, token) -> None:
+        """Copy `w` into the graph for the forward call `token`. Every forward
+        copies (a tensor can change in place without a new version, e.g.
+        through .data); a backward copies only if another forward ran since
+        its own (autograd itself rejects in-place changes of saved weights)."""
+        if token is not None and self.loaded_by is token:
+            return
         _check_tensor(w, self.arcs, self.device, "weights")
         torch.cuda.current_stream(self.device).synchronize()
         self.graph.set_weights_device(w.data_ptr())
+        self.loaded_by = token
 
 
 def _check_tensor(t, size, device, name):
@@ -58,7 +64,10 @@ def _params(damp, tol, distribute, precision, max_iterations):
 class _PageRankFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, weights, teleport, graph, fwd, bwd):
-        graph.load_weights(weights)
+        token = object()
+        graph.load_weights(weights, None)
+        graph.loaded_by = token
+        ctx.token = token
         if teleport is not None:
             _check_tensor(teleport, graph.z, graph.device, "teleport")
         out = torch.empty(graph.z, dtype=torch.float64, device=graph.device)
@@ -76,7 +85,7 @@ class _PageRankFn(torch.autograd.Function):
     def backward(ctx, grad_out):
         weights, teleport, scores = ctx.saved_tensors
         graph = ctx.graph
-        graph.load_weights(weights)
+        graph.load_weights(weights, ctx.token)
         g = grad_out.contiguous().to(torch.float64)
         want_w = ctx.needs_input_grad[0]
         want_t = ctx.needs_input_grad[1]

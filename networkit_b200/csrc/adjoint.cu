@@ -1,10 +1,11 @@
-// Differentiable PageRank: the adjoint (backward) solve and the gradients
-// with respect to the arc weights and the teleport vector. No reference
-// counterpart; the forward it differentiates is PageRank.cpp:20-104 with a
-// weighted graph (optionally distributeSinks and a personalised teleport).
+// Differentiable PageRank: the adjoint (backward) solve, the gradients with
+// respect to the arc weights and the teleport vector, and in-place weight
+// updates. No reference counterpart; the forward it differentiates is
+// PageRank.cpp:20-104 on a weighted graph (optionally distributeSinks and a
+// personalised teleport).
 //
-// Forward fixed point, in the relabelled order, with t the teleport
-// distribution (1/n without one), m the sink mask and A[u,v] = w(v->u)/wdeg[v]:
+// Forward fixed point, with t the teleport distribution (1/n without one), m
+// the sink mask and A[u,v] = w(v->u)/wdeg[v]:
 //     x = d (A x + [distributeSinks] (m.x) t) + (1-d) t,    p = x / sum(x).
 // For a loss L with g = dL/dp, with gbar = g - (g.p) 1, the adjoint lam solves
 //     (I - d M^T) lam = gbar,   M^T q = A^T q + [distributeSinks] m (t.q),
@@ -14,19 +15,23 @@
 // where sum(x) follows from p alone at the fixed point (summing the forward
 // equation over all nodes, tau = sum(t)):
 //     sum(x) = (1-d) tau / (1 - d + d (m.p) (1 - [distributeSinks] tau)).
-// (The lam here is sum(x) times the lam of the un-normalised system, which is
-// why neither gradient needs sum(x) beyond that one factor.)
+// (This lam is sum(x) times the lam of the un-normalised system, which is why
+// neither gradient needs sum(x) beyond that one factor.)
 //
 // A^T is a pull over the out-adjacency, so the graph gets a second sliced
-// layout: the out-CSR of the relabelled graph, its rows (nodes) sorted by
-// out-degree, descending, each row listing its out-arcs in the order they
-// appear in the in-CSR. The FP32 solve is the BiCGSTAB of refine.cuh with
-// OP = 1; the FP64 Jacobi sweep of the adjoint system below gives the
-// residual of the refinement, the FP64 solve and the final c.
+// layout: the out-CSR, its rows ("out-rows") the nodes sorted by out-degree,
+// descending, each listing its out-arcs in the order they appear in the
+// in-CSR, its column ids out-row numbers. Every vector of the adjoint solve
+// is indexed by out-row, so rows are written in place and only the gathers
+// are scattered. The FP32 solve is the BiCGSTAB of refine.cuh with OP = 1;
+// the FP64 Jacobi sweep below gives the refinement's residual, the FP64 solve
+// and the final c. dL/dw is then one pass over the in-adjacency's sliced
+// layout, written straight into the caller's arc order.
 #include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 
 #include "graph.hpp"
@@ -35,22 +40,42 @@
 
 namespace nkg {
 
+// Work buffers of one backward pass, kept between calls (sized for n).
+struct AdjWork {
+    DeviceArray<double> p, g, t, gbar, c, part, fix_part, chunk64, lam_f, lam[2];
+    DeviceArray<double2> qc;
+    DeviceArray<float> t32, chunk32, x, r, rhat, pv, v, sv, tv;
+    DeviceArray<unsigned char> scal;  // AdjScalars, BiScalars, AdjState
+    bool ready = false;
+};
+
 struct AdjointState {
-    SellLayout tl;                  // out-adjacency, rows in out-degree order
-    DeviceArray<uint32_t> trow;     // n: node of out-row rt
-    DeviceArray<uint32_t> tptr;     // n+1: out-CSR offsets (out-row order)
-    DeviceArray<uint32_t> tarc;     // arcs: in-CSR index of every out-CSR entry
+    SellLayout tl;                  // out-adjacency, rows = out-rows
+    DeviceArray<uint32_t> trow;     // n: relabelled id of out-row rt
+    DeviceArray<uint32_t> tinv;     // n: out-row of relabelled id v
+    DeviceArray<uint32_t> tperm;    // n: caller id of out-row rt
+    DeviceArray<uint32_t> tdegc;    // n: out-degree of out-row rt
+    DeviceArray<uint32_t> tptr;     // n+1: out-CSR offsets
+    DeviceArray<uint32_t> tarc;     // arcs: in-CSR entry of every out-CSR entry
+    DeviceArray<double> tdegw64;    // n: weighted out-degree (weighted graphs)
+    DeviceArray<float> tdegw32;     // n
     DeviceArray<float> w_sell32;    // slots (weighted graphs)
-    DeviceArray<float> degw32;      // n (weighted graphs)
     DeviceArray<uint32_t> units32, units64;
     uint32_t n_units32 = 0, n_units64 = 0;
     unsigned ctas32 = 0, ctas64 = 0;
     int shape = -1;
+    // Weight updates: caller arc index of every slot (kNone for padding) of
+    // the in-layout and of the out-layout; chunk partial sums of out-degrees.
+    DeviceArray<uint32_t> fw_map, t_map;
+    DeviceArray<double> tchunk;
+    AdjWork work;
 };
 
 void destroy_adjoint(AdjointState *a) { delete a; }
 
 namespace {
+
+constexpr int kAdjThreads = 256;
 
 // ---------------------------------------------------------------------------
 // Layout build kernels
@@ -64,19 +89,23 @@ __global__ void adj_outdeg_keys(const uint32_t *__restrict__ degc, uint32_t n,
     }
 }
 
-__global__ void adj_row_lengths(const uint32_t *__restrict__ trow, const uint32_t *__restrict__ degc,
-                                uint32_t n, uint32_t *__restrict__ tlen,
-                                uint32_t *__restrict__ tinv) {
+__global__ void adj_row_info(const uint32_t *__restrict__ trow, const uint32_t *__restrict__ degc,
+                             const uint32_t *__restrict__ perm, const double *__restrict__ degw,
+                             uint32_t n, uint32_t *__restrict__ tdegc, uint32_t *__restrict__ tinv,
+                             uint32_t *__restrict__ tperm, double *__restrict__ tdegw) {
     const uint32_t rt = blockIdx.x * blockDim.x + threadIdx.x;
     if (rt < n) {
         const uint32_t v = trow[rt];
-        tlen[rt] = degc[v];
+        tdegc[rt] = degc[v];
         tinv[v] = rt;
+        tperm[rt] = perm[v];
+        if (tdegw)
+            tdegw[rt] = degw[v];
     }
 }
 
-// Per in-arc e (row u, source v): sort key = out-row of v, value = e; and the
-// row of every arc. One warp per in-row.
+// Per in-arc k (row u, source v): sort key = out-row of v, value = k; and the
+// out-row of its target u. One warp per in-row.
 __global__ void adj_arc_keys(const uint32_t *__restrict__ row_ptr, const uint32_t *__restrict__ col,
                              const uint32_t *__restrict__ tinv, uint32_t n,
                              uint32_t *__restrict__ key, uint32_t *__restrict__ val,
@@ -86,43 +115,130 @@ __global__ void adj_arc_keys(const uint32_t *__restrict__ row_ptr, const uint32_
     const int lane = threadIdx.x & 31;
     for (uint64_t u = warp; u < n; u += nwarps) {
         const uint32_t b = row_ptr[u], e = row_ptr[u + 1];
+        const uint32_t ut = tinv[u];
         for (uint32_t k = b + lane; k < e; k += 32) {
             key[k] = tinv[col[k]];
             val[k] = k;
-            arc_row[k] = static_cast<uint32_t>(u);
+            arc_row[k] = ut;
         }
     }
 }
 
-__global__ void adj_gather_cols(const uint32_t *__restrict__ tarc,
-                                const uint32_t *__restrict__ arc_row, uint64_t arcs,
-                                uint32_t *__restrict__ tcol) {
+// out[k] = src[idx[k]]
+__global__ void adj_gather_u32(const uint32_t *__restrict__ idx, const uint32_t *__restrict__ src,
+                               uint64_t m, uint32_t *__restrict__ out) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < arcs;
+    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < m;
          k += stride)
-        tcol[k] = arc_row[tarc[k]];
+        out[k] = src[idx[k]];
 }
 
-// Weighted out-degree: one warp per out-row, lane-strided partial sums
-// combined by a fixed shuffle tree (deterministic).
-__global__ void adj_out_wdeg(const uint32_t *__restrict__ tptr, const uint32_t *__restrict__ tarc,
-                             const uint32_t *__restrict__ trow, const double *__restrict__ w,
-                             uint32_t n, double *__restrict__ degw) {
+// Caller arc index of every in-CSR entry (row r starts at row_src[r] there).
+__global__ void adj_caller_index(const uint32_t *__restrict__ row_ptr,
+                                 const uint64_t *__restrict__ row_src, uint32_t n,
+                                 uint32_t *__restrict__ out) {
     const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
     const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
-    for (uint64_t rt = warp; rt < n; rt += nwarps) {
-        double s = 0.0;
-        for (uint32_t k = tptr[rt] + lane; k < tptr[rt + 1]; k += 32)
-            s += w[tarc[k]];
-        s = warp_sum(s);
-        if (lane == 0)
-            degw[trow[rt]] = s;
+    for (uint64_t r = warp; r < n; r += nwarps) {
+        const uint32_t b = row_ptr[r], e = row_ptr[r + 1];
+        const uint64_t src = row_src[r];
+        for (uint32_t k = b + lane; k < e; k += 32)
+            out[k] = static_cast<uint32_t>(src + (k - b));
     }
 }
 
 // ---------------------------------------------------------------------------
-// FP64 Jacobi sweep of the adjoint system
+// Weight updates
+
+// w64[slot] = w[map[slot]] (0 for padding), and its FP32 copy.
+__global__ void adj_refresh_slots(const uint32_t *__restrict__ map, uint64_t slots,
+                                  const double *__restrict__ w, double *__restrict__ w64,
+                                  float *__restrict__ w32) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < slots;
+         k += stride) {
+        const uint32_t m = map[k];
+        const double v = m != kNone ? w[m] : 0.0;
+        w64[k] = v;
+        if (w32)
+            w32[k] = static_cast<float>(v);
+    }
+}
+
+struct DegreeOut {
+    const uint32_t *trow;
+    double *tdegw64;
+    float *tdegw32;
+    double *degw64;  // relabelled order (the forward's)
+    float *degw32;   // relabelled order, FP32 plane (or null)
+};
+
+__device__ __forceinline__ void put_degree(const DegreeOut &o, uint32_t rt, double d) {
+    o.tdegw64[rt] = d;
+    o.tdegw32[rt] = static_cast<float>(d);
+    const uint32_t v = o.trow[rt];
+    o.degw64[v] = d;
+    if (o.degw32)
+        o.degw32[v] = static_cast<float>(d);
+}
+
+// Weighted out-degrees from the out-layout's slot weights: every lane sums its
+// virtual row in slot order (padding weighs 0); split rows keep chunk sums.
+__global__ void adj_degree_sums(const uint32_t *__restrict__ slice_off,
+                                const double *__restrict__ w64, uint32_t slices, uint32_t s_chunk,
+                                uint32_t n_long, uint32_t n, double *__restrict__ tchunk,
+                                DegreeOut o) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t s = warp; s < slices; s += nwarps) {
+        const uint32_t off = slice_off[s], len = slice_off[s + 1] - off;
+        const double *wp = w64 + static_cast<size_t>(off) * 32 + lane;
+        double sum = 0.0;
+        uint32_t j = 0;
+        for (; j + 8 <= len; j += 8) {
+            double v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                v[k] = wp[static_cast<size_t>(j + k) * 32];
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                sum += v[k];
+        }
+        for (; j < len; ++j)
+            sum += wp[static_cast<size_t>(j) * 32];
+        if (s < s_chunk) {
+            tchunk[static_cast<size_t>(s) * 32 + lane] = sum;
+        } else {
+            const uint32_t r = n_long + (s - s_chunk) * 32 + lane;
+            if (r < n)
+                put_degree(o, r, sum);
+        }
+    }
+}
+
+__global__ void adj_degree_fix(const uint32_t *__restrict__ chunk_begin, uint32_t n_long,
+                               const double *__restrict__ tchunk, DegreeOut o) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_long)
+        return;
+    double sum = 0.0;
+    for (uint32_t k = chunk_begin[r]; k < chunk_begin[r + 1]; ++k)
+        sum += tchunk[k];
+    put_degree(o, r, sum);
+}
+
+// Weighted out-degrees given by the caller (caller ids).
+__global__ void adj_degree_given(const double *__restrict__ wdeg, const uint32_t *__restrict__ tperm,
+                                 uint32_t n, DegreeOut o) {
+    const uint32_t rt = blockIdx.x * blockDim.x + threadIdx.x;
+    if (rt < n)
+        put_degree(o, rt, wdeg[tperm[rt]]);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 Jacobi sweep of the adjoint system (out-row order)
 
 struct AdjState {
     double tdot;               // tel.lam_in (uniform teleport: times 1/n)
@@ -138,10 +254,9 @@ struct AdjArgs {
     const uint32_t *__restrict__ slice_off;
     const uint32_t *__restrict__ unit_start;
     const uint32_t *__restrict__ chunk_begin;
-    const uint32_t *__restrict__ row_label;
     const uint32_t *__restrict__ degc;
     const double *__restrict__ degw;
-    const double *__restrict__ tele;      // relabelled teleport or null
+    const double *__restrict__ tele;      // teleport or null
     const double *__restrict__ gbar;
     const double *__restrict__ lam_in;    // n+1, lam_in[n] = 0
     double *__restrict__ lam_out;         // n+1 or null (c only)
@@ -221,7 +336,7 @@ __global__ void __launch_bounds__(THREADS) adj_sweep(AdjArgs a) {
             } else {
                 const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
                 if (r < a.n)
-                    adj_row<WEIGHTED>(a, a.row_label[r], acc, tdot, res, td);
+                    adj_row<WEIGHTED>(a, r, acc, tdot, res, td);
             }
         }
     }
@@ -232,8 +347,6 @@ __global__ void __launch_bounds__(THREADS) adj_sweep(AdjArgs a) {
         a.part[2 * blockIdx.x + 1] = td;
     }
 }
-
-constexpr int kAdjThreads = 256;
 
 // Split out-rows (one thread each, chunks in order), then the last CTA
 // closes the sweep: residual, tel.lam_out for the next sweep, stopping test.
@@ -250,7 +363,7 @@ __global__ void __launch_bounds__(kAdjThreads) adj_fix(AdjArgs a) {
         double acc = 0.0;
         for (uint32_t k = a.chunk_begin[r]; k < a.chunk_begin[r + 1]; ++k)
             acc += a.chunk_val[k];
-        adj_row<WEIGHTED>(a, a.row_label[r], acc, tdot, res, td);
+        adj_row<WEIGHTED>(a, r, acc, tdot, res, td);
     }
     res = block_sum<kAdjThreads>(res, s_red);
     td = block_sum<kAdjThreads>(td, s_red);
@@ -299,27 +412,28 @@ struct AdjScalars {
     unsigned int ticket;
 };
 
-// p and g into the relabelled order; g.p, m.p and sum(t).
+// p, g (and the teleport) into out-row order; g.p, m.p and sum(t); the
+// scalars that follow from them.
 __global__ void __launch_bounds__(kAdjThreads)
     adj_inputs(const double *__restrict__ scores, const double *__restrict__ grad,
-               const double *__restrict__ tele_orig, const uint32_t *__restrict__ perm,
-               const uint32_t *__restrict__ degc, uint32_t n, double damp, int distribute,
-               double *__restrict__ p_lab, double *__restrict__ g_lab, double *__restrict__ t_lab,
+               const double *__restrict__ tele_orig, const uint32_t *__restrict__ tperm,
+               const uint32_t *__restrict__ tdegc, uint32_t n, double damp, int distribute,
+               double *__restrict__ p_t, double *__restrict__ g_t, double *__restrict__ t_t,
                float *__restrict__ t32, double *__restrict__ part, AdjScalars *sc) {
     __shared__ double s_red[32];
     __shared__ bool s_last;
     double gp = 0.0, sp = 0.0, tau = 0.0;
     for (uint32_t r = blockIdx.x * kAdjThreads + threadIdx.x; r < n; r += gridDim.x * kAdjThreads) {
-        const uint32_t o = perm[r];
+        const uint32_t o = tperm[r];
         const double pv = scores[o], gv = grad[o];
-        p_lab[r] = pv;
-        g_lab[r] = gv;
+        p_t[r] = pv;
+        g_t[r] = gv;
         gp += gv * pv;
-        if (degc[r] == 0)
+        if (tdegc[r] == 0)
             sp += pv;
         if (tele_orig) {
             const double t = tele_orig[o];
-            t_lab[r] = t;
+            t_t[r] = t;
             t32[r] = static_cast<float>(t);
             tau += t;
         }
@@ -356,10 +470,10 @@ __global__ void __launch_bounds__(kAdjThreads)
     }
 }
 
-// gbar = g - (g.p) 1 (FP64 and FP32 copies), lam0 = gbar, |gbar|_1 and
-// tel.gbar (the state of a Jacobi sweep from lam0).
+// gbar = g - (g.p) 1 (FP64 and FP32 copies), lam0 = gbar, |gbar|_1 and the
+// sweep state of lam0 (tel.gbar, not done).
 __global__ void __launch_bounds__(kAdjThreads)
-    adj_rhs(const double *__restrict__ g_lab, const double *__restrict__ t_lab, uint32_t n,
+    adj_rhs(const double *__restrict__ g_t, const double *__restrict__ t_t, uint32_t n,
             int personal, double inv_n, double *__restrict__ gbar, float *__restrict__ r32,
             double *__restrict__ lam0, double *__restrict__ part, AdjScalars *sc, AdjState *st) {
     __shared__ double s_red[32];
@@ -367,12 +481,12 @@ __global__ void __launch_bounds__(kAdjThreads)
     const double gp = sc->gp;
     double nrm = 0.0, td = 0.0;
     for (uint32_t r = blockIdx.x * kAdjThreads + threadIdx.x; r < n; r += gridDim.x * kAdjThreads) {
-        const double b = g_lab[r] - gp;
+        const double b = g_t[r] - gp;
         gbar[r] = b;
         r32[r] = static_cast<float>(b);
         lam0[r] = b;
         nrm += fabs(b);
-        td += personal ? t_lab[r] * b : b;
+        td += personal ? t_t[r] * b : b;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0)
         lam0[n] = 0.0;
@@ -397,6 +511,7 @@ __global__ void __launch_bounds__(kAdjThreads)
         st->residual = 0.0;
         st->iteration = 0;
         st->done = 0;
+        st->ticket = 0;
         sc->ticket = 0;
     }
 }
@@ -404,7 +519,7 @@ __global__ void __launch_bounds__(kAdjThreads)
 // lam64 = x32 (add = 0) or lam64 += x32 (add = 1), lam64[n] = 0, and the
 // sweep state for lam64 (tel.lam64; not done).
 __global__ void __launch_bounds__(kAdjThreads)
-    adj_to_fp64(const float *__restrict__ x32, double *__restrict__ lam, const double *t_lab,
+    adj_to_fp64(const float *__restrict__ x32, double *__restrict__ lam, const double *t_t,
                 uint32_t n, int add, int personal, double inv_n, double *__restrict__ part,
                 unsigned int *ticket, AdjState *st) {
     __shared__ double s_red[32];
@@ -413,7 +528,7 @@ __global__ void __launch_bounds__(kAdjThreads)
     for (uint32_t r = blockIdx.x * kAdjThreads + threadIdx.x; r < n; r += gridDim.x * kAdjThreads) {
         const double v = add ? lam[r] + static_cast<double>(x32[r]) : static_cast<double>(x32[r]);
         lam[r] = v;
-        td += personal ? t_lab[r] * v : v;
+        td += personal ? t_t[r] * v : v;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0)
         lam[n] = 0.0;
@@ -430,6 +545,7 @@ __global__ void __launch_bounds__(kAdjThreads)
         st->tdot = personal ? t : t * inv_n;
         st->iteration = 0;
         st->done = 0;
+        st->ticket = 0;
         *ticket = 0;
     }
 }
@@ -443,38 +559,105 @@ __global__ void adj_residual_rhs(const double *__restrict__ lam_out,
         r32[r] = static_cast<float>(lam_out[r] - lam_in[r]);
 }
 
-// dL/dw for every in-arc, written at the arc's index in the caller's in-CSR.
-// One warp per in-row u.
+// Into the relabelled (in-layout) order: lam_f[v] = lam[tinv[v]] and the pair
+// qc[v] = (d p[v] / wdeg[v], c[v]) that every out-arc of v reads; qc[n] = 0
+// for the padding slots.
 template <bool WEIGHTED>
-__global__ void adj_grad_w(const uint32_t *__restrict__ row_ptr, const uint32_t *__restrict__ col,
-                           const uint64_t *__restrict__ row_src, const double *__restrict__ p_lab,
-                           const uint32_t *__restrict__ degc, const double *__restrict__ degw,
-                           const double *__restrict__ lam, const double *__restrict__ c,
-                           uint32_t n, double damp, double *__restrict__ grad_w) {
-    const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
-    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+__global__ void adj_to_forward(const uint32_t *__restrict__ tinv, const double *__restrict__ lam_t,
+                               const double *__restrict__ c_t, const double *__restrict__ p_t,
+                               const uint32_t *__restrict__ tdegc, const double *__restrict__ tdegw,
+                               uint32_t n, double damp, double *__restrict__ lam_f,
+                               double2 *__restrict__ qc) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v > n)
+        return;
+    if (v == n) {
+        qc[n] = make_double2(0.0, 0.0);
+        return;
+    }
+    const uint32_t rt = tinv[v];
+    lam_f[v] = lam_t[rt];
+    const uint32_t dc = tdegc[rt];
+    const double deg = WEIGHTED ? tdegw[rt] : static_cast<double>(dc);
+    qc[v] = make_double2(dc ? damp * (p_t[rt] / deg) : 0.0, c_t[rt]);
+}
+
+// dL/dw over the in-layout's slices: lane = virtual row (an in-row u or a
+// chunk of one), slot j = its arc start + j with source v = col_sell, so
+// dL/dw = qc[v].x (lam[u] - qc[v].y), stored at the arc's caller index
+// row_src[u] + start + j (consecutive for a lane). One warp per slice.
+__global__ void __launch_bounds__(256)
+    adj_grad_w(const uint32_t *__restrict__ slice_off, const uint32_t *__restrict__ col_sell,
+               const uint32_t *__restrict__ chunk_begin, const uint32_t *__restrict__ row_ptr,
+               const uint64_t *__restrict__ row_src, const double *__restrict__ lam_f,
+               const double2 *__restrict__ qc, uint32_t slices, uint32_t s_chunk,
+               uint32_t n_chunks, uint32_t n_long, uint32_t n, double *__restrict__ grad_w) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
-    for (uint64_t u = warp; u < n; u += nwarps) {
-        const uint32_t b = row_ptr[u], e = row_ptr[u + 1];
-        const uint64_t dst = row_src[u];
-        const double lu = lam[u];
-        for (uint32_t k = b + lane; k < e; k += 32) {
-            const uint32_t v = col[k];
-            const double deg = WEIGHTED ? degw[v] : static_cast<double>(degc[v]);
-            grad_w[dst + (k - b)] = damp * (p_lab[v] / deg) * (lu - c[v]);
+    for (uint32_t s = warp; s < slices; s += nwarps) {
+        const uint32_t off = slice_off[s], len = slice_off[s + 1] - off;
+        uint32_t r = 0, start = 0, vlen = 0;
+        if (s < s_chunk) {
+            const uint32_t k = s * 32 + lane;
+            if (k < n_chunks) {
+                // split row of chunk k: the last r with chunk_begin[r] <= k
+                uint32_t lo = 0, hi = n_long - 1;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1) >> 1;
+                    if (chunk_begin[mid] <= k)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                r = lo;
+                start = (k - chunk_begin[r]) * kChunk;
+                const uint32_t rl = row_ptr[r + 1] - row_ptr[r];
+                vlen = rl - start < kChunk ? rl - start : kChunk;
+            }
+        } else {
+            r = n_long + (s - s_chunk) * 32 + lane;
+            if (r < n)
+                vlen = row_ptr[r + 1] - row_ptr[r];
+            else
+                r = 0;
+        }
+        const double lu = lam_f[r];
+        double *dst = grad_w + row_src[r] + start;
+        const uint32_t *cp = col_sell + static_cast<size_t>(off) * 32 + lane;
+        uint32_t j = 0;
+        for (; j + 8 <= len; j += 8) {
+            uint32_t c[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                c[k] = ld_stream(cp + static_cast<size_t>(j + k) * 32);
+            double2 q[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                q[k] = __ldg(qc + c[k]);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (j + k < vlen)
+                    dst[j + k] = q[k].x * (lu - q[k].y);
+        }
+        for (; j < len; ++j) {
+            if (j < vlen) {
+                const double2 q = __ldg(qc + ld_stream(cp + static_cast<size_t>(j) * 32));
+                dst[j] = q.x * (lu - q.y);
+            }
         }
     }
 }
 
 // dL/dt in the caller's ids (0 for ids of deleted nodes).
-__global__ void adj_grad_t(const uint32_t *__restrict__ inv, uint64_t z,
-                           const double *__restrict__ lam, const AdjScalars *sc,
-                           double *__restrict__ grad_t) {
+__global__ void adj_grad_t(const uint32_t *__restrict__ inv, const uint32_t *__restrict__ tinv,
+                           uint64_t z, const double *__restrict__ lam_t,
+                           const AdjScalars *sc, double *__restrict__ grad_t) {
     const uint64_t o = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (o >= z)
         return;
     const uint32_t r = inv[o];
-    grad_t[o] = r == kNone ? 0.0 : sc->tfac * lam[r];
+    grad_t[o] = r == kNone ? 0.0 : sc->tfac * lam_t[tinv[r]];
 }
 
 } // namespace
@@ -487,6 +670,7 @@ AdjointState &adjoint_ensure(nkg_graph *g) {
         return *g->adj;
     require(!g->arc_sorted,
             "the adjoint needs the in-rows in the caller's arc order (arc_order 0)");
+    require(!g->w64src_stale, "internal: CSR weights out of date");
     cudaStream_t s = g->stream;
     const uint32_t n = static_cast<uint32_t>(g->n);
     const uint64_t arcs = g->arcs;
@@ -508,18 +692,25 @@ AdjointState &adjoint_ensure(nkg_graph *g) {
                                                            ids.get(), A->trow.get(),
                                                            static_cast<int64_t>(n), 0, 32, s));
     }
-    DeviceArray<uint32_t> tlen(n), tinv(n);
-    adj_row_lengths<<<ceil_div(n, 256), 256, 0, s>>>(A->trow.get(), g->degc.get(), n, tlen.get(),
-                                                     tinv.get());
+    A->tinv.alloc(n);
+    A->tperm.alloc(n);
+    A->tdegc.alloc(n);
+    if (g->weighted) {
+        A->tdegw64.alloc(n);
+        A->tdegw32.alloc(n);
+    }
+    adj_row_info<<<ceil_div(n, 256), 256, 0, s>>>(A->trow.get(), g->degc.get(), g->perm.get(),
+                                                  g->degw64src.get(), n, A->tdegc.get(),
+                                                  A->tinv.get(), A->tperm.get(), A->tdegw64.get());
     NKG_CUDA(cudaGetLastError());
     A->tptr.alloc(static_cast<size_t>(n) + 1);
     NKG_CUDA(cudaMemsetAsync(A->tptr.get(), 0, sizeof(uint32_t), s));
     {
         size_t tb = 0;
-        NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, tlen.get(), A->tptr.get() + 1,
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, A->tdegc.get(), A->tptr.get() + 1,
                                                static_cast<int64_t>(n), s));
         DeviceArray<unsigned char> tmp(tb);
-        NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb, tlen.get(), A->tptr.get() + 1,
+        NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb, A->tdegc.get(), A->tptr.get() + 1,
                                                static_cast<int64_t>(n), s));
     }
 
@@ -528,7 +719,7 @@ AdjointState &adjoint_ensure(nkg_graph *g) {
     DeviceArray<uint32_t> tcol(std::max<uint64_t>(arcs, 1));
     if (arcs) {
         DeviceArray<uint32_t> key(arcs), key_s(arcs), val(arcs), arc_row(arcs);
-        adj_arc_keys<<<sms * 16, 256, 0, s>>>(g->row_ptr.get(), g->col.get(), tinv.get(), n,
+        adj_arc_keys<<<sms * 16, 256, 0, s>>>(g->row_ptr.get(), g->col.get(), A->tinv.get(), n,
                                               key.get(), val.get(), arc_row.get());
         NKG_CUDA(cudaGetLastError());
         int bits = 1;
@@ -542,47 +733,87 @@ AdjointState &adjoint_ensure(nkg_graph *g) {
         NKG_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, key.get(), key_s.get(), val.get(),
                                                  A->tarc.get(), static_cast<int64_t>(arcs), 0, bits,
                                                  s));
-        adj_gather_cols<<<sms * 8, 256, 0, s>>>(A->tarc.get(), arc_row.get(), arcs, tcol.get());
+        adj_gather_u32<<<sms * 8, 256, 0, s>>>(A->tarc.get(), arc_row.get(), arcs, tcol.get());
         NKG_CUDA(cudaGetLastError());
         NKG_CUDA(cudaStreamSynchronize(s));
     }
     build_sell(A->tl, n, A->tptr.get(), tcol.get(), g->weighted ? g->w64src.get() : nullptr,
-               A->tarc.get(), tlen.get(), g->device, s);
+               A->tarc.get(), A->tdegc.get(), g->device, s);
     if (g->weighted) {
         A->w_sell32.alloc(A->tl.slots, 4);
-        A->degw32.alloc(n);
         convert_to_float(A->tl.w_sell64.get(), A->w_sell32.get(), A->tl.slots, g->device, s);
-        convert_to_float(g->degw64src.get(), A->degw32.get(), n, g->device, s);
+        convert_to_float(A->tdegw64.get(), A->tdegw32.get(), n, g->device, s);
     }
     NKG_CUDA(cudaStreamSynchronize(s));
     g->adj.reset(A.release());
     return *g->adj;
 }
 
-void adjoint_refresh_weights(nkg_graph *g) {
-    if (!g->adj || !g->weighted)
+namespace {
+
+// Slot -> caller arc maps of both layouts (first weight update only).
+void ensure_weight_maps(nkg_graph *g, AdjointState &A) {
+    if (A.fw_map)
         return;
-    AdjointState &A = *g->adj;
+    cudaStream_t s = g->stream;
     const uint32_t n = static_cast<uint32_t>(g->n);
-    refill_sell_weights(A.tl, n, A.tptr.get(), g->w64src.get(), A.tarc.get(), g->device, g->stream);
-    convert_to_float(A.tl.w_sell64.get(), A.w_sell32.get(), A.tl.slots, g->device, g->stream);
-    convert_to_float(g->degw64src.get(), A.degw32.get(), n, g->device, g->stream);
-    NKG_CUDA(cudaStreamSynchronize(g->stream));
+    const unsigned sms = num_sms(g->device);
+    DeviceArray<uint32_t> caller(std::max<uint64_t>(g->arcs, 1)), tcaller(std::max<uint64_t>(g->arcs, 1));
+    if (g->arcs) {
+        adj_caller_index<<<sms * 16, 256, 0, s>>>(g->row_ptr.get(), g->row_src.get(), n,
+                                                  caller.get());
+        adj_gather_u32<<<sms * 8, 256, 0, s>>>(A.tarc.get(), caller.get(), g->arcs, tcaller.get());
+        NKG_CUDA(cudaGetLastError());
+    }
+    A.fw_map.alloc(std::max<uint64_t>(g->fw.slots, 1));
+    A.t_map.alloc(std::max<uint64_t>(A.tl.slots, 1));
+    build_slot_map(g->fw, n, g->row_ptr.get(), caller.get(), A.fw_map.get(), g->device, s);
+    build_slot_map(A.tl, n, A.tptr.get(), tcaller.get(), A.t_map.get(), g->device, s);
+    A.tchunk.alloc(static_cast<size_t>(A.tl.s_chunk) * 32 + 1);
+    NKG_CUDA(cudaStreamSynchronize(s));
 }
 
-void adjoint_out_wdeg(nkg_graph *g, double *degw) {
+} // namespace
+
+// Replace the arc weights (and weighted out-degrees) in place: every buffer
+// keeps its address, so captured sweep graphs stay valid. w and wdeg are
+// device arrays in the caller's order (wdeg may be null).
+void set_weights_device(nkg_graph *g, const double *w, const double *wdeg) {
     AdjointState &A = adjoint_ensure(g);
+    ensure_weight_maps(g, A);
+    cudaStream_t s = g->stream;
     const uint32_t n = static_cast<uint32_t>(g->n);
-    adj_out_wdeg<<<num_sms(g->device) * 16, 256, 0, g->stream>>>(A.tptr.get(), A.tarc.get(),
-                                                                A.trow.get(), g->w64src.get(), n,
-                                                                degw);
+    const unsigned sms = num_sms(g->device);
+    if (g->fw.slots)
+        adj_refresh_slots<<<sms * 8, 256, 0, s>>>(A.fw_map.get(), g->fw.slots, w,
+                                                  g->fw.w_sell64.get(), g->p32.w_sell.get());
+    if (A.tl.slots)
+        adj_refresh_slots<<<sms * 8, 256, 0, s>>>(A.t_map.get(), A.tl.slots, w,
+                                                  A.tl.w_sell64.get(), A.w_sell32.get());
     NKG_CUDA(cudaGetLastError());
+    DegreeOut o{A.trow.get(), A.tdegw64.get(), A.tdegw32.get(), g->degw64src.get(),
+                g->p32.degw.get()};
+    if (wdeg) {
+        adj_degree_given<<<ceil_div(n, 256), 256, 0, s>>>(wdeg, A.tperm.get(), n, o);
+    } else {
+        adj_degree_sums<<<sms * 8, 256, 0, s>>>(A.tl.slice_off.get(), A.tl.w_sell64.get(),
+                                                A.tl.slices, A.tl.s_chunk, A.tl.n_long, n,
+                                                A.tchunk.get(), o);
+        if (A.tl.n_long)
+            adj_degree_fix<<<ceil_div(A.tl.n_long, 256), 256, 0, s>>>(
+                A.tl.chunk_begin.get(), A.tl.n_long, A.tchunk.get(), o);
+    }
+    NKG_CUDA(cudaGetLastError());
+    // The relabelled CSR weights are not kept current: the sliced layouts
+    // carry the weights from here on.
+    g->w64src_stale = true;
+    NKG_CUDA(cudaStreamSynchronize(s));
 }
 
 namespace {
 
-// Grids and cost-balanced units of the two out-adjacency kernels (FP32
-// BiCGSTAB product, FP64 sweep) for the graph's launch shape.
+// Grids and cost-balanced units of the two out-layout kernels (FP32 BiCGSTAB
+// product, FP64 sweep) for the graph's launch shape.
 template <bool WEIGHTED>
 void adjoint_launch_setup(nkg_graph *g, AdjointState &A) {
     if (A.shape == g->sweep_shape)
@@ -614,8 +845,8 @@ void adjoint_launch_setup(nkg_graph *g, AdjointState &A) {
     };
     auto units = [&](unsigned c) {
         const uint64_t warps = static_cast<uint64_t>(c) * (threads / 32);
-        return static_cast<uint32_t>(
-            std::max<uint64_t>(1, std::min<uint64_t>(warps * kUnitsPerWarp, std::max<uint64_t>(slices, 1))));
+        return static_cast<uint32_t>(std::max<uint64_t>(
+            1, std::min<uint64_t>(warps * kUnitsPerWarp, std::max<uint64_t>(slices, 1))));
     };
     A.ctas32 = ctas(occ32);
     A.ctas64 = ctas(occ64);
@@ -627,11 +858,44 @@ void adjoint_launch_setup(nkg_graph *g, AdjointState &A) {
     sell_units(A.tl, A.n_units64, A.units64.get(), s);
     NKG_CUDA(cudaStreamSynchronize(s));
     A.shape = g->sweep_shape;
+    A.work.ready = false;  // partial-sum buffers depend on the grids
+}
+
+constexpr size_t kScalOffBi = 0, kScalOffAdj = 128, kScalOffSt = 256, kScalBytes = 384;
+
+void ensure_work(nkg_graph *g, AdjointState &A, unsigned vec_ctas, unsigned fix_ctas) {
+    AdjWork &W = A.work;
+    if (W.ready)
+        return;
+    const size_t n = g->n;
+    const size_t part_n = std::max<size_t>(std::max(A.ctas32, A.ctas64), vec_ctas);
+    const size_t chunks = static_cast<size_t>(A.tl.s_chunk) * 32 + 1;
+    for (auto *a : {&W.p, &W.g, &W.t, &W.gbar, &W.c, &W.lam_f})
+        a->alloc(n);
+    W.lam[0].alloc(n + 1);
+    W.lam[1].alloc(n + 1);
+    W.part.alloc(3 * part_n);
+    W.fix_part.alloc(2 * static_cast<size_t>(fix_ctas));
+    W.chunk64.alloc(chunks);
+    W.chunk32.alloc(chunks);
+    W.qc.alloc(n + 1);
+    for (auto *a : {&W.t32, &W.x, &W.r, &W.rhat, &W.v, &W.tv})
+        a->alloc(n);
+    W.pv.alloc(n + 1);
+    W.sv.alloc(n + 1);
+    W.scal.alloc(kScalBytes);
+    cudaStream_t s = g->stream;
+    NKG_CUDA(cudaMemsetAsync(W.scal.get(), 0, kScalBytes, s));
+    NKG_CUDA(cudaMemsetAsync(W.pv.get() + n, 0, sizeof(float), s));
+    NKG_CUDA(cudaMemsetAsync(W.sv.get() + n, 0, sizeof(float), s));
+    NKG_CUDA(cudaMemsetAsync(W.lam[1].get() + n, 0, sizeof(double), s));
+    NKG_CUDA(cudaStreamSynchronize(s));
+    W.ready = true;
 }
 
 struct AdjResult {
     uint64_t fp64_sweeps = 0, fp32_matvecs = 0, launches = 0;
-    double residual = 0.0, ms = 0.0;
+    double residual = 0.0, ms = 0.0, ms_solve = 0.0;
 };
 
 template <bool WEIGHTED>
@@ -645,62 +909,56 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
     const int personal = d_tele ? 1 : 0;
     const int distribute = p.distribute_sinks ? 1 : 0;
     const double inv_n = 1.0 / static_cast<double>(n);
-    AdjResult R;
-    NKG_CUDA(cudaEventRecord(g->ev0, s));
-
     const unsigned vec_ctas = std::max<unsigned>(1, std::min<unsigned>(sms * 4, ceil_div(n, kBiThreads)));
     const unsigned fix_ctas = std::max<unsigned>(1, ceil_div(A.tl.n_long, kBiThreads));
-    const unsigned part_n = std::max<unsigned>(std::max(A.ctas32, A.ctas64), vec_ctas);
-    DeviceArray<double> p_lab(n), g_lab(n), t_lab(personal ? n : 0), gbar(n), c(n), part(3ull * part_n),
-        fix_part(2ull * fix_ctas), chunk64(static_cast<size_t>(A.tl.s_chunk) * 32 + 1);
-    DeviceArray<double> lam[2] = {DeviceArray<double>(n + 1), DeviceArray<double>(n + 1)};
-    DeviceArray<float> t32(personal ? n : 0), chunk32(static_cast<size_t>(A.tl.s_chunk) * 32 + 1);
-    DeviceArray<float> bx(n), br(n), brhat(n), bp(n + 1), bv(n), bs(n + 1), bt(n);
-    DeviceArray<AdjScalars> sc(1);
-    DeviceArray<BiScalars> bsc(1);
-    DeviceArray<AdjState> st(1);
-    NKG_CUDA(cudaMemsetAsync(sc.get(), 0, sizeof(AdjScalars), s));
-    NKG_CUDA(cudaMemsetAsync(bsc.get(), 0, sizeof(BiScalars), s));
-    NKG_CUDA(cudaMemsetAsync(st.get(), 0, sizeof(AdjState), s));
-    NKG_CUDA(cudaMemsetAsync(bp.get() + n, 0, sizeof(float), s));
-    NKG_CUDA(cudaMemsetAsync(bs.get() + n, 0, sizeof(float), s));
-    NKG_CUDA(cudaMemsetAsync(lam[1].get() + n, 0, sizeof(double), s));
+    ensure_work(g, A, vec_ctas, fix_ctas);
+    AdjWork &W = A.work;
+    AdjResult R;
+    NKG_CUDA(cudaEventRecord(g->ev0, s));
+    NKG_CUDA(cudaMemsetAsync(W.scal.get(), 0, kScalBytes, s));
+    BiScalars *bsc = reinterpret_cast<BiScalars *>(W.scal.get() + kScalOffBi);
+    AdjScalars *sc = reinterpret_cast<AdjScalars *>(W.scal.get() + kScalOffAdj);
+    AdjState *st = reinterpret_cast<AdjState *>(W.scal.get() + kScalOffSt);
+    static_assert(sizeof(BiScalars) <= 128 && sizeof(AdjScalars) <= 128 && sizeof(AdjState) <= 128,
+                  "scalar blocks fit their slots");
 
-    const double *degw64 = g->degw64src.get();
-    adj_inputs<<<vec_ctas, kAdjThreads, 0, s>>>(d_scores, d_grad, d_tele, g->perm.get(),
-                                                g->degc.get(), n, p.damp, distribute, p_lab.get(),
-                                                g_lab.get(), t_lab.get(), t32.get(), part.get(),
-                                                sc.get());
-    adj_rhs<<<vec_ctas, kAdjThreads, 0, s>>>(g_lab.get(), t_lab.get(), n, personal, inv_n,
-                                             gbar.get(), br.get(), lam[0].get(), part.get(),
-                                             sc.get(), st.get());
+    adj_inputs<<<vec_ctas, kAdjThreads, 0, s>>>(d_scores, d_grad, d_tele, A.tperm.get(),
+                                                A.tdegc.get(), n, p.damp, distribute, W.p.get(),
+                                                W.g.get(), W.t.get(), W.t32.get(), W.part.get(), sc);
+    adj_rhs<<<vec_ctas, kAdjThreads, 0, s>>>(W.g.get(), W.t.get(), n, personal, inv_n,
+                                             W.gbar.get(), W.r.get(), W.lam[0].get(), W.part.get(),
+                                             sc, st);
     NKG_CUDA(cudaGetLastError());
     R.launches += 2;
-    AdjScalars *hsc = reinterpret_cast<AdjScalars *>(g->scalars_host.get());
-    static_assert(sizeof(AdjScalars) <= 16 * sizeof(double), "AdjScalars fits the pinned buffer");
-    NKG_CUDA(cudaMemcpyAsync(hsc, sc.get(), sizeof(AdjScalars), cudaMemcpyDeviceToHost, s));
+    // Pinned read-back slots (16 doubles): BiScalars at 0 (80 bytes); the
+    // adjoint's scalars and state at 12 (32 bytes).
+    double *h2 = g->scalars_host.get() + 12;
+    AdjState *hst = reinterpret_cast<AdjState *>(g->scalars_host.get() + 12);
+    static_assert(sizeof(BiScalars) <= 12 * sizeof(double) && sizeof(AdjState) <= 4 * sizeof(double),
+                  "read-back slots fit the pinned buffer");
+    static_assert(offsetof(AdjScalars, sumx) == offsetof(AdjScalars, gnorm) + sizeof(double),
+                  "gnorm and sumx are read back together");
+    NKG_CUDA(cudaMemcpyAsync(h2, &sc->gnorm, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     NKG_CUDA(cudaStreamSynchronize(s));
-    const double gnorm = hsc->gnorm;
-    require(std::isfinite(gnorm) && std::isfinite(hsc->sumx) && hsc->sumx > 0.0,
+    const double gnorm = h2[0], sumx = h2[1];
+    require(std::isfinite(gnorm) && std::isfinite(sumx) && sumx > 0.0,
             "scores / grad_scores are not finite or do not come from a converged forward run");
     const double tol_abs = p.tol * gnorm;
 
-    // FP64 sweep arguments (lam_in / lam_out / c_out set per launch).
     AdjArgs aa{};
     aa.col_sell = A.tl.col_sell.get();
     aa.w_sell = A.tl.w_sell64.get();
     aa.slice_off = A.tl.slice_off.get();
     aa.unit_start = A.units64.get();
     aa.chunk_begin = A.tl.chunk_begin.get();
-    aa.row_label = A.trow.get();
-    aa.degc = g->degc.get();
-    aa.degw = degw64;
-    aa.tele = t_lab.get();
-    aa.gbar = gbar.get();
-    aa.chunk_val = chunk64.get();
-    aa.part = part.get();
-    aa.fix_part = fix_part.get();
-    aa.st = st.get();
+    aa.degc = A.tdegc.get();
+    aa.degw = A.tdegw64.get();
+    aa.tele = personal ? W.t.get() : nullptr;
+    aa.gbar = W.gbar.get();
+    aa.chunk_val = W.chunk64.get();
+    aa.part = W.part.get();
+    aa.fix_part = W.fix_part.get();
+    aa.st = st;
     aa.damp = p.damp;
     aa.inv_n = inv_n;
     aa.tol = tol_abs;
@@ -726,12 +984,8 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
         R.launches += 2;
         ++R.fp64_sweeps;
     };
-    // Pinned read-back slots: BiScalars at 0 (80 bytes), AdjState at 96.
-    AdjState *hst = reinterpret_cast<AdjState *>(g->scalars_host.get() + 12);
-    static_assert(sizeof(BiScalars) <= 12 * sizeof(double) && sizeof(AdjState) <= 4 * sizeof(double),
-                  "read-back slots fit the pinned buffer");
     auto read_state = [&] {
-        NKG_CUDA(cudaMemcpyAsync(hst, st.get(), sizeof(AdjState), cudaMemcpyDeviceToHost, s));
+        NKG_CUDA(cudaMemcpyAsync(hst, st, sizeof(AdjState), cudaMemcpyDeviceToHost, s));
         NKG_CUDA(cudaStreamSynchronize(s));
         if (g->cancel.load()) {
             g->cancel.store(0);
@@ -739,21 +993,19 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
         }
     };
 
-    int fin = 0;  // lam[fin] is the solution
+    int fin = 0;  // W.lam[fin] holds the solution
     if (p.precision == NKG_PREC_FP64) {
         // Jacobi from lam0 = gbar until |lam' - lam|_1 <= tol |gbar|_1, in
         // batches of kSweepsPerGraph launches; the launches after the sweep
         // that meets the test return at once.
         uint64_t before = 0;
-        R.fp64_sweeps = 0;
         for (;;) {
             const int fin0 = fin;
             for (int k = 0; k < kSweepsPerGraph; ++k)
-                sweep64(lam[(fin0 + k) & 1].get(), lam[(fin0 + k + 1) & 1].get(), nullptr,
+                sweep64(W.lam[(fin0 + k) & 1].get(), W.lam[(fin0 + k + 1) & 1].get(), nullptr,
                         p.max_iterations);
             read_state();
-            const uint64_t eff = hst->iteration - before;
-            fin = fin0 ^ static_cast<int>(eff & 1);
+            fin = fin0 ^ static_cast<int>((hst->iteration - before) & 1);
             before = hst->iteration;
             if (hst->done)
                 break;
@@ -767,22 +1019,21 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
         a.slice_off = A.tl.slice_off.get();
         a.unit_start = A.units32.get();
         a.chunk_begin = A.tl.chunk_begin.get();
-        a.degc = g->degc.get();
-        a.degw = A.degw32.get();
-        a.tele = t32.get();
-        a.row_label = A.trow.get();
-        a.chunk_val = chunk32.get();
-        a.x = bx.get();
-        a.r = br.get();
-        a.rhat = brhat.get();
-        a.p = bp.get();
-        a.v = bv.get();
-        a.s = bs.get();
-        a.t = bt.get();
+        a.degc = A.tdegc.get();
+        a.degw = A.tdegw32.get();
+        a.tele = personal ? W.t32.get() : nullptr;
+        a.chunk_val = W.chunk32.get();
+        a.x = W.x.get();
+        a.r = W.r.get();
+        a.rhat = W.rhat.get();
+        a.p = W.pv.get();
+        a.v = W.v.get();
+        a.s = W.sv.get();
+        a.t = W.tv.get();
         a.g = nullptr;
-        a.part = part.get();
-        a.fix_part = fix_part.get();
-        a.sc = bsc.get();
+        a.part = W.part.get();
+        a.fix_part = W.fix_part.get();
+        a.sc = bsc;
         a.damp = p.damp;
         a.inv_n = inv_n;
         a.n = n;
@@ -800,36 +1051,38 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
         bl.sweep_ctas = A.ctas32;
         bl.vec_ctas = vec_ctas;
         bl.fix_ctas = fix_ctas;
-        bl.d_sc = bsc.get();
+        bl.d_sc = bsc;
         bl.h_sc = reinterpret_cast<BiScalars *>(g->scalars_host.get());
         bl.cancel = &g->cancel;
         if (p.precision == NKG_PREC_FP32) {
-            // FP32 alone: one solve to the FP32 floor or tol, whichever is larger.
+            // FP32 alone: one solve to tol or the FP32 floor, whichever is larger.
             bi_solve<WEIGHTED, 1>(a, bl, std::max(p.tol, 3e-7), 0.0);
-            adj_to_fp64<<<vec_ctas, kAdjThreads, 0, s>>>(bx.get(), lam[0].get(), t_lab.get(), n,
-                                                         0, personal, inv_n, part.get(),
-                                                         &sc.get()->ticket, st.get());
+            adj_to_fp64<<<vec_ctas, kAdjThreads, 0, s>>>(W.x.get(), W.lam[0].get(), W.t.get(), n,
+                                                         0, personal, inv_n, W.part.get(),
+                                                         &sc->ticket, st);
             R.launches += 1;
-            NKG_CUDA(cudaMemcpyAsync(bl.h_sc, bsc.get(), sizeof(BiScalars), cudaMemcpyDeviceToHost, s));
-            NKG_CUDA(cudaStreamSynchronize(s));
             R.residual = bl.h_sc->res;
+            // c = A^T lam for the solution.
+            sweep64(W.lam[0].get(), nullptr, W.c.get(), ~0ull);
         } else {
             // FP32 solves, FP64 Jacobi residual sweeps: stop when the FP64
-            // residual of lam is <= tol |gbar|_1 (lam is then the sweep's input).
+            // residual of lam is <= tol |gbar|_1 (lam is then the sweep's input,
+            // and the sweep has written its c).
             bi_solve<WEIGHTED, 1>(a, bl, 1e-6, 0.25 * tol_abs);
             int add = 0;
             for (int round = 0;; ++round) {
-                require(round < 40, "FP32 refinement of the adjoint did not reach the tolerance in 40 rounds");
-                adj_to_fp64<<<vec_ctas, kAdjThreads, 0, s>>>(bx.get(), lam[0].get(), t_lab.get(),
-                                                             n, add, personal, inv_n, part.get(),
-                                                             &sc.get()->ticket, st.get());
+                require(round < 40,
+                        "FP32 refinement of the adjoint did not reach the tolerance in 40 rounds");
+                adj_to_fp64<<<vec_ctas, kAdjThreads, 0, s>>>(W.x.get(), W.lam[0].get(), W.t.get(),
+                                                             n, add, personal, inv_n, W.part.get(),
+                                                             &sc->ticket, st);
                 R.launches += 1;
-                sweep64(lam[0].get(), lam[1].get(), c.get(), ~0ull);
+                sweep64(W.lam[0].get(), W.lam[1].get(), W.c.get(), ~0ull);
                 read_state();
                 if (hst->residual <= tol_abs)
                     break;
-                adj_residual_rhs<<<ceil_div(n, 256), 256, 0, s>>>(lam[1].get(), lam[0].get(), n,
-                                                                  br.get());
+                adj_residual_rhs<<<ceil_div(n, 256), 256, 0, s>>>(W.lam[1].get(), W.lam[0].get(),
+                                                                  n, W.r.get());
                 R.launches += 1;
                 bi_solve<WEIGHTED, 1>(a, bl, 1e-5, 0.25 * tol_abs);
                 add = 1;
@@ -840,27 +1093,25 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
         R.launches += bl.launches;
         fin = 0;
     }
-    // c = A^T lam for the solution (the refinement's last sweep already has it).
-    if (!(p.precision == NKG_PREC_FP32_REFINE)) {
-        NKG_CUDA(cudaMemsetAsync(st.get(), 0, sizeof(AdjState), s));
-        sweep64(lam[fin].get(), nullptr, c.get(), ~0ull);
+    if (p.precision == NKG_PREC_FP64) {
+        // c = A^T lam for the solution.
+        NKG_CUDA(cudaMemsetAsync(st, 0, sizeof(AdjState), s));
+        sweep64(W.lam[fin].get(), nullptr, W.c.get(), ~0ull);
     }
     NKG_CUDA(cudaEventRecord(g->ev1, s));
+    const double *lam_t = W.lam[fin].get();
     if (d_gw && g->arcs) {
-        if (WEIGHTED)
-            adj_grad_w<true><<<sms * 16, 256, 0, s>>>(g->row_ptr.get(), g->col.get(),
-                                                      g->row_src.get(), p_lab.get(), g->degc.get(),
-                                                      degw64, lam[fin].get(), c.get(), n, p.damp,
-                                                      d_gw);
-        else
-            adj_grad_w<false><<<sms * 16, 256, 0, s>>>(g->row_ptr.get(), g->col.get(),
-                                                       g->row_src.get(), p_lab.get(), g->degc.get(),
-                                                       nullptr, lam[fin].get(), c.get(), n, p.damp,
-                                                       d_gw);
-        R.launches += 1;
+        adj_to_forward<WEIGHTED><<<ceil_div(static_cast<uint64_t>(n) + 1, 256), 256, 0, s>>>(
+            A.tinv.get(), lam_t, W.c.get(), W.p.get(), A.tdegc.get(), A.tdegw64.get(), n, p.damp,
+            W.lam_f.get(), W.qc.get());
+        adj_grad_w<<<sms * 16, 256, 0, s>>>(
+            g->fw.slice_off.get(), g->fw.col_sell.get(), g->fw.chunk_begin.get(), g->row_ptr.get(),
+            g->row_src.get(), W.lam_f.get(), W.qc.get(), g->fw.slices, g->fw.s_chunk,
+            g->fw.n_chunks, g->fw.n_long, n, d_gw);
+        R.launches += 2;
     }
     if (d_gt) {
-        adj_grad_t<<<ceil_div(g->z, 256), 256, 0, s>>>(g->inv.get(), g->z, lam[fin].get(), sc.get(),
+        adj_grad_t<<<ceil_div(g->z, 256), 256, 0, s>>>(g->inv.get(), A.tinv.get(), g->z, lam_t, sc,
                                                        d_gt);
         R.launches += 1;
     }
@@ -870,16 +1121,18 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
     float ms = 0.f;
     NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev2));
     R.ms = ms;
+    NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    R.ms_solve = ms;
     return R;
 }
 
-// Device copy of a caller array (host arrays are uploaded; device arrays
-// are used in place).
+// Device copy of a caller array (host arrays are uploaded; device arrays are
+// used in place).
 const double *device_input(const double *p, size_t count, bool on_device, DeviceArray<double> &tmp,
                            cudaStream_t s) {
     if (!p || on_device)
         return p;
-    tmp.alloc(count);
+    tmp.alloc(std::max<size_t>(count, 1));
     if (count)
         NKG_CUDA(cudaMemcpyAsync(tmp.get(), p, count * sizeof(double), cudaMemcpyHostToDevice, s));
     return tmp.get();
@@ -891,6 +1144,21 @@ const double *device_input(const double *p, size_t count, bool on_device, Device
 using namespace nkg;
 
 extern "C" {
+
+int nkg_graph_set_weights(nkg_graph *g, const double *in_w, const double *out_wdeg, int flags) {
+    return guarded([&] {
+        require(g != nullptr && in_w != nullptr, "NULL argument");
+        require((flags & ~NKG_DEVICE_PTRS) == 0, "unknown flags");
+        require(g->weighted, "the graph was created unweighted (in_w NULL)");
+        require(!g->arc_sorted, "new weights need the in-rows in the caller's order (arc_order 0)");
+        DeviceGuard guard(g->device);
+        const bool dev = (flags & NKG_DEVICE_PTRS) != 0;
+        DeviceArray<double> w_tmp, d_tmp;
+        const double *d_w = device_input(in_w, g->arcs, dev, w_tmp, g->stream);
+        const double *d_wdeg = device_input(out_wdeg, g->z, dev, d_tmp, g->stream);
+        set_weights_device(g, d_w, d_wdeg);
+    });
+}
 
 int nkg_pagerank_adjoint(nkg_graph *g, const nkg_pr_params *p, const double *teleport,
                          const double *scores, const double *grad_scores, double *grad_w_out,
@@ -946,9 +1214,7 @@ int nkg_pagerank_adjoint(nkg_graph *g, const nkg_pr_params *p, const double *tel
             stats->iterations = R.fp64_sweeps + R.fp32_matvecs;
             stats->residual = R.residual;
             stats->ms_total = R.ms;
-            float ms = 0.f;
-            NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
-            stats->ms_iterations = ms;
+            stats->ms_iterations = R.ms_solve;
             stats->kernel_launches = R.launches;
             stats->fp64_sweeps = R.fp64_sweeps;
             stats->fp32_sweeps = R.fp32_matvecs;

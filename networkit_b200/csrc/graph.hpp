@@ -36,9 +36,10 @@ struct SellLayout {
 void build_sell(SellLayout &L, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                 const double *w, const uint32_t *w_index, const uint32_t *rowlen, int device,
                 cudaStream_t s);
-// Rewrite the FP64 slot weights of a layout built by build_sell.
-void refill_sell_weights(SellLayout &L, uint32_t n, const uint32_t *row_ptr, const double *w,
-                         const uint32_t *w_index, int device, cudaStream_t s);
+// map[slot] = index[k] for the CSR entry k each slot of L holds (kNone for
+// padding slots).
+void build_slot_map(const SellLayout &L, uint32_t n, const uint32_t *row_ptr, const uint32_t *index,
+                    uint32_t *map, int device, cudaStream_t s);
 // Cost-balanced unit boundaries over the slices of L (units+1 entries).
 void sell_units(const SellLayout &L, uint32_t units, uint32_t *unit_start, cudaStream_t s);
 void convert_to_float(const double *in, float *out, uint64_t m, int device, cudaStream_t s);
@@ -87,6 +88,7 @@ struct nkg_graph {
     nkg::SellLayout fw;
     int sweep_shape = 0;
     bool arc_sorted = false;
+    bool w64src_stale = false;  // w64src predates nkg_graph_set_weights
 
     // Out-adjacency layout and buffers of the adjoint (built on first use).
     std::unique_ptr<nkg::AdjointState, nkg::AdjointDeleter> adj;
@@ -111,9 +113,7 @@ struct nkg_graph {
 namespace nkg {
 // The out-adjacency layout of the adjoint (adjoint.cu), built on first use.
 AdjointState &adjoint_ensure(nkg_graph *g);
-// Refresh the adjoint's copies of the arc weights after w64src changed.
-void adjoint_refresh_weights(nkg_graph *g);
-// Weighted out-degree of every node (relabelled order) summed over its
-// out-arcs in the order they appear in the in-CSR.
-void adjoint_out_wdeg(nkg_graph *g, double *degw);
+// Replace the arc weights in place (device arrays in the caller's order;
+// wdeg null: summed on the device over every node's out-arcs).
+void set_weights_device(nkg_graph *g, const double *w, const double *wdeg);
 } // namespace nkg

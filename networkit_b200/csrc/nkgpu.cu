@@ -514,9 +514,27 @@ void build_sell(SellLayout &L, uint32_t n, const uint32_t *row_ptr, const uint32
     NKG_CUDA(cudaStreamSynchronize(s));
 }
 
-// Rewrite the FP64 slot weights of L from new CSR weights (same structure).
-void refill_sell_weights(SellLayout &L, uint32_t n, const uint32_t *row_ptr, const double *w,
-                         const uint32_t *w_index, int device, cudaStream_t s) {
+// map[slot] = index[k] for the CSR entry k the slot holds (kNone for padding).
+__global__ void fill_slot_map(uint32_t slices, uint32_t s_chunk, uint32_t n_chunks, uint32_t n_long,
+                              uint32_t n, const uint32_t *__restrict__ chunk_row,
+                              const uint32_t *__restrict__ chunk_idx,
+                              const uint32_t *__restrict__ row_ptr,
+                              const uint32_t *__restrict__ index,
+                              const uint32_t *__restrict__ slice_off, uint32_t *__restrict__ map) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t s = warp; s < slices; s += nwarps) {
+        const VRow v =
+            vrow_of(s, lane, s_chunk, n_chunks, n_long, n, chunk_row, chunk_idx, row_ptr);
+        const uint32_t off = slice_off[s], len = slice_off[s + 1] - off;
+        for (uint32_t j = 0; j < len; ++j)
+            map[(static_cast<size_t>(off) + j) * 32 + lane] = j < v.len ? index[v.start + j] : kNone;
+    }
+}
+
+void build_slot_map(const SellLayout &L, uint32_t n, const uint32_t *row_ptr, const uint32_t *index,
+                    uint32_t *map, int device, cudaStream_t s) {
     if (!L.slices)
         return;
     const unsigned sms = num_sms(device);
@@ -525,9 +543,9 @@ void refill_sell_weights(SellLayout &L, uint32_t n, const uint32_t *row_ptr, con
     if (L.n_long)
         expand_chunks<<<sms * 4, 256, 0, s>>>(L.chunk_begin.get(), L.n_long, chunk_row.get(),
                                               chunk_idx.get());
-    fill_slices<<<sms * 16, 256, 0, s>>>(L.slices, L.s_chunk, L.n_chunks, L.n_long, n,
-                                         chunk_row.get(), chunk_idx.get(), row_ptr, nullptr, w,
-                                         w_index, L.slice_off.get(), nullptr, L.w_sell64.get());
+    fill_slot_map<<<sms * 16, 256, 0, s>>>(L.slices, L.s_chunk, L.n_chunks, L.n_long, n,
+                                           chunk_row.get(), chunk_idx.get(), row_ptr, index,
+                                           L.slice_off.get(), map);
     NKG_CUDA(cudaGetLastError());
     NKG_CUDA(cudaStreamSynchronize(s));
 }
@@ -1209,69 +1227,6 @@ static int run_to(nkg_graph *g, const nkg_pr_params *p, const double *teleport, 
     });
 }
 
-// New arc weights (caller's in-CSR order) into the relabelled CSR; one warp
-// per row.
-__global__ void scatter_weights(const uint32_t *__restrict__ row_ptr,
-                                const uint64_t *__restrict__ row_src, const double *__restrict__ w_in,
-                                uint64_t n, double *__restrict__ w) {
-    const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
-    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    for (uint64_t r = warp; r < n; r += nwarps) {
-        const uint32_t b = row_ptr[r], e = row_ptr[r + 1];
-        const uint64_t src = row_src[r];
-        for (uint32_t k = b + lane; k < e; k += 32)
-            w[k] = w_in[src + (k - b)];
-    }
-}
-
-__global__ void permute_wdeg(const double *__restrict__ wdeg_orig, const uint32_t *__restrict__ perm,
-                             uint64_t n, double *__restrict__ degw) {
-    const uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    if (r < n)
-        degw[r] = wdeg_orig[perm[r]];
-}
-
-// Replace the arc weights (and weighted degrees) of a weighted graph in place:
-// every buffer keeps its address, so captured sweep graphs stay valid.
-static void set_weights(nkg_graph *g, const double *in_w, const double *out_wdeg, bool on_device) {
-    cudaStream_t s = g->stream;
-    const uint32_t n = static_cast<uint32_t>(g->n);
-    const unsigned sms = num_sms(g->device);
-    DeviceArray<double> w_tmp, d_tmp;
-    const double *d_w = in_w, *d_wdeg = out_wdeg;
-    if (!on_device) {
-        w_tmp.alloc(std::max<uint64_t>(g->arcs, 1));
-        if (g->arcs)
-            NKG_CUDA(cudaMemcpyAsync(w_tmp.get(), in_w, g->arcs * sizeof(double),
-                                     cudaMemcpyHostToDevice, s));
-        d_w = w_tmp.get();
-        if (out_wdeg) {
-            d_tmp.alloc(g->z);
-            NKG_CUDA(cudaMemcpyAsync(d_tmp.get(), out_wdeg, g->z * sizeof(double),
-                                     cudaMemcpyHostToDevice, s));
-            d_wdeg = d_tmp.get();
-        }
-    }
-    if (g->arcs)
-        scatter_weights<<<sms * 16, 256, 0, s>>>(g->row_ptr.get(), g->row_src.get(), d_w, n,
-                                                 g->w64src.get());
-    NKG_CUDA(cudaGetLastError());
-    if (d_wdeg)
-        permute_wdeg<<<ceil_div(n, 256), 256, 0, s>>>(d_wdeg, g->perm.get(), n,
-                                                     g->degw64src.get());
-    else
-        adjoint_out_wdeg(g, g->degw64src.get());
-    NKG_CUDA(cudaGetLastError());
-    refill_sell_weights(g->fw, n, g->row_ptr.get(), g->w64src.get(), nullptr, g->device, s);
-    if (g->p32.w_sell) {
-        convert_to_float(g->fw.w_sell64.get(), g->p32.w_sell.get(), g->fw.slots, g->device, s);
-        convert_to_float(g->degw64src.get(), g->p32.degw.get(), n, g->device, s);
-    }
-    adjoint_refresh_weights(g);
-    NKG_CUDA(cudaStreamSynchronize(s));
-}
-
 static void ranking_prepare(double *keys, uint32_t *ids, const uint32_t *inv, uint64_t z,
                             cudaStream_t s) {
     ranking_prepare_kernel<<<ceil_div(z, 256), 256, 0, s>>>(keys, ids, inv, z);
@@ -1374,17 +1329,6 @@ int nkg_pagerank_run_ex(nkg_graph *g, const nkg_pr_params *p, const double *tele
     }
     const bool host = (flags & NKG_DEVICE_PTRS) == 0;
     return run_to(g, p, teleport, host, scores_out, host, iterations_out, max_out, stats);
-}
-
-int nkg_graph_set_weights(nkg_graph *g, const double *in_w, const double *out_wdeg, int flags) {
-    return guarded([&] {
-        require(g != nullptr && in_w != nullptr, "NULL argument");
-        require((flags & ~NKG_DEVICE_PTRS) == 0, "unknown flags");
-        require(g->weighted, "the graph was created unweighted (in_w NULL)");
-        require(!g->arc_sorted, "new weights need the in-rows in the caller's order (arc_order 0)");
-        DeviceGuard guard(g->device);
-        set_weights(g, in_w, out_wdeg, (flags & NKG_DEVICE_PTRS) != 0);
-    });
 }
 
 int nkg_ranking(nkg_graph *g, const double *scores, uint64_t *ids_out, double *vals_out) {

@@ -14,7 +14,9 @@
 // differentiable form (OP = 1): the product then runs over the sliced
 // out-adjacency, M^T q = A^T q + [distributeSinks] m (t.q) with
 // (A^T q)[v] = sum_{v->u} w q[u] / wdeg[v]: the vector is gathered as it is
-// (no degree scaling) and every row is scaled after its sum.
+// (no degree scaling) and every row is scaled after its sum. All vectors of an
+// OP 1 solve are indexed in the out-adjacency's row order (degc, degw and tele
+// too), so rows are written in place.
 #pragma once
 
 #include <atomic>
@@ -44,7 +46,6 @@ struct BiArgs {
     const uint32_t *__restrict__ degc;
     const float *__restrict__ degw;
     const float *__restrict__ tele;   // personalised teleport (n) or null
-    const uint32_t *__restrict__ row_label;  // OP 1: node of each out-adjacency row
     float *__restrict__ chunk_val;
     // vectors (x-form, n entries; g is the gather form, n+1 with g[n] = 0;
     // for OP 1, p and s have n+1 entries with p[n] = s[n] = 0 and g is unused)
@@ -161,8 +162,7 @@ __global__ void __launch_bounds__(THREADS) bi_mv(BiArgs a) {
             } else {
                 const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
                 if (r < a.n)
-                    bi_mv_row<WEIGHTED, MODE, OP>(a, OP ? a.row_label[r] : r, acc, px, out, d1,
-                                                  d2);
+                    bi_mv_row<WEIGHTED, MODE, OP>(a, r, acc, px, out, d1, d2);
             }
         }
     }
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kBiThreads) bi_mv_fix(BiArgs a) {
         float acc = 0.f;
         for (uint32_t k = a.chunk_begin[r]; k < a.chunk_begin[r + 1]; ++k)
             acc += a.chunk_val[k];
-        bi_mv_row<WEIGHTED, MODE, OP>(a, OP ? a.row_label[r] : r, acc, px, out, d1, d2);
+        bi_mv_row<WEIGHTED, MODE, OP>(a, r, acc, px, out, d1, d2);
     }
     d1 = block_sum<kBiThreads>(d1, s_red);
     d2 = block_sum<kBiThreads>(d2, s_red);
