@@ -210,6 +210,45 @@ NKG_API int nkg_ppr_run(nkg_graph *g, const nkg_pr_params *p, uint32_t k, const 
                         float *scores_out, int out_on_device, uint64_t *iterations_out,
                         nkg_stats *stats);
 
+/* Many-graph batch, no reference counterpart: `count` independent graphs
+ * (each PageRank.cpp:20-104 on its own: its own n, teleport (1-damp)/n,
+ * residual and stopping test) solved together by one persistent kernel
+ * launch, captured in a CUDA graph. The graphs come as one block-diagonal
+ * in-CSR: graph i owns the node ids [node_offsets[i], node_offsets[i+1]) and
+ * every arc stays inside its graph (checked). Unweighted; all nodes exist.
+ * FP32 runs stop at tol, at max_iterations, or at the FP32 rounding floor (a
+ * residual that shrinks by less than 0.9x in one sweep, which the exact
+ * iteration never does); FP64 runs stop at tol or max_iterations.
+ * The kernel's launch shape comes from nkg_batch_tuning: thread-block
+ * cluster size, threads per CTA, and the row-split threshold (rows longer
+ * than `split` arcs are summed by a whole warp, the others one per lane in
+ * 32-row slices). nkg_batch_tune times `sweeps` sweeps of every graph for
+ * each candidate (split 32..1024, 256 or 512 threads, clusters 1..8) and
+ * keeps the fastest; results (nullable, `capacity` entries) receive every
+ * timed candidate, n_results their count.
+ * nkg_batch_run: scores_out = the total node count of doubles (caller ids,
+ * each graph normalised like PageRank.cpp:75-92), host or device memory
+ * (flags 0 / NKG_DEVICE_PTRS); iterations_out (nullable, host) = count sweep
+ * counts; floor_stops_out (nullable) = graphs stopped at the FP32 floor. */
+typedef struct nkg_batch nkg_batch;
+typedef struct {
+    uint32_t cluster;  /* CTAs per thread-block cluster: 1, 2, 4 or 8 */
+    uint32_t threads;  /* threads per CTA: 128, 256 or 512 */
+    uint32_t split;    /* row-split threshold (arcs) */
+    uint32_t reserved;
+    double ms;         /* nkg_batch_tune: device time of the timed sweeps */
+} nkg_batch_tuning;
+NKG_API int nkg_batch_create(nkg_batch **out, uint32_t count, const uint64_t *node_offsets,
+                             const uint64_t *in_row_ptr, const uint32_t *in_col, int device);
+NKG_API void nkg_batch_destroy(nkg_batch *b);
+NKG_API int nkg_batch_get_tuning(const nkg_batch *b, nkg_batch_tuning *t);
+NKG_API int nkg_batch_set_tuning(nkg_batch *b, const nkg_batch_tuning *t);
+NKG_API int nkg_batch_tune(nkg_batch *b, const nkg_pr_params *p, uint32_t sweeps,
+                           nkg_batch_tuning *results, uint32_t capacity, uint32_t *n_results,
+                           nkg_batch_tuning *best_out);
+NKG_API int nkg_batch_run(nkg_batch *b, const nkg_pr_params *p, double *scores_out, int flags,
+                          uint64_t *iterations_out, uint32_t *floor_stops_out, nkg_stats *stats);
+
 /* Centrality::ranking() (Centrality.cpp:29-41): existing nodes sorted by score
  * descending, ties by node id ascending. scores: host array of z doubles (any
  * scores, e.g. from nkg_pagerank_run); ids_out / vals_out: n entries each. */

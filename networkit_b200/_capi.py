@@ -85,6 +85,15 @@ class GraphOptions(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("cluster", C.c_uint32), ("threads", C.c_uint32), ("split", C.c_uint32),
+                ("reserved", C.c_uint32), ("ms", C.c_double)]
+
+    def as_dict(self):
+        return {"cluster": self.cluster, "threads": self.threads, "split": self.split,
+                "ms": self.ms}
+
+
 _u64p = C.POINTER(C.c_uint64)
 _u32p = C.POINTER(C.c_uint32)
 _u8p = C.POINTER(C.c_uint8)
@@ -119,6 +128,14 @@ SIGNATURES = {
     "nkg_graph_set_weights": (C.c_int, [_vp, _vp, _vp, C.c_int]),
     "nkg_pagerank_adjoint": (C.c_int, [_vp, C.POINTER(PRParams), _vp, _vp, _vp, _vp, _vp, C.c_int,
                                        _u64p, C.POINTER(Stats)]),
+    "nkg_batch_create": (C.c_int, [C.POINTER(_vp), C.c_uint32, _u64p, _u64p, _u32p, C.c_int]),
+    "nkg_batch_destroy": (None, [_vp]),
+    "nkg_batch_get_tuning": (C.c_int, [_vp, C.POINTER(BatchTuning)]),
+    "nkg_batch_set_tuning": (C.c_int, [_vp, C.POINTER(BatchTuning)]),
+    "nkg_batch_tune": (C.c_int, [_vp, C.POINTER(PRParams), C.c_uint32, C.POINTER(BatchTuning),
+                                 C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(BatchTuning)]),
+    "nkg_batch_run": (C.c_int, [_vp, C.POINTER(PRParams), _vp, C.c_int, _u64p,
+                                C.POINTER(C.c_uint32), C.POINTER(Stats)]),
 }
 
 _lib = None
@@ -318,3 +335,66 @@ class DeviceGraph:
         check(lib().nkg_profile_sweeps(self.h, int(precision), int(sweeps), C.byref(a),
                                        C.byref(b)))
         return float(a.value), float(b.value)
+
+
+class DeviceBatch:
+    """Owning wrapper of an nkg_batch handle: many graphs given as one
+    block-diagonal in-CSR plus node_offsets (graph i = nodes
+    [node_offsets[i], node_offsets[i+1]))."""
+
+    def __init__(self, csr, node_offsets, device: int = -1):
+        L = lib()
+        h = _vp()
+        offs = np.ascontiguousarray(node_offsets, np.uint64)
+        in_ptr = np.ascontiguousarray(csr.in_ptr, np.uint64)
+        in_col = np.ascontiguousarray(csr.in_col, np.uint32)
+        check(L.nkg_batch_create(C.byref(h), int(offs.shape[0] - 1), ptr(offs, _u64p),
+                                 ptr(in_ptr, _u64p), ptr(in_col, _u32p), int(device)))
+        self.h = h
+        self.count = int(offs.shape[0] - 1)
+        self.total = int(offs[-1])
+        self.node_offsets = offs
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().nkg_batch_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def tuning(self) -> dict:
+        t = BatchTuning()
+        check(lib().nkg_batch_get_tuning(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, cluster: int, threads: int, split: int):
+        t = BatchTuning(int(cluster), int(threads), int(split), 0, 0.0)
+        check(lib().nkg_batch_set_tuning(self.h, C.byref(t)))
+
+    def tune(self, p: PRParams, sweeps: int = 8, capacity: int = 64):
+        """Time every candidate launch shape; returns (best, [all timed])."""
+        res = (BatchTuning * capacity)()
+        nres = C.c_uint32(0)
+        best = BatchTuning()
+        check(lib().nkg_batch_tune(self.h, C.byref(p), int(sweeps), res, capacity, C.byref(nres),
+                                   C.byref(best)))
+        return best.as_dict(), [res[i].as_dict() for i in range(min(nres.value, capacity))]
+
+    def run(self, p: PRParams, d_out_ptr: int = 0):
+        """Returns (scores float64[total] or None when written to d_out_ptr,
+        iterations uint64[count], floor_stops, stats)."""
+        its = np.zeros(self.count, np.uint64)
+        fl = C.c_uint32(0)
+        st = Stats()
+        if d_out_ptr:
+            check(lib().nkg_batch_run(self.h, C.byref(p), _vp(d_out_ptr), NKG_DEVICE_PTRS,
+                                      ptr(its, _u64p), C.byref(fl), C.byref(st)))
+            return None, its, int(fl.value), st.as_dict()
+        out = np.empty(self.total, np.float64)
+        check(lib().nkg_batch_run(self.h, C.byref(p), _vp(out.ctypes.data), 0, ptr(its, _u64p),
+                                  C.byref(fl), C.byref(st)))
+        return out, its, int(fl.value), st.as_dict()

@@ -17,6 +17,13 @@ constexpr uint32_t kUnitsPerWarp = 8;
 // epilogue of its 32 rows).
 constexpr uint32_t kSliceOverhead = 3;
 
+// Work buffers of the FP32 refinement solve, kept between runs.
+struct RefineWork {
+    DeviceArray<float> x, r, rhat, p, v, s, t, g;  // g: n+1 (gather form, g[n] = 0)
+    DeviceArray<double> x64, part, fix_part;
+    DeviceArray<unsigned char> sc;                  // BiScalars
+};
+
 // Sliced layout (SELL-32 with chunked long rows, see sweep.cuh) of one
 // adjacency: the in-adjacency for the forward sweeps, the out-adjacency for
 // the adjoint.
@@ -95,6 +102,7 @@ struct nkg_graph {
 
     nkg::Plane<double> p64;
     nkg::Plane<float> p32;
+    nkg::RefineWork refine_work;
 
     nkg::DeviceArray<double> cta_res, cta_sink, fix_res, fix_sink;
     nkg::DeviceArray<double> out_buf;    // scores staging for host output (z)

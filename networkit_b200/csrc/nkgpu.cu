@@ -1009,15 +1009,28 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
         permute_teleport<float><<<ceil_div(n, 256), 256, 0, s>>>(d_tele, g->perm.get(),
                                                                  n, P32.tele.get());
     }
-    DeviceArray<float> bx(n), br(n), brhat(n), bp(n), bv(n), bs(n), bt(n), bg(n + 1, 4);
-    DeviceArray<double> x64(n);
     const unsigned vec_ctas = std::max<unsigned>(1, std::min<unsigned>(sms * 4, ceil_div(n, kBiThreads)));
+    RefineWork &W = g->refine_work;
+    if (!W.x64) {
+        for (auto *v : {&W.x, &W.r, &W.rhat, &W.p, &W.v, &W.s, &W.t})
+            v->alloc(n);
+        W.g.alloc(n + 1, 4);
+        W.x64.alloc(n);
+        W.sc.alloc(sizeof(BiScalars));
+        NKG_CUDA(cudaMemsetAsync(W.g.get(), 0, (n + 1 + 4) * sizeof(float), s));
+    }
+    const size_t part_n = 2 * static_cast<size_t>(std::max<unsigned>(P32.sweep_ctas, vec_ctas));
+    if (W.part.size() < part_n)
+        W.part.alloc(part_n);
+    DeviceArray<float> &bx = W.x, &br = W.r, &brhat = W.rhat, &bp = W.p, &bv = W.v, &bs = W.s,
+                       &bt = W.t, &bg = W.g;
+    DeviceArray<double> &x64 = W.x64, &part = W.part;
     const unsigned fix_ctas = std::max<unsigned>(1, ceil_div(g->fw.n_long, kBiThreads));
-    DeviceArray<double> part(2 * static_cast<size_t>(std::max<unsigned>(P32.sweep_ctas, vec_ctas)));
-    DeviceArray<double> fix_part(2 * static_cast<size_t>(fix_ctas));
-    DeviceArray<BiScalars> sc(1);
-    NKG_CUDA(cudaMemsetAsync(sc.get(), 0, sizeof(BiScalars), s));
-    NKG_CUDA(cudaMemsetAsync(bg.get(), 0, (n + 1 + 4) * sizeof(float), s));
+    if (W.fix_part.size() < 2 * static_cast<size_t>(fix_ctas))
+        W.fix_part.alloc(2 * static_cast<size_t>(fix_ctas));
+    DeviceArray<double> &fix_part = W.fix_part;
+    BiScalars *scp = reinterpret_cast<BiScalars *>(W.sc.get());
+    NKG_CUDA(cudaMemsetAsync(scp, 0, sizeof(BiScalars), s));
     BiArgs a{};
     a.col_sell = g->fw.col_sell.get();
     a.w_sell = P32.w_sell.get();
@@ -1038,7 +1051,7 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
     a.g = bg.get();
     a.part = part.get();
     a.fix_part = fix_part.get();
-    a.sc = sc.get();
+    a.sc = scp;
     a.damp = p.damp;
     a.inv_n = 1.0 / static_cast<double>(n);
     a.n = n;
@@ -1059,7 +1072,7 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
     bl.sweep_ctas = P32.sweep_ctas;
     bl.vec_ctas = vec_ctas;
     bl.fix_ctas = fix_ctas;
-    bl.d_sc = sc.get();
+    bl.d_sc = scp;
     bl.h_sc = hsc;
     bl.cancel = &g->cancel;
     // Solve (I - dM) x = r (r holds the right-hand side).
@@ -1078,7 +1091,7 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
         NKG_CUDA(cudaMemcpyAsync(g->st.get(), sh, sizeof(IterState), cudaMemcpyHostToDevice, s));
         bi_to_fp64<WEIGHTED><<<vec_ctas, kBiThreads, 0, s>>>(
             bx.get(), x64.get(), P64.y[0].get(), g->degc.get(), degw64, n, add, part.get(),
-            g->st.get(), &sc.get()->ticket, a.distribute, personal);
+            g->st.get(), &scp->ticket, a.distribute, personal);
         NKG_CUDA(cudaGraphLaunch(exec, s));
         R.launches += 1 + 2 * kSweepsPerGraph;
         ++fp64;

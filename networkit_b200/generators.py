@@ -10,6 +10,9 @@ graph on any machine and thread count.
 * :func:`erdos_renyi` - undirected G(n, p) (ErdosRenyiGenerator shape).
 * :func:`barabasi_albert` - undirected preferential attachment
   (BarabasiAlbertGenerator shape, Batagelj variant).
+* :func:`hyperbolic`, :func:`hyperbolic_batch` - undirected threshold random
+  hyperbolic graphs (HyperbolicGenerator shape at temperature 0: average
+  degree and power-law exponent given).
 """
 from __future__ import annotations
 
@@ -48,6 +51,11 @@ def _load():
         L.nkgen_erdos_renyi.argtypes = [C.c_uint64, C.c_double, C.c_uint64, C.c_int,
                                         C.POINTER(_Csr)]
         L.nkgen_barabasi_albert.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(_Csr)]
+        L.nkgen_hyperbolic.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_uint64,
+                                       C.POINTER(_Csr)]
+        L.nkgen_hyperbolic_batch.argtypes = [C.c_uint64, C.POINTER(C.c_uint64), C.c_double,
+                                             C.c_double, C.c_uint64, C.c_int, C.POINTER(_Csr),
+                                             C.POINTER(C.c_uint64)]
         _lib = L
     return _lib
 
@@ -90,6 +98,32 @@ def barabasi_albert(k: int, n: int, seed: int = 42) -> InCSR:
     out = _Csr()
     _check(_load().nkgen_barabasi_albert(int(k), int(n), int(seed), C.byref(out)))
     return _take(out, False)
+
+
+def hyperbolic(n: int, avg_deg: float = 16.0, exponent: float = 3.0, seed: int = 42) -> InCSR:
+    """Undirected random hyperbolic graph, threshold model: n points in a
+    hyperbolic disc whose radius gives expected average degree avg_deg,
+    radial density exponent-dependent (alpha = (exponent - 1) / 2), edges
+    between points at distance <= the radius."""
+    out = _Csr()
+    _check(_load().nkgen_hyperbolic(int(n), float(avg_deg), float(exponent), int(seed),
+                                    C.byref(out)))
+    return _take(out, False)
+
+
+def hyperbolic_batch(ns, avg_deg: float = 16.0, exponent: float = 3.0, seed: int = 42,
+                     nthreads: int = 0):
+    """len(ns) hyperbolic graphs (graph i with ns[i] nodes and seed + i) as one
+    block-diagonal InCSR plus node_offsets (graph i = nodes
+    [node_offsets[i], node_offsets[i+1]))."""
+    ns = np.ascontiguousarray(ns, np.uint64)
+    offs = np.zeros(ns.shape[0] + 1, np.uint64)
+    out = _Csr()
+    _check(_load().nkgen_hyperbolic_batch(
+        int(ns.shape[0]), ns.ctypes.data_as(C.POINTER(C.c_uint64)), float(avg_deg),
+        float(exponent), int(seed), int(nthreads), C.byref(out),
+        offs.ctypes.data_as(C.POINTER(C.c_uint64))))
+    return _take(out, False), offs
 
 
 def with_uniform_weights(csr: InCSR, seed: int = 43, low: float = 0.1, high: float = 1.0) -> InCSR:

@@ -62,6 +62,31 @@ class InCSR:
         return out_ptr, out_col.astype(np.uint32), order.astype(np.uint64)
 
 
+def concat_in_csr(csrs):
+    """Block-diagonal union of unweighted in-CSRs without deleted nodes (the
+    input of the many-graph batch): graph i's node v becomes
+    node_offsets[i] + v. Returns (InCSR, node_offsets uint64[len + 1])."""
+    offs = np.zeros(len(csrs) + 1, np.uint64)
+    for i, c in enumerate(csrs):
+        if c.exists is not None and not np.all(c.exists):
+            raise ValueError("graphs of a batch must not have deleted nodes")
+        offs[i + 1] = offs[i] + np.uint64(c.z)
+    arc_offs = np.cumsum([0] + [c.arcs for c in csrs]).astype(np.uint64)
+    z = int(offs[-1])
+    in_ptr = np.empty(z + 1, np.uint64)
+    in_col = np.empty(int(arc_offs[-1]), np.uint32)
+    outdeg = np.empty(z, np.uint32)
+    for i, c in enumerate(csrs):
+        a, b = int(offs[i]), int(offs[i + 1])
+        in_ptr[a:b] = c.in_ptr[:-1].astype(np.uint64) + arc_offs[i]
+        in_col[int(arc_offs[i]):int(arc_offs[i + 1])] = c.in_col.astype(np.uint64) + offs[i]
+        outdeg[a:b] = c.outdeg
+    in_ptr[z] = arc_offs[-1]
+    directed = any(c.directed for c in csrs)
+    return InCSR(z, z, in_ptr, in_col, None, outdeg.astype(np.float64), outdeg, None,
+                 directed), offs
+
+
 def in_csr_from_edges(z, src, dst, w=None, directed=False, exists=None) -> InCSR:
     """Build the in-CSR of a graph whose edges were inserted in the given
     order (Graph::addEdge, Graph.cpp:549-596)."""

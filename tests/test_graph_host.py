@@ -120,3 +120,39 @@ def test_capi_library_exports_every_header_symbol():
     assert set(syms) <= set(_capi.SIGNATURES), "every header symbol has a ctypes signature"
     L = _capi.lib()
     assert L.nkg_abi_version() == 1
+
+
+def test_hyperbolic_generator_shape():
+    """Threshold random hyperbolic graphs: symmetric, no self-loops, average
+    degree at the target in expectation, independent of the thread count in
+    batch form, and the batch equals the graphs generated one by one."""
+    degs = [generators.hyperbolic(20000, 16, 3, seed=s).arcs / 20000 for s in range(8)]
+    assert abs(np.mean(degs) - 16.0) < 0.6
+    c = generators.hyperbolic(5000, 16, 3, seed=9)
+    rows = np.repeat(np.arange(c.z, dtype=np.int64), np.diff(c.in_ptr).astype(np.int64))
+    assert not np.any(rows == c.in_col)
+    fwd = np.sort(rows * c.z + c.in_col)
+    bwd = np.sort(c.in_col.astype(np.int64) * c.z + rows)
+    np.testing.assert_array_equal(fwd, bwd)
+    ns = [300, 2000, 900]
+    b1, offs = generators.hyperbolic_batch(ns, 16, 3, seed=42, nthreads=1)
+    b4, offs4 = generators.hyperbolic_batch(ns, 16, 3, seed=42, nthreads=4)
+    np.testing.assert_array_equal(b1.in_col, b4.in_col)
+    np.testing.assert_array_equal(offs, offs4)
+    for i, n in enumerate(ns):
+        g = generators.hyperbolic(n, 16, 3, seed=42 + i)
+        a, b = int(offs[i]), int(offs[i + 1])
+        np.testing.assert_array_equal(b1.in_ptr[a:b + 1] - b1.in_ptr[a], g.in_ptr)
+        np.testing.assert_array_equal(b1.in_col[b1.in_ptr[a]:b1.in_ptr[b]] - a, g.in_col)
+
+
+def test_concat_in_csr_block_diagonal():
+    from networkit_b200.graph import concat_in_csr
+    gs = [generators.rmat_directed(5, 4, seed=s) for s in range(3)]
+    csr, offs = concat_in_csr(gs)
+    assert csr.z == sum(g.z for g in gs) and csr.arcs == sum(g.arcs for g in gs)
+    for i, g in enumerate(gs):
+        a, b = int(offs[i]), int(offs[i + 1])
+        np.testing.assert_array_equal(csr.in_ptr[a:b + 1] - csr.in_ptr[a], g.in_ptr)
+        seg = csr.in_col[csr.in_ptr[a]:csr.in_ptr[b]]
+        assert seg.min() >= a and seg.max() < b
