@@ -50,6 +50,8 @@ def parse_args():
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the companion forms (refine, ppr, adjoint, batch) of the default line")
     ap.add_argument("--profile-only", type=int, default=0, metavar="SWEEPS",
                     help="only upload the graph and run SWEEPS individually launched sweeps "
                          "(the small, fixed launch sequence used for ncu captures)")
@@ -59,7 +61,7 @@ def parse_args():
                     help="sweep launch shape (nkg_graph_options.sweep_shape; -1 default)")
     ap.add_argument("--arc-order", type=int, default=0, choices=[0, 1],
                     help="nkg_graph_options.arc_order (0 keep the reference order, 1 sorted)")
-    ap.add_argument("--form", default="", choices=["", "ppr", "refine", "adjoint"],
+    ap.add_argument("--form", default="", choices=["", "ppr", "refine", "adjoint", "batch"],
                     help="run only one companion form and print its figures")
     ap.add_argument("--fd-edges", type=int, default=64,
                     help="arcs checked by finite differences in --form adjoint")
@@ -217,8 +219,31 @@ def form_ppr(local, n=4_000_000, m=8, k=256, steps=2):
         col_sweeps = int(its.sum())
     bytes_sweep = st["bytes_per_sweep_fp32"]
     per_sweep_ms = ms / sweeps
+    # Against the plain FP64 path: one personalised FP64 run per seed
+    # (nkg_pagerank_run_device with a one-hot teleport), timed on a sample of
+    # seeds and scaled to k; the L1 error of those columns against it.
+    sample = list(range(0, k, k // 8))
+    scores = out.cpu().numpy()
+    p64 = dg.params(0.85, 1e-7, NORM_L1, False, False, _capi.NKG_PREC_FP64, 1000)
+    ref = dg.params(0.85, 1e-12, NORM_L1, False, False, _capi.NKG_PREC_FP64, 1000)
+    d_t = torch.zeros(csr.z, dtype=torch.float64, device=f"cuda:{local}")
+    d_o = torch.empty(csr.z, dtype=torch.float64, device=f"cuda:{local}")
+    plain_ms, errs = 0.0, []
+    for j in sample:
+        d_t.zero_()
+        d_t[int(seeds[j])] = 1.0
+        torch.cuda.synchronize()
+        dg.run_ex(p64, d_t.data_ptr(), d_o.data_ptr(), True)  # warm-up (graph capture)
+        _, _, st64 = dg.run_ex(p64, d_t.data_ptr(), d_o.data_ptr(), True)
+        plain_ms += st64["ms_total"]
+        dg.run_ex(ref, d_t.data_ptr(), d_o.data_ptr(), True)
+        errs.append(float(np.abs(scores[j].astype(np.float64) - d_o.cpu().numpy()).sum()))
+    plain_ms *= k / len(sample)
     dg.close()
     return {"workload": f"ppr_ba{n}_m{m}_k{k}_fp32", "n": csr.z, "arcs": csr.arcs, "k": k,
+            "plain_fp64_per_seed_ms": plain_ms, "plain_seeds_timed": len(sample),
+            "speedup_vs_plain_fp64": plain_ms / (ms / steps),
+            "l1_err_max_vs_fp64": max(errs),
             "sweeps": sweeps // steps, "column_sweeps": col_sweeps, "ms_per_run": ms / steps,
             "ms_per_sweep": per_sweep_ms,
             "gteps_per_iter": csr.arcs * k / (per_sweep_ms / 1e3) / 1e9,
@@ -384,6 +409,93 @@ def form_adjoint(local, scale=22, steps=3, fd_edges=64, only_step=False):
     return res
 
 
+def form_batch(local, count=1024, steps=3, plain_graphs=None):
+    """Many-graph batch: 1024 random hyperbolic graphs, n_i log-uniform in
+    [1e3, 2e5] (numpy seed 42), average degree 16, exponent 3, graph i from
+    seed 42 + i; FP32, damp 0.85, tol 1e-8 (L1), one persistent launch in a
+    CUDA graph with the autotuned launch shape. Against it: the plain FP64
+    path run graph by graph (nkg_pagerank_run_device on every graph, the
+    graphs already resident), and the FP64 batch for the error figures (the
+    FP64 batch is parity-tested against the oracle)."""
+    import torch
+
+    from networkit_b200 import _capi, generators
+    from networkit_b200.graph import InCSR
+
+    rng = np.random.default_rng(42)
+    ns = np.round(np.exp(rng.uniform(np.log(1e3), np.log(2e5), count))).astype(np.uint64)
+    t0 = time.perf_counter()
+    csr, offs = generators.hyperbolic_batch(ns, 16.0, 3.0, seed=42)
+    t_gen = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    db = _capi.DeviceBatch(csr, offs, device=local)
+    t_create = time.perf_counter() - t0
+    arcs_g = np.array([int(csr.in_ptr[int(offs[i + 1])] - csr.in_ptr[int(offs[i])])
+                       for i in range(count)], np.float64)
+    n_g = np.diff(offs).astype(np.float64)
+    p32 = _capi.PRParams(DAMP, 1e-8, NORM_L1, 0, 0, _capi.NKG_PREC_FP32, 10000)
+    p64 = _capi.PRParams(DAMP, 1e-8, NORM_L1, 0, 0, _capi.NKG_PREC_FP64, 10000)
+    t0 = time.perf_counter()
+    best, table = db.tune(p32, sweeps=8)
+    t_tune = time.perf_counter() - t0
+    dev = torch.device("cuda", local)
+    out = torch.empty(db.total, dtype=torch.float64, device=dev)
+    db.run(p32, out.data_ptr())  # warm-up
+    ms, its, floor = [], None, 0
+    for _ in range(steps):
+        _, its, floor, st = db.run(p32, out.data_ptr())
+        ms.append(st["ms_total"])
+    ms32 = statistics.median(ms)
+    s32 = out.cpu().numpy()
+    # e2e through the C ABI: host scores out, the graphs resident
+    t0 = time.perf_counter()
+    h32, _, _, _ = db.run(p32)
+    e2e_ms = 1e3 * (time.perf_counter() - t0)
+    _, its64, _, st64 = db.run(p64, out.data_ptr())
+    ms64_batch = st64["ms_total"]
+    ref = _capi.PRParams(DAMP, 1e-13, NORM_L1, 0, 0, _capi.NKG_PREC_FP64, 10000)
+    db.run(ref, out.data_ptr())
+    s_ref = out.cpu().numpy()
+    errs = np.array([np.abs(s32[int(offs[i]):int(offs[i + 1])] -
+                            s_ref[int(offs[i]):int(offs[i + 1])]).sum() for i in range(count)])
+    sweeps = its.astype(np.float64)
+    arc_it = float((arcs_g * sweeps).sum())
+    alg_bytes = float(((4 * arcs_g + 20 * n_g + 4) * sweeps).sum())
+    db.close()
+    # Plain FP64 path, graph by graph (each graph uploaded beforehand).
+    idx = list(range(count)) if plain_graphs is None else list(plain_graphs)
+    plain_ms = 0.0
+    pin = _capi.PRParams(DAMP, 1e-8, NORM_L1, 0, 0, _capi.NKG_PREC_FP64, 10000)
+    for i in idx:
+        a, b = int(offs[i]), int(offs[i + 1])
+        ptr = (csr.in_ptr[a:b + 1] - csr.in_ptr[a]).astype(np.uint64)
+        col = (csr.in_col[int(csr.in_ptr[a]):int(csr.in_ptr[b])] - np.uint32(a)).astype(np.uint32)
+        g = InCSR(b - a, b - a, ptr, col, None, csr.wdeg[a:b], csr.outdeg[a:b], None, False)
+        dg = _capi.DeviceGraph(g, device=local)
+        o = torch.empty(b - a, dtype=torch.float64, device=dev)
+        dg.run_device(pin, o.data_ptr())  # warm-up (sweep graph capture)
+        _, _, st = dg.run_device(pin, o.data_ptr())
+        plain_ms += st["ms_total"]
+        dg.close()
+    plain_ms *= count / len(idx)
+    peak, peak_kind = measured_peak_hbm()
+    return {"workload": f"batch_hyperbolic{count}_fp32", "graphs": count,
+            "nodes": int(offs[-1]), "arcs": int(csr.arcs), "gen_s": t_gen, "create_s": t_create,
+            "tune_s": t_tune, "tuning": best, "tuning_candidates": len(table),
+            "tuning_table_top": sorted(table, key=lambda t: t["ms"])[:6],
+            "fp32_ms": ms32, "fp32_sweeps_total": int(sweeps.sum()),
+            "fp32_sweeps_max": int(sweeps.max()), "fp32_floor_stops": floor,
+            "gteps_per_iter": arc_it / (ms32 / 1e3) / 1e9,
+            "alg_gbs": alg_bytes / (ms32 / 1e3) / 1e9, "alg_frac_of_hbm": alg_bytes / (ms32 / 1e3) / 1e9 / peak,
+            "peak_source": peak_kind,
+            "fp32_l1_err_max": float(errs.max()), "fp32_l1_err_median": float(np.median(errs)),
+            "e2e_ms_host_scores": e2e_ms,
+            "fp64_batch_ms": ms64_batch, "plain_fp64_per_graph_ms": plain_ms,
+            "plain_graphs_timed": len(idx),
+            "speedup_vs_plain_fp64": plain_ms / ms32,
+            "speedup_fp64_batch_vs_plain_fp64": plain_ms / ms64_batch}
+
+
 def run_reference_arm(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -442,6 +554,9 @@ def main():
     torch.cuda.set_device(local)
     if args.form == "ppr":
         print(json.dumps(form_ppr(local)))
+        return
+    if args.form == "batch":
+        print(json.dumps(form_batch(local)))
         return
     if args.form == "adjoint":
         print(json.dumps(form_adjoint(local, fd_edges=args.fd_edges,
@@ -540,6 +655,21 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(csr, os.cpu_count() or 1)
+    dg.close()
+
+    # Companion forms, each against the plain FP64 GPU path on the same GPU.
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        forms = {}
+        for name, fn in (("fp32_refine", lambda: form_refine(local, csr, steps=1)),
+                         ("ppr", lambda: form_ppr(local, steps=1)),
+                         ("fwd_bwd", lambda: form_adjoint(local, steps=2, fd_edges=0)),
+                         ("batch", lambda: form_batch(local, steps=2,
+                                                      plain_graphs=range(0, 1024, 8)))):
+            try:
+                forms[name] = fn()
+            except Exception as e:  # a form that fails is reported, not fatal
+                forms[name] = {"error": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
         line = {
@@ -566,8 +696,9 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
+        if forms is not None:
+            line["forms"] = forms
         print(json.dumps(line))
-    dg.close()
     if world > 1:
         import torch.distributed as dist
 
