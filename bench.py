@@ -67,6 +67,11 @@ def parse_args():
                     help="arcs checked by finite differences in --form adjoint")
     ap.add_argument("--adjoint-step-only", action="store_true",
                     help="--form adjoint: only the reference solves and one timed breakdown")
+    ap.add_argument("--adjoint-scale", type=int, default=22, help="R-MAT scale of --form adjoint")
+    ap.add_argument("--batch-graphs", type=int, default=1024, help="graphs of --form batch")
+    ap.add_argument("--batch-step-only", action="store_true",
+                    help="--form batch: no tuning and no comparison, two runs with the default "
+                         "launch shape (the short launch sequence used for ncu captures)")
     ap.add_argument("--cache", default=os.path.join(tempfile.gettempdir(), "nk_b200_graphs"))
     return ap.parse_args()
 
@@ -409,7 +414,7 @@ def form_adjoint(local, scale=22, steps=3, fd_edges=64, only_step=False):
     return res
 
 
-def form_batch(local, count=1024, steps=3, plain_graphs=None):
+def form_batch(local, count=1024, steps=3, plain_graphs=None, step_only=False):
     """Many-graph batch: 1024 random hyperbolic graphs, n_i log-uniform in
     [1e3, 2e5] (numpy seed 42), average degree 16, exponent 3, graph i from
     seed 42 + i; FP32, damp 0.85, tol 1e-8 (L1), one persistent launch in a
@@ -435,6 +440,17 @@ def form_batch(local, count=1024, steps=3, plain_graphs=None):
     n_g = np.diff(offs).astype(np.float64)
     p32 = _capi.PRParams(DAMP, 1e-8, NORM_L1, 0, 0, _capi.NKG_PREC_FP32, 10000)
     p64 = _capi.PRParams(DAMP, 1e-8, NORM_L1, 0, 0, _capi.NKG_PREC_FP64, 10000)
+    if step_only:
+        dev = torch.device("cuda", local)
+        out = torch.empty(db.total, dtype=torch.float64, device=dev)
+        db.run(p32, out.data_ptr())
+        _, its, floor, st = db.run(p32, out.data_ptr())
+        tuning = db.tuning()
+        db.close()
+        return {"workload": f"batch_hyperbolic{count}_fp32", "graphs": count,
+                "nodes": int(offs[-1]), "arcs": int(csr.arcs), "tuning": tuning,
+                "fp32_ms": st["ms_total"], "fp32_sweeps_total": int(its.sum()),
+                "fp32_floor_stops": floor}
     t0 = time.perf_counter()
     best, table = db.tune(p32, sweeps=8)
     t_tune = time.perf_counter() - t0
@@ -556,10 +572,11 @@ def main():
         print(json.dumps(form_ppr(local)))
         return
     if args.form == "batch":
-        print(json.dumps(form_batch(local)))
+        print(json.dumps(form_batch(local, count=args.batch_graphs,
+                                    step_only=args.batch_step_only)))
         return
     if args.form == "adjoint":
-        print(json.dumps(form_adjoint(local, fd_edges=args.fd_edges,
+        print(json.dumps(form_adjoint(local, scale=args.adjoint_scale, fd_edges=args.fd_edges,
                                       only_step=args.adjoint_step_only)))
         return
     if world > 1:
