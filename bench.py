@@ -462,6 +462,7 @@ def form_batch(local, count=1024, steps=3, plain_graphs=None, step_only=False):
         _, its, floor, st = db.run(p32, out.data_ptr())
         ms.append(st["ms_total"])
     ms32 = statistics.median(ms)
+    g_start, g_end = db.graph_times()
     s32 = out.cpu().numpy()
     # e2e through the C ABI: host scores out, the graphs resident
     t0 = time.perf_counter()
@@ -500,6 +501,9 @@ def form_batch(local, count=1024, steps=3, plain_graphs=None, step_only=False):
             "tune_s": t_tune, "tuning": best, "tuning_candidates": len(table),
             "tuning_table_top": sorted(table, key=lambda t: t["ms"])[:6],
             "fp32_ms": ms32, "fp32_sweeps_total": int(sweeps.sum()),
+            "critical_graph_ms": float((g_end - g_start).max()),
+            "last_graph_end_ms": float(g_end.max()),
+            "graph_busy_ms_sum": float((g_end - g_start).sum()),
             "fp32_sweeps_max": int(sweeps.max()), "fp32_floor_stops": floor,
             "gteps_per_iter": arc_it / (ms32 / 1e3) / 1e9,
             "alg_gbs": alg_bytes / (ms32 / 1e3) / 1e9, "alg_frac_of_hbm": alg_bytes / (ms32 / 1e3) / 1e9 / peak,

@@ -223,7 +223,7 @@ NKG_API int nkg_ppr_run(nkg_graph *g, const nkg_pr_params *p, uint32_t k, const 
  * cluster size, threads per CTA, and the row-split threshold (rows longer
  * than `split` arcs are summed by a whole warp, the others one per lane in
  * 32-row slices). nkg_batch_tune times `sweeps` sweeps of every graph for
- * each candidate (split 32..1024, 256 or 512 threads, clusters 1..8) and
+ * each candidate (split 32..1024, 256 or 512 threads, clusters 1..16) and
  * keeps the fastest; results (nullable, `capacity` entries) receive every
  * timed candidate, n_results their count.
  * nkg_batch_run: scores_out = the total node count of doubles (caller ids,
@@ -232,7 +232,7 @@ NKG_API int nkg_ppr_run(nkg_graph *g, const nkg_pr_params *p, uint32_t k, const 
  * counts; floor_stops_out (nullable) = graphs stopped at the FP32 floor. */
 typedef struct nkg_batch nkg_batch;
 typedef struct {
-    uint32_t cluster;  /* CTAs per thread-block cluster: 1, 2, 4 or 8 */
+    uint32_t cluster;  /* CTAs per thread-block cluster: 1, 2, 4, 8 or 16 */
     uint32_t threads;  /* threads per CTA: 128, 256 or 512 */
     uint32_t split;    /* row-split threshold (arcs) */
     uint32_t reserved;
@@ -248,6 +248,10 @@ NKG_API int nkg_batch_tune(nkg_batch *b, const nkg_pr_params *p, uint32_t sweeps
                            nkg_batch_tuning *best_out);
 NKG_API int nkg_batch_run(nkg_batch *b, const nkg_pr_params *p, double *scores_out, int flags,
                           uint64_t *iterations_out, uint32_t *floor_stops_out, nkg_stats *stats);
+/* Diagnostic: when each graph of the last run (or tuning launch) started and
+ * converged, in ms from the earliest start (device global timer); count
+ * entries each. */
+NKG_API int nkg_batch_graph_times(nkg_batch *b, double *start_ms, double *end_ms);
 
 /* Centrality::ranking() (Centrality.cpp:29-41): existing nodes sorted by score
  * descending, ties by node id ascending. scores: host array of z doubles (any

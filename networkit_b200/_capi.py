@@ -136,6 +136,7 @@ SIGNATURES = {
                                  C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(BatchTuning)]),
     "nkg_batch_run": (C.c_int, [_vp, C.POINTER(PRParams), _vp, C.c_int, _u64p,
                                 C.POINTER(C.c_uint32), C.POINTER(Stats)]),
+    "nkg_batch_graph_times": (C.c_int, [_vp, _f64p, _f64p]),
 }
 
 _lib = None
@@ -383,6 +384,13 @@ class DeviceBatch:
         check(lib().nkg_batch_tune(self.h, C.byref(p), int(sweeps), res, capacity, C.byref(nres),
                                    C.byref(best)))
         return best.as_dict(), [res[i].as_dict() for i in range(min(nres.value, capacity))]
+
+    def graph_times(self):
+        """(start_ms, end_ms) of every graph in the last launch."""
+        a = np.empty(self.count, np.float64)
+        b = np.empty(self.count, np.float64)
+        check(lib().nkg_batch_graph_times(self.h, ptr(a, _f64p), ptr(b, _f64p)))
+        return a, b
 
     def run(self, p: PRParams, d_out_ptr: int = 0):
         """Returns (scores float64[total] or None when written to d_out_ptr,

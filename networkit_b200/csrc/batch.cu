@@ -49,7 +49,7 @@ namespace cg = cooperative_groups;
 namespace nkg {
 namespace {
 
-constexpr int kMaxCluster = 8;
+constexpr unsigned kMaxCluster = 16;  // 16 is above the portable 8: opted in per kernel
 
 struct BatchParams {
     double damp;
@@ -87,6 +87,7 @@ struct BatchArgs {
     double *out;                              // scores, caller ids
     unsigned long long *iterations;           // per graph
     double *residual;                         // per graph
+    unsigned long long *times;                // per graph: start and end (global timer, ns)
     unsigned int *queue;                      // next queue position
     unsigned int *floor_stops;                // graphs stopped at the FP32 floor
     const BatchParams *prm;
@@ -101,6 +102,12 @@ struct ClusterShared {
     int done;
     double sink_coef, sumx, sink, res;
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
 
 template <typename T>
 __device__ __forceinline__ T ld_iter(const T *p) {
@@ -157,6 +164,8 @@ __global__ void __launch_bounds__(THREADS) batch_kernel(BatchArgs<T> a) {
         }
         const uint32_t gi = a.order[q];
         const GraphMeta m = a.meta[gi];
+        if (crank == 0 && threadIdx.x == 0)
+            a.times[2 * gi] = global_ns();
         const T tele = static_cast<T>((1.0 - prm.damp) / static_cast<double>(m.n));
         // x = 1/n in gather form (PageRank.cpp:26)
         const T x0 = static_cast<T>(1.0 / static_cast<double>(m.n));
@@ -264,6 +273,7 @@ __global__ void __launch_bounds__(THREADS) batch_kernel(BatchArgs<T> a) {
                 sh.sink = t2;
                 sh.sink_coef = prm.distribute ? t2 / static_cast<double>(m.n) : 0.0;
                 if (done && crank == 0) {
+                    a.times[2 * gi + 1] = global_ns();
                     a.iterations[gi] = done_it;
                     a.residual[gi] = norm;
                     if (at_floor)
@@ -461,6 +471,7 @@ struct nkg_batch {
     DeviceArray<double> y64[2];
     DeviceArray<double> out_buf, residual;
     DeviceArray<unsigned long long> iterations;
+    DeviceArray<unsigned long long> times;     // per graph: start, end (ns)
     DeviceArray<unsigned int> counters;        // queue, floor stops
     DeviceArray<BatchParams> prm;
     PinnedHost<BatchParams> prm_h;
@@ -538,6 +549,13 @@ bool batch_launch(nkg_batch *b, const nkg_batch_tuning &t, T *y0, T *y1, double 
     with_batch_threads(t.threads, [&](auto TH) {
         constexpr int threads = decltype(TH)::value;
         auto kfn = batch_kernel<T, threads, kBatchUnroll>;
+        if (t.cluster > 8 &&
+            cudaFuncSetAttribute(kfn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            ok = false;
+            return;
+        }
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -573,6 +591,7 @@ bool batch_launch(nkg_batch *b, const nkg_batch_tuning &t, T *y0, T *y1, double 
         a.out = out;
         a.iterations = b->iterations.get();
         a.residual = b->residual.get();
+        a.times = b->times.get();
         a.queue = b->counters.get();
         a.floor_stops = b->counters.get() + 1;
         a.prm = b->prm.get();
@@ -748,6 +767,7 @@ nkg_batch *batch_create(uint32_t count, const uint64_t *node_off, const uint64_t
     b->out_buf.alloc(total);
     b->residual.alloc(count);
     b->iterations.alloc(count);
+    b->times.alloc(2 * static_cast<size_t>(count));
     b->counters.alloc(2);
     b->prm.alloc(1);
     b->prm_h.alloc(1);
@@ -768,8 +788,9 @@ void check_batch_params(const nkg_pr_params *p) {
 }
 
 void check_tuning(const nkg_batch_tuning &t) {
-    require(t.cluster == 1 || t.cluster == 2 || t.cluster == 4 || t.cluster == 8,
-            "cluster must be 1, 2, 4 or 8");
+    require(t.cluster == 1 || t.cluster == 2 || t.cluster == 4 || t.cluster == 8 ||
+                t.cluster == kMaxCluster,
+            "cluster must be 1, 2, 4, 8 or 16");
     require(t.threads == 128 || t.threads == 256 || t.threads == 512,
             "threads must be 128, 256 or 512");
     require(t.split >= 1, "split must be >= 1");
@@ -890,7 +911,7 @@ int nkg_batch_tune(nkg_batch *b, const nkg_pr_params *p, uint32_t sweeps,
         upload_params(b, tp);
         const uint32_t splits[] = {32, 64, 128, 256, 1024};
         const uint32_t threads[] = {256, 512};
-        const uint32_t clusters[] = {1, 2, 4, 8};
+        const uint32_t clusters[] = {1, 2, 4, 8, 16};
         nkg_batch_tuning best{};
         best.ms = 1e300;
         uint32_t nres = 0;
@@ -929,6 +950,24 @@ int nkg_batch_tune(nkg_batch *b, const nkg_pr_params *p, uint32_t sweeps,
             *n_results = nres;
         if (best_out)
             *best_out = best;
+    });
+}
+
+int nkg_batch_graph_times(nkg_batch *b, double *start_ms, double *end_ms) {
+    return guarded([&] {
+        require(b != nullptr && start_ms != nullptr && end_ms != nullptr, "NULL argument");
+        DeviceGuard guard(b->device);
+        std::vector<unsigned long long> t(2 * static_cast<size_t>(b->count));
+        NKG_CUDA(cudaMemcpyAsync(t.data(), b->times.get(), t.size() * 8, cudaMemcpyDeviceToHost,
+                                 b->stream));
+        NKG_CUDA(cudaStreamSynchronize(b->stream));
+        unsigned long long t0 = ~0ull;
+        for (uint32_t i = 0; i < b->count; ++i)
+            t0 = std::min(t0, t[2 * i]);
+        for (uint32_t i = 0; i < b->count; ++i) {
+            start_ms[i] = static_cast<double>(t[2 * i] - t0) * 1e-6;
+            end_ms[i] = static_cast<double>(t[2 * i + 1] - t0) * 1e-6;
+        }
     });
 }
 

@@ -51,7 +51,8 @@ def check(oracle_mod, gs, offs, scores, its, prec, norm, tol, distribute, normal
             assert err <= 2e-6 * scale, (i, err)
 
 
-@pytest.mark.parametrize("shape", [(1, 128, 4), (2, 256, 32), (4, 512, 128), (8, 256, 1024)])
+@pytest.mark.parametrize("shape", [(1, 128, 4), (2, 256, 32), (4, 512, 128), (8, 256, 1024),
+                                   (16, 256, 64)])
 @pytest.mark.parametrize("prec", [_capi.NKG_PREC_FP64, _capi.NKG_PREC_FP32])
 def test_batch_matches_oracle_per_graph(oracle_mod, batch, shape, prec):
     gs, csr, offs, db = batch
@@ -63,6 +64,8 @@ def test_batch_matches_oracle_per_graph(oracle_mod, batch, shape, prec):
     assert st["iterations"] == int(its.sum())
     if prec == _capi.NKG_PREC_FP64:
         assert floor == 0
+    start, end = db.graph_times()
+    assert np.all(start >= 0) and np.all(end >= start) and end.max() <= st["ms_total"] + 1.0
 
 
 @pytest.mark.parametrize("variant", ["l2", "distribute", "normalized"])
@@ -101,7 +104,7 @@ def test_batch_tuner(batch):
     assert best["ms"] == min(t["ms"] for t in table)
     assert db.tuning()["split"] == best["split"]
     for t in table:
-        assert t["cluster"] in (1, 2, 4, 8) and t["threads"] in (256, 512)
+        assert t["cluster"] in (1, 2, 4, 8, 16) and t["threads"] in (256, 512)
 
 
 def test_batch_rejects_bad_input():
