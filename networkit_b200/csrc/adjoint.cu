@@ -64,6 +64,10 @@ struct AdjointState {
     uint32_t n_units32 = 0, n_units64 = 0;
     unsigned ctas32 = 0, ctas64 = 0;
     int shape = -1;
+    // dL/dw pass: source and row (relabelled) of every arc in the caller's
+    // order, and the grid of that pass.
+    DeviceArray<uint32_t> gw_src, gw_row;
+    unsigned gw_ctas = 0;
     // Weight updates: caller arc index of every slot (kNone for padding) of
     // the in-layout and of the out-layout; chunk partial sums of out-degrees.
     DeviceArray<uint32_t> fw_map, t_map;
@@ -582,70 +586,58 @@ __global__ void adj_to_forward(const uint32_t *__restrict__ tinv, const double *
     qc[v] = make_double2(dc ? damp * (p_t[rt] / deg) : 0.0, c_t[rt]);
 }
 
-// dL/dw over the in-layout's slices: lane = virtual row (an in-row u or a
-// chunk of one), slot j = its arc start + j with source v = col_sell, so
-// dL/dw = qc[v].x (lam[u] - qc[v].y), stored at the arc's caller index
-// row_src[u] + start + j (consecutive for a lane). One warp per slice.
-__global__ void __launch_bounds__(256)
-    adj_grad_w(const uint32_t *__restrict__ slice_off, const uint32_t *__restrict__ col_sell,
-               const uint32_t *__restrict__ chunk_begin, const uint32_t *__restrict__ row_ptr,
-               const uint64_t *__restrict__ row_src, const double *__restrict__ lam_f,
-               const double2 *__restrict__ qc, uint32_t slices, uint32_t s_chunk,
-               uint32_t n_chunks, uint32_t n_long, uint32_t n, double *__restrict__ grad_w) {
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+constexpr int kGradThreads = 256;
+
+// The arcs in the caller's order: source (relabelled) and row (relabelled)
+// of caller arc e, scattered once from the relabelled in-CSR (one warp per row).
+__global__ void adj_caller_arcs(const uint32_t *__restrict__ row_ptr,
+                                const uint64_t *__restrict__ row_src,
+                                const uint32_t *__restrict__ col, uint32_t n,
+                                uint32_t *__restrict__ src_c, uint32_t *__restrict__ row_c) {
+    const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
-    for (uint32_t s = warp; s < slices; s += nwarps) {
-        const uint32_t off = slice_off[s], len = slice_off[s + 1] - off;
-        uint32_t r = 0, start = 0, vlen = 0;
-        if (s < s_chunk) {
-            const uint32_t k = s * 32 + lane;
-            if (k < n_chunks) {
-                // split row of chunk k: the last r with chunk_begin[r] <= k
-                uint32_t lo = 0, hi = n_long - 1;
-                while (lo < hi) {
-                    const uint32_t mid = (lo + hi + 1) >> 1;
-                    if (chunk_begin[mid] <= k)
-                        lo = mid;
-                    else
-                        hi = mid - 1;
-                }
-                r = lo;
-                start = (k - chunk_begin[r]) * kChunk;
-                const uint32_t rl = row_ptr[r + 1] - row_ptr[r];
-                vlen = rl - start < kChunk ? rl - start : kChunk;
-            }
-        } else {
-            r = n_long + (s - s_chunk) * 32 + lane;
-            if (r < n)
-                vlen = row_ptr[r + 1] - row_ptr[r];
-            else
-                r = 0;
+    for (uint64_t r = warp; r < n; r += nwarps) {
+        const uint32_t b = row_ptr[r], e = row_ptr[r + 1];
+        const uint64_t dst = row_src[r];
+        for (uint32_t k = b + lane; k < e; k += 32) {
+            src_c[dst + (k - b)] = col[k];
+            row_c[dst + (k - b)] = static_cast<uint32_t>(r);
         }
-        const double lu = lam_f[r];
-        double *dst = grad_w + row_src[r] + start;
-        const uint32_t *cp = col_sell + static_cast<size_t>(off) * 32 + lane;
-        uint32_t j = 0;
-        for (; j + 8 <= len; j += 8) {
-            uint32_t c[8];
+    }
+}
+
+
+// dL/dw in the caller's arc order: arc e (source v, row u) gets
+// qc[v].x (lam[u] - qc[v].y). Index reads and stores are coalesced; the pair
+// qc[v] is the one scattered load per arc (lam[u] repeats along a row).
+__global__ void __launch_bounds__(kGradThreads)
+    adj_grad_w(const uint32_t *__restrict__ src_c, const uint32_t *__restrict__ row_c,
+               const double *__restrict__ lam_f, const double2 *__restrict__ qc, uint64_t arcs,
+               double *__restrict__ grad_w) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * kGradThreads;
+    uint64_t e = blockIdx.x * static_cast<uint64_t>(kGradThreads) + threadIdx.x;
+    for (; e + 3 * stride < arcs; e += 4 * stride) {
+        uint32_t v[4], u[4];
 #pragma unroll
-            for (int k = 0; k < 8; ++k)
-                c[k] = ld_stream(cp + static_cast<size_t>(j + k) * 32);
-            double2 q[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k)
-                q[k] = __ldg(qc + c[k]);
-#pragma unroll
-            for (int k = 0; k < 8; ++k)
-                if (j + k < vlen)
-                    dst[j + k] = q[k].x * (lu - q[k].y);
+        for (int k = 0; k < 4; ++k) {
+            v[k] = ld_stream(src_c + e + k * stride);
+            u[k] = ld_stream(row_c + e + k * stride);
         }
-        for (; j < len; ++j) {
-            if (j < vlen) {
-                const double2 q = __ldg(qc + ld_stream(cp + static_cast<size_t>(j) * 32));
-                dst[j] = q.x * (lu - q.y);
-            }
+        double2 q[4];
+        double l[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            q[k] = __ldg(qc + v[k]);
+            l[k] = __ldg(lam_f + u[k]);
         }
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            __stcs(grad_w + e + k * stride, q[k].x * (l[k] - q[k].y));
+    }
+    for (; e < arcs; e += stride) {
+        const double2 q = __ldg(qc + ld_stream(src_c + e));
+        __stcs(grad_w + e, q.x * (__ldg(lam_f + ld_stream(row_c + e)) - q.y));
     }
 }
 
@@ -856,6 +848,11 @@ void adjoint_launch_setup(nkg_graph *g, AdjointState &A) {
     A.units64.alloc(static_cast<size_t>(A.n_units64) + 1);
     sell_units(A.tl, A.n_units32, A.units32.get(), s);
     sell_units(A.tl, A.n_units64, A.units64.get(), s);
+    // dL/dw pass: a full grid of the arc-parallel kernel
+    int occg = 0;
+    NKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occg, adj_grad_w, kGradThreads, 0));
+    require(occg >= 1, "adjoint kernels do not fit on an SM");
+    A.gw_ctas = static_cast<unsigned>(occg) * sms;
     NKG_CUDA(cudaStreamSynchronize(s));
     A.shape = g->sweep_shape;
     A.work.ready = false;  // partial-sum buffers depend on the grids
@@ -903,6 +900,14 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
                       const double *d_scores, const double *d_grad, double *d_gw, double *d_gt) {
     AdjointState &A = adjoint_ensure(g);
     adjoint_launch_setup<WEIGHTED>(g, A);
+    if (d_gw && !A.gw_src && g->arcs) {
+        A.gw_src.alloc(g->arcs);
+        A.gw_row.alloc(g->arcs);
+        adj_caller_arcs<<<num_sms(g->device) * 16, 256, 0, g->stream>>>(
+            g->row_ptr.get(), g->row_src.get(), g->col.get(), static_cast<uint32_t>(g->n),
+            A.gw_src.get(), A.gw_row.get());
+        NKG_CUDA(cudaGetLastError());
+    }
     cudaStream_t s = g->stream;
     const uint32_t n = static_cast<uint32_t>(g->n);
     const unsigned sms = num_sms(g->device);
@@ -1104,10 +1109,8 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
         adj_to_forward<WEIGHTED><<<ceil_div(static_cast<uint64_t>(n) + 1, 256), 256, 0, s>>>(
             A.tinv.get(), lam_t, W.c.get(), W.p.get(), A.tdegc.get(), A.tdegw64.get(), n, p.damp,
             W.lam_f.get(), W.qc.get());
-        adj_grad_w<<<sms * 16, 256, 0, s>>>(
-            g->fw.slice_off.get(), g->fw.col_sell.get(), g->fw.chunk_begin.get(), g->row_ptr.get(),
-            g->row_src.get(), W.lam_f.get(), W.qc.get(), g->fw.slices, g->fw.s_chunk,
-            g->fw.n_chunks, g->fw.n_long, n, d_gw);
+        adj_grad_w<<<A.gw_ctas, kGradThreads, 0, s>>>(A.gw_src.get(), A.gw_row.get(),
+                                                       W.lam_f.get(), W.qc.get(), g->arcs, d_gw);
         R.launches += 2;
     }
     if (d_gt) {
