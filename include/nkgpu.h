@@ -223,8 +223,8 @@ NKG_API int nkg_ppr_run(nkg_graph *g, const nkg_pr_params *p, uint32_t k, const 
  * cluster size, threads per CTA, and the row-split threshold (rows longer
  * than `split` arcs are summed by a whole warp, the others one per lane in
  * 32-row slices). nkg_batch_tune times `sweeps` sweeps of every graph for
- * each candidate (split 32..1024, 256 or 512 threads, clusters 1..16) and
- * keeps the fastest; results (nullable, `capacity` entries) receive every
+ * each candidate (split 32..1024, 256 or 512 threads, clusters 1..16), then
+ * the kernel variants on the best of those, and keeps the fastest; results (nullable, `capacity` entries) receive every
  * timed candidate, n_results their count.
  * nkg_batch_run: scores_out = the total node count of doubles (caller ids,
  * each graph normalised like PageRank.cpp:75-92), host or device memory
@@ -235,7 +235,8 @@ typedef struct {
     uint32_t cluster;  /* CTAs per thread-block cluster: 1, 2, 4, 8 or 16 */
     uint32_t threads;  /* threads per CTA: 128, 256 or 512 */
     uint32_t split;    /* row-split threshold (arcs) */
-    uint32_t reserved;
+    uint32_t variant;  /* kernel variant bits: 1 = 16 slots per batch of gathers
+                          (else 8), 2 = iterate loads through L2 only */
     double ms;         /* nkg_batch_tune: device time of the timed sweeps */
 } nkg_batch_tuning;
 NKG_API int nkg_batch_create(nkg_batch **out, uint32_t count, const uint64_t *node_offsets,

@@ -87,11 +87,11 @@ class GraphOptions(C.Structure):
 
 class BatchTuning(C.Structure):
     _fields_ = [("cluster", C.c_uint32), ("threads", C.c_uint32), ("split", C.c_uint32),
-                ("reserved", C.c_uint32), ("ms", C.c_double)]
+                ("variant", C.c_uint32), ("ms", C.c_double)]
 
     def as_dict(self):
         return {"cluster": self.cluster, "threads": self.threads, "split": self.split,
-                "ms": self.ms}
+                "variant": self.variant, "ms": self.ms}
 
 
 _u64p = C.POINTER(C.c_uint64)
@@ -372,8 +372,8 @@ class DeviceBatch:
         check(lib().nkg_batch_get_tuning(self.h, C.byref(t)))
         return t.as_dict()
 
-    def set_tuning(self, cluster: int, threads: int, split: int):
-        t = BatchTuning(int(cluster), int(threads), int(split), 0, 0.0)
+    def set_tuning(self, cluster: int, threads: int, split: int, variant: int = 0):
+        t = BatchTuning(int(cluster), int(threads), int(split), int(variant), 0.0)
         check(lib().nkg_batch_set_tuning(self.h, C.byref(t)))
 
     def tune(self, p: PRParams, sweeps: int = 8, capacity: int = 64):

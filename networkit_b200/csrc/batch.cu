@@ -50,6 +50,9 @@ namespace nkg {
 namespace {
 
 constexpr unsigned kMaxCluster = 16;  // 16 is above the portable 8: opted in per kernel
+// nkg_batch_tuning.variant bits
+constexpr uint32_t kVariantUnroll16 = 1;  // 16 slots per batch of gathers (else 8)
+constexpr uint32_t kVariantL2Only = 2;    // iterate loads bypass L1
 
 struct BatchParams {
     double damp;
@@ -109,15 +112,25 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-template <typename T>
-__device__ __forceinline__ T ld_iter(const T *p) {
-    return *p;  // coherent load: the iterate is written during the kernel
+// Coherent loads of the iterate (it is written during the kernel): through
+// L1 (CG = false) or L2 only (CG = true).
+template <bool CG>
+__device__ __forceinline__ float ld_iter(const float *p) {
+    if (CG)
+        return __ldcg(p);
+    return *p;
+}
+template <bool CG>
+__device__ __forceinline__ double ld_iter(const double *p) {
+    if (CG)
+        return __ldcg(p);
+    return *p;
 }
 
 // Row r of graph (tele, sink_coef): the update of PageRank.cpp:64-65 in gather
 // form (y = x/deg for rows with out-arcs, x for sinks), accumulating the
 // residual, the sum and the sink mass of the new iterate.
-template <typename T>
+template <typename T, bool CG>
 __device__ __forceinline__ void batch_finish(const BatchArgs<T> &a, const T *yin, T *yout,
                                              uint32_t r, T acc, T damp, T tele, T sink_coef,
                                              bool distribute, bool l2, double &res, double &sumx,
@@ -126,7 +139,7 @@ __device__ __forceinline__ void batch_finish(const BatchArgs<T> &a, const T *yin
     if (distribute)
         acc = t_add(acc, sink_coef);
     const T x = t_add(t_mul(acc, damp), tele);
-    const T yo = ld_iter(yin + r);
+    const T yo = ld_iter<CG>(yin + r);
     const T xo = dc ? t_mul(yo, static_cast<T>(dc)) : yo;
     const double d = static_cast<double>(xo) - static_cast<double>(x);
     res += l2 ? d * d : fabs(d);
@@ -139,7 +152,7 @@ __device__ __forceinline__ void batch_finish(const BatchArgs<T> &a, const T *yin
     }
 }
 
-template <typename T, int THREADS, int UNROLL>
+template <typename T, int THREADS, int UNROLL, bool CG>
 __global__ void __launch_bounds__(THREADS) batch_kernel(BatchArgs<T> a) {
     __shared__ ClusterShared sh;
     cg::cluster_group cluster = cg::this_cluster();
@@ -200,18 +213,18 @@ __global__ void __launch_bounds__(THREADS) batch_kernel(BatchArgs<T> a) {
                         T v[4];
 #pragma unroll
                         for (int u = 0; u < 4; ++u)
-                            v[u] = ld_iter(yin + c[u]);
+                            v[u] = ld_iter<CG>(yin + c[u]);
 #pragma unroll
                         for (int u = 0; u < 4; ++u)
                             acc += v[u];
                     }
                     for (; k < e; k += 32)
-                        acc += ld_iter(yin + __ldg(a.col + k));
+                        acc += ld_iter<CG>(yin + __ldg(a.col + k));
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1)
                         acc += __shfl_xor_sync(0xffffffffu, acc, o);
                     if (lane == 0)
-                        batch_finish<T>(a, yin, yout, r, acc, damp, tele, sink_coef,
+                        batch_finish<T, CG>(a, yin, yout, r, acc, damp, tele, sink_coef,
                                         prm.distribute, prm.l2, res, sumx, sink);
                 } else {
                     const uint32_t s = m.slice0 + (item - m.n_long);
@@ -227,16 +240,16 @@ __global__ void __launch_bounds__(THREADS) batch_kernel(BatchArgs<T> a) {
                         T v[UNROLL];
 #pragma unroll
                         for (int u = 0; u < UNROLL; ++u)
-                            v[u] = ld_iter(yin + c[u]);
+                            v[u] = ld_iter<CG>(yin + c[u]);
 #pragma unroll
                         for (int u = 0; u < UNROLL; ++u)
                             acc += v[u];
                     }
                     for (; j < len; ++j)
-                        acc += ld_iter(yin + __ldg(cp + static_cast<size_t>(j) * 32));
+                        acc += ld_iter<CG>(yin + __ldg(cp + static_cast<size_t>(j) * 32));
                     const uint32_t i = m.n_long + (item - m.n_long) * 32 + lane;
                     if (i < m.n)
-                        batch_finish<T>(a, yin, yout, m.base + i, acc, damp, tele, sink_coef,
+                        batch_finish<T, CG>(a, yin, yout, m.base + i, acc, damp, tele, sink_coef,
                                         prm.distribute, prm.l2, res, sumx, sink);
                 }
             }
@@ -294,7 +307,7 @@ __global__ void __launch_bounds__(THREADS) batch_kernel(BatchArgs<T> a) {
         const T *yfin = (it & 1) ? a.y1 : a.y0;
         for (uint32_t i = crank * THREADS + threadIdx.x; i < m.n; i += csize * THREADS) {
             const uint32_t r = m.base + i, dc = a.degc[r];
-            const T yv = ld_iter(yfin + r);
+            const T yv = ld_iter<CG>(yfin + r);
             const double x = dc ? static_cast<double>(t_mul(yv, static_cast<T>(dc)))
                                 : static_cast<double>(yv);
             a.out[a.perm[r]] = x / factor;
@@ -447,7 +460,7 @@ using namespace nkg;
 
 struct BatchGraph {
     cudaGraphExec_t exec = nullptr;
-    uint32_t cluster = 0, threads = 0, split = 0;
+    uint32_t cluster = 0, threads = 0, split = 0, variant = 0;
     uint64_t layout_gen = 0;
 };
 
@@ -528,16 +541,27 @@ void batch_layout(nkg_batch *b, uint32_t split) {
     ++b->layout_gen;
 }
 
-template <typename F>
-void with_batch_threads(uint32_t threads, F &&f) {
-    switch (threads) {
-    case 128: f(std::integral_constant<int, 128>{}); break;
-    case 512: f(std::integral_constant<int, 512>{}); break;
-    default: f(std::integral_constant<int, 256>{}); break;
+template <typename T, int TH, typename F>
+void with_batch_variant(uint32_t variant, F &&f) {
+    const std::integral_constant<int, TH> th{};
+    switch (variant & 3u) {
+    case kVariantUnroll16: f(batch_kernel<T, TH, 16, false>, th); break;
+    case kVariantL2Only: f(batch_kernel<T, TH, 8, true>, th); break;
+    case kVariantUnroll16 | kVariantL2Only: f(batch_kernel<T, TH, 16, true>, th); break;
+    default: f(batch_kernel<T, TH, 8, false>, th); break;
     }
 }
 
-constexpr int kBatchUnroll = 8;
+// Calls f(kernel, threads) for the kernel of a tuning.
+template <typename T, typename F>
+void with_batch_kernel(const nkg_batch_tuning &t, F &&f) {
+    switch (t.threads) {
+    case 128: with_batch_variant<T, 128>(t.variant, f); break;
+    case 512: with_batch_variant<T, 512>(t.variant, f); break;
+    default: with_batch_variant<T, 256>(t.variant, f); break;
+    }
+}
+
 
 // Launch the persistent kernel (queue reset first). Returns false when the
 // cluster shape does not fit.
@@ -546,9 +570,8 @@ bool batch_launch(nkg_batch *b, const nkg_batch_tuning &t, T *y0, T *y1, double 
                   bool check_only = false) {
     cudaStream_t s = b->stream;
     bool ok = true;
-    with_batch_threads(t.threads, [&](auto TH) {
+    with_batch_kernel<T>(t, [&](auto kfn, auto TH) {
         constexpr int threads = decltype(TH)::value;
-        auto kfn = batch_kernel<T, threads, kBatchUnroll>;
         if (t.cluster > 8 &&
             cudaFuncSetAttribute(kfn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
                 cudaSuccess) {
@@ -794,6 +817,7 @@ void check_tuning(const nkg_batch_tuning &t) {
     require(t.threads == 128 || t.threads == 256 || t.threads == 512,
             "threads must be 128, 256 or 512");
     require(t.split >= 1, "split must be >= 1");
+    require((t.variant & ~3u) == 0, "unknown variant bits");
 }
 
 // The queue reset and the persistent kernel, captured as one CUDA graph per
@@ -802,7 +826,7 @@ template <typename T>
 cudaGraphExec_t batch_graph(nkg_batch *b, const nkg_batch_tuning &t) {
     BatchGraph &G = b->graphs[sizeof(T) == 8 ? 1 : 0];
     if (G.exec && G.cluster == t.cluster && G.threads == t.threads && G.split == t.split &&
-        G.layout_gen == b->layout_gen)
+        G.variant == t.variant && G.layout_gen == b->layout_gen)
         return G.exec;
     if (G.exec)
         cudaGraphExecDestroy(G.exec);
@@ -820,6 +844,7 @@ cudaGraphExec_t batch_graph(nkg_batch *b, const nkg_batch_tuning &t) {
     G.cluster = t.cluster;
     G.threads = t.threads;
     G.split = t.split;
+    G.variant = t.variant;
     G.layout_gen = b->layout_gen;
     return G.exec;
 }
@@ -944,6 +969,32 @@ int nkg_batch_tune(nkg_batch *b, const nkg_pr_params *p, uint32_t sweeps,
                         best = t;
                 }
         require(nres > 0, "no cluster shape fits on this GPU");
+        // Second stage: the kernel variants on the best shape.
+        for (uint32_t var = 1; var <= 3; ++var) {
+            nkg_batch_tuning t = best;
+            t.variant = var;
+            t.ms = 0.0;
+            const bool fits =
+                p->precision == NKG_PREC_FP64
+                    ? batch_launch<double>(b, t, nullptr, nullptr, nullptr, true)
+                    : batch_launch<float>(b, t, nullptr, nullptr, nullptr, true);
+            if (!fits)
+                continue;
+            float ms;
+            if (p->precision == NKG_PREC_FP64) {
+                batch_timed<double>(b, t);
+                ms = batch_timed<double>(b, t);
+            } else {
+                batch_timed<float>(b, t);
+                ms = batch_timed<float>(b, t);
+            }
+            t.ms = ms;
+            if (results && nres < capacity)
+                results[nres] = t;
+            ++nres;
+            if (ms < best.ms)
+                best = t;
+        }
         b->tuning = best;
         batch_layout(b, best.split);
         if (n_results)

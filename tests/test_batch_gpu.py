@@ -51,8 +51,8 @@ def check(oracle_mod, gs, offs, scores, its, prec, norm, tol, distribute, normal
             assert err <= 2e-6 * scale, (i, err)
 
 
-@pytest.mark.parametrize("shape", [(1, 128, 4), (2, 256, 32), (4, 512, 128), (8, 256, 1024),
-                                   (16, 256, 64)])
+@pytest.mark.parametrize("shape", [(1, 128, 4, 0), (2, 256, 32, 1), (4, 512, 128, 2), (8, 256, 1024, 3),
+                                   (16, 256, 64, 0)])
 @pytest.mark.parametrize("prec", [_capi.NKG_PREC_FP64, _capi.NKG_PREC_FP32])
 def test_batch_matches_oracle_per_graph(oracle_mod, batch, shape, prec):
     gs, csr, offs, db = batch
