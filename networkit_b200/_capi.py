@@ -223,10 +223,17 @@ class DeviceGraph:
         return PRParams(float(damp), float(tol), int(norm), int(bool(normalized)),
                         int(bool(distribute_sinks)), int(precision), int(max_iterations))
 
-    def run(self, p: PRParams, teleport=None):
-        """Run to convergence; returns (scores[z], iterations, maximum, stats)."""
+    def run(self, p: PRParams, teleport=None, out=None):
+        """Run to convergence; returns (scores[z], iterations, maximum, stats).
+        `out`: optional float64[z] host array to receive the scores (pinned
+        memory makes the read-back a direct DMA)."""
         L = lib()
-        scores = np.empty(self.z, np.float64)
+        if out is not None:
+            if out.dtype != np.float64 or out.shape != (self.z,) or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous float64 array of z entries")
+            scores = out
+        else:
+            scores = np.empty(self.z, np.float64)
         it = C.c_uint64(0)
         mx = C.c_double(0.0)
         st = Stats()
