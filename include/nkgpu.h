@@ -134,6 +134,19 @@ NKG_API int nkg_graph_create(nkg_graph **out, uint64_t z, uint64_t arcs, const u
 NKG_API int nkg_graph_create_ex(nkg_graph **out, uint64_t z, uint64_t arcs, const uint64_t *in_row_ptr,
                         const uint32_t *in_col, const double *in_w, const double *out_wdeg,
                         const uint8_t *exists, int directed, const nkg_graph_options *opts);
+/* The same graph from its edge list, built on the device: edge e = (src[e],
+ * dst[e]) with weight w[e] (w NULL: unweighted), in the order Graph::addEdge
+ * was called (Graph.cpp:549-596). The in-adjacency is what Graph stores: for
+ * directed graphs row v lists the sources of v's in-edges, for undirected
+ * graphs row x lists the other endpoint of every edge at x (a self-loop
+ * once), in edge order; weighted degrees are summed in edge order, as the
+ * host builder does. Duplicate edges stay (as addEdge keeps them). flags: 0
+ * (host arrays) or NKG_DEVICE_PTRS (src, dst, w, exists in device memory).
+ * No reference counterpart as a single call (GPU ingest). */
+NKG_API int nkg_graph_create_from_edges(nkg_graph **out, uint64_t z, uint64_t m,
+                                        const uint32_t *src, const uint32_t *dst, const double *w,
+                                        const uint8_t *exists, int directed, int flags,
+                                        const nkg_graph_options *opts);
 NKG_API void nkg_graph_destroy(nkg_graph *g);
 NKG_API int nkg_graph_get_info(const nkg_graph *g, nkg_graph_info *info);
 

@@ -108,6 +108,9 @@ SIGNATURES = {
                                    _f64p, _u8p, C.c_int]),
     "nkg_graph_create_ex": (C.c_int, [C.POINTER(_vp), C.c_uint64, C.c_uint64, _u64p, _u32p,
                                       _f64p, _f64p, _u8p, C.c_int, C.POINTER(GraphOptions)]),
+    "nkg_graph_create_from_edges": (C.c_int, [C.POINTER(_vp), C.c_uint64, C.c_uint64, _vp, _vp,
+                                              _vp, _vp, C.c_int, C.c_int,
+                                              C.POINTER(GraphOptions)]),
     "nkg_graph_destroy": (None, [_vp]),
     "nkg_graph_get_info": (C.c_int, [_vp, C.POINTER(GraphInfo)]),
     "nkg_pagerank_run": (C.c_int, [_vp, C.POINTER(PRParams), _f64p, _u64p, _f64p,
@@ -201,6 +204,46 @@ class DeviceGraph:
         self.h = h
         self.z = int(csr.z)
         self.n = int(csr.n)
+
+    @classmethod
+    def from_edges(cls, z, src, dst, w=None, directed=False, exists=None, device: int = -1,
+                   sweep_shape: int = -1):
+        """Build the graph on the device from host edge arrays in insertion
+        order (nkg_graph_create_from_edges)."""
+        s = np.ascontiguousarray(src, np.uint32)
+        d = np.ascontiguousarray(dst, np.uint32)
+        if s.shape != d.shape:
+            raise ValueError("src and dst differ in length")
+        ww = None if w is None else np.ascontiguousarray(w, np.float64)
+        ex = None if exists is None else np.ascontiguousarray(exists, np.uint8)
+        return cls._from_edge_pointers(
+            z, int(s.shape[0]), s.ctypes.data, d.ctypes.data, 0 if ww is None else ww.ctypes.data,
+            0 if ex is None else ex.ctypes.data, directed, False, device, sweep_shape)
+
+    @classmethod
+    def from_device_edges(cls, z, m, src_ptr, dst_ptr, w_ptr=0, exists_ptr=0, directed=False,
+                          device: int = -1, sweep_shape: int = -1):
+        """The same from device arrays (raw pointers; uint32 src/dst, float64
+        w, uint8 exists)."""
+        return cls._from_edge_pointers(z, m, src_ptr, dst_ptr, w_ptr, exists_ptr, directed, True,
+                                       device, sweep_shape)
+
+    @classmethod
+    def _from_edge_pointers(cls, z, m, src_p, dst_p, w_p, ex_p, directed, on_device, device,
+                            sweep_shape):
+        self = cls.__new__(cls)
+        h = _vp()
+        opts = GraphOptions()
+        opts.device = int(device)
+        opts.sweep_shape = int(sweep_shape)
+        check(lib().nkg_graph_create_from_edges(
+            C.byref(h), int(z), int(m), _vp(src_p or None), _vp(dst_p or None), _vp(w_p or None),
+            _vp(ex_p or None), int(bool(directed)), NKG_DEVICE_PTRS if on_device else 0,
+            C.byref(opts)))
+        self.h = h
+        self.z = int(z)
+        self.n = int(self.info()["n"])
+        return self
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:

@@ -286,6 +286,95 @@ __global__ void convert_array(const double *__restrict__ in, T *__restrict__ out
 }
 
 // ---------------------------------------------------------------------------
+// Edge-list ingest (nkg_graph_create_from_edges): the in-CSR that
+// Graph::addEdge builds (Graph.cpp:549-596), on the device.
+
+// One key per arc: (row << 32) | edge index. Directed: row = dst. Undirected:
+// both endpoints, a self-loop once (the second copy gets the sentinel key).
+__global__ void ingest_keys(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                            uint64_t m, uint64_t z, int directed, uint64_t *__restrict__ keys,
+                            int *__restrict__ err) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < m;
+         e += stride) {
+        const uint32_t u = src[e], v = dst[e];
+        if (u >= z || v >= z) {
+            atomicCAS(err, 0, 1);
+            continue;
+        }
+        if (directed) {
+            keys[e] = (static_cast<uint64_t>(v) << 32) | e;
+        } else {
+            keys[2 * e] = (static_cast<uint64_t>(u) << 32) | e;
+            keys[2 * e + 1] = u == v ? ~0ull : (static_cast<uint64_t>(v) << 32) | e;
+        }
+    }
+}
+
+// Sorted keys -> in_col / in_w and the row histogram.
+__global__ void ingest_fill(const uint64_t *__restrict__ keys, uint64_t arcs,
+                            const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                            const double *__restrict__ w, int directed, uint32_t *__restrict__ col,
+                            double *__restrict__ in_w, unsigned long long *__restrict__ counts) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < arcs;
+         k += stride) {
+        const uint64_t key = keys[k];
+        const uint32_t row = static_cast<uint32_t>(key >> 32), e = static_cast<uint32_t>(key);
+        const uint32_t u = src[e], v = dst[e];
+        col[k] = directed ? u : (row == u ? v : u);
+        if (w)
+            in_w[k] = w[e];
+        atomicAdd(counts + row, 1ull);
+    }
+}
+
+__global__ void count_below(const uint64_t *__restrict__ keys, uint64_t count, uint64_t bound,
+                            unsigned long long *__restrict__ cnt) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    unsigned long long c = 0;
+    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < count;
+         k += stride)
+        c += keys[k] < bound;
+    c = static_cast<unsigned long long>(warp_sum(static_cast<double>(c)));
+    if ((threadIdx.x & 31) == 0 && c)
+        atomicAdd(cnt, c);
+}
+
+// Sequential sum of vals[b..e) per segment (deterministic, in the given order).
+__global__ void segment_sums(const uint64_t *__restrict__ ptr, const double *__restrict__ vals,
+                             uint64_t segs, double *__restrict__ out) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= segs)
+        return;
+    double sum = 0.0;
+    for (uint64_t k = ptr[i]; k < ptr[i + 1]; ++k)
+        sum += vals[k];
+    out[i] = sum;
+}
+
+// Directed weighted degrees: out-weights of every source in edge order.
+__global__ void ingest_out_keys(const uint32_t *__restrict__ src, uint64_t m,
+                                uint64_t *__restrict__ keys) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < m;
+         e += stride)
+        keys[e] = (static_cast<uint64_t>(src[e]) << 32) | e;
+}
+
+__global__ void ingest_out_vals(const uint64_t *__restrict__ keys, uint64_t m,
+                                const double *__restrict__ w, double *__restrict__ vals,
+                                unsigned long long *__restrict__ counts) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < m;
+         k += stride) {
+        const uint64_t key = keys[k];
+        vals[k] = w[static_cast<uint32_t>(key)];
+        atomicAdd(counts + (key >> 32), 1ull);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Per-run kernels
 
 // PageRank.cpp:26: x = 1/n, stored in gather form.
@@ -564,31 +653,47 @@ void convert_to_float(const double *in, float *out, uint64_t m, int device, cuda
     NKG_CUDA(cudaGetLastError());
 }
 
-static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr,
-                               const uint32_t *in_col, const double *in_w, const double *wdeg,
-                               const uint8_t *exists, int directed, const nkg_graph_options *opt) {
-    require(z >= 1, "graph must have at least one node id (z >= 1)");
-    require(z < 0xffffffffull, "node ids must fit in 32 bits (z < 2^32 - 1)");
-    require(arcs < 0xfffffff0ull, "graphs with 2^32 or more arcs are not supported");
-    require(in_ptr != nullptr, "in_row_ptr is NULL");
-    require(arcs == 0 || in_col != nullptr, "in_col is NULL");
-    require(in_w == nullptr || wdeg != nullptr, "weighted graph needs out_wdeg");
-    require(in_ptr[0] == 0 && in_ptr[z] == arcs, "in_row_ptr must start at 0 and end at arcs");
-
+static int option_device(const nkg_graph_options *opt) {
     int dev = opt && opt->device >= 0 ? opt->device : -1;
     if (dev < 0)
         NKG_CUDA(cudaGetDevice(&dev));
-    DeviceGuard guard(dev);
+    return dev;
+}
+
+// A handle with its device, stream and events (dev current); no graph data yet.
+static std::unique_ptr<nkg_graph> graph_shell(int dev, uint64_t z, uint64_t arcs, bool weighted,
+                                              int directed) {
+    require(z >= 1, "graph must have at least one node id (z >= 1)");
+    require(z < 0xffffffffull, "node ids must fit in 32 bits (z < 2^32 - 1)");
+    require(arcs < 0xfffffff0ull, "graphs with 2^32 or more arcs are not supported");
     std::unique_ptr<nkg_graph> g(new nkg_graph());
     g->device = dev;
     g->z = z;
     g->arcs = arcs;
-    g->weighted = in_w != nullptr;
+    g->weighted = weighted;
     g->directed = directed != 0;
     NKG_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
     NKG_CUDA(cudaEventCreate(&g->ev0));
     NKG_CUDA(cudaEventCreate(&g->ev1));
     NKG_CUDA(cudaEventCreate(&g->ev2));
+    return g;
+}
+
+static nkg_graph *build_graph(std::unique_ptr<nkg_graph> g, DeviceArray<uint64_t> &d_ptr,
+                              DeviceArray<uint32_t> &d_col, DeviceArray<double> &d_w,
+                              DeviceArray<double> &d_wdeg, DeviceArray<uint8_t> &d_ex,
+                              const uint8_t *exists, const nkg_graph_options *opt);
+
+static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr,
+                               const uint32_t *in_col, const double *in_w, const double *wdeg,
+                               const uint8_t *exists, int directed, const nkg_graph_options *opt) {
+    require(in_ptr != nullptr, "in_row_ptr is NULL");
+    require(arcs == 0 || in_col != nullptr, "in_col is NULL");
+    require(in_w == nullptr || wdeg != nullptr, "weighted graph needs out_wdeg");
+    DeviceGuard guard(option_device(opt));
+    std::unique_ptr<nkg_graph> g = graph_shell(option_device(opt), z, arcs, in_w != nullptr,
+                                               directed);
+    require(in_ptr[0] == 0 && in_ptr[z] == arcs, "in_row_ptr must start at 0 and end at arcs");
     cudaStream_t s = g->stream;
 
     // Upload.
@@ -614,6 +719,19 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
         NKG_CUDA(cudaMemcpyAsync(d_ex.get(), exists, z, cudaMemcpyHostToDevice, s));
     }
     NKG_CUDA(cudaEventRecord(g->ev0, s));
+    return build_graph(std::move(g), d_ptr, d_col, d_w, d_wdeg, d_ex, exists, opt);
+}
+
+// The rest of the upload from the in-CSR in device memory: validation,
+// relabelling, sliced layout, per-run buffers. `exists` (host, nullable) is
+// the existence mask d_ex holds on the device.
+static nkg_graph *build_graph(std::unique_ptr<nkg_graph> g, DeviceArray<uint64_t> &d_ptr,
+                              DeviceArray<uint32_t> &d_col, DeviceArray<double> &d_w,
+                              DeviceArray<double> &d_wdeg, DeviceArray<uint8_t> &d_ex,
+                              const uint8_t *exists, const nkg_graph_options *opt) {
+    const uint64_t z = g->z, arcs = g->arcs;
+    const int dev = g->device;
+    cudaStream_t s = g->stream;
 
     // Validate + out-degree count.
     DeviceArray<uint32_t> outdeg(z);
@@ -722,6 +840,142 @@ static nkg_graph *create_graph(uint64_t z, uint64_t arcs, const uint64_t *in_ptr
     g->scalars_host.alloc(16);
     NKG_CUDA(cudaStreamSynchronize(s));
     return g.release();
+}
+
+static void sort_keys64(DeviceArray<uint64_t> &keys, uint64_t count, int end_bit, cudaStream_t s) {
+    DeviceArray<uint64_t> out(std::max<uint64_t>(count, 1));
+    size_t tb = 0;
+    NKG_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, keys.get(), out.get(),
+                                            static_cast<int64_t>(count), 0, end_bit, s));
+    DeviceArray<unsigned char> tmp(tb);
+    NKG_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), tb, keys.get(), out.get(),
+                                            static_cast<int64_t>(count), 0, end_bit, s));
+    keys = std::move(out);
+}
+
+// counts (z) -> offsets (z + 1).
+static void counts_to_ptr(const unsigned long long *counts, uint64_t z, uint64_t *ptr,
+                          cudaStream_t s) {
+    NKG_CUDA(cudaMemsetAsync(ptr, 0, sizeof(uint64_t), s));
+    size_t tb = 0;
+    NKG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, counts, ptr + 1,
+                                           static_cast<int64_t>(z), s));
+    DeviceArray<unsigned char> tmp(tb);
+    NKG_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tb, counts, ptr + 1,
+                                           static_cast<int64_t>(z), s));
+}
+
+// The graph of m edges inserted in the given order (src[e], dst[e], weight
+// w[e]), as nkg_graph_create would get it from Graph::forInEdgesOf.
+static nkg_graph *create_from_edges(uint64_t z, uint64_t m, const uint32_t *src,
+                                    const uint32_t *dst, const double *w, const uint8_t *exists,
+                                    int directed, bool on_device, const nkg_graph_options *opt) {
+    require(m == 0 || (src != nullptr && dst != nullptr), "src / dst is NULL");
+    require(m < 0x7fffffffull, "edge lists of 2^31 or more edges are not supported");
+    DeviceGuard guard(option_device(opt));
+    const uint64_t max_arcs = directed ? m : 2 * m;
+    std::unique_ptr<nkg_graph> g0 = graph_shell(option_device(opt), z, 0, w != nullptr, directed);
+    cudaStream_t s = g0->stream;
+    const unsigned sms = num_sms(g0->device);
+    DeviceArray<uint32_t> d_src, d_dst;
+    DeviceArray<double> d_ew;
+    const uint32_t *ps = src, *pd = dst;
+    const double *pw = w;
+    if (!on_device && m) {
+        d_src.alloc(m);
+        d_dst.alloc(m);
+        NKG_CUDA(cudaMemcpyAsync(d_src.get(), src, m * 4, cudaMemcpyHostToDevice, s));
+        NKG_CUDA(cudaMemcpyAsync(d_dst.get(), dst, m * 4, cudaMemcpyHostToDevice, s));
+        ps = d_src.get();
+        pd = d_dst.get();
+        if (w) {
+            d_ew.alloc(m);
+            NKG_CUDA(cudaMemcpyAsync(d_ew.get(), w, m * 8, cudaMemcpyHostToDevice, s));
+            pw = d_ew.get();
+        }
+    }
+    std::vector<uint8_t> ex_host;
+    DeviceArray<uint8_t> d_ex;
+    const uint8_t *exh = nullptr;
+    if (exists) {
+        d_ex.alloc(z);
+        ex_host.resize(z);
+        if (on_device) {
+            NKG_CUDA(cudaMemcpyAsync(ex_host.data(), exists, z, cudaMemcpyDeviceToHost, s));
+            NKG_CUDA(cudaMemcpyAsync(d_ex.get(), exists, z, cudaMemcpyDeviceToDevice, s));
+        } else {
+            std::memcpy(ex_host.data(), exists, z);
+            NKG_CUDA(cudaMemcpyAsync(d_ex.get(), exists, z, cudaMemcpyHostToDevice, s));
+        }
+        exh = ex_host.data();
+    }
+    NKG_CUDA(cudaEventRecord(g0->ev0, s));
+
+    int zbits = 1;
+    while (zbits < 32 && (1ull << zbits) < z)
+        ++zbits;
+    DeviceArray<uint64_t> keys(std::max<uint64_t>(max_arcs, 1));
+    DeviceArray<int> err(1);
+    NKG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
+    if (m)
+        ingest_keys<<<sms * 8, 256, 0, s>>>(ps, pd, m, z, directed, keys.get(), err.get());
+    NKG_CUDA(cudaGetLastError());
+    require(read_scalar(err.get(), s) == 0, "an edge endpoint is >= z");
+    // Self-loop copies carry the all-ones key and sort behind every arc.
+    sort_keys64(keys, max_arcs, directed ? 32 + zbits : 64, s);
+    uint64_t arcs = max_arcs;
+    if (!directed && m) {
+        // arcs = number of keys below the sentinel: find it on the host side of a
+        // small read-back (the sentinel keys form the tail).
+        DeviceArray<unsigned long long> cnt(1);
+        NKG_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(unsigned long long), s));
+        count_below<<<sms * 8, 256, 0, s>>>(keys.get(), max_arcs, ~0ull, cnt.get());
+        NKG_CUDA(cudaGetLastError());
+        arcs = read_scalar(cnt.get(), s);
+    }
+    require(arcs < 0xfffffff0ull, "graphs with 2^32 or more arcs are not supported");
+    g0->arcs = arcs;
+    DeviceArray<uint64_t> d_ptr(z + 1);
+    DeviceArray<uint32_t> d_col(std::max<uint64_t>(arcs, 1));
+    DeviceArray<double> d_w, d_wdeg;
+    DeviceArray<unsigned long long> counts(z);
+    NKG_CUDA(cudaMemsetAsync(counts.get(), 0, z * sizeof(unsigned long long), s));
+    if (w) {
+        d_w.alloc(std::max<uint64_t>(arcs, 1));
+        d_wdeg.alloc(z);
+    }
+    if (arcs)
+        ingest_fill<<<sms * 8, 256, 0, s>>>(keys.get(), arcs, ps, pd, pw, directed, d_col.get(),
+                                            d_w.get(), counts.get());
+    NKG_CUDA(cudaGetLastError());
+    counts_to_ptr(counts.get(), z, d_ptr.get(), s);
+    if (w) {
+        if (directed) {
+            // out-weights of every source in edge order
+            DeviceArray<uint64_t> okeys(std::max<uint64_t>(m, 1));
+            DeviceArray<double> ovals(std::max<uint64_t>(m, 1));
+            DeviceArray<uint64_t> optr(z + 1);
+            NKG_CUDA(cudaMemsetAsync(counts.get(), 0, z * sizeof(unsigned long long), s));
+            if (m) {
+                ingest_out_keys<<<sms * 8, 256, 0, s>>>(ps, m, okeys.get());
+                sort_keys64(okeys, m, 32 + zbits, s);
+                ingest_out_vals<<<sms * 8, 256, 0, s>>>(okeys.get(), m, pw, ovals.get(),
+                                                        counts.get());
+            }
+            counts_to_ptr(counts.get(), z, optr.get(), s);
+            segment_sums<<<ceil_div(z, 256), 256, 0, s>>>(optr.get(), ovals.get(), z,
+                                                          d_wdeg.get());
+        } else {
+            segment_sums<<<ceil_div(z, 256), 256, 0, s>>>(d_ptr.get(), d_w.get(), z,
+                                                          d_wdeg.get());
+        }
+        NKG_CUDA(cudaGetLastError());
+    }
+    keys.reset();
+    d_src.reset();
+    d_dst.reset();
+    d_ew.reset();
+    return build_graph(std::move(g0), d_ptr, d_col, d_w, d_wdeg, d_ex, exh, opt);
 }
 
 static void destroy_plane_graphs(nkg_graph *g) {
@@ -1264,6 +1518,18 @@ int nkg_graph_create_ex(nkg_graph **out, uint64_t z, uint64_t arcs, const uint64
         require(out != nullptr, "out is NULL");
         *out = nullptr;
         *out = create_graph(z, arcs, in_row_ptr, in_col, in_w, out_wdeg, exists, directed, opts);
+    });
+}
+
+int nkg_graph_create_from_edges(nkg_graph **out, uint64_t z, uint64_t m, const uint32_t *src,
+                                const uint32_t *dst, const double *w, const uint8_t *exists,
+                                int directed, int flags, const nkg_graph_options *opts) {
+    return guarded([&] {
+        require(out != nullptr, "out is NULL");
+        require((flags & ~NKG_DEVICE_PTRS) == 0, "unknown flags");
+        *out = nullptr;
+        *out = create_from_edges(z, m, src, dst, w, exists, directed,
+                                 (flags & NKG_DEVICE_PTRS) != 0, opts);
     });
 }
 
