@@ -671,6 +671,25 @@ def main():
             e2e_t.append(dt)
             e2e_it.append(it2)
     e2e_value = world * arcs * sum(e2e_it) / sum(e2e_t) / 1e9 if e2e_t else None
+    # The same from the edge list (COO in insertion order, pinned): the in-CSR is
+    # built on the device (nkg_graph_create_from_edges).
+    e2e_edges = None
+    if args.e2e_steps > 0:
+        e_src = pin(csr.in_col)
+        e_dst = pin(np.repeat(np.arange(n, dtype=np.uint32),
+                              np.diff(csr.in_ptr).astype(np.int64)))
+        ts = []
+        for i in range(2):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            g3 = _capi.DeviceGraph.from_edges(n, e_src, e_dst, directed=True, device=local)
+            _, it3, _, _ = g3.run(p, out=h_out)
+            g3.close()
+            if i > 0:
+                ts.append(time.perf_counter() - t1)
+        e2e_edges = {"value": world * arcs * it3 / ts[0] / 1e9, "unit": UNIT,
+                     "ms_per_step": 1e3 * ts[0], "h2d_bytes_per_step": 8 * arcs,
+                     "d2h_bytes_per_step": 8 * n}
     h2d = 8 * (n + 1) + 4 * arcs
     d2h = 8 * n
 
@@ -713,7 +732,8 @@ def main():
                          "ms_per_iteration": ms_iter, "peak_source": peak_kind},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
-                    "ms_per_step": 1e3 * sum(e2e_t) / len(e2e_t) if e2e_t else None},
+                    "ms_per_step": 1e3 * sum(e2e_t) / len(e2e_t) if e2e_t else None,
+                    "from_edge_list": e2e_edges},
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,

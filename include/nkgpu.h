@@ -267,6 +267,21 @@ NKG_API int nkg_batch_run(nkg_batch *b, const nkg_pr_params *p, double *scores_o
  * entries each. */
 NKG_API int nkg_batch_graph_times(nkg_batch *b, double *start_ms, double *end_ms);
 
+/* EigenvectorCentrality(G, tol).run() + scores() (EigenvectorCentrality.cpp:20-60,
+ * centrality.pyx:1950-1968) and KatzCentrality(G, alpha, beta, tol) with
+ * edgeDirection 0 (InEdges) or 1 (OutEdges) (KatzCentrality.cpp:20-72,
+ * centrality.pyx:1678-1712; alpha 0 = 1 / (1 + maxDegree); a negative alpha
+ * is rejected with the reference's message), on the graph's weights, FP64.
+ * The reference has no iteration cap; max_iterations (UINT64_MAX = none)
+ * bounds the loop. scores_out: z doubles, host or device (flags 0 /
+ * NKG_DEVICE_PTRS); deleted ids keep 1.0 as in the reference. */
+NKG_API int nkg_eigenvector_run(nkg_graph *g, double tol, uint64_t max_iterations,
+                                double *scores_out, int flags, uint64_t *iterations_out,
+                                nkg_stats *stats);
+NKG_API int nkg_katz_run(nkg_graph *g, double alpha, double beta, double tol, int edge_direction,
+                         uint64_t max_iterations, double *scores_out, int flags,
+                         uint64_t *iterations_out, nkg_stats *stats);
+
 /* Centrality::ranking() (Centrality.cpp:29-41): existing nodes sorted by score
  * descending, ties by node id ascending. scores: host array of z doubles (any
  * scores, e.g. from nkg_pagerank_run); ids_out / vals_out: n entries each. */

@@ -131,6 +131,10 @@ SIGNATURES = {
     "nkg_graph_set_weights": (C.c_int, [_vp, _vp, _vp, C.c_int]),
     "nkg_pagerank_adjoint": (C.c_int, [_vp, C.POINTER(PRParams), _vp, _vp, _vp, _vp, _vp, C.c_int,
                                        _u64p, C.POINTER(Stats)]),
+    "nkg_eigenvector_run": (C.c_int, [_vp, C.c_double, C.c_uint64, _vp, C.c_int, _u64p,
+                                      C.POINTER(Stats)]),
+    "nkg_katz_run": (C.c_int, [_vp, C.c_double, C.c_double, C.c_double, C.c_int, C.c_uint64, _vp,
+                               C.c_int, _u64p, C.POINTER(Stats)]),
     "nkg_batch_create": (C.c_int, [C.POINTER(_vp), C.c_uint32, _u64p, _u64p, _u32p, C.c_int]),
     "nkg_batch_destroy": (None, [_vp]),
     "nkg_batch_get_tuning": (C.c_int, [_vp, C.POINTER(BatchTuning)]),
@@ -352,6 +356,25 @@ class DeviceGraph:
                                          _vp(gt_ptr or None), NKG_DEVICE_PTRS, C.byref(it),
                                          C.byref(st)))
         return int(it.value), st.as_dict()
+
+    def eigenvector(self, tol=1e-9, max_iterations=UINT64_MAX):
+        """EigenvectorCentrality scores (z), iterations, stats."""
+        out = np.empty(self.z, np.float64)
+        it = C.c_uint64(0)
+        st = Stats()
+        check(lib().nkg_eigenvector_run(self.h, float(tol), int(max_iterations),
+                                        _vp(out.ctypes.data), 0, C.byref(it), C.byref(st)))
+        return out, int(it.value), st.as_dict()
+
+    def katz(self, alpha=0.0, beta=0.1, tol=1e-8, edge_direction=0, max_iterations=UINT64_MAX):
+        """KatzCentrality scores (z), iterations, stats."""
+        out = np.empty(self.z, np.float64)
+        it = C.c_uint64(0)
+        st = Stats()
+        check(lib().nkg_katz_run(self.h, float(alpha), float(beta), float(tol),
+                                 int(edge_direction), int(max_iterations), _vp(out.ctypes.data),
+                                 0, C.byref(it), C.byref(st)))
+        return out, int(it.value), st.as_dict()
 
     def ppr(self, seeds, p: PRParams, d_out_ptr: int = 0):
         """Batched personalised PageRank (one column per seed). Returns

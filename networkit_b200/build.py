@@ -23,7 +23,7 @@ INCLUDE = os.path.join(ROOT, "include")
 GPU_LIB = os.path.join(LIBDIR, "libnkgpu.so")
 GEN_LIB = os.path.join(LIBDIR, "libnkgen.so")
 
-GPU_SOURCES = ["nkgpu.cu", "noalloc.cu", "ppr.cu", "adjoint.cu", "batch.cu"]
+GPU_SOURCES = ["nkgpu.cu", "noalloc.cu", "ppr.cu", "adjoint.cu", "batch.cu", "centrality.cu"]
 GPU_HEADERS = ["common.cuh", "sweep.cuh", "refine.cuh", "graph.hpp", "host.hpp"]
 GEN_SOURCES = ["graphgen.cpp"]
 

@@ -1,4 +1,5 @@
-"""``networkit.centrality.PageRank`` on the B200 path.
+"""``networkit.centrality.PageRank`` (and the centralities that share its
+sweep: EigenvectorCentrality, KatzCentrality) on the B200 path.
 
 Mirrors the reference's Cython surface for this path
 (networkit/centrality.pyx:24-100 Centrality, :1970-2037 Norm/PageRank,
@@ -224,6 +225,113 @@ class PageRank(Centrality):
         if self._scores.shape[0] == 0:
             return np.zeros(0, np.uint64), np.zeros(0)
         return self._device_graph().ranking(self._scores)
+
+
+class _SweepCentrality(Centrality):
+    """Shared upload / ranking of the centralities that run the pull sweep."""
+
+    def __init__(self, G: Graph, device: int = -1):
+        super().__init__()
+        if not isinstance(G, Graph):
+            raise TypeError("G must be a networkit_b200.Graph")
+        self._G = G
+        self._device = int(device)
+        self._dg: Optional[_capi.DeviceGraph] = None
+        self._dg_key = None
+        self._iterations = 0
+        self.lastStats: dict = {}
+
+    def _device_graph(self) -> _capi.DeviceGraph:
+        csr = self._G.inCSR()
+        if self._dg is None or self._dg_key != id(csr):
+            self._dg = _capi.DeviceGraph(csr, device=self._device)
+            self._dg_key = id(csr)
+            self._csr = csr
+        return self._dg
+
+    def _finish(self, scores, it, st):
+        self._scores = scores
+        self._iterations = it
+        self.lastStats = st
+        self._hasRun = True
+        return self
+
+    def numberOfIterations(self) -> int:
+        """Iterations of the last run (the reference keeps no count)."""
+        self._assureFinished()
+        return self._iterations
+
+    def rankingArrays(self):
+        self._assureFinished()
+        if self._scores.shape[0] == 0:
+            return np.zeros(0, np.uint64), np.zeros(0)
+        return self._device_graph().ranking(self._scores)
+
+
+class EigenvectorCentrality(_SweepCentrality):
+    """Leading eigenvector of the adjacency matrix, normalised in the 2-norm.
+
+    EigenvectorCentrality(G, tol=1e-9) (centrality.pyx:1950-1968;
+    EigenvectorCentrality.cpp:20-60): power iteration over the in-adjacency
+    with the edge weights until the 2-norm of the product changes by at most
+    tol."""
+
+    def __init__(self, G: Graph, tol: float = 1e-9, device: int = -1):
+        super().__init__(G, device)
+        self._tol = float(tol)
+
+    def run(self):
+        csr = self._G.inCSR()
+        self._exists = csr.exists
+        if csr.n == 0:
+            return self._finish(np.ones(csr.z), 0, {})
+        scores, it, st = self._device_graph().eigenvector(self._tol)
+        return self._finish(scores, it, st)
+
+
+class EdgeDirection:
+    """KatzCentrality::edgeDirection (KatzCentrality.hpp: InEdges = 0, OutEdges = 1)."""
+
+    InEdges = 0
+    OutEdges = 1
+
+
+class KatzCentrality(_SweepCentrality):
+    """Katz centrality.
+
+    KatzCentrality(G, alpha=0, beta=0.1, tol=1e-8) (centrality.pyx:1678-1712;
+    KatzCentrality.cpp:20-72). alpha 0 picks 1 / (1 + maximum degree); a
+    negative alpha raises like the reference. ``edgeDirection`` counts in-edges
+    (default) or out-edges."""
+
+    def __init__(self, G: Graph, alpha: float = 0, beta: float = 0.1, tol: float = 1e-8,
+                 device: int = -1):
+        if alpha < 0:
+            raise RuntimeError("Alpha must be non negative.")
+        super().__init__(G, device)
+        self._alpha = float(alpha)
+        self._beta = float(beta)
+        self._tol = float(tol)
+        self._edgeDirection = EdgeDirection.InEdges
+
+    @property
+    def edgeDirection(self) -> int:
+        return self._edgeDirection
+
+    @edgeDirection.setter
+    def edgeDirection(self, d: int):
+        if d not in (EdgeDirection.InEdges, EdgeDirection.OutEdges):
+            raise ValueError("edgeDirection must be EdgeDirection.InEdges or OutEdges")
+        self._edgeDirection = int(d)
+
+    def run(self):
+        csr = self._G.inCSR()
+        self._exists = csr.exists
+        if csr.n == 0:
+            return self._finish(np.ones(csr.z), 0, {})
+        scores, it, st = self._device_graph().katz(self._alpha, self._beta, self._tol,
+                                                   self._edgeDirection)
+        return self._finish(scores, it, st)
 
 
 def rankPerNode(ranking):

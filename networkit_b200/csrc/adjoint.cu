@@ -741,6 +741,11 @@ AdjointState &adjoint_ensure(nkg_graph *g) {
     return *g->adj;
 }
 
+OutLayoutView adjoint_out_layout(nkg_graph *g) {
+    AdjointState &A = adjoint_ensure(g);
+    return OutLayoutView{&A.tl, A.tinv.get()};
+}
+
 namespace {
 
 // Slot -> caller arc maps of both layouts (first weight update only).

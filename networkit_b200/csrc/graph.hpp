@@ -121,6 +121,13 @@ struct nkg_graph {
 namespace nkg {
 // The out-adjacency layout of the adjoint (adjoint.cu), built on first use.
 AdjointState &adjoint_ensure(nkg_graph *g);
+// Read-only view of that layout for other kernels: rows are the nodes in
+// out-degree order (tinv: relabelled id -> row), columns row numbers.
+struct OutLayoutView {
+    const SellLayout *tl;
+    const uint32_t *tinv;
+};
+OutLayoutView adjoint_out_layout(nkg_graph *g);
 // Replace the arc weights in place (device arrays in the caller's order;
 // wdeg null: summed on the device over every node's out-arcs).
 void set_weights_device(nkg_graph *g, const double *w, const double *wdeg);

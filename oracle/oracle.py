@@ -74,6 +74,12 @@ def oracle_lib():
         lib.nko_pagerank_adjoint.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _f64p, _u32p, _f64p,
                                              C.c_double, C.c_int, _f64p, _f64p, C.c_double,
                                              C.c_uint64, _f64p, _f64p, _f64p]
+        lib.nko_eigenvector.restype = C.c_int64
+        lib.nko_eigenvector.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _u8p, C.c_double,
+                                        C.c_uint64, _f64p]
+        lib.nko_katz.restype = C.c_int64
+        lib.nko_katz.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _u8p, C.c_double, C.c_double,
+                                 C.c_double, C.c_uint64, _f64p]
         _oracle = lib
     return _oracle
 
@@ -104,6 +110,11 @@ def ref_lib():
         lib.nkref_graph_export.restype = C.c_int
         lib.nkref_graph_export.argtypes = [C.c_void_p, _u64p, _u32p, _f64p, _u64p, _u32p, _f64p,
                                            _u8p]
+        lib.nkref_eigenvector.restype = C.c_int
+        lib.nkref_eigenvector.argtypes = [C.c_void_p, C.c_double, C.c_int, _f64p, _f64p]
+        lib.nkref_katz.restype = C.c_int
+        lib.nkref_katz.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int,
+                                   C.c_int, _f64p, _u64p, _f64p]
         lib.nkref_pagerank.restype = C.c_int
         lib.nkref_pagerank.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_int,
                                        C.c_uint64, C.c_int, _f64p, _u64p, _f64p, _u64p, _f64p,
@@ -154,6 +165,40 @@ def ranking(scores, exists=None):
     ex = None if exists is None else np.ascontiguousarray(exists, np.uint8)
     lib.nko_ranking(z, _ptr(sc, _f64p), _ptr(ex, _u8p), _ptr(ids, _u64p), _ptr(vals, _f64p))
     return ids, vals
+
+
+def eigenvector(csr, tol=1e-9, max_iterations=100000):
+    """EigenvectorCentrality (C restatement); returns (scores, iterations)."""
+    lib = oracle_lib()
+    z = int(csr.z)
+    scores = np.empty(z, np.float64)
+    ex = None if csr.exists is None else np.ascontiguousarray(csr.exists, np.uint8)
+    it = lib.nko_eigenvector(z, _ptr(np.ascontiguousarray(csr.in_ptr, np.uint64), _u64p),
+                             _ptr(np.ascontiguousarray(csr.in_col, np.uint32), _u32p),
+                             _ptr(csr.in_w, _f64p), _ptr(ex, _u8p), tol, max_iterations,
+                             _ptr(scores, _f64p))
+    if it < 0:
+        raise RuntimeError("oracle eigenvector failed")
+    return scores, int(it)
+
+
+def katz(z, ptr, col, w=None, exists=None, alpha=0.0, beta=0.1, tol=1e-8, max_degree=None,
+         max_iterations=100000):
+    """KatzCentrality (C restatement) over the adjacency (ptr, col, w): the
+    in-CSR for InEdges, the out-CSR for OutEdges. alpha 0 = 1/(1 + max_degree)
+    (KatzCentrality.cpp:15-17). Returns (scores, iterations)."""
+    lib = oracle_lib()
+    if alpha == 0:
+        alpha = 1.0 / (1.0 + max_degree)
+    scores = np.empty(int(z), np.float64)
+    ex = None if exists is None else np.ascontiguousarray(exists, np.uint8)
+    ww = None if w is None else np.ascontiguousarray(w, np.float64)
+    it = lib.nko_katz(int(z), _ptr(np.ascontiguousarray(ptr, np.uint64), _u64p),
+                      _ptr(np.ascontiguousarray(col, np.uint32), _u32p), _ptr(ww, _f64p),
+                      _ptr(ex, _u8p), alpha, beta, tol, max_iterations, _ptr(scores, _f64p))
+    if it < 0:
+        raise RuntimeError("oracle katz failed")
+    return scores, int(it)
 
 
 def adjoint(csr, x, g, damp=0.85, distribute_sinks=True, teleport=None, tol=1e-14,
@@ -260,6 +305,26 @@ class RefGraph:
             raise RuntimeError(lib.nkref_last_error().decode())
         return dict(out_ptr=out_ptr, out_adj=out_adj, out_w=out_w, in_ptr=in_ptr, in_adj=in_adj,
                     in_w=in_w, exists=exists, directed=directed, weighted=self.weighted)
+
+    def eigenvector(self, tol=1e-9, nthreads=0):
+        lib = ref_lib()
+        scores = np.empty(self.z, np.float64)
+        secs = C.c_double(0.0)
+        if lib.nkref_eigenvector(self.h, tol, int(nthreads), _ptr(scores, _f64p),
+                                 C.byref(secs)) != 0:
+            raise RuntimeError(lib.nkref_last_error().decode())
+        return scores
+
+    def katz(self, alpha=0.0, beta=0.1, tol=1e-8, out_edges=False, nthreads=0):
+        """(scores, ranking ids)"""
+        lib = ref_lib()
+        scores = np.empty(self.z, np.float64)
+        ids = np.empty(self.n, np.uint64)
+        secs = C.c_double(0.0)
+        if lib.nkref_katz(self.h, alpha, beta, tol, int(bool(out_edges)), int(nthreads),
+                          _ptr(scores, _f64p), _ptr(ids, _u64p), C.byref(secs)) != 0:
+            raise RuntimeError(lib.nkref_last_error().decode())
+        return scores, ids
 
     def pagerank(self, damp=0.85, tol=1e-8, normalized=False, norm=1, max_iterations=2**64 - 1,
                  nthreads=0, want_ranking=True):

@@ -8,7 +8,9 @@
  * (oracle/_ref/libnkref.so) run on one OpenMP thread; tests/test_oracle.py
  * checks that on every golden fixture. The distributeSinks term, the
  * personalised teleport and the adjoint have no reference implementation
- * (parity unpinned); they extend the same loop. */
+ * (parity unpinned); they extend the same loop. EigenvectorCentrality and
+ * KatzCentrality (EigenvectorCentrality.cpp, KatzCentrality.cpp) are
+ * restated the same way and pinned against the reference library. */
 #include "pagerank_oracle.h"
 
 #include <math.h>
@@ -277,4 +279,94 @@ int64_t nko_pagerank_adjoint(uint64_t z, const uint64_t *in_ptr, const uint32_t 
     free(c);
     free(lam2);
     return sweeps;
+}
+
+/* NumericTools::equal (NumericTools.cpp:16-18). */
+static int num_equal(double x, double y, double error) {
+    return (x <= (y + error)) && (x >= (y - error));
+}
+
+static double length_of(uint64_t z, const uint8_t *exists, const double *v) {
+    double sum = 0.0;
+    for (uint64_t u = 0; u < z; ++u)
+        if (exists_at(exists, u))
+            sum += v[u] * v[u];
+    return sqrt(sum);
+}
+
+int64_t nko_eigenvector(uint64_t z, const uint64_t *in_ptr, const uint32_t *in_col,
+                        const double *in_w, const uint8_t *exists, double tol, uint64_t max_iter,
+                        double *scores) {
+    if (!in_ptr || !scores || z == 0)
+        return -1;
+    double *values = (double *)malloc(z * sizeof(double));
+    double *x = (double *)malloc(z * sizeof(double));
+    if (!values || !x) {
+        free(values);
+        free(x);
+        return -1;
+    }
+    for (uint64_t u = 0; u < z; ++u)
+        values[u] = x[u] = 1.0;
+    double length = 0.0, old_length = 0.0;
+    int64_t it = 0;
+    do {
+        old_length = length;
+        for (uint64_t u = 0; u < z; ++u) {
+            if (!exists_at(exists, u))
+                continue;
+            values[u] = 0.0;
+            for (uint64_t e = in_ptr[u]; e < in_ptr[u + 1]; ++e)
+                values[u] += (in_w ? in_w[e] : 1.0) * x[in_col[e]];
+        }
+        length = length_of(z, exists, values);
+        for (uint64_t u = 0; u < z; ++u)
+            if (exists_at(exists, u))
+                values[u] /= length;
+        double *t = x;
+        x = values;
+        values = t;
+        ++it;
+    } while (!num_equal(length, old_length, tol) && (uint64_t)it < max_iter);
+    if (x[0] < 0)
+        for (uint64_t u = 0; u < z; ++u)
+            if (exists_at(exists, u))
+                x[u] = fabs(x[u]);
+    memcpy(scores, x, z * sizeof(double));
+    free(values);
+    free(x);
+    return it;
+}
+
+int64_t nko_katz(uint64_t z, const uint64_t *ptr, const uint32_t *col, const double *w,
+                 const uint8_t *exists, double alpha, double beta, double tol, uint64_t max_iter,
+                 double *scores) {
+    if (!ptr || !scores || z == 0)
+        return -1;
+    double *values = (double *)malloc(z * sizeof(double));
+    if (!values)
+        return -1;
+    for (uint64_t u = 0; u < z; ++u)
+        values[u] = scores[u] = 1.0;
+    double length = 0.0, old_length = 0.0;
+    int64_t it = 0;
+    do {
+        old_length = length;
+        for (uint64_t u = 0; u < z; ++u) {
+            if (!exists_at(exists, u))
+                continue;
+            values[u] = 0.0;
+            for (uint64_t e = ptr[u]; e < ptr[u + 1]; ++e)
+                values[u] += (w ? w[e] : 1.0) * alpha * (1 + scores[col[e]]);
+            values[u] += beta;
+        }
+        length = length_of(z, exists, values);
+        memcpy(scores, values, z * sizeof(double));
+        ++it;
+    } while (!num_equal(length, old_length, tol) && (uint64_t)it < max_iter);
+    for (uint64_t u = 0; u < z; ++u)
+        if (exists_at(exists, u))
+            scores[u] /= length;
+    free(values);
+    return it;
 }

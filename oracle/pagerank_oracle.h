@@ -68,6 +68,27 @@ int64_t nko_pagerank_adjoint(uint64_t z, const uint64_t *in_ptr, const uint32_t 
                              const double *x, const double *g, double tol, uint64_t max_iter,
                              double *lam, double *grad_w, double *grad_t);
 
+/* EigenvectorCentrality::run() (EigenvectorCentrality.cpp:20-60): x = 1 for
+ * all z ids; repeat values[u] = sum over in-arcs of w * x[v] (arc order),
+ * length = sqrt(sum of values^2 over existing nodes, id order), values /=
+ * length, swap; until |length - oldLength| <= tol (NumericTools::equal,
+ * NumericTools.cpp:16-18); finally |x| if x[0] < 0. Deleted ids keep 1.
+ * Returns the number of iterations (capped at max_iter), -1 on bad input. */
+int64_t nko_eigenvector(uint64_t z, const uint64_t *in_ptr, const uint32_t *in_col,
+                        const double *in_w, const uint8_t *exists, double tol, uint64_t max_iter,
+                        double *scores);
+
+/* KatzCentrality::run() (KatzCentrality.cpp:28-72) over the given adjacency
+ * (the in-CSR for EdgeDirection::InEdges, the out-CSR for OutEdges):
+ * x = 1; repeat values[u] = sum of w * alpha * (1 + x[v]) + beta, length =
+ * sqrt(sum of values^2), x = values; until |length - oldLength| <= tol;
+ * finally x /= length on existing nodes (deleted ids keep 1). alpha must
+ * already be resolved (the reference's 0 = 1 / (1 + maxDegree)). Returns the
+ * number of iterations (capped at max_iter), -1 on bad input. */
+int64_t nko_katz(uint64_t z, const uint64_t *ptr, const uint32_t *col, const double *w,
+                 const uint8_t *exists, double alpha, double beta, double tol, uint64_t max_iter,
+                 double *scores);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,8 @@
 
 #include <omp.h>
 
+#include <networkit/centrality/EigenvectorCentrality.hpp>
+#include <networkit/centrality/KatzCentrality.hpp>
 #include <networkit/centrality/PageRank.hpp>
 #include <networkit/graph/Graph.hpp>
 #include <networkit/io/GMLGraphReader.hpp>
@@ -108,6 +110,57 @@ int nkref_pagerank(void *g, double damp, double tol, int normalized, int norm,
                 if (ranking_vals_out)
                     ranking_vals_out[i] = r[i].second;
             }
+        }
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// Run the reference EigenvectorCentrality (EigenvectorCentrality.cpp:20-60);
+// scores_out has upperNodeIdBound() entries.
+int nkref_eigenvector(void *g, double tol, int nthreads, double *scores_out,
+                      double *run_seconds_out) {
+    try {
+        if (nthreads > 0)
+            omp_set_num_threads(nthreads);
+        auto &G = *static_cast<RefGraph *>(g)->G;
+        NetworKit::EigenvectorCentrality ec(G, tol);
+        auto t0 = std::chrono::steady_clock::now();
+        ec.run();
+        auto t1 = std::chrono::steady_clock::now();
+        if (run_seconds_out)
+            *run_seconds_out = std::chrono::duration<double>(t1 - t0).count();
+        const auto &sc = ec.scores();
+        std::memcpy(scores_out, sc.data(), sc.size() * sizeof(double));
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// Run the reference KatzCentrality (KatzCentrality.cpp:20-72); out_edges
+// selects EdgeDirection::OutEdges. ranking_ids_out (nullable) gets ranking().
+int nkref_katz(void *g, double alpha, double beta, double tol, int out_edges, int nthreads,
+               double *scores_out, uint64_t *ranking_ids_out, double *run_seconds_out) {
+    try {
+        if (nthreads > 0)
+            omp_set_num_threads(nthreads);
+        auto &G = *static_cast<RefGraph *>(g)->G;
+        NetworKit::KatzCentrality kc(G, alpha, beta, tol);
+        kc.edgeDirection = out_edges ? NetworKit::EdgeDirection::OutEdges
+                                     : NetworKit::EdgeDirection::InEdges;
+        auto t0 = std::chrono::steady_clock::now();
+        kc.run();
+        auto t1 = std::chrono::steady_clock::now();
+        if (run_seconds_out)
+            *run_seconds_out = std::chrono::duration<double>(t1 - t0).count();
+        const auto &sc = kc.scores();
+        std::memcpy(scores_out, sc.data(), sc.size() * sizeof(double));
+        if (ranking_ids_out) {
+            auto r = kc.ranking();
+            for (size_t i = 0; i < r.size(); ++i)
+                ranking_ids_out[i] = r[i].first;
         }
         return 0;
     } catch (const std::exception &e) {

@@ -9,8 +9,9 @@ reads the reference's own test inputs with the reference's own readers
 (SNAP: input/wiki-Vote.txt, METIS: input/celegans_metabolic.graph, GML:
 input/looptest1.gml, input/looptest2.gml), builds the 8-node weighted graph of
 CentralityGTest.cpp:582-607, runs NetworKit::PageRank on one OpenMP thread for
-every (norm, normalized) combination and stores, per graph, the in-adjacency in
-storage order plus the reference results in ``<name>.npz``. The GPU box has no
+every (norm, normalized) combination (plus EigenvectorCentrality and
+KatzCentrality in both edge directions) and stores, per graph, the in- and
+out-adjacency in storage order plus the reference results in ``<name>.npz``. The GPU box has no
 reference checkout: the tests read only these files.
 """
 from __future__ import annotations
@@ -46,7 +47,9 @@ def export_to_arrays(g):
     return dict(z=np.int64(z), in_ptr=ptr.astype(np.uint64), in_col=adj.astype(np.uint32),
                 in_w=(w.astype(np.float64) if ex["weighted"] else np.zeros(0)),
                 weighted=np.bool_(ex["weighted"]), wdeg=wdeg, outdeg=outdeg,
-                exists=ex["exists"].astype(np.uint8), directed=np.bool_(ex["directed"]))
+                exists=ex["exists"].astype(np.uint8), directed=np.bool_(ex["directed"]),
+                out_ptr=ex["out_ptr"].astype(np.uint64), out_col=ex["out_adj"].astype(np.uint32),
+                out_w=(ex["out_w"].astype(np.float64) if ex["weighted"] else np.zeros(0)))
 
 
 def run_all(g, arrays, tag, damp=0.85, tol=1e-8):
@@ -67,6 +70,16 @@ def run_all(g, arrays, tag, damp=0.85, tol=1e-8):
             out[key + "_max2_iterations"] = np.int64(r2["iterations"])
             print(f"  {tag} norm={norm} normalized={normalized}: it={r['iterations']} "
                   f"top={r['ranking_ids'][0]} {r['ranking_vals'][0]:.6g}")
+    # EigenvectorCentrality (tol 1e-9, centrality.pyx:1966) and KatzCentrality
+    # (alpha 0 = default, beta 0.1, tol 1e-8, centrality.pyx:1700) in both edge
+    # directions, and Katz with alpha 5e-4 (CentralityGTest.cpp:216-225).
+    out["ec_scores"] = g.eigenvector(tol=1e-9, nthreads=1)
+    out["katz_in_scores"], ids = g.katz(0.0, 0.1, 1e-8, False, nthreads=1)
+    out["katz_in_rank_ids"] = ids.astype(np.uint32)
+    out["katz_out_scores"], _ = g.katz(0.0, 0.1, 1e-8, True, nthreads=1)
+    out["katz5e4_scores"], ids = g.katz(5e-4, 0.1, 1e-8, False, nthreads=1)
+    out["katz5e4_rank_ids"] = ids.astype(np.uint32)
+    print(f"  {tag} katz(5e-4) top={ids[0]}")
     return out
 
 
