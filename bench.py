@@ -61,7 +61,8 @@ def parse_args():
                     help="sweep launch shape (nkg_graph_options.sweep_shape; -1 default)")
     ap.add_argument("--arc-order", type=int, default=0, choices=[0, 1],
                     help="nkg_graph_options.arc_order (0 keep the reference order, 1 sorted)")
-    ap.add_argument("--form", default="", choices=["", "ppr", "refine", "adjoint", "batch"],
+    ap.add_argument("--form", default="",
+                    choices=["", "ppr", "refine", "adjoint", "batch", "centrality"],
                     help="run only one companion form and print its figures")
     ap.add_argument("--fd-edges", type=int, default=64,
                     help="arcs checked by finite differences in --form adjoint")
@@ -516,6 +517,28 @@ def form_batch(local, count=1024, steps=3, plain_graphs=None, step_only=False):
             "speedup_fp64_batch_vs_plain_fp64": plain_ms / ms64_batch}
 
 
+def form_centrality(local, csr):
+    """EigenvectorCentrality (tol 1e-9) and KatzCentrality (alpha 0 = 1/(1 +
+    max degree), beta 0.1, tol 1e-8, in- and out-edges) on the R-MAT scale-24
+    graph, FP64, graph resident: device time per run and per iteration."""
+    from networkit_b200 import _capi
+
+    dg = _capi.DeviceGraph(csr, device=local)
+    res = {"workload": "eigenvector_katz_rmat24_fp64", "arcs": csr.arcs}
+    runs = (("eigenvector", lambda: dg.eigenvector(1e-9)),
+            ("katz_in", lambda: dg.katz(0.0, 0.1, 1e-8, 0)),
+            ("katz_out", lambda: dg.katz(0.0, 0.1, 1e-8, 1)))
+    for name, fn in runs:
+        fn()  # warm-up (out-layout build for katz_out)
+        _, it, st = fn()
+        ms = st["ms_total"]
+        res[name] = {"ms": ms, "iterations": it, "ms_per_iteration": ms / max(it, 1),
+                     "gteps_per_iter": csr.arcs * it / (ms / 1e3) / 1e9,
+                     "gpu_launches": st["kernel_launches"]}
+    dg.close()
+    return res
+
+
 def run_reference_arm(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -602,6 +625,9 @@ def main():
     csr = make_graph(args.scale, args.cache, rank, barrier)
     if args.form == "refine":
         print(json.dumps(form_refine(local, csr)))
+        return
+    if args.form == "centrality":
+        print(json.dumps(form_centrality(local, csr)))
         return
     arcs, n = csr.arcs, csr.z
     dg = _capi.DeviceGraph(csr, device=local, sweep_shape=args.shape, arc_order=args.arc_order)
@@ -705,6 +731,7 @@ def main():
         for name, fn in (("fp32_refine", lambda: form_refine(local, csr, steps=1)),
                          ("ppr", lambda: form_ppr(local, steps=1)),
                          ("fwd_bwd", lambda: form_adjoint(local, steps=2, fd_edges=0)),
+                         ("eigenvector_katz", lambda: form_centrality(local, csr)),
                          ("batch", lambda: form_batch(local, steps=2,
                                                       plain_graphs=range(0, 1024, 8)))):
             try:

@@ -2,8 +2,9 @@
 
 * ``_lib/libnkgpu.so``  - the CUDA PageRank library behind include/nkgpu.h,
   compiled for sm_100a only.
-* ``_lib/libnkgen.so``  - host-side synthetic graph generators (C++/OpenMP),
-  used by the benchmarks and tests to make their inputs.
+* ``_lib/libnkgen.so``  - host-side synthetic graph generators and the
+  NetworkitBinaryGraph file decoder (C++/OpenMP), used by the benchmarks and
+  tests to make their inputs and by :mod:`networkit_b200.graphio`.
 
 ``python -m networkit_b200.build`` rebuilds whatever is out of date.
 """
@@ -25,7 +26,7 @@ GEN_LIB = os.path.join(LIBDIR, "libnkgen.so")
 
 GPU_SOURCES = ["nkgpu.cu", "noalloc.cu", "ppr.cu", "adjoint.cu", "batch.cu", "centrality.cu"]
 GPU_HEADERS = ["common.cuh", "sweep.cuh", "refine.cuh", "graph.hpp", "host.hpp"]
-GEN_SOURCES = ["graphgen.cpp"]
+GEN_SOURCES = ["graphgen.cpp", "graphio.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -110,6 +110,10 @@ def ref_lib():
         lib.nkref_graph_export.restype = C.c_int
         lib.nkref_graph_export.argtypes = [C.c_void_p, _u64p, _u32p, _f64p, _u64p, _u32p, _f64p,
                                            _u8p]
+        lib.nkref_write_nkbg.restype = C.c_int
+        lib.nkref_write_nkbg.argtypes = [C.c_void_p, C.c_char_p, C.c_uint64, C.c_int]
+        lib.nkref_read_nkbg.restype = C.c_int
+        lib.nkref_read_nkbg.argtypes = [C.POINTER(C.c_void_p), C.c_char_p]
         lib.nkref_eigenvector.restype = C.c_int
         lib.nkref_eigenvector.argtypes = [C.c_void_p, C.c_double, C.c_int, _f64p, _f64p]
         lib.nkref_katz.restype = C.c_int
@@ -305,6 +309,21 @@ class RefGraph:
             raise RuntimeError(lib.nkref_last_error().decode())
         return dict(out_ptr=out_ptr, out_adj=out_adj, out_w=out_w, in_ptr=in_ptr, in_adj=in_adj,
                     in_w=in_w, exists=exists, directed=directed, weighted=self.weighted)
+
+    def write_nkbg(self, path, chunks=32, weights=5):
+        """weights: 0 none, 1 unsigned varint, 2 signed varint, 3 double,
+        4 float, 5 auto-detect (NetworkitBinaryWriter.hpp:17-24)."""
+        lib = ref_lib()
+        if lib.nkref_write_nkbg(self.h, path.encode(), int(chunks), int(weights)) != 0:
+            raise RuntimeError(lib.nkref_last_error().decode())
+
+    @classmethod
+    def read_nkbg(cls, path):
+        lib = ref_lib()
+        h = C.c_void_p()
+        if lib.nkref_read_nkbg(C.byref(h), path.encode()) != 0:
+            raise RuntimeError(lib.nkref_last_error().decode())
+        return cls(h)
 
     def eigenvector(self, tol=1e-9, nthreads=0):
         lib = ref_lib()

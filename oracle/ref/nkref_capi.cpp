@@ -26,6 +26,8 @@
 #include <networkit/centrality/PageRank.hpp>
 #include <networkit/graph/Graph.hpp>
 #include <networkit/io/GMLGraphReader.hpp>
+#include <networkit/io/NetworkitBinaryReader.hpp>
+#include <networkit/io/NetworkitBinaryWriter.hpp>
 #include <networkit/io/METISGraphReader.hpp>
 #include <networkit/io/SNAPGraphReader.hpp>
 
@@ -162,6 +164,35 @@ int nkref_katz(void *g, double alpha, double beta, double tol, int out_edges, in
             for (size_t i = 0; i < r.size(); ++i)
                 ranking_ids_out[i] = r[i].first;
         }
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// Write the graph in the NetworkitBinaryGraph format (NetworkitBinaryWriter,
+// `chunks` node chunks; `weights` = the NetworkitBinaryWeights value: 0 none,
+// 1 unsigned varint, 2 signed varint, 3 double, 4 float, 5 auto-detect).
+int nkref_write_nkbg(void *g, const char *path, uint64_t chunks, int weights) {
+    try {
+        if (weights < 0 || weights > 5)
+            throw std::runtime_error("weights must be in 0..5");
+        NetworKit::NetworkitBinaryWriter w(chunks,
+                                           static_cast<NetworKit::NetworkitBinaryWeights>(weights));
+        w.write(*static_cast<RefGraph *>(g)->G, path);
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// Read a NetworkitBinaryGraph file with the reference's reader.
+int nkref_read_nkbg(void **out, const char *path) {
+    try {
+        NetworKit::NetworkitBinaryReader r;
+        auto *rg = new RefGraph();
+        rg->G.reset(new NetworKit::Graph(r.read(path)));
+        *out = rg;
         return 0;
     } catch (const std::exception &e) {
         return fail(e);

@@ -11,7 +11,11 @@ input/looptest1.gml, input/looptest2.gml), builds the 8-node weighted graph of
 CentralityGTest.cpp:582-607, runs NetworKit::PageRank on one OpenMP thread for
 every (norm, normalized) combination (plus EigenvectorCentrality and
 KatzCentrality in both edge directions) and stores, per graph, the in- and
-out-adjacency in storage order plus the reference results in ``<name>.npz``. The GPU box has no
+out-adjacency in storage order plus the reference results in ``<name>.npz``.
+It also writes every graph with the reference's NetworkitBinaryWriter
+(``<name>.nkbg``) and stores the adjacency the reference's reader builds from
+that file (keys ``nkbg_*``), plus one file per weight encoding of the format
+(``nkbg_<case>.nkbg``, ``nkbg_formats.npz``). The GPU box has no
 reference checkout: the tests read only these files.
 """
 from __future__ import annotations
@@ -109,7 +113,68 @@ def main():
         arrays = export_to_arrays(g)
         print(f"{name}: z={g.z} n={g.n} m={g.m} directed={g.directed} weighted={g.weighted}")
         res = run_all(g, arrays, name)
+        # NetworkitBinaryGraph round trip: the reference writer (4 node chunks)
+        # and the adjacency the reference reader stores for that file.
+        nkbg = os.path.join(HERE, f"{name}.nkbg")
+        g.write_nkbg(nkbg, chunks=4)
+        back = export_to_arrays(O.RefGraph.read_nkbg(nkbg))
+        res.update({"nkbg_" + k: back[k] for k in NKBG_KEYS})
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **arrays, **res)
+    nkbg_formats(O)
+
+
+NKBG_KEYS = ("in_ptr", "in_col", "in_w", "wdeg", "outdeg", "exists", "directed", "weighted")
+
+
+def nkbg_formats(O):
+    """One small file per weight encoding of the binary format (none,
+    unsigned varint, signed varint, double, float), with isolated nodes,
+    self-loops, duplicate edges, several chunk counts and ids / weights that
+    need every varint length (1..9 bytes). Stored: the files
+    (``nkbg_<case>.nkbg``) and the adjacency the reference reader builds from
+    each (``nkbg_formats.npz``, keys ``<case>_<field>``).
+
+    No case has deleted nodes: the reference writer lists only existing nodes
+    (forNodes) under ids 0..numberOfNodes()-1 (NetworkitBinaryWriter.cpp:128,
+    :253-290), so such a graph does not round trip, and the reference reader
+    asserts that a node exists before preallocating its lists
+    (Graph.cpp:173), so a file with a cleared flag byte stops it."""
+    rng = np.random.default_rng(2024)
+    out = {}
+    cases = [
+        # name, nodes, edges, directed, weights type, chunks
+        ("unsigned_dir", 3000, 12000, True, 1, 5),
+        ("signed_undir", 2500, 9000, False, 2, 3),
+        ("double_undir", 1800, 7000, False, 3, 7),
+        ("float_dir", 2200, 8000, True, 4, 2),
+        ("none_undir", 70000, 6000, False, 0, 9),
+        ("none_dir", 500, 3000, True, 0, 1),
+    ]
+    for name, z, m, directed, wtype, chunks in cases:
+        # endpoints below z - 40: the top 40 ids stay isolated
+        src = ((z - 40) * rng.random(m) ** 2).astype(np.uint32)
+        dst = ((z - 40) * rng.random(m)).astype(np.uint32)
+        src[:25] = dst[:25]  # self-loops
+        src = np.concatenate([src, src[:30]])  # duplicates
+        dst = np.concatenate([dst, dst[:30]])
+        w = None
+        if wtype == 1:
+            w = rng.integers(0, 300, src.shape[0]).astype(np.float64)
+            w[:4] = [2.0 ** 20, 2.0 ** 40, 2.0 ** 55, 2.0 ** 60]
+        elif wtype == 2:
+            w = rng.integers(-200, 200, src.shape[0]).astype(np.float64)
+            w[:3] = [-(2.0 ** 50), 2.0 ** 45, -1.0]
+        elif wtype == 3:
+            w = rng.random(src.shape[0]) * 10 - 2
+        elif wtype == 4:
+            w = rng.integers(-4000, 4000, src.shape[0]) / 8.0
+        g = O.RefGraph.from_edges(z, src, dst, w, directed=directed, weighted=w is not None)
+        path = os.path.join(HERE, f"nkbg_{name}.nkbg")
+        g.write_nkbg(path, chunks=chunks, weights=wtype)
+        back = export_to_arrays(O.RefGraph.read_nkbg(path))
+        out.update({f"{name}_{k}": back[k] for k in NKBG_KEYS})
+        print(f"nkbg_{name}: z={z} m={src.shape[0]} {os.path.getsize(path)} bytes")
+    np.savez_compressed(os.path.join(HERE, "nkbg_formats.npz"), **out)
 
 
 if __name__ == "__main__":
