@@ -62,7 +62,7 @@ def parse_args():
     ap.add_argument("--arc-order", type=int, default=0, choices=[0, 1],
                     help="nkg_graph_options.arc_order (0 keep the reference order, 1 sorted)")
     ap.add_argument("--form", default="",
-                    choices=["", "ppr", "refine", "adjoint", "batch", "centrality"],
+                    choices=["", "ppr", "refine", "adjoint", "batch", "centrality", "local"],
                     help="run only one companion form and print its figures")
     ap.add_argument("--fd-edges", type=int, default=64,
                     help="arcs checked by finite differences in --form adjoint")
@@ -539,6 +539,58 @@ def form_centrality(local, csr):
     return res
 
 
+def form_local(local, n=1_000_000, deg=16, seeds=4096, alpha=0.1, eps=1e-5, ref_sample=48):
+    """PageRankNibble(G, 0.1, 1e-5) (the SelectiveCDGTest.cpp parameters),
+    one community per seed (SelectiveCommunityDetector::run) for `seeds`
+    random seeds of an undirected threshold hyperbolic graph (n nodes,
+    average degree `deg`, exponent 3): device time, end-to-end time through
+    the C ABI (host seeds in, host communities out), pushes per second, and
+    the reference's own PageRankNibble on a sample of the seeds (one core: the
+    reference runs the seeds one after another)."""
+    from networkit_b200 import _capi, generators
+
+    g = generators.hyperbolic(n, deg, 3, seed=11)
+    dl = _capi.DeviceLocal(g.z, g.in_ptr, g.in_col, None, None, False, device=local)
+    rng = np.random.default_rng(5)
+    sd = np.sort(rng.choice(g.z, seeds, replace=False))
+    problems = [[int(s)] for s in sd]
+    dl.run(problems[:256], alpha, eps, nibble=True)  # warm-up: slots, pool, module
+    t0 = time.perf_counter()
+    sups, sets, st = dl.run(problems, alpha, eps, nibble=True)
+    wall = time.perf_counter() - t0
+    res = {"workload": f"pagerank_nibble_hyperbolic{n}_deg{deg}_seeds{seeds}",
+           "alpha": alpha, "epsilon": eps, "n": g.z, "arcs": g.arcs, "seeds": seeds,
+           "slots": st["slots"], "pushes": st["pushes"],
+           "mean_support": st["support"] / seeds,
+           "mean_set": float(np.mean([s.shape[0] for s in sets])),
+           "ms_device": st["ms_total"], "ms_push_kernel": st["ms_push"],
+           "seeds_per_s": seeds / (st["ms_total"] / 1e3),
+           "pushes_per_s": st["pushes"] / (st["ms_push"] / 1e3),
+           "e2e_seeds_per_s": seeds / wall, "e2e_ms": 1e3 * wall,
+           "gpu_launches": st["kernel_launches"]}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if oracle.ref_available():
+        # Insert the edges (u < v, lexicographic: the generator's order) so
+        # that every reference row lists its neighbours in the same order.
+        rows = np.repeat(np.arange(g.z, dtype=np.uint32), np.diff(g.in_ptr).astype(np.int64))
+        keep = rows < g.in_col
+        rg = oracle.RefGraph.from_edges(g.z, rows[keep], g.in_col[keep], directed=False)
+        sample = sd[:: max(1, seeds // ref_sample)][:ref_sample]
+        ref_sets, secs = rg.prn(alpha, eps, sample)
+        idx = np.searchsorted(sd, sample)
+        same = sum(int(np.array_equal(ref_sets[i], sets[j])) for i, j in enumerate(idx))
+        res["reference"] = {"seeds": int(sample.shape[0]), "seconds": secs,
+                            "seeds_per_s": sample.shape[0] / secs, "cores": 1,
+                            "kind": "reference",
+                            "sets_identical": same}
+        res["speedup_vs_reference_device"] = res["seeds_per_s"] / res["reference"]["seeds_per_s"]
+        res["speedup_vs_reference_e2e"] = res["e2e_seeds_per_s"] / res["reference"]["seeds_per_s"]
+    dl.close()
+    return res
+
+
 def run_reference_arm(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -601,6 +653,9 @@ def main():
     if args.form == "batch":
         print(json.dumps(form_batch(local, count=args.batch_graphs,
                                     step_only=args.batch_step_only)))
+        return
+    if args.form == "local":
+        print(json.dumps(form_local(local)))
         return
     if args.form == "adjoint":
         print(json.dumps(form_adjoint(local, scale=args.adjoint_scale, fd_edges=args.fd_edges,
@@ -732,6 +787,7 @@ def main():
                          ("ppr", lambda: form_ppr(local, steps=1)),
                          ("fwd_bwd", lambda: form_adjoint(local, steps=2, fd_edges=0)),
                          ("eigenvector_katz", lambda: form_centrality(local, csr)),
+                         ("pagerank_nibble", lambda: form_local(local)),
                          ("batch", lambda: form_batch(local, steps=2,
                                                       plain_graphs=range(0, 1024, 8)))):
             try:

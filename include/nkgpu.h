@@ -323,6 +323,58 @@ NKG_API int nkg_pagerank_csr_noalloc(uint64_t n, uint64_t arcs, const uint64_t *
                                      double *d_scores_out, uint64_t *iterations_out,
                                      void *stream);
 
+/* Local (seeded) PageRank: ApproximatePageRank (scd/ApproximatePageRank.cpp:18-55,
+ * scd.pyx:87-136) and PageRankNibble (scd/PageRankNibble.cpp:28-89,
+ * scd.pyx:138-151), many independent problems per call.
+ *
+ * nkg_local_create uploads the neighbour CSR in Graph::forNeighborsOf order
+ * (undirected graphs: the neighbour lists, self-loops once; directed graphs:
+ * the out-lists in insertion order), weights w (NULL: unweighted), the
+ * existence mask (NULL: all exist) and the graph kind. It computes
+ * weightedDegree(u, true) of every node (Graph.cpp:427-453) and
+ * 2 * totalEdgeWeight() (Graph.cpp:860-868). memory_budget bounds the
+ * per-problem state, 28 bytes per node for every problem in flight
+ * (0: half the free device memory, at most 48 GiB).
+ *
+ * nkg_local_run: problem k has the seeds seeds[seed_ptr[k] .. seed_ptr[k+1])
+ * (ascending, no duplicates: the reference's std::set<node>) and runs
+ * ApproximatePageRank(G, alpha, epsilon).run(seeds) in the reference's push
+ * order, bit for bit. With NKG_LOCAL_NIBBLE it also runs
+ * PageRankNibble::bestSweepSet on each result (ties of p/vol broken by
+ * ascending node id). One problem per seed is SelectiveCommunityDetector::run
+ * (SelectiveCommunityDetector.cpp:15-23); one problem of all seeds is
+ * expandOneCommunity(seeds). max_pushes bounds the pushes of one problem
+ * (UINT64_MAX: none); a problem that reaches it fails the call with
+ * NKG_ERR_TIMEOUT. epsilon must be > 0. support_sizes_out / set_sizes_out
+ * (nullable, host) receive per-problem counts.
+ * nkg_local_support: the supports of the last run (every node the result
+ * map holds), problem after problem, each ascending by id, with its value
+ * (values_out nullable); sum of support sizes entries.
+ * nkg_local_sets: the PageRankNibble sets of the last run, problem after
+ * problem, each ascending. */
+typedef struct nkg_local nkg_local;
+#define NKG_LOCAL_NIBBLE 2
+typedef struct {
+    uint64_t pushes;          /* pushes over all problems */
+    uint64_t support;         /* sum of the support sizes */
+    uint64_t slots;           /* problems in flight (resident warps) */
+    uint64_t reruns;          /* push launches repeated to grow the result pool */
+    double ms_push;           /* device time of the push kernel(s) */
+    double ms_sweep;          /* device time of the sorts and the sweep */
+    double ms_total;
+    uint64_t kernel_launches;
+} nkg_local_stats;
+NKG_API int nkg_local_create(nkg_local **out, uint64_t z, const uint64_t *row_ptr,
+                             const uint32_t *col, const double *w, const uint8_t *exists,
+                             int directed, int device, uint64_t memory_budget);
+NKG_API void nkg_local_destroy(nkg_local *h);
+NKG_API int nkg_local_run(nkg_local *h, double alpha, double epsilon, uint64_t problems,
+                          const uint64_t *seed_ptr, const uint32_t *seeds, int flags,
+                          uint64_t max_pushes, uint64_t *support_sizes_out,
+                          uint64_t *set_sizes_out, nkg_local_stats *stats);
+NKG_API int nkg_local_support(nkg_local *h, uint32_t *nodes_out, double *values_out);
+NKG_API int nkg_local_sets(nkg_local *h, uint32_t *nodes_out);
+
 /* Message of the last failure on the calling thread ("" if none). */
 NKG_API const char *nkg_last_error(void);
 

@@ -94,6 +94,17 @@ class BatchTuning(C.Structure):
                 "variant": self.variant, "ms": self.ms}
 
 
+class LocalStats(C.Structure):
+    _fields_ = [("pushes", C.c_uint64), ("support", C.c_uint64), ("slots", C.c_uint64),
+                ("reruns", C.c_uint64), ("ms_push", C.c_double), ("ms_sweep", C.c_double),
+                ("ms_total", C.c_double), ("kernel_launches", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+NKG_LOCAL_NIBBLE = 2
+
 _u64p = C.POINTER(C.c_uint64)
 _u32p = C.POINTER(C.c_uint32)
 _u8p = C.POINTER(C.c_uint8)
@@ -144,6 +155,13 @@ SIGNATURES = {
     "nkg_batch_run": (C.c_int, [_vp, C.POINTER(PRParams), _vp, C.c_int, _u64p,
                                 C.POINTER(C.c_uint32), C.POINTER(Stats)]),
     "nkg_batch_graph_times": (C.c_int, [_vp, _f64p, _f64p]),
+    "nkg_local_create": (C.c_int, [C.POINTER(_vp), C.c_uint64, _u64p, _u32p, _f64p, _u8p, C.c_int,
+                                   C.c_int, C.c_uint64]),
+    "nkg_local_destroy": (None, [_vp]),
+    "nkg_local_run": (C.c_int, [_vp, C.c_double, C.c_double, C.c_uint64, _u64p, _u32p, C.c_int,
+                                C.c_uint64, _u64p, _u64p, C.POINTER(LocalStats)]),
+    "nkg_local_support": (C.c_int, [_vp, _u32p, _f64p]),
+    "nkg_local_sets": (C.c_int, [_vp, _u32p]),
 }
 
 _lib = None
@@ -479,3 +497,70 @@ class DeviceBatch:
         check(lib().nkg_batch_run(self.h, C.byref(p), _vp(out.ctypes.data), 0, ptr(its, _u64p),
                                   C.byref(fl), C.byref(st)))
         return out, its, int(fl.value), st.as_dict()
+
+
+class DeviceLocal:
+    """Owning wrapper of an nkg_local handle: the neighbour CSR (forNeighborsOf
+    order) for ApproximatePageRank / PageRankNibble runs."""
+
+    def __init__(self, z, row_ptr, col, w=None, exists=None, directed=False, device: int = -1,
+                 memory_budget: int = 0):
+        L = lib()
+        h = _vp()
+        self._ptr = np.ascontiguousarray(row_ptr, np.uint64)
+        self._col = np.ascontiguousarray(col, np.uint32)
+        self._w = None if w is None else np.ascontiguousarray(w, np.float64)
+        self._ex = None if exists is None else np.ascontiguousarray(exists, np.uint8)
+        check(L.nkg_local_create(C.byref(h), int(z), ptr(self._ptr, _u64p), ptr(self._col, _u32p),
+                                 ptr(self._w, _f64p), ptr(self._ex, _u8p), int(bool(directed)),
+                                 int(device), int(memory_budget)))
+        self.h = h
+        self.z = int(z)
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().nkg_local_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, seed_sets, alpha, epsilon, nibble=False, max_pushes=UINT64_MAX):
+        """seed_sets: list of seed collections (each made a sorted set).
+        Returns (supports, sets, stats): supports = [(nodes, values)] per
+        problem (ascending ids); sets = [nodes] per problem or None."""
+        sets_ = [np.unique(np.atleast_1d(np.asarray(list(s) if isinstance(s, (set, frozenset))
+                                                    else s, np.int64))) for s in seed_sets]
+        seed_ptr = np.zeros(len(sets_) + 1, np.uint64)
+        np.cumsum([x.shape[0] for x in sets_], out=seed_ptr[1:])
+        seeds = (np.concatenate(sets_) if sets_ else np.zeros(0)).astype(np.uint32)
+        if seeds.size and (np.concatenate(sets_).min() < 0):
+            raise NkgError(NKG_ERR_INVALID_ARG, "negative seed id")
+        k = len(sets_)
+        sup = np.zeros(k, np.uint64)
+        setc = np.zeros(k, np.uint64)
+        st = LocalStats()
+        check(lib().nkg_local_run(self.h, float(alpha), float(epsilon), k, ptr(seed_ptr, _u64p),
+                                  ptr(seeds, _u32p), NKG_LOCAL_NIBBLE if nibble else 0,
+                                  int(max_pushes), ptr(sup, _u64p),
+                                  ptr(setc, _u64p) if nibble else None, C.byref(st)))
+        tot = int(sup.sum())
+        nodes = np.empty(max(tot, 1), np.uint32)
+        vals = np.empty(max(tot, 1), np.float64)
+        check(lib().nkg_local_support(self.h, ptr(nodes, _u32p), ptr(vals, _f64p)))
+        offs = np.zeros(k + 1, np.int64)
+        np.cumsum(sup.astype(np.int64), out=offs[1:])
+        supports = [(nodes[offs[i]:offs[i + 1]].copy(), vals[offs[i]:offs[i + 1]].copy())
+                    for i in range(k)]
+        sets_out = None
+        if nibble:
+            ts = int(setc.sum())
+            sn = np.empty(max(ts, 1), np.uint32)
+            check(lib().nkg_local_sets(self.h, ptr(sn, _u32p)))
+            so = np.zeros(k + 1, np.int64)
+            np.cumsum(setc.astype(np.int64), out=so[1:])
+            sets_out = [sn[so[i]:so[i + 1]].copy() for i in range(k)]
+        return supports, sets_out, st.as_dict()

@@ -24,7 +24,8 @@ INCLUDE = os.path.join(ROOT, "include")
 GPU_LIB = os.path.join(LIBDIR, "libnkgpu.so")
 GEN_LIB = os.path.join(LIBDIR, "libnkgen.so")
 
-GPU_SOURCES = ["nkgpu.cu", "noalloc.cu", "ppr.cu", "adjoint.cu", "batch.cu", "centrality.cu"]
+GPU_SOURCES = ["nkgpu.cu", "noalloc.cu", "ppr.cu", "adjoint.cu", "batch.cu", "centrality.cu",
+               "local.cu"]
 GPU_HEADERS = ["common.cuh", "sweep.cuh", "refine.cuh", "graph.hpp", "host.hpp"]
 GEN_SOURCES = ["graphgen.cpp", "graphio.cpp"]
 
@@ -67,10 +68,11 @@ def build_gpu(force: bool = False, verbose: bool = False) -> str:
 
 def build_gen(force: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in GEN_SOURCES]
-    if not force and not _stale(GEN_LIB, srcs + [__file__]):
+    if not force and not _stale(GEN_LIB, srcs + [os.path.join(INCLUDE, "nkgio.h"), __file__]):
         return GEN_LIB
     os.makedirs(LIBDIR, exist_ok=True)
     cmd = [_host_cxx(), "-std=c++17", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared",
+           "-I", INCLUDE,
            "-o", GEN_LIB + ".tmp", *srcs]
     subprocess.run(cmd, check=True)
     os.replace(GEN_LIB + ".tmp", GEN_LIB)

@@ -20,6 +20,8 @@
 // sum of v's out-list weights in list order; undirected graphs: row v = v's
 // out list, then its transpose list without self-loops; weighted degree = sum
 // over that row in row order.
+#include "nkgio.h"
+
 #include <omp.h>
 
 #include <algorithm>
@@ -119,19 +121,6 @@ struct ChunkOut {
 } // namespace
 
 extern "C" {
-
-struct nkgen_graph {
-    uint64_t z;
-    uint64_t arcs;
-    uint64_t *in_ptr;
-    uint32_t *in_col;
-    uint32_t *outdeg;
-    double *w;       // NULL when unweighted
-    double *wdeg;
-    uint8_t *exists;
-    int directed;
-    int weighted;
-};
 
 const char *nkgen_io_last_error(void) { return g_io_err.c_str(); }
 

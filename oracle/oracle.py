@@ -80,6 +80,14 @@ def oracle_lib():
         lib.nko_katz.restype = C.c_int64
         lib.nko_katz.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _u8p, C.c_double, C.c_double,
                                  C.c_double, C.c_uint64, _f64p]
+        lib.nko_volumes.restype = C.c_int
+        lib.nko_volumes.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _f64p]
+        lib.nko_apr.restype = C.c_int64
+        lib.nko_apr.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _f64p, C.c_double, C.c_double,
+                                _u32p, C.c_uint64, C.c_uint64, _u32p, _f64p, _u64p]
+        lib.nko_sweep_set.restype = C.c_int64
+        lib.nko_sweep_set.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _f64p, C.c_double,
+                                      C.c_uint64, C.c_uint64, _u32p, _f64p, _u32p]
         _oracle = lib
     return _oracle
 
@@ -123,6 +131,12 @@ def ref_lib():
         lib.nkref_pagerank.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_int,
                                        C.c_uint64, C.c_int, _f64p, _u64p, _f64p, _u64p, _f64p,
                                        _f64p]
+        lib.nkref_apr.restype = C.c_int
+        lib.nkref_apr.argtypes = [C.c_void_p, C.c_double, C.c_double, _u32p, C.c_uint64,
+                                  C.c_uint64, _u32p, _f64p, _u64p, _f64p]
+        lib.nkref_prn.restype = C.c_int
+        lib.nkref_prn.argtypes = [C.c_void_p, C.c_double, C.c_double, _u32p, C.c_uint64, C.c_int,
+                                  C.c_uint64, _u64p, _u32p, _u64p, _f64p]
         _ref = lib
     return _ref
 
@@ -231,6 +245,65 @@ def adjoint(csr, x, g, damp=0.85, distribute_sinks=True, teleport=None, tol=1e-1
 # The reference library (oracle/_ref)
 
 
+def volumes(z, ptr, col, w=None):
+    """weightedDegree(u, true) of every node of a neighbour CSR."""
+    vol = np.empty(int(z), np.float64)
+    oracle_lib().nko_volumes(int(z), _ptr(np.ascontiguousarray(ptr, np.uint64), _u64p),
+                             _ptr(np.ascontiguousarray(col, np.uint32), _u32p),
+                             _ptr(None if w is None else np.ascontiguousarray(w, np.float64),
+                                  _f64p), _ptr(vol, _f64p))
+    return vol
+
+
+@dataclass
+class AprResult:
+    nodes: np.ndarray   # support, ascending ids
+    values: np.ndarray  # p of each support node
+    pushes: int
+
+
+def apr(z, ptr, col, w, seeds, alpha, eps, vol=None):
+    """ApproximatePageRank(G, alpha, eps).run(seeds) over the neighbour CSR
+    (forNeighborsOf order); seeds: any iterable (made a sorted set)."""
+    ptr = np.ascontiguousarray(ptr, np.uint64)
+    col = np.ascontiguousarray(col, np.uint32)
+    w = None if w is None else np.ascontiguousarray(w, np.float64)
+    if vol is None:
+        vol = volumes(z, ptr, col, w)
+    sd = np.unique(np.asarray(list(seeds) if not np.isscalar(seeds) else [seeds],
+                              np.int64)).astype(np.uint32)
+    cap = 1 << 16
+    pushes = C.c_uint64(0)
+    while True:
+        nodes = np.empty(cap, np.uint32)
+        vals = np.empty(cap, np.float64)
+        cnt = oracle_lib().nko_apr(int(z), _ptr(ptr, _u64p), _ptr(col, _u32p), _ptr(w, _f64p),
+                                   _ptr(vol, _f64p), float(alpha), float(eps), _ptr(sd, _u32p),
+                                   sd.shape[0], cap, _ptr(nodes, _u32p), _ptr(vals, _f64p),
+                                   C.byref(pushes))
+        if cnt < 0:
+            raise ValueError("bad APR input")
+        if cnt <= cap:
+            return AprResult(nodes[:cnt].copy(), vals[:cnt].copy(), int(pushes.value))
+        cap = int(cnt)
+
+
+def sweep_set(z, ptr, col, w, vol, total_volume, n_nodes, nodes, values):
+    """PageRankNibble::bestSweepSet over an APR support; ascending ids."""
+    nodes = np.ascontiguousarray(nodes, np.uint32)
+    values = np.ascontiguousarray(values, np.float64)
+    out = np.empty(max(1, nodes.shape[0]), np.uint32)
+    k = oracle_lib().nko_sweep_set(
+        int(z), _ptr(np.ascontiguousarray(ptr, np.uint64), _u64p),
+        _ptr(np.ascontiguousarray(col, np.uint32), _u32p),
+        _ptr(None if w is None else np.ascontiguousarray(w, np.float64), _f64p),
+        _ptr(np.ascontiguousarray(vol, np.float64), _f64p), float(total_volume), int(n_nodes),
+        nodes.shape[0], _ptr(nodes, _u32p), _ptr(values, _f64p), _ptr(out, _u32p))
+    if k < 0:
+        raise ValueError("bad sweep input")
+    return out[:k].copy()
+
+
 class RefGraph:
     """A NetworKit::Graph owned by the reference library."""
 
@@ -324,6 +397,47 @@ class RefGraph:
         if lib.nkref_read_nkbg(C.byref(h), path.encode()) != 0:
             raise RuntimeError(lib.nkref_last_error().decode())
         return cls(h)
+
+    def apr(self, alpha, eps, seeds):
+        """The reference's ApproximatePageRank(G, alpha, eps).run(seeds):
+        (nodes ascending, values, seconds)."""
+        lib = ref_lib()
+        sd = np.ascontiguousarray(np.atleast_1d(np.asarray(seeds, np.int64)), np.uint32)
+        cap = 1 << 16
+        while True:
+            nodes = np.empty(cap, np.uint32)
+            vals = np.empty(cap, np.float64)
+            cnt = C.c_uint64(0)
+            secs = C.c_double(0.0)
+            if lib.nkref_apr(self.h, float(alpha), float(eps), _ptr(sd, _u32p), sd.shape[0], cap,
+                             _ptr(nodes, _u32p), _ptr(vals, _f64p), C.byref(cnt),
+                             C.byref(secs)) != 0:
+                raise RuntimeError(lib.nkref_last_error().decode())
+            if cnt.value <= cap:
+                k = int(cnt.value)
+                return nodes[:k].copy(), vals[:k].copy(), secs.value
+            cap = int(cnt.value)
+
+    def prn(self, alpha, eps, seeds, joint=False):
+        """The reference's PageRankNibble(G, alpha, eps): one community per
+        seed (run(seeds), seeds ascending) or, with joint, one community of
+        the seed set. Returns (list of ascending id arrays, seconds)."""
+        lib = ref_lib()
+        sd = np.ascontiguousarray(np.atleast_1d(np.asarray(seeds, np.int64)), np.uint32)
+        k = 1 if joint else np.unique(sd).shape[0]
+        cap = 1 << 16
+        while True:
+            offs = np.zeros(k + 1, np.uint64)
+            sets = np.empty(cap, np.uint32)
+            tot = C.c_uint64(0)
+            secs = C.c_double(0.0)
+            if lib.nkref_prn(self.h, float(alpha), float(eps), _ptr(sd, _u32p), sd.shape[0],
+                             int(bool(joint)), cap, _ptr(offs, _u64p), _ptr(sets, _u32p),
+                             C.byref(tot), C.byref(secs)) != 0:
+                raise RuntimeError(lib.nkref_last_error().decode())
+            if tot.value <= cap:
+                return [sets[int(offs[i]):int(offs[i + 1])].copy() for i in range(k)], secs.value
+            cap = int(tot.value)
 
     def eigenvector(self, tol=1e-9, nthreads=0):
         lib = ref_lib()

@@ -370,3 +370,202 @@ int64_t nko_katz(uint64_t z, const uint64_t *ptr, const uint32_t *col, const dou
     free(values);
     return it;
 }
+
+/* ---------------------------------------------------------------------------
+ * Local PageRank: ApproximatePageRank (ApproximatePageRank.cpp:18-55) and the
+ * sweep of PageRankNibble (PageRankNibble.cpp:28-82).
+ * ------------------------------------------------------------------------- */
+
+int nko_volumes(uint64_t z, const uint64_t *ptr, const uint32_t *col, const double *w,
+                double *vol) {
+    for (uint64_t u = 0; u < z; ++u) {
+        if (w) {
+            double sum = 0.0;
+            for (uint64_t k = ptr[u]; k < ptr[u + 1]; ++k)
+                sum += (col[k] == u) ? 2. * w[k] : w[k];
+            vol[u] = sum;
+        } else {
+            uint64_t sum = ptr[u + 1] - ptr[u];
+            for (uint64_t k = ptr[u]; k < ptr[u + 1]; ++k)
+                sum += (col[k] == u);
+            vol[u] = (double)sum;
+        }
+    }
+    return 0;
+}
+
+typedef struct {
+    uint32_t *buf;
+    uint64_t cap, head, size;
+} fifo_t;
+
+static int fifo_push(fifo_t *q, uint32_t v) {
+    if (q->size == q->cap) {
+        uint64_t ncap = q->cap ? 2 * q->cap : 64;
+        uint32_t *nb = (uint32_t *)malloc(ncap * sizeof(uint32_t));
+        if (!nb)
+            return -1;
+        for (uint64_t i = 0; i < q->size; ++i)
+            nb[i] = q->buf[(q->head + i) % q->cap];
+        free(q->buf);
+        q->buf = nb;
+        q->cap = ncap;
+        q->head = 0;
+    }
+    q->buf[(q->head + q->size) % q->cap] = v;
+    q->size++;
+    return 0;
+}
+
+static uint32_t fifo_pop(fifo_t *q) {
+    uint32_t v = q->buf[q->head];
+    q->head = (q->head + 1) % q->cap;
+    q->size--;
+    return v;
+}
+
+int64_t nko_apr(uint64_t z, const uint64_t *ptr, const uint32_t *col, const double *w,
+                const double *vol, double alpha, double eps, const uint32_t *seeds,
+                uint64_t nseeds, uint64_t cap, uint32_t *nodes, double *values,
+                uint64_t *pushes) {
+    if (nseeds == 0)
+        return -1;
+    for (uint64_t i = 0; i < nseeds; ++i)
+        if (seeds[i] >= z || (i && seeds[i] <= seeds[i - 1]))
+            return -1;
+    double *r = (double *)calloc(z ? z : 1, sizeof(double));
+    double *p = (double *)calloc(z ? z : 1, sizeof(double));
+    uint8_t *in_map = (uint8_t *)calloc(z ? z : 1, 1);
+    fifo_t q = {NULL, 0, 0, 0};
+    int64_t ret = -1;
+    uint64_t npush = 0;
+    if (!r || !p || !in_map)
+        goto done;
+    const double init_res = 1.0 / (double)nseeds;
+    for (uint64_t i = 0; i < nseeds; ++i) {
+        const uint32_t s = seeds[i];
+        in_map[s] = 1;
+        p[s] = 0.0;
+        r[s] = init_res;
+        if (fifo_push(&q, s))
+            goto done;
+    }
+    while (q.size) {
+        const uint32_t u = fifo_pop(&q);
+        const double res = r[u];
+        const double volume = vol[u];
+        for (uint64_t k = ptr[u]; k < ptr[u + 1]; ++k) {
+            const uint32_t v = col[k];
+            const double wk = w ? w[k] : 1.0;
+            const double mass = (1.0 - alpha) * res * wk / (2.0 * volume);
+            const double vol_v = vol[v];
+            in_map[v] = 1;
+            if (r[v] < vol_v * eps && (r[v] + mass) >= eps * vol_v)
+                if (fifo_push(&q, v))
+                    goto done;
+            r[v] += mass;
+        }
+        p[u] = p[u] + alpha * res;
+        r[u] = (1.0 - alpha) * res / 2;
+        if ((r[u] / volume) >= eps)
+            if (fifo_push(&q, u))
+                goto done;
+        npush++;
+    }
+    {
+        uint64_t cnt = 0;
+        for (uint64_t v = 0; v < z; ++v)
+            if (in_map[v]) {
+                if (cnt < cap) {
+                    nodes[cnt] = (uint32_t)v;
+                    values[cnt] = p[v];
+                }
+                cnt++;
+            }
+        ret = (int64_t)cnt;
+    }
+done:
+    if (pushes)
+        *pushes = npush;
+    free(r);
+    free(p);
+    free(in_map);
+    free(q.buf);
+    return ret;
+}
+
+/* Order-preserving map of a double onto uint64 (sign-magnitude to offset
+ * binary): numeric order, -0 before +0, NaNs at the ends. */
+static uint64_t order_bits(double d) {
+    uint64_t u;
+    memcpy(&u, &d, 8);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+
+typedef struct {
+    uint64_t key;
+    uint32_t node;
+} sweep_item;
+
+static int sweep_cmp(const void *a, const void *b) {
+    const sweep_item *x = (const sweep_item *)a, *y = (const sweep_item *)b;
+    if (x->key != y->key)
+        return x->key > y->key ? -1 : 1;
+    return x->node < y->node ? -1 : (x->node > y->node);
+}
+
+static int u32_cmp(const void *a, const void *b) {
+    const uint32_t x = *(const uint32_t *)a, y = *(const uint32_t *)b;
+    return x < y ? -1 : (x > y);
+}
+
+int64_t nko_sweep_set(uint64_t z, const uint64_t *ptr, const uint32_t *col, const double *w,
+                      const double *vol, double total_volume, uint64_t n_nodes,
+                      uint64_t support, const uint32_t *nodes, const double *values,
+                      uint32_t *set) {
+    sweep_item *it = (sweep_item *)malloc((support ? support : 1) * sizeof(sweep_item));
+    uint8_t *within = (uint8_t *)calloc(z ? z : 1, 1);
+    int64_t ret = -1;
+    if (!it || !within)
+        goto done;
+    for (uint64_t i = 0; i < support; ++i) {
+        if (nodes[i] >= z)
+            goto done;
+        it[i].node = nodes[i];
+        it[i].key = order_bits(values[i] / vol[nodes[i]]);
+    }
+    qsort(it, support, sizeof(sweep_item), sweep_cmp);
+    {
+        double best_cond = 1.79769313486231570815e+308; /* DBL_MAX */
+        double cut = 0.0, volume = 0.0;
+        uint64_t best = 0;
+        for (uint64_t i = 0; i < support; ++i) {
+            const uint32_t v = it[i].node;
+            double wdeg = 0.0;
+            for (uint64_t k = ptr[v]; k < ptr[v + 1]; ++k) {
+                const double wk = w ? w[k] : 1.0;
+                wdeg += wk;
+                if (!within[col[k]])
+                    cut += wk;
+                else
+                    cut -= wk;
+            }
+            volume += wdeg;
+            within[v] = 1;
+            const double other = total_volume - volume;
+            const double cond = cut / ((other < volume) ? other : volume); /* std::min */
+            if ((cond < best_cond) && (i + 1 < n_nodes)) {
+                best_cond = cond;
+                best = i + 1;
+            }
+        }
+        for (uint64_t i = 0; i < best; ++i)
+            set[i] = it[i].node;
+        qsort(set, best, sizeof(uint32_t), u32_cmp);
+        ret = (int64_t)best;
+    }
+done:
+    free(it);
+    free(within);
+    return ret;
+}

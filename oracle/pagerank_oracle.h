@@ -89,6 +89,41 @@ int64_t nko_katz(uint64_t z, const uint64_t *ptr, const uint32_t *col, const dou
                  const uint8_t *exists, double alpha, double beta, double tol, uint64_t max_iter,
                  double *scores);
 
+/* Graph::weightedDegree(u, true) (Graph.cpp:427-453) over a neighbour CSR
+ * in forNeighborsOf order: weighted: sum of w, self-loops counted twice, in
+ * row order; unweighted: degree + number of self-loops. Returns 0. */
+int nko_volumes(uint64_t z, const uint64_t *ptr, const uint32_t *col, const double *w,
+                double *vol);
+
+/* ApproximatePageRank::run(seeds) (ApproximatePageRank.cpp:18-55): the FIFO
+ * push of Andersen-Chung-Lang on the lazy walk. Every seed (ascending, no
+ * duplicates; a std::set) starts with residual 1/|seeds| and is queued; a
+ * push of u adds (1-alpha)*res*w/(2*vol u) to each neighbour's residual in
+ * row order, queueing a neighbour whose residual crosses eps*vol from below,
+ * then sets (p, r)(u) = (p + alpha*res, (1-alpha)*res/2) (a self-loop's share
+ * added during the loop is overwritten) and queues u again while
+ * r/vol >= eps. Output: every node the map holds (seeds and neighbours of
+ * pushed nodes) with its p, ascending by id, at most `cap` of them. Returns
+ * the support size (may exceed cap: nothing past cap is written), -1 on bad
+ * input. *pushes = number of pushes. */
+int64_t nko_apr(uint64_t z, const uint64_t *ptr, const uint32_t *col, const double *w,
+                const double *vol, double alpha, double eps, const uint32_t *seeds,
+                uint64_t nseeds, uint64_t cap, uint32_t *nodes, double *values,
+                uint64_t *pushes);
+
+/* PageRankNibble::bestSweepSet (PageRankNibble.cpp:28-82) on an APR support:
+ * values p/vol, ordered descending (ties: ascending node id - the reference's
+ * unstable sort leaves tie order open); prefix sets swept in that order with
+ * cut += w for a neighbour outside the prefix (the node itself included),
+ * cut -= w inside, volume += the row's weight sum, conductance
+ * cut / min(volume, total_volume - volume); the first strict minimum over
+ * prefixes smaller than n_nodes wins. Writes the chosen set ascending by id
+ * into `set`; returns its size, -1 on bad input. */
+int64_t nko_sweep_set(uint64_t z, const uint64_t *ptr, const uint32_t *col, const double *w,
+                      const double *vol, double total_volume, uint64_t n_nodes,
+                      uint64_t support, const uint32_t *nodes, const double *values,
+                      uint32_t *set);
+
 #ifdef __cplusplus
 }
 #endif

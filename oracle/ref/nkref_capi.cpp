@@ -15,7 +15,9 @@
 #include <cstdint>
 #include <cstring>
 #include <exception>
+#include <algorithm>
 #include <memory>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -30,6 +32,8 @@
 #include <networkit/io/NetworkitBinaryWriter.hpp>
 #include <networkit/io/METISGraphReader.hpp>
 #include <networkit/io/SNAPGraphReader.hpp>
+#include <networkit/scd/ApproximatePageRank.hpp>
+#include <networkit/scd/PageRankNibble.hpp>
 
 namespace {
 thread_local std::string g_err;
@@ -164,6 +168,76 @@ int nkref_katz(void *g, double alpha, double beta, double tol, int out_edges, in
             for (size_t i = 0; i < r.size(); ++i)
                 ranking_ids_out[i] = r[i].first;
         }
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// ApproximatePageRank(G, alpha, eps).run(seeds) (ApproximatePageRank.cpp:18-55):
+// the support (every node the result holds) ascending by id with its value.
+// *count = support size; nothing is written when it exceeds cap.
+int nkref_apr(void *g, double alpha, double eps, const uint32_t *seeds, uint64_t nseeds,
+              uint64_t cap, uint32_t *nodes, double *values, uint64_t *count,
+              double *run_seconds_out) {
+    try {
+        auto &G = *static_cast<RefGraph *>(g)->G;
+        std::set<NetworKit::node> s(seeds, seeds + nseeds);
+        NetworKit::ApproximatePageRank apr(G, alpha, eps);
+        auto t0 = std::chrono::steady_clock::now();
+        auto pr = apr.run(s);
+        auto t1 = std::chrono::steady_clock::now();
+        if (run_seconds_out)
+            *run_seconds_out = std::chrono::duration<double>(t1 - t0).count();
+        std::sort(pr.begin(), pr.end());
+        *count = pr.size();
+        if (pr.size() <= cap)
+            for (size_t i = 0; i < pr.size(); ++i) {
+                nodes[i] = static_cast<uint32_t>(pr[i].first);
+                values[i] = pr[i].second;
+            }
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// PageRankNibble(G, alpha, eps): one community per seed, as
+// SelectiveCommunityDetector::run(seeds) builds them
+// (SelectiveCommunityDetector.cpp:15-23, PageRankNibble.cpp:84-89), or one
+// community of the whole seed set (expandOneCommunity(seeds)) when `joint`.
+// Sets are ascending, concatenated; offsets[k..k+1] delimit set k.
+// *total = sum of the set sizes; nothing past cap is written.
+int nkref_prn(void *g, double alpha, double eps, const uint32_t *seeds, uint64_t nseeds,
+              int joint, uint64_t cap, uint64_t *offsets, uint32_t *sets, uint64_t *total,
+              double *run_seconds_out) {
+    try {
+        auto &G = *static_cast<RefGraph *>(g)->G;
+        std::set<NetworKit::node> s(seeds, seeds + nseeds);
+        NetworKit::PageRankNibble prn(G, alpha, eps);
+        std::vector<std::set<NetworKit::node>> out;
+        auto t0 = std::chrono::steady_clock::now();
+        if (joint) {
+            out.push_back(prn.expandOneCommunity(s));
+        } else {
+            auto res = prn.run(s);
+            for (NetworKit::node x : s)
+                out.push_back(res[x]);
+        }
+        auto t1 = std::chrono::steady_clock::now();
+        if (run_seconds_out)
+            *run_seconds_out = std::chrono::duration<double>(t1 - t0).count();
+        uint64_t pos = 0;
+        offsets[0] = 0;
+        for (size_t k = 0; k < out.size(); ++k) {
+            for (NetworKit::node x : out[k]) {
+                if (pos < cap)
+                    sets[pos] = static_cast<uint32_t>(x);
+                ++pos;
+            }
+            offsets[k + 1] = pos;
+        }
+        *total = pos;
         return 0;
     } catch (const std::exception &e) {
         return fail(e);

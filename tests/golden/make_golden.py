@@ -15,7 +15,9 @@ out-adjacency in storage order plus the reference results in ``<name>.npz``.
 It also writes every graph with the reference's NetworkitBinaryWriter
 (``<name>.nkbg``) and stores the adjacency the reference's reader builds from
 that file (keys ``nkbg_*``), plus one file per weight encoding of the format
-(``nkbg_<case>.nkbg``, ``nkbg_formats.npz``). The GPU box has no
+(``nkbg_<case>.nkbg``, ``nkbg_formats.npz``), and the reference's
+ApproximatePageRank and PageRankNibble results on the reference's SCD test
+graphs (``local_ppr.npz``). The GPU box has no
 reference checkout: the tests read only these files.
 """
 from __future__ import annotations
@@ -121,6 +123,58 @@ def main():
         res.update({"nkbg_" + k: back[k] for k in NKBG_KEYS})
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **arrays, **res)
     nkbg_formats(O)
+    local_ppr(O, inp)
+
+
+# (alpha, epsilon, seeds) of the local PageRank fixtures. SelectiveCDGTest.cpp
+# runs ApproximatePageRank(G, 0.4) from seed 0 on wiki-Vote (epsilon default
+# 1e-12) and PageRankNibble(G, 0.1, 1e-5) from seed 50 on hep-th.
+LOCAL_CASES = [(0.4, 1e-12, [0]), (0.1, 1e-5, [50]), (0.1, 1e-7, [3, 17, 50]),
+               (0.05, 1e-6, [100]), (0.2, 1e-4, [1, 2, 5, 8, 13, 21])]
+
+
+def local_ppr(O, inp):
+    """ApproximatePageRank and PageRankNibble fixtures (``local_ppr.npz``):
+    per graph its neighbour CSR in forNeighborsOf order (``<g>_ptr``,
+    ``<g>_col``, ``<g>_w``, ``<g>_directed``, ``<g>_m``, ``<g>_n``) and per
+    case the reference's result: ``<g>_<c>_apr_nodes`` / ``_apr_values``
+    (ascending ids), ``<g>_<c>_joint`` (expandOneCommunity(seeds)) and
+    ``<g>_<c>_each_<seed>`` (run(seeds), one community per seed; undirected
+    graphs only)."""
+    import json
+    graphs = [
+        ("hepth", O.RefGraph.read(os.path.join(inp, "hep-th.graph"), 1)),
+        ("wikivote_undirected", O.RefGraph.read(os.path.join(inp, "wiki-Vote.txt"), 0, False)),
+        ("wikivote_directed", O.RefGraph.read(os.path.join(inp, "wiki-Vote.txt"), 0, True)),
+        ("celegans", O.RefGraph.read(os.path.join(inp, "celegans_metabolic.graph"), 1)),
+        ("matlab8", O.RefGraph.from_edges(
+            8, [0, 1, 2, 2, 2, 3, 4, 5, 5], [2, 2, 3, 4, 5, 5, 5, 6, 7],
+            [3, 2, 3, 2, 1.5, 3, 2, 3, 2], directed=False, weighted=True)),
+    ]
+    out = {"cases": np.array(json.dumps(LOCAL_CASES)),
+           "graphs": np.array(json.dumps([g for g, _ in graphs]))}
+    for gname, g in graphs:
+        ex = g.export()
+        out[f"{gname}_ptr"] = ex["out_ptr"].astype(np.uint64)
+        out[f"{gname}_col"] = ex["out_adj"].astype(np.uint32)
+        out[f"{gname}_w"] = ex["out_w"].astype(np.float64) if ex["weighted"] else np.zeros(0)
+        out[f"{gname}_directed"] = np.bool_(ex["directed"])
+        out[f"{gname}_m"] = np.int64(g.m)
+        out[f"{gname}_n"] = np.int64(g.n)
+        for c, (alpha, eps, seeds) in enumerate(LOCAL_CASES):
+            seeds = [s for s in seeds if s < g.z]
+            nodes, vals, _ = g.apr(alpha, eps, seeds)
+            out[f"{gname}_{c}_apr_nodes"] = nodes
+            out[f"{gname}_{c}_apr_values"] = vals
+            if ex["directed"]:
+                continue
+            sets, _ = g.prn(alpha, eps, seeds, joint=True)
+            out[f"{gname}_{c}_joint"] = sets[0]
+            each, _ = g.prn(alpha, eps, seeds)
+            for sd, st in zip(sorted(seeds), each):
+                out[f"{gname}_{c}_each_{sd}"] = st
+        print(f"local_ppr {gname}: z={g.z} m={g.m}")
+    np.savez_compressed(os.path.join(HERE, "local_ppr.npz"), **out)
 
 
 NKBG_KEYS = ("in_ptr", "in_col", "in_w", "wdeg", "outdeg", "exists", "directed", "weighted")

@@ -134,3 +134,19 @@ def test_pagerank_on_decoded_graph(oracle_mod, name):
         o = oracle_mod.pagerank(csr, tol=1e-10, norm=norm)
         assert float(np.abs(s - o.scores).sum()) <= 1e-10
         assert abs(int(it) - o.iterations) <= 1
+
+
+def test_reader_library_exports_header_symbols():
+    """libnkgen.so exports every entry point include/nkgio.h declares."""
+    import ctypes
+    import re
+
+    from networkit_b200 import build
+
+    src = open(os.path.join(os.path.dirname(os.path.dirname(HERE)), "include", "nkgio.h")).read()
+    syms = sorted(set(re.findall(r"NKGEN_API\s+[\w\s\*]+?\b(nkgen_\w+)\s*\(", src)))
+    assert len(syms) == 3, syms
+    build.build_gen()
+    lib = ctypes.CDLL(build.GEN_LIB)
+    for s in syms:
+        assert hasattr(lib, s), s
