@@ -554,9 +554,13 @@ def form_local(local, n=1_000_000, deg=16, seeds=4096, alpha=0.1, eps=1e-5, ref_
     rng = np.random.default_rng(5)
     sd = np.sort(rng.choice(g.z, seeds, replace=False))
     problems = [[int(s)] for s in sd]
-    dl.run(problems[:256], alpha, eps, nibble=True)  # warm-up: slots, pool, module
+    # Per-problem bound: alpha * eps * vol >= 1e-6 moves into p per push
+    # (unweighted, vol >= 1), so no problem takes more than 1 / (alpha * eps)
+    # pushes, plus about 1100 halvings for an isolated seed.
+    maxp = int(1.0 / (alpha * eps)) + 2000
+    dl.run(problems[:256], alpha, eps, nibble=True, max_pushes=maxp)  # warm-up: slots, pool
     t0 = time.perf_counter()
-    sups, sets, st = dl.run(problems, alpha, eps, nibble=True)
+    sups, sets, st = dl.run(problems, alpha, eps, nibble=True, max_pushes=maxp)
     wall = time.perf_counter() - t0
     res = {"workload": f"pagerank_nibble_hyperbolic{n}_deg{deg}_seeds{seeds}",
            "alpha": alpha, "epsilon": eps, "n": g.z, "arcs": g.arcs, "seeds": seeds,

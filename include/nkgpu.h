@@ -345,7 +345,11 @@ NKG_API int nkg_pagerank_csr_noalloc(uint64_t n, uint64_t arcs, const uint64_t *
  * (SelectiveCommunityDetector.cpp:15-23); one problem of all seeds is
  * expandOneCommunity(seeds). max_pushes bounds the pushes of one problem
  * (UINT64_MAX: none); a problem that reaches it fails the call with
- * NKG_ERR_TIMEOUT. epsilon must be > 0. support_sizes_out / set_sizes_out
+ * NKG_ERR_TIMEOUT. epsilon must be > 0, alpha in (0, 1] and the weights
+ * non-negative: then the loop ends (each push moves alpha * r >= alpha *
+ * epsilon * vol into the values, which sum to at most 1); the reference does
+ * not check these, and its loop need not end without them.
+ * support_sizes_out / set_sizes_out
  * (nullable, host) receive per-problem counts.
  * nkg_local_support: the supports of the last run (every node the result
  * map holds), problem after problem, each ascending by id, with its value

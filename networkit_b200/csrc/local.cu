@@ -722,6 +722,10 @@ int nkg_local_create(nkg_local **out, uint64_t z, const uint64_t *row_ptr, const
             for (uint64_t k = row_ptr[u]; k < row_ptr[u + 1]; ++k) {
                 const uint32_t v = col[k];
                 require(v < z, "neighbour id >= z");
+                // With alpha in (0, 1], epsilon > 0 and weights >= 0 the push
+                // loop ends: each push moves alpha * r_u >= alpha * eps * vol_u
+                // into p, whose total stays <= 1 (Andersen-Chung-Lang).
+                require(w == nullptr || w[k] >= 0.0, "weights must be non-negative numbers");
                 require(exists == nullptr || exists[v], "an arc ends at a non-existent node");
                 loops += (v == u);
                 // totalEdgeWeight(): forEdges order (Graph.cpp:860-868,
@@ -809,6 +813,8 @@ int nkg_local_run(nkg_local *h, double alpha, double epsilon, uint64_t problems,
         require(problems >= 1, "no problems");
         require(seeds != nullptr, "seeds is NULL");
         require(epsilon > 0.0, "epsilon must be > 0 (the push loop does not end otherwise)");
+        require(alpha > 0.0 && alpha <= 1.0,
+                "alpha must be in (0, 1] (the push loop need not end otherwise)");
         require((flags & ~NKG_LOCAL_NIBBLE) == 0, "unknown flags");
         DeviceGuard guard(h->device);
         const bool nibble = (flags & NKG_LOCAL_NIBBLE) != 0;

@@ -53,6 +53,9 @@ class _Local:
         self.alpha = float(alpha)
         self.epsilon = float(epsilon)
         self._dev = None
+        # Pushes one problem may take (the reference has no bound);
+        # nkg_local_run fails with NKG_ERR_TIMEOUT past it.
+        self.maxPushes = _capi.UINT64_MAX
 
     def _device(self) -> _capi.DeviceLocal:
         if self._dev is None:
@@ -87,7 +90,8 @@ class ApproximatePageRank(_Local):
         """One independent run per entry (a node or an iterable of nodes),
         all in one launch: [(nodes ascending, values)]."""
         sets = [_seed_list(s) for s in seed_sets]
-        supports, _, self.stats = self._device().run(sets, self.alpha, self.epsilon)
+        supports, _, self.stats = self._device().run(sets, self.alpha, self.epsilon,
+                                                     max_pushes=self.maxPushes)
         return supports
 
 
@@ -99,18 +103,19 @@ class PageRankNibble(_Local):
         """SelectiveCommunityDetector::run: one community per seed."""
         sl = _seed_list(seeds)
         _, sets, self.stats = self._device().run([[s] for s in sl], self.alpha, self.epsilon,
-                                                 nibble=True)
+                                                 nibble=True, max_pushes=self.maxPushes)
         return {s: set(c.tolist()) for s, c in zip(sl, sets)}
 
     def expandOneCommunity(self, seeds) -> Set[int]:
         """One community around a seed node or a set of seed nodes."""
         _, sets, self.stats = self._device().run([_seed_list(seeds)], self.alpha, self.epsilon,
-                                                 nibble=True)
+                                                 nibble=True, max_pushes=self.maxPushes)
         return set(sets[0].tolist())
 
     def expandMany(self, seed_sets: Iterable) -> List[np.ndarray]:
         """One community per entry (a node or a set of nodes), all in one
         launch; each ascending."""
         sets_in = [_seed_list(s) for s in seed_sets]
-        _, sets, self.stats = self._device().run(sets_in, self.alpha, self.epsilon, nibble=True)
+        _, sets, self.stats = self._device().run(sets_in, self.alpha, self.epsilon, nibble=True,
+                                                 max_pushes=self.maxPushes)
         return sets

@@ -119,11 +119,12 @@ def test_errors(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", GRAPH_CASES + ["nkbg_unsigned_dir", "nkbg_none_undir",
-                                                "nkbg_none_dir"])
+@pytest.mark.parametrize("name", GRAPH_CASES + ["nkbg_none_undir", "nkbg_none_dir"])
 def test_pagerank_on_decoded_graph(oracle_mod, name):
     """File -> host decode -> device graph -> PageRank, against the oracle on
-    the decoded in-CSR: FP64 L1 <= 1e-10, iterations within 1."""
+    the decoded in-CSR: FP64 L1 <= 1e-10, iterations within 1. (The weight
+    encoding files hold zero and 2^60 weights, made for the decoder, on which
+    PageRank need not converge.)"""
     from networkit_b200 import _capi
 
     csr = graphio.read_nkbg(os.path.join(HERE, f"{name}.nkbg"))
@@ -131,7 +132,7 @@ def test_pagerank_on_decoded_graph(oracle_mod, name):
     for norm in (0, 1):
         p = dg.params(0.85, 1e-10, norm, False, False, _capi.NKG_PREC_FP64, 10000)
         s, it, _, _ = dg.run(p)
-        o = oracle_mod.pagerank(csr, tol=1e-10, norm=norm)
+        o = oracle_mod.pagerank(csr, tol=1e-10, norm=norm, max_iterations=10000)
         assert float(np.abs(s - o.scores).sum()) <= 1e-10
         assert abs(int(it) - o.iterations) <= 1
 

@@ -14,11 +14,13 @@ import numpy as np
 import pytest
 
 from networkit_b200 import _capi, scd
-from networkit_b200.graph import Graph, in_csr_from_edges
+from networkit_b200.graph import Graph
 
 pytestmark = pytest.mark.gpu
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+# Every run is bounded: far above the pushes of any case here (< 10^6).
+MAXP = 50_000_000
 D = np.load(os.path.join(HERE, "local_ppr.npz"))
 CASES = json.loads(str(D["cases"]))
 GRAPHS = json.loads(str(D["graphs"]))
@@ -55,7 +57,7 @@ def test_apr_matches_reference_fixtures(name):
         seeds = [s for s in seeds if s < z]
         if not seeds:
             continue
-        (sup,), _, st = dl.run([seeds], alpha, eps)
+        (sup,), _, st = dl.run([seeds], alpha, eps, max_pushes=MAXP)
         np.testing.assert_array_equal(sup[0], D[f"{name}_{c}_apr_nodes"])
         np.testing.assert_array_equal(bits(sup[1]), bits(D[f"{name}_{c}_apr_values"]))
         assert st["support"] == sup[0].shape[0]
@@ -74,7 +76,7 @@ def test_nibble_matches_oracle_and_reference(oracle_mod, name):
             continue
         problems = [seeds] + [[s] for s in seeds]
         keys = ["joint"] + [f"each_{s}" for s in seeds]
-        sups, sets, _ = dl.run(problems, alpha, eps, nibble=True)
+        sups, sets, _ = dl.run(problems, alpha, eps, nibble=True, max_pushes=MAXP)
         for pr, key, (nodes, vals), got in zip(problems, keys, sups, sets):
             want = oracle_mod.sweep_set(z, ptr, col, w, vol, tv, n, nodes, vals)
             if w is None:
@@ -119,7 +121,7 @@ def test_many_problems_against_oracle(oracle_mod, directed, weighted):
     problems += [[z - 10], [z - 5, 3], [0, z - 2]]  # isolated ids
     dl = _capi.DeviceLocal(z, ptr, col, w, ex, dr)
     for alpha, eps in [(0.1, 1e-5), (0.3, 1e-7)]:
-        sups, _, st = dl.run(problems, alpha, eps)
+        sups, _, st = dl.run(problems, alpha, eps, max_pushes=MAXP)
         assert st["slots"] >= 1
         pushes = 0
         for pr, (nodes, vals) in zip(problems, sups):
@@ -138,7 +140,7 @@ def test_small_budget_and_reuse(oracle_mod):
     dl = _capi.DeviceLocal(z, ptr, col, w, ex, dr, memory_budget=1)
     problems = [[5], [5], [7, 9], [5]]
     for _ in range(2):
-        sups, _, st = dl.run(problems, 0.15, 1e-6)
+        sups, _, st = dl.run(problems, 0.15, 1e-6, max_pushes=MAXP)
         assert st["slots"] == 1
         for pr, (nodes, vals) in zip(problems, sups):
             o = oracle_mod.apr(z, ptr, col, w, pr, 0.15, 1e-6)
@@ -149,10 +151,12 @@ def test_small_budget_and_reuse(oracle_mod):
 def test_python_mirror():
     g = random_graph(2000, 12000, 5, False, False, dups=False)
     apr = scd.ApproximatePageRank(g, 0.2, 1e-6)
+    apr.maxPushes = MAXP
     res = apr.run(17)
     assert res and all(a < b for (a, _), (b, _) in zip(res, res[1:]))
     assert dict(res) == dict(apr.run({17}))
     prn = scd.PageRankNibble(g, 0.1, 1e-5)
+    prn.maxPushes = MAXP
     comm = prn.run({3, 17})
     assert set(comm) == {3, 17}
     assert comm[17] == prn.expandOneCommunity(17)
@@ -165,15 +169,20 @@ def test_errors():
     z, ptr, col, w, ex, dr = scd.neighbour_csr(g)
     dl = _capi.DeviceLocal(z, ptr, col, w, ex, dr)
     with pytest.raises(_capi.NkgError, match="epsilon"):
-        dl.run([[1]], 0.1, 0.0)
+        dl.run([[1]], 0.1, 0.0, max_pushes=MAXP)
     with pytest.raises(_capi.NkgError, match="seed id"):
-        dl.run([[z + 3]], 0.1, 1e-4)
+        dl.run([[z + 3]], 0.1, 1e-4, max_pushes=MAXP)
     with pytest.raises(_capi.NkgError, match="non-existent"):
-        dl.run([[z - 1]], 0.1, 1e-4)
+        dl.run([[z - 1]], 0.1, 1e-4, max_pushes=MAXP)
+    with pytest.raises(_capi.NkgError, match="alpha"):
+        dl.run([[1]], 0.0, 1e-4, max_pushes=MAXP)
+    with pytest.raises(_capi.NkgError, match="non-negative"):
+        _capi.DeviceLocal(3, np.array([0, 1, 1, 1], np.uint64), np.array([2], np.uint32),
+                          np.array([-1.0]))
     with pytest.raises(_capi.NkgError, match="push limit"):
         dl.run([[1]], 0.1, 1e-9, max_pushes=3)
     with pytest.raises(_capi.NkgError, match="neighbour id"):
         _capi.DeviceLocal(3, np.array([0, 1, 1, 1], np.uint64), np.array([7], np.uint32))
     # the handle stays usable after an error
-    sups, _, _ = dl.run([[1]], 0.1, 1e-4)
+    sups, _, _ = dl.run([[1]], 0.1, 1e-4, max_pushes=MAXP)
     assert sups[0][0].shape[0] >= 1
