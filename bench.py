@@ -62,7 +62,8 @@ def parse_args():
     ap.add_argument("--arc-order", type=int, default=0, choices=[0, 1],
                     help="nkg_graph_options.arc_order (0 keep the reference order, 1 sorted)")
     ap.add_argument("--form", default="",
-                    choices=["", "ppr", "refine", "adjoint", "batch", "centrality", "local"],
+                    choices=["", "ppr", "refine", "adjoint", "batch", "centrality", "local",
+                             "reader"],
                     help="run only one companion form and print its figures")
     ap.add_argument("--fd-edges", type=int, default=64,
                     help="arcs checked by finite differences in --form adjoint")
@@ -73,6 +74,11 @@ def parse_args():
     ap.add_argument("--batch-step-only", action="store_true",
                     help="--form batch: no tuning and no comparison, two runs with the default "
                          "launch shape (the short launch sequence used for ncu captures)")
+    ap.add_argument("--local-n", type=int, default=1_000_000, help="graph nodes of --form local")
+    ap.add_argument("--local-seeds", type=int, default=16384, help="seeds of --form local")
+    ap.add_argument("--local-ref-sample", type=int, default=48,
+                    help="seeds the reference runs in --form local (0: none)")
+    ap.add_argument("--local-runs", type=int, default=2, help="timed calls of --form local")
     ap.add_argument("--cache", default=os.path.join(tempfile.gettempdir(), "nk_b200_graphs"))
     return ap.parse_args()
 
@@ -539,7 +545,8 @@ def form_centrality(local, csr):
     return res
 
 
-def form_local(local, n=1_000_000, deg=16, seeds=4096, alpha=0.1, eps=1e-5, ref_sample=48):
+def form_local(local, n=1_000_000, deg=16, seeds=16384, alpha=0.1, eps=1e-5, ref_sample=48,
+               runs=2):
     """PageRankNibble(G, 0.1, 1e-5) (the SelectiveCDGTest.cpp parameters),
     one community per seed (SelectiveCommunityDetector::run) for `seeds`
     random seeds of an undirected threshold hyperbolic graph (n nodes,
@@ -553,18 +560,21 @@ def form_local(local, n=1_000_000, deg=16, seeds=4096, alpha=0.1, eps=1e-5, ref_
     dl = _capi.DeviceLocal(g.z, g.in_ptr, g.in_col, None, None, False, device=local)
     rng = np.random.default_rng(5)
     sd = np.sort(rng.choice(g.z, seeds, replace=False))
-    problems = [[int(s)] for s in sd]
+    problems = sd  # one single-seed problem per entry
     # Per-problem bound: alpha * eps * vol >= 1e-6 moves into p per push
     # (unweighted, vol >= 1), so no problem takes more than 1 / (alpha * eps)
     # pushes, plus about 1100 halvings for an isolated seed.
     maxp = int(1.0 / (alpha * eps)) + 2000
-    dl.run(problems[:256], alpha, eps, nibble=True, max_pushes=maxp)  # warm-up: slots, pool
-    t0 = time.perf_counter()
-    sups, sets, st = dl.run(problems, alpha, eps, nibble=True, max_pushes=maxp)
-    wall = time.perf_counter() - t0
+    walls = []
+    for _ in range(runs):  # the first call sizes the map and result pools
+        t0 = time.perf_counter()
+        sups, sets, st = dl.run(problems, alpha, eps, nibble=True, max_pushes=maxp)
+        walls.append(time.perf_counter() - t0)
+    wall = walls[-1]
     res = {"workload": f"pagerank_nibble_hyperbolic{n}_deg{deg}_seeds{seeds}",
            "alpha": alpha, "epsilon": eps, "n": g.z, "arcs": g.arcs, "seeds": seeds,
-           "slots": st["slots"], "pushes": st["pushes"],
+           "slots": st["slots"], "pushes": st["pushes"], "arc_visits": st["arc_visits"],
+           "map_entries": st["table_entries"], "reruns": st["reruns"],
            "mean_support": st["support"] / seeds,
            "mean_set": float(np.mean([s.shape[0] for s in sets])),
            "ms_device": st["ms_total"], "ms_push_kernel": st["ms_push"],
@@ -575,7 +585,7 @@ def form_local(local, n=1_000_000, deg=16, seeds=4096, alpha=0.1, eps=1e-5, ref_
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
-    if oracle.ref_available():
+    if oracle.ref_available() and ref_sample:
         # Insert the edges (u < v, lexicographic: the generator's order) so
         # that every reference row lists its neighbours in the same order.
         rows = np.repeat(np.arange(g.z, dtype=np.uint32), np.diff(g.in_ptr).astype(np.int64))
@@ -592,6 +602,64 @@ def form_local(local, n=1_000_000, deg=16, seeds=4096, alpha=0.1, eps=1e-5, ref_
         res["speedup_vs_reference_device"] = res["seeds_per_s"] / res["reference"]["seeds_per_s"]
         res["speedup_vs_reference_e2e"] = res["e2e_seeds_per_s"] / res["reference"]["seeds_per_s"]
     dl.close()
+    return res
+
+
+def form_reader(local, csr, chunks=32, runs=3):
+    """NetworkitBinaryGraph input on the R-MAT scale-24 graph: the file
+    written by the project's writer (byte-identical to the reference
+    writer's), then decoded three ways, best of `runs` each (the file in the
+    page cache): the decoder alone (file -> in-CSR arrays), the decoder plus
+    the device upload (file -> resident graph -> PageRank-ready), and the
+    reference's NetworkitBinaryReader::read (file -> Graph; all host cores)."""
+    from networkit_b200 import _capi, graphio
+
+    path = os.path.join(tempfile.gettempdir(), f"nk_b200_rmat{csr.z}.nkbg")
+    out_ptr, out_col, _ = csr.out_csr()
+    t0 = time.perf_counter()
+    graphio.write_nkbg(path, csr.z, out_ptr, out_col, None, csr.in_ptr, csr.in_col, None,
+                       directed=True, chunks=chunks)
+    t_write = time.perf_counter() - t0
+    del out_ptr, out_col
+    size = os.path.getsize(path)
+    res = {"workload": f"nkbg_read_rmat24_chunks{chunks}", "file_bytes": size, "arcs": csr.arcs,
+           "n": csr.z, "write_s": t_write, "cores": os.cpu_count() or 1}
+    best = float("inf")
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        g = graphio.read_nkbg(path)
+        best = min(best, time.perf_counter() - t0)
+    assert g.arcs == csr.arcs and np.array_equal(g.in_col, csr.in_col)
+    res["decode_s"] = best
+    res["decode_gb_per_s"] = size / best / 1e9
+    res["decode_marcs_per_s"] = csr.arcs / best / 1e6
+    best = float("inf")
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        g = graphio.read_nkbg(path)
+        dg = _capi.DeviceGraph(g, device=local)
+        import torch
+
+        torch.cuda.synchronize()
+        best = min(best, time.perf_counter() - t0)
+        dg.close()
+    res["file_to_device_graph_s"] = best
+    del g
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if oracle.ref_available():
+        best = float("inf")
+        for _ in range(2):
+            t0 = time.perf_counter()
+            rg = oracle.RefGraph.read_nkbg(path)
+            best = min(best, time.perf_counter() - t0)
+            del rg
+        res["reference"] = {"read_s": best, "marcs_per_s": csr.arcs / best / 1e6,
+                            "kind": "reference", "cores": os.cpu_count() or 1,
+                            "sample": "NetworkitBinaryReader::read of the same file"}
+        res["speedup_decode_vs_reference"] = best / res["decode_s"]
+    os.remove(path)
     return res
 
 
@@ -659,7 +727,8 @@ def main():
                                     step_only=args.batch_step_only)))
         return
     if args.form == "local":
-        print(json.dumps(form_local(local)))
+        print(json.dumps(form_local(local, n=args.local_n, seeds=args.local_seeds,
+                                    ref_sample=args.local_ref_sample, runs=args.local_runs)))
         return
     if args.form == "adjoint":
         print(json.dumps(form_adjoint(local, scale=args.adjoint_scale, fd_edges=args.fd_edges,
@@ -687,6 +756,9 @@ def main():
         return
     if args.form == "centrality":
         print(json.dumps(form_centrality(local, csr)))
+        return
+    if args.form == "reader":
+        print(json.dumps(form_reader(local, csr)))
         return
     arcs, n = csr.arcs, csr.z
     dg = _capi.DeviceGraph(csr, device=local, sweep_shape=args.shape, arc_order=args.arc_order)
@@ -792,6 +864,7 @@ def main():
                          ("fwd_bwd", lambda: form_adjoint(local, steps=2, fd_edges=0)),
                          ("eigenvector_katz", lambda: form_centrality(local, csr)),
                          ("pagerank_nibble", lambda: form_local(local)),
+                         ("nkbg_reader", lambda: form_reader(local, csr)),
                          ("batch", lambda: form_batch(local, steps=2,
                                                       plain_graphs=range(0, 1024, 8)))):
             try:

@@ -333,8 +333,10 @@ NKG_API int nkg_pagerank_csr_noalloc(uint64_t n, uint64_t arcs, const uint64_t *
  * existence mask (NULL: all exist) and the graph kind. It computes
  * weightedDegree(u, true) of every node (Graph.cpp:427-453) and
  * 2 * totalEdgeWeight() (Graph.cpp:860-868). memory_budget bounds the
- * per-problem state, 28 bytes per node for every problem in flight
- * (0: half the free device memory, at most 48 GiB).
+ * problems in flight (0: half the free device memory, at most 48 GiB): each
+ * holds a hash map of 40 bytes per entry, 1024 entries at first, doubled when
+ * half full; the map pool grows past the budget when one problem's support
+ * needs it.
  *
  * nkg_local_run: problem k has the seeds seeds[seed_ptr[k] .. seed_ptr[k+1])
  * (ascending, no duplicates: the reference's std::set<node>) and runs
@@ -360,11 +362,13 @@ typedef struct nkg_local nkg_local;
 #define NKG_LOCAL_NIBBLE 2
 typedef struct {
     uint64_t pushes;          /* pushes over all problems */
+    uint64_t arc_visits;      /* arcs the pushes walked (sum of the pushed rows) */
     uint64_t support;         /* sum of the support sizes */
     uint64_t slots;           /* problems in flight (resident warps) */
-    uint64_t reruns;          /* push launches repeated to grow the result pool */
-    double ms_push;           /* device time of the push kernel(s) */
-    double ms_sweep;          /* device time of the sorts and the sweep */
+    uint64_t table_entries;   /* map entries the last push launch took from the pool */
+    uint64_t reruns;          /* push launches repeated to grow the map or result pool */
+    double ms_push;           /* device time of the (last) push launch */
+    double ms_sweep;          /* ms_total - ms_push: re-runs, sorts and the sweep */
     double ms_total;
     uint64_t kernel_launches;
 } nkg_local_stats;

@@ -95,9 +95,10 @@ class BatchTuning(C.Structure):
 
 
 class LocalStats(C.Structure):
-    _fields_ = [("pushes", C.c_uint64), ("support", C.c_uint64), ("slots", C.c_uint64),
-                ("reruns", C.c_uint64), ("ms_push", C.c_double), ("ms_sweep", C.c_double),
-                ("ms_total", C.c_double), ("kernel_launches", C.c_uint64)]
+    _fields_ = [("pushes", C.c_uint64), ("arc_visits", C.c_uint64), ("support", C.c_uint64),
+                ("slots", C.c_uint64), ("table_entries", C.c_uint64), ("reruns", C.c_uint64),
+                ("ms_push", C.c_double), ("ms_sweep", C.c_double), ("ms_total", C.c_double),
+                ("kernel_launches", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -529,17 +530,24 @@ class DeviceLocal:
             pass
 
     def run(self, seed_sets, alpha, epsilon, nibble=False, max_pushes=UINT64_MAX):
-        """seed_sets: list of seed collections (each made a sorted set).
-        Returns (supports, sets, stats): supports = [(nodes, values)] per
-        problem (ascending ids); sets = [nodes] per problem or None."""
-        sets_ = [np.unique(np.atleast_1d(np.asarray(list(s) if isinstance(s, (set, frozenset))
-                                                    else s, np.int64))) for s in seed_sets]
-        seed_ptr = np.zeros(len(sets_) + 1, np.uint64)
-        np.cumsum([x.shape[0] for x in sets_], out=seed_ptr[1:])
-        seeds = (np.concatenate(sets_) if sets_ else np.zeros(0)).astype(np.uint32)
-        if seeds.size and (np.concatenate(sets_).min() < 0):
-            raise NkgError(NKG_ERR_INVALID_ARG, "negative seed id")
-        k = len(sets_)
+        """seed_sets: a 1-D integer array (one single-seed problem per entry) or
+        a list of seed collections (each made a sorted set). Returns
+        (supports, sets, stats): supports = [(nodes, values)] per problem
+        (ascending ids); sets = [nodes] per problem or None."""
+        if isinstance(seed_sets, np.ndarray) and seed_sets.ndim == 1:
+            if seed_sets.size and seed_sets.min() < 0:
+                raise NkgError(NKG_ERR_INVALID_ARG, "negative seed id")
+            seeds = np.ascontiguousarray(seed_sets, np.uint32)
+            seed_ptr = np.arange(seeds.shape[0] + 1, dtype=np.uint64)
+        else:
+            sets_ = [np.unique(np.atleast_1d(np.asarray(list(x) if isinstance(x, (set, frozenset))
+                                                        else x, np.int64))) for x in seed_sets]
+            if any(x.size and x.min() < 0 for x in sets_):
+                raise NkgError(NKG_ERR_INVALID_ARG, "negative seed id")
+            seed_ptr = np.zeros(len(sets_) + 1, np.uint64)
+            np.cumsum([x.shape[0] for x in sets_], out=seed_ptr[1:])
+            seeds = (np.concatenate(sets_) if sets_ else np.zeros(0)).astype(np.uint32)
+        k = seed_ptr.shape[0] - 1
         sup = np.zeros(k, np.uint64)
         setc = np.zeros(k, np.uint64)
         st = LocalStats()
@@ -551,16 +559,12 @@ class DeviceLocal:
         nodes = np.empty(max(tot, 1), np.uint32)
         vals = np.empty(max(tot, 1), np.float64)
         check(lib().nkg_local_support(self.h, ptr(nodes, _u32p), ptr(vals, _f64p)))
-        offs = np.zeros(k + 1, np.int64)
-        np.cumsum(sup.astype(np.int64), out=offs[1:])
-        supports = [(nodes[offs[i]:offs[i + 1]].copy(), vals[offs[i]:offs[i + 1]].copy())
-                    for i in range(k)]
+        cut = np.cumsum(sup.astype(np.int64))[:-1]
+        supports = list(zip(np.split(nodes[:tot], cut), np.split(vals[:tot], cut)))
         sets_out = None
         if nibble:
             ts = int(setc.sum())
             sn = np.empty(max(ts, 1), np.uint32)
             check(lib().nkg_local_sets(self.h, ptr(sn, _u32p)))
-            so = np.zeros(k + 1, np.int64)
-            np.cumsum(setc.astype(np.int64), out=so[1:])
-            sets_out = [sn[so[i]:so[i + 1]].copy() for i in range(k)]
+            sets_out = np.split(sn[:ts], np.cumsum(setc.astype(np.int64))[:-1])
         return supports, sets_out, st.as_dict()

@@ -10,18 +10,17 @@
 // SelectiveCommunityDetector::run takes the seeds one after another
 // (SelectiveCommunityDetector.cpp:15-23).
 //
-// Per-problem state is dense: one slot of z entries per resident warp, holding
-//   r, p     residual and value (the reference's unordered_map pair),
-//   stamp    the problem's epoch. An entry is in the map iff its stamp equals
-//            the epoch, so slots are never cleared between problems,
-//   touched  the support in first-touch order,
-//   queue    the FIFO ring (z entries: with non-negative weights a node is
-//            queued at most once at a time).
-// That is 28 bytes per node per slot; the number of slots follows a memory
-// budget.
+// Per-problem state is a hash map per warp, the reference's unordered_map
+// made compact: open addressing with linear probing, 32-byte entries (node
+// tagged with the problem's epoch, residual, value), taken from a
+// bump-allocated pool and doubled whenever it is half full. Its
+// footprint follows the support, not the graph, so the maps of thousands of
+// problems in flight stay in L2. Tags carry the problem's epoch, so a warp
+// reuses its table for the next problem without clearing it. The FIFO queue
+// is a ring of entry indices beside the table.
 //
 // PageRankNibble's sweep (bestSweepSet) then runs as:
-//   (1) per support node, in the push kernel while the slot is live: its key
+//   (1) per support node, in the push kernel while the map is live: its key
 //       p/vol as an order-preserving integer, and its cut change
 //       dcut = sum over its row of (+w, or -w for a neighbour that precedes it
 //       in the sweep order), summed in row order;
@@ -93,6 +92,16 @@ __global__ void local_volumes(uint64_t z, const uint64_t *__restrict__ ptr,
     }
 }
 
+// One entry of a problem's map (the reference's unordered_map<node,
+// pair<double, double>>), 32 bytes: the node tagged with the problem's epoch
+// (an entry with another epoch is empty for this problem), residual r, value
+// p and, during a rehash, the entry's index in the new table.
+struct __align__(32) MapEntry {
+    unsigned long long tag;
+    double r, p;
+    uint32_t fwd, pad;
+};
+
 struct PushArgs {
     const uint64_t *ptr;
     const uint32_t *col;
@@ -104,44 +113,146 @@ struct PushArgs {
     uint64_t problems;
     const uint64_t *seed_ptr;
     const uint32_t *seeds;
-    // slots
-    uint64_t slots;
-    double *r, *p;
-    uint32_t *stamp, *touched, *queue, *epoch;
-    // results
+    uint32_t epoch_base;  // problem k runs with epoch epoch_base + k + 1
+    uint32_t init_cap;    // first table size of a warp (power of two)
+    // Table pool: a region of `cap` entries, `cap` support indices and a FIFO
+    // ring of `cap` entry indices, handed out by a bump counter; a warp keeps
+    // its last region for its next problem and takes a twice larger one when
+    // the table is half full or the ring is full.
+    MapEntry *ent_pool;
+    uint32_t *idx_pool, *ring_pool;
     uint64_t pool_cap;
     unsigned long long *pool_used;
     unsigned long long *next;
+    // results
+    uint64_t out_cap;
+    unsigned long long *out_used;
     uint32_t *out_node;
     double *out_p;
     uint64_t *out_key;
     double *out_dcut;
-    uint64_t *sup_off, *sup_cnt, *pushes;
-    int *err;  // 1: queue overflow (negative weights), 2: push limit reached
+    uint64_t *sup_off, *sup_cnt, *pushes, *visits;
+    int *err;  // 2: push limit reached, 3: table pool exhausted, 4: table too large
     int nibble;
 };
 
-// One warp = one slot; the warp takes problems from a global counter until
-// none are left.
+__device__ __forceinline__ uint32_t map_home(uint32_t v, uint32_t bits) {
+    return (v * 2654435769u) >> (32 - bits);  // Fibonacci hashing
+}
+
+// Index of v's entry in the table, or kNone if v has none and !insert.
+// With insert, an absent v gets an entry (r = p = 0) and
+// `fresh` is set. Lanes of one warp may insert distinct nodes at once: the
+// claim of an empty entry is a compare-and-swap of its tag. Returns kNone - 1
+// if the table is full (never at the load factor kept, 1/2). The tag and the
+// residual come in one 16-byte load from L2 (r_out: v's residual, 0 when
+// fresh).
+__device__ __forceinline__ uint32_t map_find(MapEntry *tab, uint32_t cap, uint32_t bits,
+                                             uint32_t epoch, uint32_t v, bool insert,
+                                             bool &fresh, double &r_out) {
+    const unsigned long long tag = (static_cast<unsigned long long>(epoch) << 32) | v;
+    uint32_t h = map_home(v, bits);
+    fresh = false;
+    r_out = 0.0;
+    for (uint32_t i = 0; i < cap; ++i) {
+        const double2 tr = __ldcg(reinterpret_cast<const double2 *>(&tab[h]));
+        const unsigned long long t = static_cast<unsigned long long>(__double_as_longlong(tr.x));
+        if (t == tag) {
+            r_out = tr.y;
+            return h;
+        }
+        if (static_cast<uint32_t>(t >> 32) != epoch) {
+            if (!insert)
+                return kNone;
+            const unsigned long long old = atomicCAS(&tab[h].tag, t, tag);
+            if (old == t) {
+                tab[h].r = 0.0;
+                tab[h].p = 0.0;
+                fresh = true;
+                return h;
+            }
+            if (old == tag) {
+                r_out = __ldcg(&tab[h].r);
+                return h;
+            }
+        }
+        h = (h + 1) & (cap - 1);
+    }
+    return kNone - 1;
+}
+
+// The warp's table: entries, support list (entry indices in first-touch
+// order), FIFO ring (entry indices; positions are counters modulo cap), size.
+// The FIFO is a ring, not a list through the entries: a node can be queued
+// twice, as in the reference, because the test that queues a node again
+// after its push (r / vol >= eps) and the test that queues a neighbour
+// (r < vol * eps) round differently.
+struct WarpMap {
+    MapEntry *tab;
+    uint32_t *tl, *ring;
+    uint32_t cap, bits;
+};
+
+// Move the warp's table into a fresh region of at least `need_cap` entries
+// (a power of two): every entry of this epoch is inserted anew, the support
+// list rewritten, the queued entries [qh, qt) copied in order to the new
+// ring's front and `cur` translated through `fwd`. Returns 0, 3 if the pool
+// is exhausted, 4 if the table would pass 2^31 entries.
+__device__ int map_grow(const PushArgs &a, WarpMap &m, uint64_t need_cap, uint32_t epoch,
+                        uint64_t T, uint64_t &qh, uint64_t &qt, uint32_t &cur, unsigned lane) {
+    if (need_cap > (1ull << 31))
+        return 4;
+    uint32_t ncap = m.cap, nbits = m.bits;
+    while (ncap < need_cap) {
+        ncap <<= 1;
+        ++nbits;
+    }
+    unsigned long long off = 0;
+    if (lane == 0)
+        off = atomicAdd(a.pool_used, static_cast<unsigned long long>(ncap));
+    off = __shfl_sync(kFull, off, 0);
+    if (off + ncap > a.pool_cap)
+        return 3;
+    WarpMap n{a.ent_pool + off, a.idx_pool + off, a.ring_pool + off, ncap, nbits};
+    if (T) {
+        for (uint64_t i = lane; i < T; i += 32) {
+            const uint32_t oi = m.tl[i];
+            const MapEntry e = m.tab[oi];
+            bool fresh;
+            double rr;
+            const uint32_t nh = map_find(n.tab, n.cap, n.bits, epoch,
+                                         static_cast<uint32_t>(e.tag), true, fresh, rr);
+            n.tab[nh].r = e.r;
+            n.tab[nh].p = e.p;
+            m.tab[oi].fwd = nh;
+            n.tl[i] = nh;
+        }
+        __syncwarp();
+        const uint64_t len = qt - qh;
+        for (uint64_t i = lane; i < len; i += 32)
+            n.ring[i] = m.tab[m.ring[(qh + i) & (m.cap - 1)]].fwd;
+        if (cur != kNone)
+            cur = m.tab[cur].fwd;
+        qh = 0;
+        qt = len;
+        __syncwarp();
+    }
+    m = n;
+    return 0;
+}
+
+// One warp runs one problem at a time, taking problems from a global counter
+// until none are left.
 template <bool WEIGHTED>
 __global__ void __launch_bounds__(kLocalThreads) local_push(PushArgs a) {
     const unsigned lane = threadIdx.x & 31;
-    const uint64_t slot = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
-    if (slot >= a.slots)
-        return;
-    const uint64_t z = a.z;
-    double *__restrict__ r = a.r + slot * z;
-    double *__restrict__ p = a.p + slot * z;
-    uint32_t *__restrict__ stamp = a.stamp + slot * z;
-    uint32_t *__restrict__ touched = a.touched + slot * z;
-    uint32_t *__restrict__ queue = a.queue + slot * z;
     const uint64_t *__restrict__ ptr = a.ptr;
     const uint32_t *__restrict__ col = a.col;
     const double *__restrict__ vol = a.vol;
-    uint32_t epoch = a.epoch[slot];
     const double oma = 1.0 - a.alpha;
     const double eps = a.eps;
     const unsigned lt = lanemask_lt();
+    WarpMap m{nullptr, nullptr, nullptr, 0, 0};
 
     for (;;) {
         unsigned long long k = 0;
@@ -150,39 +261,62 @@ __global__ void __launch_bounds__(kLocalThreads) local_push(PushArgs a) {
         k = __shfl_sync(kFull, k, 0);
         if (k >= a.problems)
             break;
-        ++epoch;
-        // Seeds: ascending, each with residual 1/|seeds|, queued in order.
-        const uint64_t s0 = a.seed_ptr[k], s1 = a.seed_ptr[k + 1];
-        const double init = 1.0 / static_cast<double>(s1 - s0);
-        for (uint64_t i = s0 + lane; i < s1; i += 32) {
-            const uint32_t v = a.seeds[i];
-            stamp[v] = epoch;
-            r[v] = init;
-            p[v] = 0.0;
-            touched[i - s0] = v;
-            queue[i - s0] = v;
-        }
-        uint64_t T = s1 - s0, head = 0, tail = s1 - s0, npush = 0;
+        const uint32_t epoch = a.epoch_base + static_cast<uint32_t>(k) + 1;
+        const uint64_t s0 = a.seed_ptr[k], s1 = a.seed_ptr[k + 1], ns = s1 - s0;
+        uint64_t T = 0, npush = 0, qh = 0, qt = 0, nvisit = 0;
+        uint32_t uidx = kNone;
         int fail = 0;
-        __syncwarp();
+        // A table of at least init_cap entries, at least 4 per seed.
+        const uint64_t want = max(static_cast<uint64_t>(a.init_cap), 4 * ns);
+        if (m.cap < want) {
+            if (m.tab == nullptr) {
+                m.cap = 1;
+                m.bits = 0;
+            }
+            fail = map_grow(a, m, want, epoch, 0, qh, qt, uidx, lane);
+        }
+        if (!fail) {
+            // Seeds: ascending, residual 1/|seeds| each, queued in order.
+            const double init = 1.0 / static_cast<double>(ns);
+            for (uint64_t i = lane; i < ns; i += 32) {
+                bool fresh;
+                double rr;
+                const uint32_t h = map_find(m.tab, m.cap, m.bits, epoch, a.seeds[s0 + i], true,
+                                            fresh, rr);
+                m.tab[h].r = init;
+                m.tl[i] = h;
+                m.ring[i] = h;
+            }
+            T = ns;
+            qt = ns;
+            __syncwarp();
+        }
 
-        while (head < tail) {
+        while (!fail && qh < qt) {
             if (npush >= a.max_pushes) {
                 fail = 2;
                 break;
             }
-            const uint32_t u = queue[head % z];
-            ++head;
-            const double res = r[u];
-            const double pu = p[u];
+            uidx = m.ring[qh & (m.cap - 1)];
+            ++qh;
+            const MapEntry ue = m.tab[uidx];
+            const uint32_t u = static_cast<uint32_t>(ue.tag);
+            const double res = ue.r;
             const double volume = vol[u];
             const uint64_t b = ptr[u], e = ptr[u + 1];
             const double a1 = __dmul_rn(oma, res);  // (1.0 - alpha) * res
             const double d2 = __dmul_rn(2.0, volume);
+            nvisit += e - b;
             for (uint64_t base = b; base < e; base += 32) {
+                // Room for 32 new entries at load <= 1/2 and 32 queued ones.
+                if (T + 32 > m.cap / 2 || qt - qh + 32 > m.cap) {
+                    fail = map_grow(a, m, 2ull * m.cap, epoch, T, qh, qt, uidx, lane);
+                    if (fail)
+                        break;
+                }
                 const uint64_t q = base + lane;
                 const bool act = q < e;
-                uint32_t v = kNone;
+                uint32_t v = kNone, h = 0;
                 double mass = 0.0, volv = 0.0, rv = 0.0;
                 bool fresh = false;
                 if (act) {
@@ -190,17 +324,12 @@ __global__ void __launch_bounds__(kLocalThreads) local_push(PushArgs a) {
                     const double wk = WEIGHTED ? a.w[q] : 1.0;
                     mass = __ddiv_rn(__dmul_rn(a1, wk), d2);
                     volv = vol[v];
-                    const uint32_t st = stamp[v];
-                    const double rraw = r[v];
-                    fresh = st != epoch;
-                    rv = fresh ? 0.0 : rraw;
                 }
                 const unsigned peers = __match_any_sync(kFull, v);
                 const bool dup = act && __popc(peers) > 1;
                 if (__any_sync(kFull, dup)) {
                     // A node twice in this chunk (a multi-edge): lane 0 takes
                     // the chunk in row order.
-                    __syncwarp();
                     if (lane == 0) {
                         const uint64_t qe = min(e, base + 32);
                         for (uint64_t qq = base; qq < qe; ++qq) {
@@ -208,83 +337,100 @@ __global__ void __launch_bounds__(kLocalThreads) local_push(PushArgs a) {
                             const double w2 = WEIGHTED ? a.w[qq] : 1.0;
                             const double m2 = __ddiv_rn(__dmul_rn(a1, w2), d2);
                             const double vv = vol[v2];
-                            const bool fr = stamp[v2] != epoch;
-                            const double old = fr ? 0.0 : r[v2];
-                            if (fr) {
-                                stamp[v2] = epoch;
-                                p[v2] = 0.0;
-                                touched[T++] = v2;
+                            bool fr;
+                            double old;
+                            const uint32_t h2 = map_find(m.tab, m.cap, m.bits, epoch, v2, true, fr,
+                                                         old);
+                            if (h2 >= kNone - 1) {
+                                fail = 4;
+                                break;
                             }
-                            if (old < __dmul_rn(vv, eps) && __dadd_rn(old, m2) >= __dmul_rn(eps, vv)) {
-                                queue[tail % z] = v2;
-                                ++tail;
-                            }
-                            r[v2] = __dadd_rn(old, m2);
+                            if (fr)
+                                m.tl[T++] = h2;
+                            if (old < __dmul_rn(vv, eps) && __dadd_rn(old, m2) >= __dmul_rn(eps, vv))
+                                m.ring[qt++ & (m.cap - 1)] = h2;
+                            m.tab[h2].r = __dadd_rn(old, m2);
                         }
                     }
                     T = __shfl_sync(kFull, T, 0);
-                    tail = __shfl_sync(kFull, tail, 0);
-                } else {
-                    bool cond = false;
-                    if (act) {
-                        cond = (rv < __dmul_rn(volv, eps)) &&
-                               (__dadd_rn(rv, mass) >= __dmul_rn(eps, volv));
-                        r[v] = __dadd_rn(rv, mass);
-                    }
-                    const unsigned fm = __ballot_sync(kFull, act && fresh);
-                    if (act && fresh) {
-                        stamp[v] = epoch;
-                        p[v] = 0.0;
-                        touched[T + __popc(fm & lt)] = v;
-                    }
-                    T += __popc(fm);
-                    const unsigned cm = __ballot_sync(kFull, cond);
-                    if (cond)
-                        queue[(tail + __popc(cm & lt)) % z] = v;
-                    tail += __popc(cm);
+                    qt = __shfl_sync(kFull, qt, 0);
+                    fail = __shfl_sync(kFull, fail, 0);
+                    __syncwarp();
+                    if (fail)
+                        break;
+                    continue;
                 }
+                if (act) {
+                    h = map_find(m.tab, m.cap, m.bits, epoch, v, true, fresh, rv);
+                    if (h >= kNone - 1)
+                        fail = 4;
+                }
+                if (__any_sync(kFull, fail != 0)) {
+                    fail = 4;
+                    break;
+                }
+                bool cond = false;
+                if (act) {
+                    cond = (rv < __dmul_rn(volv, eps)) &&
+                           (__dadd_rn(rv, mass) >= __dmul_rn(eps, volv));
+                    m.tab[h].r = __dadd_rn(rv, mass);
+                }
+                const unsigned fm = __ballot_sync(kFull, fresh);
+                if (fresh)
+                    m.tl[T + __popc(fm & lt)] = h;
+                T += __popc(fm);
+                // Queue the crossing lanes in lane (= row) order.
+                const unsigned cm = __ballot_sync(kFull, cond);
+                if (cond)
+                    m.ring[(qt + __popc(cm & lt)) & (m.cap - 1)] = h;
+                qt += __popc(cm);
                 __syncwarp();
             }
+            if (fail)
+                break;
             // prRes[u] = (p + alpha*res, (1-alpha)*res/2); queue u again while
             // r/vol >= eps. A self-loop's share added above is overwritten.
             const double ru = __ddiv_rn(__dmul_rn(oma, res), 2.0);
+            const bool again = __ddiv_rn(ru, volume) >= eps;
+            if (again && qt - qh + 1 > m.cap) {
+                fail = map_grow(a, m, 2ull * m.cap, epoch, T, qh, qt, uidx, lane);
+                if (fail)
+                    break;
+            }
             if (lane == 0) {
-                p[u] = __dadd_rn(pu, __dmul_rn(a.alpha, res));
-                r[u] = ru;
+                m.tab[uidx].p = __dadd_rn(ue.p, __dmul_rn(a.alpha, res));
+                m.tab[uidx].r = ru;
+                if (again)
+                    m.ring[qt & (m.cap - 1)] = uidx;
             }
-            if (__ddiv_rn(ru, volume) >= eps) {
-                if (lane == 0)
-                    queue[tail % z] = u;
-                ++tail;
-            }
+            qt += again;
             ++npush;
-            if (tail - head > z) {
-                fail = 1;
-                break;
-            }
             __syncwarp();
         }
         __syncwarp();
 
         unsigned long long off = 0;
         if (lane == 0) {
-            off = atomicAdd(a.pool_used, static_cast<unsigned long long>(T));
+            off = atomicAdd(a.out_used, static_cast<unsigned long long>(T));
             a.sup_off[k] = off;
             a.sup_cnt[k] = T;
             a.pushes[k] = npush;
+            a.visits[k] = nvisit;
             if (fail)
                 atomicMax(a.err, fail);
         }
         off = __shfl_sync(kFull, off, 0);
-        if (fail || off + T > a.pool_cap)
-            continue;  // the host sees the error or the shortfall and re-runs
+        if (fail == 3)
+            break;  // no region for this warp; the host grows the pool and re-runs
+        if (fail || off + T > a.out_cap)
+            continue;  // the host sees the error or the shortfall
         for (uint64_t i = lane; i < T; i += 32) {
-            const uint32_t v = touched[i];
-            const double pv = p[v];
+            const MapEntry ev = m.tab[m.tl[i]];
+            const uint32_t v = static_cast<uint32_t>(ev.tag);
             a.out_node[off + i] = v;
-            a.out_p[off + i] = pv;
+            a.out_p[off + i] = ev.p;
             if (a.nibble) {
-                const uint64_t kv = order_bits(pv / vol[v]);
+                const uint64_t kv = order_bits(__ddiv_rn(ev.p, vol[v]));
                 a.out_key[off + i] = kv;
                 // Cut change of v: +w for a neighbour outside the prefix that
                 // ends before v (v itself included), -w inside; row order.
@@ -294,9 +440,14 @@ __global__ void __launch_bounds__(kLocalThreads) local_push(PushArgs a) {
                     const uint32_t x = col[qq];
                     const double wq = WEIGHTED ? a.w[qq] : 1.0;
                     bool before = false;
-                    if (x != v && stamp[x] == epoch) {
-                        const uint64_t kx = order_bits(p[x] / vol[x]);
-                        before = kx > kv || (kx == kv && x < v);
+                    if (x != v) {
+                        bool fr;
+                        double rx;
+                        const uint32_t hx = map_find(m.tab, m.cap, m.bits, epoch, x, false, fr, rx);
+                        if (hx < kNone - 1) {
+                            const uint64_t kx = order_bits(__ddiv_rn(m.tab[hx].p, vol[x]));
+                            before = kx > kv || (kx == kv && x < v);
+                        }
                     }
                     acc = before ? __dsub_rn(acc, wq) : __dadd_rn(acc, wq);
                 }
@@ -305,8 +456,6 @@ __global__ void __launch_bounds__(kLocalThreads) local_push(PushArgs a) {
         }
         __syncwarp();
     }
-    if (lane == 0)
-        a.epoch[slot] = epoch;
 }
 
 // bestSweepSet (PageRankNibble.cpp:48-79) per problem over the support in
@@ -414,7 +563,7 @@ __global__ void local_gather_u64(const uint32_t *__restrict__ idx, const uint64_
 struct nkg_local {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
     uint64_t z = 0, arcs = 0, n_nodes = 0;
     bool weighted = false;
     double total_volume = 0.0;  // 2 * totalEdgeWeight() (PageRankNibble.cpp:46)
@@ -422,52 +571,53 @@ struct nkg_local {
     DeviceArray<uint64_t> ptr;
     DeviceArray<uint32_t> col;
     DeviceArray<double> w, vol, wsum;
-    // per-problem slots
-    uint64_t budget = 0, slots = 0, epochs_used = 0;
-    DeviceArray<double> r, p;
-    DeviceArray<uint32_t> stamp, touched, queue, epoch;
+    // per-problem maps: the table pool and the epoch counter
+    uint64_t budget = 0;
+    uint64_t table_cap = 0;       // entries of the table pool
+    uint32_t epoch_base = 0;      // epochs below this one are spent
+    DeviceArray<MapEntry> ent_pool;
+    DeviceArray<uint32_t> idx_pool, ring_pool;
     // result pool
-    uint64_t pool_cap = 0, nibble_cap = 0;
+    uint64_t out_cap = 0, nibble_cap = 0;
     DeviceArray<uint32_t> out_node, node_sorted, ord_node, ord_sweep, set_node, set_sorted, iota;
     DeviceArray<double> out_p, out_dcut;
     DeviceArray<uint64_t> out_key, key_sorted;
-    DeviceArray<unsigned long long> counters;  // pool_used, next
+    DeviceArray<unsigned long long> counters;  // out_used, next problem, table pool used
     DeviceArray<int> err;
     DeviceArray<uint8_t> sort_tmp;
     // last run
     uint64_t problems = 0;
     bool nibble = false;
     std::vector<uint64_t> sup_off, sup_cnt, set_cnt;
-    DeviceArray<uint64_t> d_sup_off, d_sup_cnt, d_sup_end, d_set_cnt, d_set_end, d_pushes;
+    DeviceArray<uint64_t> d_sup_off, d_sup_cnt, d_sup_end, d_set_cnt, d_set_end, d_pushes, d_visits;
+    uint64_t table_need = 0;  // table entries the last launch asked for
 };
 
 namespace {
 
-constexpr uint64_t kSlotBytesPerNode = 8 + 8 + 4 + 4 + 4;
+constexpr uint32_t kInitCap = 1024;    // first table of a warp: 40 KB
+constexpr unsigned kWarpsPerSm = 32;   // 4 CTAs of 8 warps at <= 64 registers
 
-void ensure_slots(nkg_local *h, uint64_t want) {
-    uint64_t fit = std::max<uint64_t>(1, h->budget / (kSlotBytesPerNode * h->z));
-    want = std::max<uint64_t>(1, std::min(want, fit));
-    if (h->slots >= want)
+// Table pool of at least `cap` entries (40 bytes each with the support index
+// and the ring slot). A new pool holds only zero tags, which match no epoch.
+void ensure_tables(nkg_local *h, uint64_t cap) {
+    if (h->table_cap >= cap)
         return;
-    const size_t n = static_cast<size_t>(want * h->z);
-    h->r.reset(), h->p.reset(), h->stamp.reset(), h->touched.reset(), h->queue.reset();
-    h->slots = 0;
-    h->r.alloc(n);
-    h->p.alloc(n);
-    h->stamp.alloc(n);
-    h->touched.alloc(n);
-    h->queue.alloc(n);
-    h->epoch.alloc(want);
-    NKG_CUDA(cudaMemsetAsync(h->stamp.get(), 0, n * 4, h->stream));
-    NKG_CUDA(cudaMemsetAsync(h->epoch.get(), 0, want * 4, h->stream));
-    h->slots = want;
-    h->epochs_used = 0;
+    h->ent_pool.reset();
+    h->idx_pool.reset();
+    h->ring_pool.reset();
+    h->table_cap = 0;
+    h->ent_pool.alloc(cap);
+    h->idx_pool.alloc(cap);
+    h->ring_pool.alloc(cap);
+    NKG_CUDA(cudaMemsetAsync(h->ent_pool.get(), 0, cap * sizeof(MapEntry), h->stream));
+    h->table_cap = cap;
+    h->epoch_base = 0;
 }
 
 // Result pool of `cap` entries; the sweep arrays only when `nibble`.
-void ensure_pool(nkg_local *h, uint64_t cap, bool nibble) {
-    if (h->pool_cap < cap) {
+void ensure_out(nkg_local *h, uint64_t cap, bool nibble) {
+    if (h->out_cap < cap) {
         h->out_node.alloc(cap);
         h->node_sorted.alloc(cap);
         h->ord_node.alloc(cap);
@@ -475,10 +625,10 @@ void ensure_pool(nkg_local *h, uint64_t cap, bool nibble) {
         h->out_p.alloc(cap);
         local_iota<<<ceil_div(cap, 256), 256, 0, h->stream>>>(h->iota.get(), cap);
         NKG_CUDA(cudaGetLastError());
-        h->pool_cap = cap;
+        h->out_cap = cap;
     }
-    if (nibble && h->nibble_cap < h->pool_cap) {
-        const uint64_t c = h->pool_cap;
+    if (nibble && h->nibble_cap < h->out_cap) {
+        const uint64_t c = h->out_cap;
         h->set_node.alloc(c);
         h->set_sorted.alloc(c);
         h->out_key.alloc(c);
@@ -507,6 +657,7 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 void run_local(nkg_local *h, double alpha, double eps, uint64_t problems, const uint64_t *seed_ptr,
                const uint32_t *seeds, bool nibble, uint64_t max_pushes, nkg_local_stats *st) {
     cudaStream_t s = h->stream;
+    require(problems <= static_cast<uint64_t>(INT_MAX), "too many problems in one call");
     const uint64_t nseeds = seed_ptr[problems];
     require(seed_ptr[0] == 0, "seed_ptr must start at 0");
     for (uint64_t k = 0; k < problems; ++k) {
@@ -519,7 +670,11 @@ void run_local(nkg_local *h, double alpha, double eps, uint64_t problems, const 
         }
     }
     const unsigned sms = num_sms(h->device);
-    ensure_slots(h, std::min<uint64_t>(problems, static_cast<uint64_t>(sms) * 16));
+    // Problems in flight: one per warp, at most 32 warps per SM, and as many
+    // as the memory budget gives first tables (with room to double twice).
+    const uint64_t by_budget = h->budget / (4ull * kInitCap * (sizeof(MapEntry) + 8));
+    const uint64_t warps = std::max<uint64_t>(
+        1, std::min<uint64_t>({problems, static_cast<uint64_t>(sms) * kWarpsPerSm, by_budget}));
     DeviceArray<uint64_t> d_seed_ptr(problems + 1);
     DeviceArray<uint32_t> d_seeds(nseeds);
     NKG_CUDA(cudaMemcpyAsync(d_seed_ptr.get(), seed_ptr, (problems + 1) * 8, cudaMemcpyHostToDevice, s));
@@ -530,25 +685,26 @@ void run_local(nkg_local *h, double alpha, double eps, uint64_t problems, const 
     h->d_set_cnt.alloc(problems);
     h->d_set_end.alloc(problems);
     h->d_pushes.alloc(problems);
+    h->d_visits.alloc(problems);
     if (!h->counters)
-        h->counters.alloc(2);
+        h->counters.alloc(3);
     if (!h->err)
         h->err.alloc(1);
-    ensure_pool(h, std::max<uint64_t>(h->pool_cap, std::max<uint64_t>(1 << 20, problems * 256)),
-                nibble);
+    // Tables: what the last call asked for, at least 16 first tables a warp.
+    ensure_tables(h, std::max<uint64_t>(warps * kInitCap * 16, h->table_need));
+    ensure_out(h, std::max<uint64_t>(h->out_cap, std::max<uint64_t>(1 << 20, problems * 256)),
+               nibble);
 
     uint64_t launches = 0, reruns = 0, used = 0;
     NKG_CUDA(cudaEventRecord(h->ev0, s));
     for (;;) {
-        // A slot's epoch grows by one per problem it takes; restart the
-        // stamps before any could wrap.
-        if (h->epochs_used + problems >= 0xfffffff0ull) {
-            NKG_CUDA(cudaMemsetAsync(h->stamp.get(), 0, h->slots * h->z * 4, s));
-            NKG_CUDA(cudaMemsetAsync(h->epoch.get(), 0, h->slots * 4, s));
-            h->epochs_used = 0;
+        // Every launch takes fresh epochs (a re-run must not see the tags
+        // of the failed launch); restart the tags before they could wrap.
+        if (static_cast<uint64_t>(h->epoch_base) + problems + 1 >= 0xffffffffull) {
+            NKG_CUDA(cudaMemsetAsync(h->ent_pool.get(), 0, h->table_cap * sizeof(MapEntry), s));
+            h->epoch_base = 0;
         }
-        h->epochs_used += problems;
-        NKG_CUDA(cudaMemsetAsync(h->counters.get(), 0, 2 * sizeof(unsigned long long), s));
+        NKG_CUDA(cudaMemsetAsync(h->counters.get(), 0, 3 * sizeof(unsigned long long), s));
         NKG_CUDA(cudaMemsetAsync(h->err.get(), 0, sizeof(int), s));
         PushArgs a{};
         a.ptr = h->ptr.get();
@@ -562,16 +718,16 @@ void run_local(nkg_local *h, double alpha, double eps, uint64_t problems, const 
         a.problems = problems;
         a.seed_ptr = d_seed_ptr.get();
         a.seeds = d_seeds.get();
-        a.slots = h->slots;
-        a.r = h->r.get();
-        a.p = h->p.get();
-        a.stamp = h->stamp.get();
-        a.touched = h->touched.get();
-        a.queue = h->queue.get();
-        a.epoch = h->epoch.get();
-        a.pool_cap = h->pool_cap;
-        a.pool_used = h->counters.get();
+        a.epoch_base = h->epoch_base;
+        a.init_cap = kInitCap;
+        a.ent_pool = h->ent_pool.get();
+        a.idx_pool = h->idx_pool.get();
+        a.ring_pool = h->ring_pool.get();
+        a.pool_cap = h->table_cap;
+        a.pool_used = h->counters.get() + 2;
         a.next = h->counters.get() + 1;
+        a.out_cap = h->out_cap;
+        a.out_used = h->counters.get();
         a.out_node = h->out_node.get();
         a.out_p = h->out_p.get();
         a.out_key = h->out_key.get();
@@ -579,9 +735,12 @@ void run_local(nkg_local *h, double alpha, double eps, uint64_t problems, const 
         a.sup_off = h->d_sup_off.get();
         a.sup_cnt = h->d_sup_cnt.get();
         a.pushes = h->d_pushes.get();
+        a.visits = h->d_visits.get();
         a.err = h->err.get();
         a.nibble = nibble ? 1 : 0;
-        const unsigned blocks = ceil_div(h->slots * 32, kLocalThreads);
+        h->epoch_base += static_cast<uint32_t>(problems);
+        NKG_CUDA(cudaEventRecord(h->ev3, s));
+        const unsigned blocks = ceil_div(warps * 32, kLocalThreads);
         if (h->weighted)
             local_push<true><<<blocks, kLocalThreads, 0, s>>>(a);
         else
@@ -589,15 +748,23 @@ void run_local(nkg_local *h, double alpha, double eps, uint64_t problems, const 
         NKG_CUDA(cudaGetLastError());
         ++launches;
         const int e = read_scalar(h->err.get(), s);
-        if (e == 1)
-            throw Error(NKG_ERR_INVALID_ARG,
-                        "push queue overflow: a node was queued twice (negative weights?)");
         if (e == 2)
             throw Error(NKG_ERR_TIMEOUT, "push limit reached before the residuals fell below epsilon");
+        if (e == 4)
+            throw Error(NKG_ERR_INVALID_ARG, "a problem's support passed 2^30 nodes");
+        // The pool counter keeps the entries every warp asked for, granted or
+        // not: the next pool holds them all.
+        h->table_need = read_scalar(h->counters.get() + 2, s);
+        if (e == 3) {
+            ensure_tables(h, std::max<uint64_t>(2 * h->table_cap,
+                                                h->table_need + h->table_need / 4));
+            ++reruns;
+            continue;
+        }
         used = read_scalar(h->counters.get(), s);
-        if (used <= h->pool_cap)
+        if (used <= h->out_cap)
             break;
-        ensure_pool(h, used + used / 8, nibble);
+        ensure_out(h, used + used / 8, nibble);
         ++reruns;
     }
     NKG_CUDA(cudaEventRecord(h->ev1, s));
@@ -605,7 +772,6 @@ void run_local(nkg_local *h, double alpha, double eps, uint64_t problems, const 
             "the supports of one call exceed 2^31 entries; pass fewer seed sets per call");
     const int items = static_cast<int>(used);
     const int segs = static_cast<int>(problems);
-    require(problems <= static_cast<uint64_t>(INT_MAX), "too many problems in one call");
     local_seg_ends<<<ceil_div(problems, 256), 256, 0, s>>>(problems, h->d_sup_off.get(),
                                                           h->d_sup_cnt.get(), h->d_sup_end.get());
     ++launches;
@@ -642,12 +808,14 @@ void run_local(nkg_local *h, double alpha, double eps, uint64_t problems, const 
     NKG_CUDA(cudaEventRecord(h->ev2, s));
     h->sup_off.resize(problems);
     h->sup_cnt.resize(problems);
-    std::vector<uint64_t> pushes(problems);
+    std::vector<uint64_t> pushes(problems), visits(problems);
     NKG_CUDA(cudaMemcpyAsync(h->sup_off.data(), h->d_sup_off.get(), problems * 8,
                              cudaMemcpyDeviceToHost, s));
     NKG_CUDA(cudaMemcpyAsync(h->sup_cnt.data(), h->d_sup_cnt.get(), problems * 8,
                              cudaMemcpyDeviceToHost, s));
     NKG_CUDA(cudaMemcpyAsync(pushes.data(), h->d_pushes.get(), problems * 8,
+                             cudaMemcpyDeviceToHost, s));
+    NKG_CUDA(cudaMemcpyAsync(visits.data(), h->d_visits.get(), problems * 8,
                              cudaMemcpyDeviceToHost, s));
     if (nibble) {
         h->set_cnt.resize(problems);
@@ -659,12 +827,16 @@ void run_local(nkg_local *h, double alpha, double eps, uint64_t problems, const 
     h->nibble = nibble;
     if (st) {
         st->pushes = 0;
+        st->arc_visits = 0;
         for (uint64_t x : pushes)
             st->pushes += x;
+        for (uint64_t x : visits)
+            st->arc_visits += x;
+        st->table_entries = h->table_need;
         st->support = used;
-        st->slots = h->slots;
+        st->slots = warps;
         st->reruns = reruns;
-        st->ms_push = elapsed(h->ev0, h->ev1);
+        st->ms_push = elapsed(h->ev3, h->ev1);  // the last push launch
         st->ms_total = elapsed(h->ev0, h->ev2);
         st->ms_sweep = st->ms_total - st->ms_push;
         st->kernel_launches = launches;
@@ -754,6 +926,7 @@ int nkg_local_create(nkg_local **out, uint64_t z, const uint64_t *row_ptr, const
         NKG_CUDA(cudaEventCreate(&h->ev0));
         NKG_CUDA(cudaEventCreate(&h->ev1));
         NKG_CUDA(cudaEventCreate(&h->ev2));
+        NKG_CUDA(cudaEventCreate(&h->ev3));
         cudaStream_t s = h->stream;
         h->ptr.alloc(z + 1);
         h->col.alloc(std::max<uint64_t>(arcs, 1));
@@ -797,6 +970,8 @@ void nkg_local_destroy(nkg_local *h) {
         cudaEventDestroy(h->ev1);
     if (h->ev2)
         cudaEventDestroy(h->ev2);
+    if (h->ev3)
+        cudaEventDestroy(h->ev3);
     cudaStream_t s = h->stream;
     delete h;
     if (s)

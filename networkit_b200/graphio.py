@@ -1,8 +1,9 @@
 """Graph file input for the PageRank path: the NetworkitBinaryGraph format.
 
 Mirrors the part of ``networkit.graphio`` (graphio.pyx:145-151
-``NetworkitBinaryReader``, :724-747 ``Format``, :786-812 ``readGraph``) that
-loads the reference's own binary format, decoded by host C++/OpenMP
+``NetworkitBinaryReader``, :153-159 ``NetworkitBinaryWriter``, :724-747
+``Format``, :786-812 ``readGraph``) that reads and writes the reference's own
+binary format, decoded and encoded by host C++/OpenMP
 (``_lib/libnkgen.so``, one thread per file chunk) straight into the in-CSR the
 device graph is built from - no intermediate edge list, no Graph object.
 
@@ -49,6 +50,11 @@ def _load():
         L.nkgen_io_last_error.restype = C.c_char_p
         L.nkgen_graph_free.argtypes = [C.POINTER(_Graph)]
         L.nkgen_read_nkbg.argtypes = [C.c_char_p, C.c_int, C.POINTER(_Graph)]
+        _u64 = C.POINTER(C.c_uint64)
+        _u32 = C.POINTER(C.c_uint32)
+        _f64 = C.POINTER(C.c_double)
+        L.nkgen_write_nkbg.argtypes = [C.c_char_p, C.c_uint64, C.c_int, _u64, _u32, _f64, _u64,
+                                       _u32, _f64, C.c_uint64, C.c_int, C.c_int]
         _lib = L
     return _lib
 
@@ -82,6 +88,64 @@ def read_nkbg(path: str, nthreads: int = 0) -> InCSR:
         L.nkgen_graph_free(C.byref(g))
     n = int(exists.sum())
     return InCSR(z, n, in_ptr, in_col, in_w, wdeg, outdeg, None if n == z else exists, directed)
+
+
+class NetworkitBinaryWeights(enum.IntEnum):
+    """NetworkitBinaryWriter.hpp:17-24."""
+
+    none = 0
+    unsignedFormat = 1
+    signedFormat = 2
+    doubleFormat = 3
+    floatFormat = 4
+    autoDetect = 5
+
+
+def _p(a, t):
+    return None if a is None else a.ctypes.data_as(C.POINTER(t))
+
+
+def write_nkbg(path: str, n: int, out_ptr, out_col, out_w=None, in_ptr=None, in_col=None,
+               in_w=None, directed: bool = False, chunks: int = 32,
+               weights: int = NetworkitBinaryWeights.autoDetect, nthreads: int = 0) -> None:
+    """Write a graph given as its out-lists (outEdges order; neighbour lists
+    for undirected graphs) and, when directed, its in-lists (inEdges order)
+    in the NetworkitBinaryGraph format, byte for byte as the reference's
+    NetworkitBinaryWriter."""
+    c = lambda a, t: None if a is None else np.ascontiguousarray(a, t)  # noqa: E731
+    op, oc, ow = c(out_ptr, np.uint64), c(out_col, np.uint32), c(out_w, np.float64)
+    ip, ic, iw = c(in_ptr, np.uint64), c(in_col, np.uint32), c(in_w, np.float64)
+    L = _load()
+    if L.nkgen_write_nkbg(os.fsencode(path), int(n), int(bool(directed)), _p(op, C.c_uint64),
+                          _p(oc, C.c_uint32), _p(ow, C.c_double), _p(ip, C.c_uint64),
+                          _p(ic, C.c_uint32), _p(iw, C.c_double), int(chunks), int(weights),
+                          int(nthreads)) != 0:
+        raise RuntimeError(L.nkgen_io_last_error().decode())
+
+
+class NetworkitBinaryWriter:
+    """``networkit.graphio.NetworkitBinaryWriter(chunks=32, weightsType=autoDetect)``
+    (NetworkitBinaryWriter.hpp:34): ``write(G, path)`` for a
+    :class:`~networkit_b200.graph.Graph` without deleted nodes."""
+
+    def __init__(self, chunks: int = 32, weightsType=NetworkitBinaryWeights.autoDetect):
+        self._chunks = int(chunks)
+        self._weights = int(weightsType)
+
+    def write(self, G: Graph, path: str) -> None:
+        from .scd import neighbour_csr
+
+        csr = G.inCSR()
+        if csr.exists is not None:
+            raise RuntimeError("the binary format numbers only existing nodes: remove the "
+                               "deleted ids first (the reference writer does not round trip them)")
+        z, optr, ocol, ow, _, directed = neighbour_csr(G)
+        if directed:
+            write_nkbg(path, z, optr, ocol, ow, csr.in_ptr, csr.in_col, csr.in_w, True,
+                       self._chunks, self._weights)
+        else:
+            write_nkbg(path, z, optr, ocol, ow, directed=False, chunks=self._chunks,
+                       weights=self._weights)
 
 
 class NetworkitBinaryReader:

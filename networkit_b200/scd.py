@@ -102,8 +102,9 @@ class PageRankNibble(_Local):
     def run(self, seeds) -> Dict[int, Set[int]]:
         """SelectiveCommunityDetector::run: one community per seed."""
         sl = _seed_list(seeds)
-        _, sets, self.stats = self._device().run([[s] for s in sl], self.alpha, self.epsilon,
-                                                 nibble=True, max_pushes=self.maxPushes)
+        _, sets, self.stats = self._device().run(np.asarray(sl, np.int64), self.alpha,
+                                                 self.epsilon, nibble=True,
+                                                 max_pushes=self.maxPushes)
         return {s: set(c.tolist()) for s, c in zip(sl, sets)}
 
     def expandOneCommunity(self, seeds) -> Set[int]:

@@ -146,8 +146,84 @@ def test_reader_library_exports_header_symbols():
 
     src = open(os.path.join(os.path.dirname(os.path.dirname(HERE)), "include", "nkgio.h")).read()
     syms = sorted(set(re.findall(r"NKGEN_API\s+[\w\s\*]+?\b(nkgen_\w+)\s*\(", src)))
-    assert len(syms) == 3, syms
+    assert len(syms) == 4, syms
     build.build_gen()
     lib = ctypes.CDLL(build.GEN_LIB)
     for s in syms:
         assert hasattr(lib, s), s
+
+
+@pytest.mark.parametrize("name", GRAPH_CASES)
+def test_writer_bytes_match_reference_writer(tmp_path, name):
+    """The writer, given a reference test graph's storage-order adjacency,
+    produces the very bytes the reference's NetworkitBinaryWriter wrote
+    (4 chunks, weight format auto-detected)."""
+    d = np.load(os.path.join(HERE, f"{name}.npz"))
+    directed = bool(d["directed"])
+    w_out = d["out_w"] if bool(d["weighted"]) else None
+    w_in = d["in_w"] if bool(d["weighted"]) else None
+    out = tmp_path / "w.nkbg"
+    if directed:
+        graphio.write_nkbg(str(out), int(d["z"]), d["out_ptr"], d["out_col"], w_out,
+                           d["in_ptr"], d["in_col"], w_in, directed=True, chunks=4)
+    else:
+        graphio.write_nkbg(str(out), int(d["z"]), d["out_ptr"], d["out_col"], w_out,
+                           directed=False, chunks=4)
+    assert out.read_bytes() == open(os.path.join(HERE, f"{name}.nkbg"), "rb").read()
+
+
+@pytest.mark.parametrize("name,chunks", [("unsigned_dir", 5), ("float_dir", 2), ("none_dir", 1)])
+def test_writer_round_trip_formats(tmp_path, name, chunks):
+    """Directed files of every weight encoding: decode, encode again with the
+    same chunks and encoding -> the same bytes."""
+    src = os.path.join(HERE, f"nkbg_{name}.nkbg")
+    fmt = (features(src) & 0xE) >> 1
+    g = graphio.read_nkbg(src)  # in-lists = the file's transpose lists
+    data = open(src, "rb").read()
+    optr, ocol, ow = _file_out_lists(data)  # the file's adjacency lists, in order
+    out = tmp_path / "w.nkbg"
+    graphio.write_nkbg(str(out), g.z, optr, ocol, ow, g.in_ptr, g.in_col, g.in_w,
+                       directed=True, chunks=chunks, weights=fmt)
+    assert out.read_bytes() == data
+
+
+def _file_out_lists(data):
+    """(ptr, col, w) of a directed file's adjacency lists in file order, via
+    the reader on a copy whose adjacency and transpose sections are swapped
+    (its in-rows are then the file's out-lists)."""
+    import tempfile
+
+    b = bytearray(data)
+    adj_off, tr_off, w_off, wt_off = struct.unpack("<4Q", bytes(b[48:80]))
+    struct.pack_into("<4Q", b, 48, tr_off, adj_off, wt_off, w_off)
+    with tempfile.NamedTemporaryFile(suffix=".nkbg", delete=False) as f:
+        f.write(bytes(b))
+        path = f.name
+    try:
+        g = graphio.read_nkbg(path)
+    finally:
+        os.unlink(path)
+    return g.in_ptr, g.in_col, g.in_w
+
+
+def test_writer_graph_api_and_errors(tmp_path):
+    from networkit_b200.graph import Graph
+
+    g = Graph(5, weighted=True, directed=True)
+    for u, v, w in [(0, 1, 2.0), (1, 2, 3.5), (2, 0, 1.0), (4, 4, 7.0), (0, 3, 1.0)]:
+        g.addEdge(u, v, w)
+    p = tmp_path / "g.nkbg"
+    graphio.NetworkitBinaryWriter(chunks=3).write(g, str(p))
+    assert (features(str(p)) & 0xE) >> 1 == 4  # all weights are floats
+    back = graphio.read_nkbg(str(p))
+    ref = g.inCSR()
+    np.testing.assert_array_equal(back.in_ptr, ref.in_ptr)
+    np.testing.assert_array_equal(back.in_col, ref.in_col)
+    np.testing.assert_array_equal(back.in_w, ref.in_w)
+    np.testing.assert_array_equal(back.wdeg, ref.wdeg)
+    h = Graph(3)
+    h.removeNode(2)
+    with pytest.raises(RuntimeError, match="existing nodes"):
+        graphio.NetworkitBinaryWriter().write(h, str(p))
+    with pytest.raises(RuntimeError, match="weights"):
+        graphio.write_nkbg(str(p), 2, [0, 1, 1], [1], weights=9)
