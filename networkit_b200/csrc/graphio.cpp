@@ -215,19 +215,6 @@ int nkgen_read_nkbg(const char *path, int nthreads, nkgen_graph *out) {
             return c ? load_u64(b + sec + (c - 1) * 8) : 0;
         };
         const size_t fixed_w = fmt == kDouble ? 8 : fmt == kFloat ? 4 : 0;
-        auto skip_weight = [&](const uint8_t *&p) {
-            if (fmt == kVarint || fmt == kZigzag) {
-                const size_t k = varint_len(p, end);
-                if (!k)
-                    throw std::runtime_error("truncated weights");
-                p += k;
-            } else if (fixed_w) {
-                if (p + fixed_w > end)
-                    throw std::runtime_error("truncated weights");
-                p += fixed_w;
-            }
-        };
-        (void)skip_weight;
         if (nthreads > 0)
             omp_set_num_threads(nthreads);
 
@@ -242,51 +229,68 @@ int nkgen_read_nkbg(const char *path, int nthreads, nkgen_graph *out) {
         if (!out->in_ptr || !out->outdeg || !out->wdeg || !out->exists)
             throw std::bad_alloc();
 
-        // Pass 1: row lengths. Directed: the transpose count. Undirected: the
-        // adjacency count plus the transpose entries that are not self-loops.
-        // in_ptr[v + 1] holds the row length until the scan below.
+        // Pass 1, per file chunk (the chunks are the format's only entry
+        // points): row lengths (directed: the transpose count; undirected: the
+        // adjacency count plus the transpose entries that are not
+        // self-loops), the out-degrees, and where each node's lists and
+        // weights start in the four streams. in_ptr[v + 1] holds the chunk's
+        // running arc count until the chunk offsets are added.
+        std::vector<uint64_t> pos_adj(z), pos_tr(z), pos_wa(fmt ? z : 0), pos_wt(fmt ? z : 0);
         std::vector<uint64_t> chunk_arcs(chunks + 1, 0);
         std::string err;
+        auto skip_varints = [&](Cursor &cu, uint64_t n) {
+            for (uint64_t j = 0; j < n; ++j) {
+                const size_t k = varint_len(cu.base + cu.off, end);
+                if (!k)
+                    throw std::runtime_error("truncated list data");
+                cu.off += k;
+            }
+        };
+        auto skip_weights = [&](Cursor &cu, uint64_t n) {
+            if (fmt == kVarint || fmt == kZigzag) {
+                skip_varints(cu, n);
+            } else if (fixed_w) {
+                cu.off += n * fixed_w;
+                if (cu.base + cu.off > end)
+                    throw std::runtime_error("truncated weights");
+            }
+        };
 #pragma omp parallel for schedule(dynamic, 1)
         for (int64_t ci = 0; ci < static_cast<int64_t>(chunks); ++ci) {
             try {
                 const uint64_t c = static_cast<uint64_t>(ci);
                 Cursor adj{b + off_adj, end, chunk_off(off_adj, c) + hdr + 8};
                 Cursor tr{b + off_tr, end, chunk_off(off_tr, c) + hdr + 8};
+                Cursor wa{b + off_w, end, fmt ? chunk_off(off_w, c) + hdr : 0};
+                Cursor wt{b + off_wt, end, fmt ? chunk_off(off_wt, c) + hdr : 0};
                 uint64_t sum = 0;
                 for (uint64_t v = first[c]; v < first[c + 1]; ++v) {
+                    pos_adj[v] = adj.off;
+                    pos_tr[v] = tr.off;
+                    if (fmt) {
+                        pos_wa[v] = wa.off;
+                        pos_wt[v] = wt.off;
+                    }
                     const uint64_t n_out = adj.next_varint();
                     const uint64_t n_in = tr.next_varint();
                     uint64_t len;
+                    skip_varints(adj, n_out);
                     if (directed) {
                         len = n_in;
-                        for (uint64_t j = 0; j < n_out; ++j) {
-                            const size_t k = varint_len(adj.base + adj.off, end);
-                            if (!k)
-                                throw std::runtime_error("truncated list data");
-                            adj.off += k;
-                        }
-                        for (uint64_t j = 0; j < n_in; ++j) {
-                            const size_t k = varint_len(tr.base + tr.off, end);
-                            if (!k)
-                                throw std::runtime_error("truncated list data");
-                            tr.off += k;
-                        }
+                        skip_varints(tr, n_in);
                         out->outdeg[v] = static_cast<uint32_t>(n_out);
                     } else {
                         len = n_out;
-                        for (uint64_t j = 0; j < n_out; ++j) {
-                            const size_t k = varint_len(adj.base + adj.off, end);
-                            if (!k)
-                                throw std::runtime_error("truncated list data");
-                            adj.off += k;
-                        }
                         for (uint64_t j = 0; j < n_in; ++j)
                             len += tr.next_varint() != v;
                         out->outdeg[v] = static_cast<uint32_t>(len);
                     }
-                    out->in_ptr[v + 1] = len;
+                    if (fmt) {
+                        skip_weights(wa, n_out);
+                        skip_weights(wt, n_in);
+                    }
                     sum += len;
+                    out->in_ptr[v + 1] = sum;
                 }
                 chunk_arcs[c + 1] = sum;
             } catch (const std::exception &e) {
@@ -303,6 +307,12 @@ int nkgen_read_nkbg(const char *path, int nthreads, nkgen_graph *out) {
             throw std::runtime_error("arc count must fit in 32 bits");
         out->arcs = arcs;
         out->in_ptr[0] = 0;
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int64_t ci = 0; ci < static_cast<int64_t>(chunks); ++ci) {
+            const uint64_t c = static_cast<uint64_t>(ci);
+            for (uint64_t v = first[c]; v < first[c + 1]; ++v)
+                out->in_ptr[v + 1] += chunk_arcs[c];
+        }
         out->in_col = static_cast<uint32_t *>(malloc(std::max<uint64_t>(arcs, 1) * 4));
         if (!out->in_col)
             throw std::bad_alloc();
@@ -311,20 +321,40 @@ int nkgen_read_nkbg(const char *path, int nthreads, nkgen_graph *out) {
             if (!out->w)
                 throw std::bad_alloc();
         }
-        // Pass 2: every list decoded straight to its place.
+        // Pass 2: node ranges of about equal arc counts (a power-law graph
+        // puts most arcs in a few chunks), each decoded from its recorded
+        // stream positions straight to its rows.
+        const int threads = std::max(1, omp_get_max_threads());
+        const uint64_t parts = std::min<uint64_t>(z, static_cast<uint64_t>(threads) * 16);
+        std::vector<uint64_t> cut(parts + 1, z);
+        cut[0] = 0;
+        for (uint64_t k = 1; k < parts; ++k) {
+            const uint64_t target = arcs / parts * k + (arcs % parts) * k / parts;
+            cut[k] = static_cast<uint64_t>(
+                std::upper_bound(out->in_ptr, out->in_ptr + z + 1, target) - out->in_ptr) - 1;
+            cut[k] = std::max(cut[k], cut[k - 1]);
+        }
 #pragma omp parallel for schedule(dynamic, 1)
-        for (int64_t ci = 0; ci < static_cast<int64_t>(chunks); ++ci) {
+        for (int64_t pi = 0; pi < static_cast<int64_t>(parts); ++pi) {
             try {
-                const uint64_t c = static_cast<uint64_t>(ci);
-                Cursor adj{b + off_adj, end, chunk_off(off_adj, c) + hdr + 8};
-                Cursor tr{b + off_tr, end, chunk_off(off_tr, c) + hdr + 8};
-                Cursor wa{b + off_w, end, fmt ? chunk_off(off_w, c) + hdr : 0};
-                Cursor wt{b + off_wt, end, fmt ? chunk_off(off_wt, c) + hdr : 0};
-                uint64_t pos = chunk_arcs[c];
-                for (uint64_t v = first[c]; v < first[c + 1]; ++v) {
+                const uint64_t v0 = cut[pi], v1 = cut[pi + 1];
+                if (v0 >= v1)
+                    continue;
+                Cursor adj{b + off_adj, end, pos_adj[v0]};
+                Cursor tr{b + off_tr, end, pos_tr[v0]};
+                Cursor wa{b + off_w, end, fmt ? pos_wa[v0] : 0};
+                Cursor wt{b + off_wt, end, fmt ? pos_wt[v0] : 0};
+                for (uint64_t v = v0; v < v1; ++v) {
+                    // A node that starts a chunk: its streams start there.
+                    adj.off = pos_adj[v];
+                    tr.off = pos_tr[v];
+                    if (fmt) {
+                        wa.off = pos_wa[v];
+                        wt.off = pos_wt[v];
+                    }
                     out->exists[v] = b[off_base + v] & 1u;
-                    const uint64_t len = out->in_ptr[v + 1];
-                    const uint64_t row0 = pos;
+                    const uint64_t row0 = out->in_ptr[v];
+                    uint64_t pos = row0;
                     const uint64_t n_out = adj.next_varint();
                     const uint64_t n_in = tr.next_varint();
                     double osum = 0.0;
@@ -353,9 +383,8 @@ int nkgen_read_nkbg(const char *path, int nthreads, nkgen_graph *out) {
                             out->w[pos] = w;
                         ++pos;
                     }
-                    if (pos - row0 != len)
+                    if (pos != out->in_ptr[v + 1])
                         throw std::runtime_error("inconsistent list lengths");
-                    out->in_ptr[v + 1] = pos;
                     if (directed) {
                         out->wdeg[v] = fmt ? osum : static_cast<double>(n_out);
                     } else {

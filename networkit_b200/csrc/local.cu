@@ -301,9 +301,9 @@ __global__ void __launch_bounds__(kLocalThreads) local_push(PushArgs a) {
             ++qh;
             const MapEntry ue = m.tab[uidx];
             const uint32_t u = static_cast<uint32_t>(ue.tag);
-            const double res = ue.r;
             const double volume = vol[u];
             const uint64_t b = ptr[u], e = ptr[u + 1];
+            const double res = ue.r;
             const double a1 = __dmul_rn(oma, res);  // (1.0 - alpha) * res
             const double d2 = __dmul_rn(2.0, volume);
             nvisit += e - b;
@@ -596,7 +596,6 @@ struct nkg_local {
 namespace {
 
 constexpr uint32_t kInitCap = 1024;    // first table of a warp: 40 KB
-constexpr unsigned kWarpsPerSm = 32;   // 4 CTAs of 8 warps at <= 64 registers
 
 // Table pool of at least `cap` entries (40 bytes each with the support index
 // and the ring slot). A new pool holds only zero tags, which match no epoch.
@@ -670,11 +669,20 @@ void run_local(nkg_local *h, double alpha, double eps, uint64_t problems, const 
         }
     }
     const unsigned sms = num_sms(h->device);
-    // Problems in flight: one per warp, at most 32 warps per SM, and as many
-    // as the memory budget gives first tables (with room to double twice).
+    // Problems in flight: one per resident warp, and as many as the memory
+    // budget gives first tables (with room to double twice).
+    int ctas_per_sm = 0;
+    if (h->weighted)
+        NKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, local_push<true>,
+                                                               kLocalThreads, 0));
+    else
+        NKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, local_push<false>,
+                                                               kLocalThreads, 0));
+    const uint64_t resident = static_cast<uint64_t>(sms) * std::max(ctas_per_sm, 1) *
+                              (kLocalThreads / 32);
     const uint64_t by_budget = h->budget / (4ull * kInitCap * (sizeof(MapEntry) + 8));
-    const uint64_t warps = std::max<uint64_t>(
-        1, std::min<uint64_t>({problems, static_cast<uint64_t>(sms) * kWarpsPerSm, by_budget}));
+    const uint64_t warps =
+        std::max<uint64_t>(1, std::min<uint64_t>({problems, resident, by_budget}));
     DeviceArray<uint64_t> d_seed_ptr(problems + 1);
     DeviceArray<uint32_t> d_seeds(nseeds);
     NKG_CUDA(cudaMemcpyAsync(d_seed_ptr.get(), seed_ptr, (problems + 1) * 8, cudaMemcpyHostToDevice, s));
