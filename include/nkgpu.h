@@ -383,6 +383,14 @@ NKG_API int nkg_local_run(nkg_local *h, double alpha, double epsilon, uint64_t p
 NKG_API int nkg_local_support(nkg_local *h, uint32_t *nodes_out, double *values_out);
 NKG_API int nkg_local_sets(nkg_local *h, uint32_t *nodes_out);
 
+/* Device memory: the library keeps the blocks it frees in a per-device
+ * cache keyed by size and hands them out again (a block at most 1/8 larger
+ * than the request), so that creating and destroying graphs does not map and
+ * unmap device memory each time; an allocation that fails first empties the
+ * cache. This returns the cached blocks of `device` (-1: the current device)
+ * to the driver; blocks still owned by live handles stay. */
+NKG_API int nkg_release_cached_memory(int device);
+
 /* Message of the last failure on the calling thread ("" if none). */
 NKG_API const char *nkg_last_error(void);
 

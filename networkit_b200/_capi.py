@@ -156,6 +156,7 @@ SIGNATURES = {
     "nkg_batch_run": (C.c_int, [_vp, C.POINTER(PRParams), _vp, C.c_int, _u64p,
                                 C.POINTER(C.c_uint32), C.POINTER(Stats)]),
     "nkg_batch_graph_times": (C.c_int, [_vp, _f64p, _f64p]),
+    "nkg_release_cached_memory": (C.c_int, [C.c_int]),
     "nkg_local_create": (C.c_int, [C.POINTER(_vp), C.c_uint64, _u64p, _u32p, _f64p, _u8p, C.c_int,
                                    C.c_int, C.c_uint64]),
     "nkg_local_destroy": (None, [_vp]),

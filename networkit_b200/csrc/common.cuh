@@ -42,8 +42,16 @@ inline void require(bool ok, const std::string &msg) {
         throw Error(NKG_ERR_INVALID_ARG, msg);
 }
 
-// Owning device allocation (cudaMalloc/cudaFree). Sizes are in elements; the
-// allocation is padded by `pad` elements so that vectorised or bulk copies
+// Device memory of the library: cudaMalloc'ed blocks that are kept, once
+// freed, in a per-device cache keyed by size, so that graph create / destroy
+// cycles do not map and unmap gigabytes each time. device_free first waits
+// for the device, as cudaFree does, then files the block in the cache.
+// nkg_release_cached_memory hands the cached blocks back.
+void *device_alloc(size_t bytes, int &device);
+void device_free(void *p, int device);
+
+// Owning device allocation (device_alloc/device_free). Sizes are in elements;
+// the allocation is padded by `pad` elements so that vectorised or bulk copies
 // that round an end offset up stay inside it.
 template <typename T>
 class DeviceArray {
@@ -52,7 +60,7 @@ class DeviceArray {
     explicit DeviceArray(size_t n, size_t pad = 0) { alloc(n, pad); }
     DeviceArray(const DeviceArray &) = delete;
     DeviceArray &operator=(const DeviceArray &) = delete;
-    DeviceArray(DeviceArray &&o) noexcept : p_(o.p_), n_(o.n_) {
+    DeviceArray(DeviceArray &&o) noexcept : p_(o.p_), n_(o.n_), dev_(o.dev_) {
         o.p_ = nullptr;
         o.n_ = 0;
     }
@@ -61,6 +69,7 @@ class DeviceArray {
             reset();
             p_ = o.p_;
             n_ = o.n_;
+            dev_ = o.dev_;
             o.p_ = nullptr;
             o.n_ = 0;
         }
@@ -71,14 +80,13 @@ class DeviceArray {
     void alloc(size_t n, size_t pad = 0) {
         reset();
         const size_t bytes = (n + pad) * sizeof(T);
-        if (bytes) {
-            NKG_CUDA(cudaMalloc(reinterpret_cast<void **>(&p_), bytes));
-        }
+        if (bytes)
+            p_ = static_cast<T *>(device_alloc(bytes, dev_));
         n_ = n;
     }
     void reset() {
         if (p_)
-            cudaFree(p_);
+            device_free(p_, dev_);
         p_ = nullptr;
         n_ = 0;
     }
@@ -89,6 +97,7 @@ class DeviceArray {
   private:
     T *p_ = nullptr;
     size_t n_ = 0;
+    int dev_ = 0;
 };
 
 // Pinned host buffer (cudaHostAlloc) for status read-back.

@@ -7,6 +7,9 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <unordered_map>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -24,6 +27,86 @@ namespace nkg {
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string &m) { g_last_error = m; }
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::unordered_map<void *, size_t> g_block_size;  // every block the cache handed out
+
+// Freed blocks kept for reuse, per device, by size: an allocation takes the
+// smallest cached block of at least its size and at most 1/8 larger, so a
+// graph created and destroyed in a loop gets the same blocks back.
+struct BlockCache {
+    std::multimap<size_t, void *> free_blocks;
+    size_t cached_bytes = 0;
+};
+
+std::mutex g_cache_mutex;
+BlockCache g_cache[kMaxDevices];
+
+void release_blocks(BlockCache &c) {
+    for (auto &kv : c.free_blocks) {
+        g_block_size.erase(kv.second);
+        cudaFree(kv.second);
+    }
+    c.free_blocks.clear();
+    c.cached_bytes = 0;
+}
+
+}  // namespace
+
+void *device_alloc(size_t bytes, int &device) {
+    NKG_CUDA(cudaGetDevice(&device));
+    require(device >= 0 && device < kMaxDevices, "device ordinal out of range");
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mutex);
+        BlockCache &c = g_cache[device];
+        auto it = c.free_blocks.lower_bound(bytes);
+        if (it != c.free_blocks.end() && it->first <= bytes + bytes / 8) {
+            void *p = it->second;
+            c.cached_bytes -= it->first;
+            c.free_blocks.erase(it);
+            return p;
+        }
+    }
+    // Blocks carry their size in a side table so that a free files them
+    // under the size they were allocated with.
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        std::lock_guard<std::mutex> lock(g_cache_mutex);
+        release_blocks(g_cache[device]);
+        e = cudaMalloc(&p, bytes);
+    }
+    NKG_CUDA(e);
+    std::lock_guard<std::mutex> lock(g_cache_mutex);
+    g_block_size[p] = bytes;
+    return p;
+}
+
+void device_free(void *p, int device) {
+    if (!p)
+        return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != device)
+        cudaSetDevice(device);
+    // As cudaFree: no work still in flight may use the block.
+    cudaDeviceSynchronize();
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mutex);
+        auto it = g_block_size.find(p);
+        if (it != g_block_size.end()) {
+            g_cache[device].free_blocks.emplace(it->second, p);
+            g_cache[device].cached_bytes += it->second;
+        } else {
+            cudaFree(p);
+        }
+    }
+    if (prev != device && prev >= 0)
+        cudaSetDevice(prev);
+}
 
 // ---------------------------------------------------------------------------
 // Graph build kernels
@@ -1510,6 +1593,19 @@ extern "C" {
 const char *nkg_last_error(void) { return nkg::g_last_error.c_str(); }
 
 int nkg_abi_version(void) { return NKG_ABI_VERSION; }
+
+int nkg_release_cached_memory(int device) {
+    return guarded([&] {
+        int dev = device;
+        if (dev < 0)
+            NKG_CUDA(cudaGetDevice(&dev));
+        require(dev >= 0 && dev < kMaxDevices, "device ordinal out of range");
+        DeviceGuard guard(dev);
+        NKG_CUDA(cudaDeviceSynchronize());
+        std::lock_guard<std::mutex> lock(g_cache_mutex);
+        release_blocks(g_cache[dev]);
+    });
+}
 
 int nkg_graph_create_ex(nkg_graph **out, uint64_t z, uint64_t arcs, const uint64_t *in_row_ptr,
                         const uint32_t *in_col, const double *in_w, const double *out_wdeg,

@@ -246,3 +246,28 @@ def test_repeated_runs_are_bit_identical():
     b = dg.run(p)
     np.testing.assert_array_equal(a[0], b[0])
     assert a[1] == b[1]
+
+
+def test_memory_pool_reuse_and_release(oracle_mod):
+    """Graphs created and destroyed in a loop reuse the library's cached
+    device memory and give the same scores; nkg_release_cached_memory hands
+    the cache back to the driver."""
+    import torch
+
+    from networkit_b200 import generators
+
+    csr = generators.rmat_directed(14, 8, seed=5)
+    free0 = torch.cuda.mem_get_info()[0]
+    first = None
+    for _ in range(3):
+        g = _capi.DeviceGraph(csr)
+        p = g.params(0.85, 1e-10, 0, False, False, _capi.NKG_PREC_FP64, 1000)
+        s, it, _, _ = g.run(p)
+        g.close()
+        if first is None:
+            first = (s, it)
+        np.testing.assert_array_equal(s, first[0])
+    _capi.check(_capi.lib().nkg_release_cached_memory(-1))
+    assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)
+    o = oracle_mod.pagerank(csr, tol=1e-10, norm=0)
+    assert np.abs(first[0] - o.scores).sum() <= 1e-10
