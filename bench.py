@@ -207,9 +207,32 @@ def profiled_traffic(kernel_tag):
     return None
 
 
-def cpu_baseline_port(csr, nthreads, target_s=15.0):
-    """The oracle's C restatement on the host cores, over a bounded number of
-    iterations of the same workload."""
+def host_cpu():
+    """Model, logical CPUs and physical cores of this host (from /proc/cpuinfo)."""
+    model, phys = None, set()
+    cur = {}
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if ":" not in line:
+                    if "core id" in cur:
+                        phys.add((cur.get("physical id"), cur["core id"]))
+                    cur = {}
+                    continue
+                k, v = (x.strip() for x in line.split(":", 1))
+                cur[k] = v
+                if k == "model name" and model is None:
+                    model = v
+        if "core id" in cur:
+            phys.add((cur.get("physical id"), cur["core id"]))
+    except OSError:
+        pass
+    return {"model": model, "logical": os.cpu_count() or 1, "physical": len(phys) or None}
+
+
+def cpu_baseline_port(csr, nthreads, target_s=4.0, runs=3):
+    """The oracle's C restatement on the host cores over a bounded number of
+    iterations of the same workload: the median of `runs` timed runs."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
@@ -217,14 +240,20 @@ def cpu_baseline_port(csr, nthreads, target_s=15.0):
     oracle.pagerank(csr, damp=DAMP, tol=TOL, norm=NORM_L1, max_iterations=1, nthreads=nthreads)
     t1 = time.perf_counter() - t0
     iters = int(max(2, min(20, target_s / max(t1, 1e-3))))
-    t0 = time.perf_counter()
-    r = oracle.pagerank(csr, damp=DAMP, tol=TOL, norm=NORM_L1, max_iterations=iters,
-                        nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    return {"value": csr.arcs * r.iterations / dt / 1e9, "unit": UNIT, "cores": nthreads,
-            "kind": "port",
-            "sample": f"{r.iterations} iterations of the same R-MAT scale-{int(np.log2(csr.z))} "
-                      f"FP64 run (oracle C restatement, OpenMP rows), {dt:.1f} s"}
+    rates, secs = [], []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        r = oracle.pagerank(csr, damp=DAMP, tol=TOL, norm=NORM_L1, max_iterations=iters,
+                            nthreads=nthreads)
+        dt = time.perf_counter() - t0
+        rates.append(csr.arcs * r.iterations / dt / 1e9)
+        secs.append(dt)
+    cpu = host_cpu()
+    return {"value": statistics.median(rates), "unit": UNIT, "cores": nthreads,
+            "kind": "port", "cpu_model": cpu["model"], "physical_cores": cpu["physical"],
+            "sample": f"median of {runs} runs of {iters} iterations of the same R-MAT "
+                      f"scale-{int(np.log2(csr.z))} FP64 run (oracle C restatement, OpenMP rows; "
+                      f"{min(secs):.1f}-{max(secs):.1f} s each)"}
 
 
 def form_ppr(local, n=4_000_000, m=8, k=256, steps=2):
@@ -733,6 +762,7 @@ def run_reference_arm(args):
                    "edgefactor": EDGEFACTOR, "n": csr.z, "arcs": csr.arcs, "damp": DAMP,
                    "tol": TOL, "norm": "L1", "iterations_per_step": iters},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "cpu_model": host_cpu()["model"], "physical_cores": host_cpu()["physical"],
                          "sample": f"{iters} iterations of NetworKit::PageRank::run() per step "
                                    f"(maxIterations={iters}) on the same graph"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -876,7 +906,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_port(csr, os.cpu_count() or 1)
+        cpu = cpu_baseline_port(csr, host_cpu()["physical"] or os.cpu_count() or 1)
     dg.close()
 
     # Companion forms, each against the plain FP64 GPU path on the same GPU.
