@@ -590,7 +590,58 @@ def form_centrality(local, csr):
                      "gteps_per_iter": csr.arcs * it / (ms / 1e3) / 1e9,
                      "gpu_launches": st["kernel_launches"]}
     dg.close()
+    res["reference_scale21"] = centrality_vs_reference(local)
     return res
+
+
+def centrality_vs_reference(local, scale=21):
+    """The reference's own CPU paths beside ours on directed R-MAT `scale`
+    (same generator and seed as the headline, all host cores): building the
+    graph from its edge list (Graph::addEdge in a loop against
+    nkg_graph_create_from_edges from host arrays, both to a graph ready for
+    the run), EigenvectorCentrality::run (tol 1e-9) and KatzCentrality::run
+    (alpha = 1/(1 + maxDegree), beta 0.1, tol 1e-8, in-edges). Device runs
+    timed with CUDA events, reference runs around run() only."""
+    from networkit_b200 import _capi, generators
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if not oracle.ref_available():
+        return {"unavailable": "oracle/_ref/libnkref.so is not built"}
+    import torch
+
+    csr = generators.rmat_directed(scale, EDGEFACTOR, *RMAT, seed=SEED)
+    rows = np.repeat(np.arange(csr.z, dtype=np.uint32), np.diff(csr.in_ptr).astype(np.int64))
+    cores = os.cpu_count() or 1
+    out = {"workload": f"rmat{scale}_fp64", "n": csr.z, "arcs": csr.arcs, "cores": cores,
+           "kind": "reference"}
+    t0 = time.perf_counter()
+    rg = oracle.RefGraph.from_edges(csr.z, csr.in_col, rows, directed=True)
+    ref_build = time.perf_counter() - t0
+    best = float("inf")
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g = _capi.DeviceGraph.from_edges(csr.z, csr.in_col, rows, directed=True, device=local)
+        torch.cuda.synchronize()
+        best = min(best, time.perf_counter() - t0)
+        g.close()
+    out["ingest"] = {"reference_s": ref_build, "ours_s": best, "speedup": ref_build / best}
+    dg = _capi.DeviceGraph(csr, device=local)
+    _, ref_s = rg.eigenvector(1e-9, nthreads=cores, timed=True)
+    dg.eigenvector(1e-9)
+    _, it, st = dg.eigenvector(1e-9)
+    out["eigenvector"] = {"reference_s": ref_s, "ours_ms": st["ms_total"], "iterations": it,
+                          "speedup": ref_s / (st["ms_total"] / 1e3)}
+    _, _, ref_s = rg.katz(0.0, 0.1, 1e-8, out_edges=False, nthreads=cores, timed=True)
+    dg.katz(0.0, 0.1, 1e-8, 0)
+    _, it, st = dg.katz(0.0, 0.1, 1e-8, 0)
+    out["katz_in"] = {"reference_s": ref_s, "ours_ms": st["ms_total"], "iterations": it,
+                      "speedup": ref_s / (st["ms_total"] / 1e3)}
+    dg.close()
+    del rg
+    return out
 
 
 def form_local(local, n=1_000_000, deg=16, seeds=16384, alpha=0.1, eps=1e-5, ref_sample=48,

@@ -439,17 +439,18 @@ class RefGraph:
                 return [sets[int(offs[i]):int(offs[i + 1])].copy() for i in range(k)], secs.value
             cap = int(tot.value)
 
-    def eigenvector(self, tol=1e-9, nthreads=0):
+    def eigenvector(self, tol=1e-9, nthreads=0, timed=False):
+        """scores (and, with timed, the seconds of run())."""
         lib = ref_lib()
         scores = np.empty(self.z, np.float64)
         secs = C.c_double(0.0)
         if lib.nkref_eigenvector(self.h, tol, int(nthreads), _ptr(scores, _f64p),
                                  C.byref(secs)) != 0:
             raise RuntimeError(lib.nkref_last_error().decode())
-        return scores
+        return (scores, secs.value) if timed else scores
 
-    def katz(self, alpha=0.0, beta=0.1, tol=1e-8, out_edges=False, nthreads=0):
-        """(scores, ranking ids)"""
+    def katz(self, alpha=0.0, beta=0.1, tol=1e-8, out_edges=False, nthreads=0, timed=False):
+        """(scores, ranking ids) (and, with timed, the seconds of run())."""
         lib = ref_lib()
         scores = np.empty(self.z, np.float64)
         ids = np.empty(self.n, np.uint64)
@@ -457,7 +458,7 @@ class RefGraph:
         if lib.nkref_katz(self.h, alpha, beta, tol, int(bool(out_edges)), int(nthreads),
                           _ptr(scores, _f64p), _ptr(ids, _u64p), C.byref(secs)) != 0:
             raise RuntimeError(lib.nkref_last_error().decode())
-        return scores, ids
+        return (scores, ids, secs.value) if timed else (scores, ids)
 
     def pagerank(self, damp=0.85, tol=1e-8, normalized=False, norm=1, max_iterations=2**64 - 1,
                  nthreads=0, want_ranking=True):
