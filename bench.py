@@ -910,6 +910,9 @@ def main():
 
     # Roofline of the dominant kernel (the sweep), timed alone with events.
     ms_kernel, ms_iter = dg.profile_sweeps(_capi.NKG_PREC_FP64, 20)
+    # The random-gather bound: the sweep's gathers alone (same slot stream,
+    # same iterate), a floor under the sweep time.
+    ms_gather = dg.profile_gathers(_capi.NKG_PREC_FP64, 20)
     bytes_sweep = st["bytes_per_sweep_fp64"]
     peak, peak_kind = measured_peak_hbm()
     achieved = bytes_sweep / (ms_kernel / 1e3) / 1e9
@@ -994,7 +997,9 @@ def main():
                              f"sweep_fp64_rmat{args.scale}"),
                          "kernel": "sweep_kernel<double> (SELL-32 pull SpMV)",
                          "bytes_per_launch": bytes_sweep, "ms_per_launch": ms_kernel,
-                         "ms_per_iteration": ms_iter, "peak_source": peak_kind},
+                         "ms_per_iteration": ms_iter, "peak_source": peak_kind,
+                         "gather_bound_ms": ms_gather,
+                         "frac_of_gather_bound": ms_gather / ms_kernel},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "ms_per_step": 1e3 * sum(e2e_t) / len(e2e_t) if e2e_t else None,

@@ -301,6 +301,14 @@ NKG_API void nkg_cancel(nkg_graph *g);
 NKG_API int nkg_profile_sweeps(nkg_graph *g, int precision, int sweeps, double *ms_sweep_kernel,
                                double *ms_iteration);
 
+/* Diagnostic, no reference counterpart: only the gathers of one sweep - the
+ * sliced layout's column stream in storage order, padding included, read
+ * from the current iterate and summed per thread, eight gathers in flight
+ * per thread - timed with CUDA events over `reps` launches (after one
+ * untimed launch). Its mean launch time is the random-gather bound of this
+ * graph on this GPU, the floor under nkg_profile_sweeps' sweep time. */
+NKG_API int nkg_profile_gathers(nkg_graph *g, int precision, int reps, double *ms_gather_kernel);
+
 /* PageRank without any device allocation; no counterpart in the reference.
  * For callers that cannot allocate device memory when they call in: a
  * framework whose caching allocator owns the device memory, a service with

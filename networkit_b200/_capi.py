@@ -134,6 +134,7 @@ SIGNATURES = {
     "nkg_ranking": (C.c_int, [_vp, _f64p, _u64p, _f64p]),
     "nkg_cancel": (None, [_vp]),
     "nkg_profile_sweeps": (C.c_int, [_vp, C.c_int, C.c_int, _f64p, _f64p]),
+    "nkg_profile_gathers": (C.c_int, [_vp, C.c_int, C.c_int, _f64p]),
     "nkg_pagerank_csr_noalloc": (C.c_int, [C.c_uint64, C.c_uint64, _vp, _vp, C.POINTER(PRParams),
                                            _vp, _u64p, _vp]),
     "nkg_ppr_run": (C.c_int, [_vp, C.POINTER(PRParams), C.c_uint32, _u32p, _vp, C.c_int, _u64p,
@@ -429,6 +430,13 @@ class DeviceGraph:
         check(lib().nkg_profile_sweeps(self.h, int(precision), int(sweeps), C.byref(a),
                                        C.byref(b)))
         return float(a.value), float(b.value)
+
+    def profile_gathers(self, precision: int, reps: int = 20) -> float:
+        """ms per launch of the gathers-only diagnostic kernel (the random
+        gather bound of the sweep on this graph)."""
+        a = C.c_double(0.0)
+        check(lib().nkg_profile_gathers(self.h, int(precision), int(reps), C.byref(a)))
+        return float(a.value)
 
 
 class DeviceBatch:

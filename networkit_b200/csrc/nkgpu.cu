@@ -1543,6 +1543,65 @@ static void profile_sweeps(nkg_graph *g, int sweeps, double *ms_kernel, double *
     *ms_iter = sweeps > 1 ? total / (sweeps - 1) : sum;
 }
 
+// Diagnostic: only the gathers of a sweep - the same slot stream (the sliced
+// layout's columns in storage order, padding included) into the same
+// iterate - summed per thread, eight gathers in flight per thread. Its time
+// is the random-gather bound of the graph on this GPU.
+template <typename T>
+__global__ void __launch_bounds__(256) gather_bound_kernel(const uint32_t *__restrict__ col,
+                                                           uint64_t slots, const T *__restrict__ y,
+                                                           T *__restrict__ sink) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t t = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    uint64_t i = t;
+    T acc = 0;
+    for (; i + 7 * stride < slots; i += 8 * stride) {
+        uint32_t c[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            c[k] = col[i + k * stride];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            acc += y[c[k]];
+    }
+    for (; i < slots; i += stride)
+        acc += y[col[i]];
+    sink[t] = acc;
+}
+
+template <typename T, bool WEIGHTED>
+static double profile_gathers(nkg_graph *g, int reps) {
+    cudaStream_t s = g->stream;
+    sweep_setup<T, WEIGHTED>(g);
+    Plane<T> &P = plane<T>(g);
+    nkg_pr_params p{};
+    p.damp = 0.85;
+    p.tol = -1.0;
+    p.norm = NKG_NORM_L1;
+    p.max_iterations = ~0ull;
+    upload_run_state<T, WEIGHTED>(g, p, 0, nullptr);
+    const unsigned blocks = num_sms(g->device) * 8;
+    DeviceArray<T> sink(static_cast<size_t>(blocks) * 256);
+    const uint64_t slots = g->fw.slots;  // entries of col_sell
+    cudaEvent_t e0, e1;
+    NKG_CUDA(cudaEventCreate(&e0));
+    NKG_CUDA(cudaEventCreate(&e1));
+    gather_bound_kernel<T><<<blocks, 256, 0, s>>>(g->fw.col_sell.get(), slots, P.y[0].get(),
+                                                  sink.get());  // warm-up
+    NKG_CUDA(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; ++r)
+        gather_bound_kernel<T><<<blocks, 256, 0, s>>>(g->fw.col_sell.get(), slots,
+                                                      P.y[r & 1].get(), sink.get());
+    NKG_CUDA(cudaEventRecord(e1, s));
+    NKG_CUDA(cudaGetLastError());
+    NKG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    NKG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return ms / reps;
+}
+
 static int run_to(nkg_graph *g, const nkg_pr_params *p, const double *teleport, bool tele_is_host,
                   double *out, bool out_is_host, uint64_t *iters, double *max_out,
                   nkg_stats *stats) {
@@ -1763,6 +1822,22 @@ int nkg_profile_sweeps(nkg_graph *g, int precision, int sweeps, double *ms_sweep
             else
                 profile_sweeps<float, false>(g, sweeps, ms_sweep_kernel, ms_iteration);
         }
+    });
+}
+
+int nkg_profile_gathers(nkg_graph *g, int precision, int reps, double *ms_gather_kernel) {
+    return guarded([&] {
+        require(g != nullptr && ms_gather_kernel != nullptr, "NULL argument");
+        require(reps >= 1 && reps <= 100000, "reps must be in [1, 100000]");
+        require(precision == NKG_PREC_FP64 || precision == NKG_PREC_FP32,
+                "precision must be FP64 or FP32");
+        DeviceGuard guard(g->device);
+        if (precision == NKG_PREC_FP64)
+            *ms_gather_kernel = g->weighted ? profile_gathers<double, true>(g, reps)
+                                            : profile_gathers<double, false>(g, reps);
+        else
+            *ms_gather_kernel = g->weighted ? profile_gathers<float, true>(g, reps)
+                                            : profile_gathers<float, false>(g, reps);
     });
 }
 
