@@ -236,9 +236,11 @@ NKG_API int nkg_ppr_run(nkg_graph *g, const nkg_pr_params *p, uint32_t k, const 
  * cluster size, threads per CTA, and the row-split threshold (rows longer
  * than `split` arcs are summed by a whole warp, the others one per lane in
  * 32-row slices). nkg_batch_tune times `sweeps` sweeps of every graph for
- * each candidate (split 32..1024, 256 or 512 threads, clusters 1..16), then
- * the kernel variants on the best of those, and keeps the fastest; results (nullable, `capacity` entries) receive every
- * timed candidate, n_results their count.
+ * each candidate (split 32..1024, 256 or 512 threads, clusters 1..16), or
+ * with sweeps = 0 the whole run to convergence under *p (the real objective:
+ * it sees the largest graphs' critical path), then the kernel variants on
+ * the best of those, and keeps the fastest; results (nullable, `capacity`
+ * entries) receive every timed candidate, n_results their count.
  * nkg_batch_run: scores_out = the total node count of doubles (caller ids,
  * each graph normalised like PageRank.cpp:75-92), host or device memory
  * (flags 0 / NKG_DEVICE_PTRS); iterations_out (nullable, host) = count sweep

@@ -4,10 +4,11 @@
 //
 // The graphs are given as one block-diagonal in-CSR (graph i owns the node
 // ids [node_offsets[i], node_offsets[i+1])). Each graph is relabelled by
-// in-degree, descending, inside its own id range. With a row-split threshold
-// T, its rows longer than T ("long rows", a prefix) are summed by a whole warp
+// in-degree bucket (half-octaves), descending, inside its own id range,
+// keeping the id order inside a bucket. With a row-split threshold T, its
+// rows longer than T ("long rows", a prefix) are summed by a whole warp
 // each; the others sit in SELL-32 slices (32 rows, column-major slots, one
-// row per lane; slice length = its first row's length).
+// row per lane; slice length = its longest row's length).
 //
 // The kernel is persistent and cluster-based: every thread-block cluster of
 // C CTAs takes the next graph from a queue ordered by arc count, descending,
@@ -327,6 +328,21 @@ __global__ void bt_node_graph(const uint64_t *__restrict__ node_off, uint32_t co
             node_graph[v] = i;
 }
 
+// Relabelling bucket of an in-degree d: half-octaves of d - 1 (0 for d <= 1),
+// so that d > T for a power of two T is exactly bucket >= 2 log2(T) + 1 and
+// the rows longer than any power-of-two split stay a prefix. Inside a
+// bucket rows keep their id order: on graphs whose ids follow geometry
+// (hyperbolic graphs number nodes by angle) neighbouring rows then gather
+// from neighbouring ids, and the lanes of a warp share sectors.
+__device__ __forceinline__ uint32_t degree_bucket(uint32_t d) {
+    if (d <= 1)
+        return 0;
+    const uint32_t x = d - 1;
+    const uint32_t e = 31 - __clz(x);
+    const uint32_t half = static_cast<uint64_t>(x) * x >= (1ull << (2 * e + 1)) ? 1u : 0u;
+    return 2 * e + half + 1;
+}
+
 __global__ void bt_validate(const uint64_t *__restrict__ in_ptr, const uint32_t *__restrict__ in_col,
                             const uint32_t *__restrict__ node_graph, uint32_t total, uint64_t arcs,
                             uint32_t *__restrict__ outdeg, uint64_t *__restrict__ keys,
@@ -343,8 +359,8 @@ __global__ void bt_validate(const uint64_t *__restrict__ in_ptr, const uint32_t 
         }
         const uint32_t gv = node_graph[v];
         if (lane == 0) {
-            const uint64_t d = e - b;
-            keys[v] = (static_cast<uint64_t>(gv) << 32) | (0xffffffffu - static_cast<uint32_t>(d));
+            keys[v] = (static_cast<uint64_t>(gv) << 32) |
+                      (0xffffffffu - degree_bucket(static_cast<uint32_t>(e - b)));
             ids[v] = static_cast<uint32_t>(v);
         }
         for (uint64_t k = b + lane; k < e; k += 32) {
@@ -391,8 +407,9 @@ __global__ void bt_relabel(const uint32_t *__restrict__ perm, const uint64_t *__
     }
 }
 
-// Per graph (one thread each): rows longer than T (a prefix: rows are sorted
-// by length, descending, inside a graph) and rows without out-arcs.
+// Per graph (one thread each): rows longer than T, a prefix of the graph's
+// rows when T is a power of two (rows are ordered by degree bucket,
+// descending; any other T gives a correct split with more padding).
 __global__ void bt_split(GraphMeta *__restrict__ meta, uint32_t count,
                          const uint32_t *__restrict__ rowlen, uint32_t split) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -419,14 +436,19 @@ __global__ void bt_sinks(const uint32_t *__restrict__ degc, const uint32_t *__re
         atomicAdd(sinks + node_graph[r], 1u);
 }
 
-// Slice lengths (= the first row's length) and the graph of every slice.
+// Slice lengths (the longest of the slice's rows) and the graph of every
+// slice.
 __global__ void bt_slice_len(const GraphMeta *__restrict__ meta, uint32_t count,
                              const uint32_t *__restrict__ rowlen, uint32_t *__restrict__ slen,
                              uint32_t *__restrict__ slice_graph) {
     for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
         const GraphMeta m = meta[i];
         for (uint32_t k = threadIdx.x; k < m.slices; k += blockDim.x) {
-            slen[m.slice0 + k] = rowlen[m.base + m.n_long + 32 * k];
+            const uint32_t r0 = m.n_long + 32 * k, r1 = min(m.n, r0 + 32);
+            uint32_t len = 0;
+            for (uint32_t r = r0; r < r1; ++r)
+                len = max(len, rowlen[m.base + r]);
+            slen[m.slice0 + k] = len;
             slice_graph[m.slice0 + k] = i;
         }
     }
@@ -928,11 +950,13 @@ int nkg_batch_tune(nkg_batch *b, const nkg_pr_params *p, uint32_t sweeps,
     return guarded([&] {
         require(b != nullptr, "batch is NULL");
         check_batch_params(p);
-        require(sweeps >= 1 && sweeps <= 1000, "sweeps must be in [1, 1000]");
+        require(sweeps <= 1000, "sweeps must be in [0, 1000]");
         DeviceGuard guard(b->device);
         nkg_pr_params tp = *p;
-        tp.tol = -1.0;               // no stopping test: every graph runs `sweeps` sweeps
-        tp.max_iterations = sweeps;
+        if (sweeps) {
+            tp.tol = -1.0;  // no stopping test: every graph runs `sweeps` sweeps
+            tp.max_iterations = sweeps;
+        }  // else every candidate runs the batch to convergence, as a real run does
         upload_params(b, tp);
         const uint32_t splits[] = {32, 64, 128, 256, 1024};
         const uint32_t threads[] = {256, 512};

@@ -247,7 +247,9 @@ double rhg_radius(uint64_t n, double avg_deg, double alpha) {
     return 0.5 * (lo + hi);
 }
 
-// One graph: its neighbour lists (rows ascending), node ids = draw order.
+// One graph: its neighbour lists (rows ascending). Node ids follow the
+// points sorted by angle, then radius, as HyperbolicGenerator numbers them
+// (HyperbolicGenerator.cpp:75-92): angularly close nodes get close ids.
 // Bands of radial width 1 counted from the rim (the inner band takes the
 // rest) hold their points sorted by angle; a point queries every band over
 // the angular window that the band's inner radius allows, then tests each
@@ -259,15 +261,26 @@ void rhg_rows(uint64_t n, double avg_deg, double exponent, uint64_t seed,
     const double R = rhg_radius(n, avg_deg, alpha);
     const double chR = std::cosh(R);
     const double span = std::cosh(alpha * R) - 1.0;
-    std::vector<RhgPoint> pts(n);
+    std::vector<RhgPoint> drawn(n);
     for (uint64_t i = 0; i < n; ++i) {
         const uint64_t h1 = hash3(seed, 1, i), h2 = hash3(seed, 2, i);
-        RhgPoint &p = pts[i];
+        RhgPoint &p = drawn[i];
         p.theta = 2.0 * M_PI * u01(h1);
         p.r = std::acosh(1.0 + u01(h2) * span) / alpha;
         p.ch = std::cosh(p.r);
         p.sh = std::sinh(p.r);
     }
+    std::vector<uint32_t> by_angle(n);
+    std::iota(by_angle.begin(), by_angle.end(), 0u);
+    std::sort(by_angle.begin(), by_angle.end(), [&](uint32_t x, uint32_t y) {
+        return drawn[x].theta < drawn[y].theta ||
+               (drawn[x].theta == drawn[y].theta &&
+                (drawn[x].r < drawn[y].r || (drawn[x].r == drawn[y].r && x < y)));
+    });
+    std::vector<RhgPoint> pts(n);
+    for (uint64_t j = 0; j < n; ++j)
+        pts[j] = drawn[by_angle[j]];
+    drawn.clear();
     const int nb = std::max(1, static_cast<int>(std::ceil(R)));
     std::vector<double> inner(nb);
     for (int b = 0; b < nb; ++b)

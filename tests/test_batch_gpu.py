@@ -105,6 +105,12 @@ def test_batch_tuner(batch):
     assert db.tuning()["split"] == best["split"]
     for t in table:
         assert t["cluster"] in (1, 2, 4, 8, 16) and t["threads"] in (256, 512)
+    # sweeps = 0: every candidate runs to convergence; the chosen shape then
+    # gives the same results as any other within the bars.
+    best0, table0 = db.tune(p, sweeps=0)
+    assert best0["ms"] == min(t["ms"] for t in table0)
+    scores, its, _, _ = db.run(p)
+    check(__import__("oracle"), gs, offs, scores, its, _capi.NKG_PREC_FP32, 0, 1e-8, False, False)
 
 
 def test_batch_rejects_bad_input():
