@@ -63,7 +63,7 @@ def parse_args():
                     help="nkg_graph_options.arc_order (0 keep the reference order, 1 sorted)")
     ap.add_argument("--form", default="",
                     choices=["", "ppr", "refine", "adjoint", "batch", "centrality", "local",
-                             "reader"],
+                             "reader", "locality"],
                     help="run only one companion form and print its figures")
     ap.add_argument("--fd-edges", type=int, default=64,
                     help="arcs checked by finite differences in --form adjoint")
@@ -644,6 +644,31 @@ def centrality_vs_reference(local, scale=21):
     return out
 
 
+def form_locality(local, n=4_000_000, deg=16):
+    """PageRank FP64 (tol 1e-10, L1) on an undirected threshold hyperbolic graph
+    numbered by angle (as HyperbolicGenerator numbers its nodes): the sliced
+    layout with in-degree relabelling (row_order 0) against half-octave
+    in-degree buckets that keep the id order inside a bucket (row_order 1,
+    the automatic choice for this graph). Device time per run, graph resident."""
+    from networkit_b200 import _capi, generators
+
+    g = generators.hyperbolic(n, deg, 3, seed=21)
+    res = {"workload": f"pagerank_hyperbolic{n}_deg{deg}_fp64", "n": g.z, "arcs": g.arcs}
+    for ro in (0, 1, -1):
+        dg = _capi.DeviceGraph(g, device=local, row_order=ro)
+        p = dg.params(DAMP, TOL, NORM_L1, False, False, _capi.NKG_PREC_FP64, _capi.UINT64_MAX)
+        dg.run(p)
+        _, it, _, st = dg.run(p)
+        info = dg.info()
+        k, _ = dg.profile_sweeps(_capi.NKG_PREC_FP64, 10)
+        res[f"row_order_{ro}"] = {"resolved": info["row_order"], "ms": st["ms_total"],
+                                  "iterations": it, "slots": info["slots"], "ms_per_sweep": k,
+                                  "gteps_per_iter": g.arcs * it / (st["ms_total"] / 1e3) / 1e9}
+        dg.close()
+    res["speedup_buckets"] = res["row_order_0"]["ms"] / res["row_order_1"]["ms"]
+    return res
+
+
 def form_local(local, n=1_000_000, deg=16, seeds=16384, alpha=0.1, eps=1e-5, ref_sample=48,
                runs=2):
     """PageRankNibble(G, 0.1, 1e-5) (the SelectiveCDGTest.cpp parameters),
@@ -837,6 +862,9 @@ def main():
         print(json.dumps(form_batch(local, count=args.batch_graphs,
                                     step_only=args.batch_step_only)))
         return
+    if args.form == "locality":
+        print(json.dumps(form_locality(local)))
+        return
     if args.form == "local":
         print(json.dumps(form_local(local, n=args.local_n, seeds=args.local_seeds,
                                     ref_sample=args.local_ref_sample, runs=args.local_runs)))
@@ -972,6 +1000,7 @@ def main():
                          ("fwd_bwd", lambda: form_adjoint(local, steps=2, fd_edges=0)),
                          ("eigenvector_katz", lambda: form_centrality(local, csr)),
                          ("pagerank_nibble", lambda: form_local(local)),
+                         ("locality", lambda: form_locality(local)),
                          ("nkbg_reader", lambda: form_reader(local, csr)),
                          ("batch", lambda: form_batch(local, steps=2,
                                                       plain_graphs=range(0, 1024, 8)))):

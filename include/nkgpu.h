@@ -95,7 +95,7 @@ typedef struct {
     int32_t weighted;
     int32_t directed;
     int32_t device;
-    int32_t reserved;
+    int32_t row_order;   /* the relabelling used (nkg_graph_options.row_order, resolved) */
     double ms_create;    /* device time of nkg_graph_create after the copies */
 } nkg_graph_info;
 
@@ -109,7 +109,16 @@ typedef struct {
                             which is the reference's summation order; 1: sort
                             each in-row by source after relabelling (faster
                             gathers, sums rounded in a different order) */
-    int32_t reserved;    /* must be 0 */
+    int32_t row_order;   /* relabelling of the rows for the sliced layout: 0 (default)
+                            in-degree, descending; 1 half-octave in-degree buckets,
+                            descending, keeping the caller's id order inside a bucket
+                            (for numberings that carry locality - geometric, crawl or
+                            mesh order: neighbouring rows then gather from neighbouring
+                            ids and share sectors; slices pad a little more); -1
+                            automatic: 1 when more than 1/4 of 65,536 sampled arcs join
+                            ids closer than max(64, z/1024), else 0; nkg_graph_create
+                            (no options) uses -1. Results do not depend on it beyond
+                            the order of the reductions */
 } nkg_graph_options;
 
 /* Upload a graph given as its in-adjacency CSR.

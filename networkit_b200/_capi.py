@@ -72,7 +72,7 @@ class GraphInfo(C.Structure):
         ("weighted", C.c_int32),
         ("directed", C.c_int32),
         ("device", C.c_int32),
-        ("reserved", C.c_int32),
+        ("row_order", C.c_int32),
         ("ms_create", C.c_double),
     ]
 
@@ -82,7 +82,7 @@ class GraphInfo(C.Structure):
 
 class GraphOptions(C.Structure):
     _fields_ = [("device", C.c_int32), ("sweep_shape", C.c_int32), ("arc_order", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("row_order", C.c_int32)]
 
 
 class BatchTuning(C.Structure):
@@ -210,7 +210,8 @@ def ptr(a, t):
 class DeviceGraph:
     """Owning wrapper of an nkg_graph handle."""
 
-    def __init__(self, csr, device: int = -1, sweep_shape: int = -1, arc_order: int = 0):
+    def __init__(self, csr, device: int = -1, sweep_shape: int = -1, arc_order: int = 0,
+                 row_order: int = -1):
         L = lib()
         h = _vp()
         in_ptr = np.ascontiguousarray(csr.in_ptr, np.uint64)
@@ -222,6 +223,7 @@ class DeviceGraph:
         opts.device = int(device)
         opts.sweep_shape = int(sweep_shape)
         opts.arc_order = int(arc_order)
+        opts.row_order = int(row_order)
         check(L.nkg_graph_create_ex(C.byref(h), int(csr.z), int(in_col.shape[0]),
                                     ptr(in_ptr, _u64p), ptr(in_col, _u32p), ptr(in_w, _f64p),
                                     ptr(wdeg, _f64p), ptr(ex, _u8p), int(bool(csr.directed)),
@@ -232,7 +234,7 @@ class DeviceGraph:
 
     @classmethod
     def from_edges(cls, z, src, dst, w=None, directed=False, exists=None, device: int = -1,
-                   sweep_shape: int = -1):
+                   sweep_shape: int = -1, row_order: int = -1):
         """Build the graph on the device from host edge arrays in insertion
         order (nkg_graph_create_from_edges)."""
         s = np.ascontiguousarray(src, np.uint32)
@@ -260,6 +262,7 @@ class DeviceGraph:
         h = _vp()
         opts = GraphOptions()
         opts.device = int(device)
+        opts.row_order = int(row_order)
         opts.sweep_shape = int(sweep_shape)
         check(lib().nkg_graph_create_from_edges(
             C.byref(h), int(z), int(m), _vp(src_p or None), _vp(dst_p or None), _vp(w_p or None),

@@ -328,21 +328,10 @@ __global__ void bt_node_graph(const uint64_t *__restrict__ node_off, uint32_t co
             node_graph[v] = i;
 }
 
-// Relabelling bucket of an in-degree d: half-octaves of d - 1 (0 for d <= 1),
-// so that d > T for a power of two T is exactly bucket >= 2 log2(T) + 1 and
-// the rows longer than any power-of-two split stay a prefix. Inside a
-// bucket rows keep their id order: on graphs whose ids follow geometry
-// (hyperbolic graphs number nodes by angle) neighbouring rows then gather
-// from neighbouring ids, and the lanes of a warp share sectors.
-__device__ __forceinline__ uint32_t degree_bucket(uint32_t d) {
-    if (d <= 1)
-        return 0;
-    const uint32_t x = d - 1;
-    const uint32_t e = 31 - __clz(x);
-    const uint32_t half = static_cast<uint64_t>(x) * x >= (1ull << (2 * e + 1)) ? 1u : 0u;
-    return 2 * e + half + 1;
-}
-
+// Graphs are relabelled by degree_bucket (common.cuh): inside a bucket rows
+// keep their id order, so on graphs whose ids follow geometry (hyperbolic
+// graphs number nodes by angle) neighbouring rows gather from neighbouring
+// ids and the lanes of a warp share sectors.
 __global__ void bt_validate(const uint64_t *__restrict__ in_ptr, const uint32_t *__restrict__ in_col,
                             const uint32_t *__restrict__ node_graph, uint32_t total, uint64_t arcs,
                             uint32_t *__restrict__ outdeg, uint64_t *__restrict__ keys,

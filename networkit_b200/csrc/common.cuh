@@ -126,6 +126,20 @@ class PinnedHost {
 
 constexpr uint32_t kNone = 0xffffffffu;
 
+// Relabelling bucket of an in-degree d: half-octaves of d - 1 (0 for d <= 1).
+// d > T for a power of two T is exactly bucket >= 2 log2(T) + 1, so rows
+// longer than any power-of-two threshold stay a prefix of a bucket order.
+__host__ __device__ inline uint32_t degree_bucket(uint32_t d) {
+    if (d <= 1)
+        return 0;
+    const uint32_t x = d - 1;
+    uint32_t e = 0;
+    while ((x >> e) > 1)
+        ++e;
+    const uint32_t half = static_cast<uint64_t>(x) * x >= (1ull << (2 * e + 1)) ? 1u : 0u;
+    return 2 * e + half + 1;
+}
+
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return static_cast<unsigned>((a + b - 1) / b); }
 
 // ---------------------------------------------------------------------------

@@ -80,6 +80,7 @@ struct nkg_graph {
     uint64_t z = 0, n = 0, arcs = 0, sinks = 0;
     bool weighted = false, directed = false;
     double ms_create = 0.0;
+    int row_order = 0;  // relabelling used: 0 in-degree, 1 in-degree buckets
 
     nkg::DeviceArray<uint32_t> perm;     // new id -> original id (n)
     nkg::DeviceArray<uint32_t> inv;      // original id -> new id (z), kNone if absent

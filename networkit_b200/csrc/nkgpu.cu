@@ -144,9 +144,11 @@ __global__ void validate_and_count(const uint64_t *__restrict__ in_ptr,
 }
 
 // Sort key per original id: deleted nodes 0 (sorted last), existing nodes
-// in-degree + 1. Counts sinks (existing, out-degree 0).
+// in-degree + 1, or with `bucketed` degree_bucket(in-degree) + 1 (the stable
+// sort then keeps the caller's order inside a bucket). Counts sinks
+// (existing, out-degree 0).
 __global__ void make_keys(const uint64_t *__restrict__ in_ptr, const uint32_t *__restrict__ outdeg,
-                          const uint8_t *__restrict__ exists, uint64_t z,
+                          const uint8_t *__restrict__ exists, uint64_t z, int bucketed,
                           uint32_t *__restrict__ keys, uint32_t *__restrict__ ids,
                           unsigned long long *__restrict__ sinks) {
     const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
@@ -154,13 +156,42 @@ __global__ void make_keys(const uint64_t *__restrict__ in_ptr, const uint32_t *_
     if (i < z) {
         const bool ex = exists == nullptr || exists[i];
         const uint64_t d = in_ptr[i + 1] - in_ptr[i];
-        keys[i] = ex ? static_cast<uint32_t>(d + 1) : 0u;
+        const uint32_t k = bucketed ? degree_bucket(static_cast<uint32_t>(d))
+                                    : static_cast<uint32_t>(d);
+        keys[i] = ex ? k + 1 : 0u;
         ids[i] = static_cast<uint32_t>(i);
         sink = ex && outdeg[i] == 0;
     }
     const int c = __syncthreads_count(sink);
     if (threadIdx.x == 0 && c)
         atomicAdd(sinks, static_cast<unsigned long long>(c));
+}
+
+// Id locality of the caller's numbering: over `samples` arcs spread evenly
+// across the CSR, how many join ids closer than `window` (the row of arc a
+// is found by binary search in in_ptr).
+__global__ void locality_sample(const uint64_t *__restrict__ in_ptr,
+                                const uint32_t *__restrict__ in_col, uint64_t z, uint64_t arcs,
+                                uint32_t samples, uint64_t window,
+                                unsigned long long *__restrict__ close) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    bool c = false;
+    if (s < samples && arcs) {
+        const uint64_t a = arcs * s / samples;
+        uint64_t lo = 0, hi = z;  // last row with in_ptr[row] <= a
+        while (hi - lo > 1) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (in_ptr[mid] <= a)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const uint64_t v = in_col[a];
+        c = (v > lo ? v - lo : lo - v) < window;
+    }
+    const int cnt = __syncthreads_count(c);
+    if (threadIdx.x == 0 && cnt)
+        atomicAdd(close, static_cast<unsigned long long>(cnt));
 }
 
 // Ranking input: deleted ids get -inf so that they sort behind every score.
@@ -836,10 +867,26 @@ static nkg_graph *build_graph(std::unique_ptr<nkg_graph> g, DeviceArray<uint64_t
     default: throw Error(NKG_ERR_INVALID_ARG, "a non-existent node has in-arcs");
     }
 
-    // Relabelling order: in-degree descending, ties by id.
+    // Relabelling order: in-degree descending (row_order 0) or half-octave
+    // in-degree buckets descending (row_order 1), ties by id; -1 picks 1 when
+    // the caller's ids carry locality (more than 1/4 of 65,536 sampled arcs
+    // join ids closer than max(64, z/1024)).
+    int row_order = opt ? opt->row_order : -1;  // no options: automatic
+    require(row_order >= -1 && row_order <= 1, "row_order must be -1, 0 or 1");
+    if (row_order < 0) {
+        constexpr uint32_t kSamples = 65536;
+        DeviceArray<unsigned long long> close(1);
+        NKG_CUDA(cudaMemsetAsync(close.get(), 0, sizeof(unsigned long long), s));
+        locality_sample<<<kSamples / 256, 256, 0, s>>>(d_ptr.get(), d_col.get(), z, arcs, kSamples,
+                                                       std::max<uint64_t>(64, z / 1024),
+                                                       close.get());
+        NKG_CUDA(cudaGetLastError());
+        row_order = (arcs && read_scalar(close.get(), s) * 4 > kSamples) ? 1 : 0;
+    }
+    g->row_order = row_order;
     DeviceArray<uint32_t> keys(z), ids(z), keys_s(z), ids_s(z);
-    make_keys<<<ceil_div(z, 256), 256, 0, s>>>(d_ptr.get(), outdeg.get(), d_ex.get(), z, keys.get(),
-                                               ids.get(), cnt.get());
+    make_keys<<<ceil_div(z, 256), 256, 0, s>>>(d_ptr.get(), outdeg.get(), d_ex.get(), z,
+                                               row_order, keys.get(), ids.get(), cnt.get());
     NKG_CUDA(cudaGetLastError());
     size_t tmp_bytes = 0;
     NKG_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, keys.get(), keys_s.get(),
@@ -889,7 +936,6 @@ static nkg_graph *build_graph(std::unique_ptr<nkg_graph> g, DeviceArray<uint64_t
                                               g->w64src.get());
     NKG_CUDA(cudaGetLastError());
     if (opt) {
-        require(opt->reserved == 0, "reserved options must be 0");
         require(opt->sweep_shape >= -1 && opt->sweep_shape < kNumSweepShapes,
                 "unknown sweep shape");
         require(opt->arc_order == 0 || opt->arc_order == 1, "arc_order must be 0 or 1");
@@ -1731,6 +1777,7 @@ int nkg_graph_get_info(const nkg_graph *g, nkg_graph_info *info) {
         info->directed = g->directed;
         info->device = g->device;
         info->ms_create = g->ms_create;
+        info->row_order = g->row_order;
     });
 }
 

@@ -271,3 +271,27 @@ def test_memory_pool_reuse_and_release(oracle_mod):
     assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)
     o = oracle_mod.pagerank(csr, tol=1e-10, norm=0)
     assert np.abs(first[0] - o.scores).sum() <= 1e-10
+
+
+@pytest.mark.parametrize("row_order", [0, 1, -1])
+def test_row_order_relabelling(oracle_mod, row_order):
+    """The half-octave bucket relabelling (and its automatic choice) changes
+    only the layout: FP64 scores within 1e-10 L1 of the oracle and the
+    iteration count within 1, on an angle-numbered hyperbolic graph (auto
+    picks buckets) and on R-MAT (auto keeps in-degree order)."""
+    from networkit_b200 import generators
+
+    hyp = generators.hyperbolic(30000, 16, 3, seed=4)
+    rmat = generators.rmat_directed(14, 16, seed=9)
+    for csr, auto_pick in ((hyp, 1), (rmat, 0)):
+        dg = _capi.DeviceGraph(csr, row_order=row_order)
+        assert dg.info()["row_order"] == (auto_pick if row_order == -1 else row_order)
+        p = dg.params(0.85, 1e-10, 0, False, False, _capi.NKG_PREC_FP64, 10000)
+        s, it, _, _ = dg.run(p)
+        o = oracle_mod.pagerank(csr, tol=1e-10, norm=0)
+        assert np.abs(s - o.scores).sum() <= 1e-10
+        assert abs(it - o.iterations) <= 1
+        p32 = dg.params(0.85, 1e-10, 0, False, False, _capi.NKG_PREC_FP32_REFINE, 10000)
+        s32, _, _, _ = dg.run(p32)
+        assert np.abs(s32 - o.scores).sum() <= 1e-9
+        dg.close()
