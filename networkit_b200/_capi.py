@@ -245,19 +245,19 @@ class DeviceGraph:
         ex = None if exists is None else np.ascontiguousarray(exists, np.uint8)
         return cls._from_edge_pointers(
             z, int(s.shape[0]), s.ctypes.data, d.ctypes.data, 0 if ww is None else ww.ctypes.data,
-            0 if ex is None else ex.ctypes.data, directed, False, device, sweep_shape)
+            0 if ex is None else ex.ctypes.data, directed, False, device, sweep_shape, row_order)
 
     @classmethod
     def from_device_edges(cls, z, m, src_ptr, dst_ptr, w_ptr=0, exists_ptr=0, directed=False,
-                          device: int = -1, sweep_shape: int = -1):
+                          device: int = -1, sweep_shape: int = -1, row_order: int = -1):
         """The same from device arrays (raw pointers; uint32 src/dst, float64
         w, uint8 exists)."""
         return cls._from_edge_pointers(z, m, src_ptr, dst_ptr, w_ptr, exists_ptr, directed, True,
-                                       device, sweep_shape)
+                                       device, sweep_shape, row_order)
 
     @classmethod
     def _from_edge_pointers(cls, z, m, src_p, dst_p, w_p, ex_p, directed, on_device, device,
-                            sweep_shape):
+                            sweep_shape, row_order=-1):
         self = cls.__new__(cls)
         h = _vp()
         opts = GraphOptions()
