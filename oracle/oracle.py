@@ -1,15 +1,17 @@
 """Test infrastructure only (the oracle).
 
 ctypes bindings for
-  * ``lib/libnkoracle.so`` - the plain-C restatement of the reference PageRank
-    path (``pagerank_oracle.c``), and
-  * ``_ref/libnkref.so`` - the reference's own PageRank compiled from the
-    reference sources (``Makefile``, ``ref/nkref_capi.cpp``), present only
+  * ``lib/libnkoracle.so`` - the plain-C restatement of the reference paths
+    (``pagerank_oracle.c``: PageRank, its adjoint, EigenvectorCentrality,
+    KatzCentrality, ApproximatePageRank and PageRankNibble's sweep), and
+  * ``_ref/libnkref.so`` - the reference's own implementations compiled from
+    the reference sources (``Makefile``, ``ref/nkref_capi.cpp``), present only
     where it was built.
 
-Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` import this module, and only as the checker / baseline. The
-product path never does.
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline legs of
+``bench.py`` (the reference arm, and the reference's own runs timed beside
+each companion form) import this module, and only as the checker or the
+baseline. The product path never does.
 """
 from __future__ import annotations
 
