@@ -247,6 +247,57 @@ __device__ __forceinline__ void bi_vec_entry(const BiArgs &a, uint32_t i, float 
     }
 }
 
+// Four consecutive vector entries, moved as one 16-byte access. Every vector of
+// a solve is its own allocation (256-byte aligned), so quad q of any of them
+// starts on a 16-byte boundary; the vector kernels walk the n/4 full quads and
+// leave the n % 4 tail to the first threads of CTA 0.
+struct Quad {
+    float v[4];
+};
+
+__device__ __forceinline__ Quad ld_quad(const float *p, uint32_t q) {
+    const float4 t = reinterpret_cast<const float4 *>(p)[q];
+    return Quad{{t.x, t.y, t.z, t.w}};
+}
+
+__device__ __forceinline__ void st_quad(float *p, uint32_t q, const Quad &f) {
+    reinterpret_cast<float4 *>(p)[q] = make_float4(f.v[0], f.v[1], f.v[2], f.v[3]);
+}
+
+// bi_vec_entry over quad q (entries 4q .. 4q+3, in that order).
+template <bool WEIGHTED, int OP>
+__device__ __forceinline__ void bi_vec_quad(const BiArgs &a, uint32_t q, const Quad &vv, double &sk) {
+    if (OP == 0) {
+        const uint4 dc = reinterpret_cast<const uint4 *>(a.degc)[q];
+        const uint32_t c[4] = {dc.x, dc.y, dc.z, dc.w};
+        Quad d;
+        if (WEIGHTED) {
+            d = ld_quad(a.degw, q);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                d.v[k] = static_cast<float>(c[k]);
+        }
+        Quad gq;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            gq.v[k] = c[k] ? vv.v[k] / d.v[k] : vv.v[k];
+            if (!c[k])
+                sk += vv.v[k];
+        }
+        st_quad(a.g, q, gq);
+    } else if (a.personal) {
+        const Quad t = ld_quad(a.tele, q);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            sk += static_cast<double>(t.v[k]) * static_cast<double>(vv.v[k]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            sk += static_cast<double>(vv.v[k]);
+    }
+}
+
 template <int OP>
 __device__ __forceinline__ double bi_sink_total(const BiArgs &a, double t) {
     return OP == 1 && !a.personal ? t * a.inv_n : t;
@@ -263,9 +314,22 @@ __global__ void __launch_bounds__(kBiThreads) bi_vec_p(BiArgs a) {
         return;
     const double beta = (sc->rho / sc->rho_prev) * (sc->alpha / sc->omega);
     const float b = static_cast<float>(beta), om = static_cast<float>(sc->omega);
+    auto step = [b, om](float r, float p, float v) {
+        return __fadd_rn(r, __fmul_rn(b, __fsub_rn(p, __fmul_rn(om, v))));
+    };
     double sk = 0.0;
-    for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < a.n; i += gridDim.x * kBiThreads) {
-        const float pv = __fadd_rn(a.r[i], __fmul_rn(b, __fsub_rn(a.p[i], __fmul_rn(om, a.v[i]))));
+    const uint32_t n4 = a.n >> 2, stride = gridDim.x * kBiThreads, tid = blockIdx.x * kBiThreads + threadIdx.x;
+    for (uint32_t q = tid; q < n4; q += stride) {
+        const Quad r = ld_quad(a.r, q), pp = ld_quad(a.p, q), v = ld_quad(a.v, q);
+        Quad pv;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            pv.v[k] = step(r.v[k], pp.v[k], v.v[k]);
+        st_quad(a.p, q, pv);
+        bi_vec_quad<WEIGHTED, OP>(a, q, pv, sk);
+    }
+    for (uint32_t i = 4 * n4 + tid; i < a.n; i += stride) {
+        const float pv = step(a.r[i], a.p[i], a.v[i]);
         a.p[i] = pv;
         bi_vec_entry<WEIGHTED, OP>(a, i, pv, sk);
     }
@@ -296,7 +360,17 @@ __global__ void __launch_bounds__(kBiThreads) bi_vec_s(BiArgs a) {
         return;
     const float al = static_cast<float>(sc->alpha);
     double sk = 0.0;
-    for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < a.n; i += gridDim.x * kBiThreads) {
+    const uint32_t n4 = a.n >> 2, stride = gridDim.x * kBiThreads, tid = blockIdx.x * kBiThreads + threadIdx.x;
+    for (uint32_t q = tid; q < n4; q += stride) {
+        const Quad r = ld_quad(a.r, q), v = ld_quad(a.v, q);
+        Quad sv;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            sv.v[k] = __fsub_rn(r.v[k], __fmul_rn(al, v.v[k]));
+        st_quad(a.s, q, sv);
+        bi_vec_quad<WEIGHTED, OP>(a, q, sv, sk);
+    }
+    for (uint32_t i = 4 * n4 + tid; i < a.n; i += stride) {
         const float sv = __fsub_rn(a.r[i], __fmul_rn(al, a.v[i]));
         a.s[i] = sv;
         bi_vec_entry<WEIGHTED, OP>(a, i, sv, sk);
@@ -325,13 +399,32 @@ static __global__ void __launch_bounds__(kBiThreads) bi_vec_x(BiArgs a) {
         return;
     const float al = static_cast<float>(sc->alpha), om = static_cast<float>(sc->omega);
     double nr = 0.0, rr = 0.0;
-    for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < a.n; i += gridDim.x * kBiThreads) {
+    auto acc = [&](float rv, float rh) {
+        const double d = rv;
+        nr += a.l2 ? d * d : fabs(d);
+        rr += static_cast<double>(rh) * d;
+    };
+    const uint32_t n4 = a.n >> 2, stride = gridDim.x * kBiThreads, tid = blockIdx.x * kBiThreads + threadIdx.x;
+    for (uint32_t q = tid; q < n4; q += stride) {
+        const Quad x = ld_quad(a.x, q), p = ld_quad(a.p, q), sv = ld_quad(a.s, q), t = ld_quad(a.t, q),
+                   rh = ld_quad(a.rhat, q);
+        Quad xn, rn;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            xn.v[k] = __fadd_rn(x.v[k], __fadd_rn(__fmul_rn(al, p.v[k]), __fmul_rn(om, sv.v[k])));
+            rn.v[k] = __fsub_rn(sv.v[k], __fmul_rn(om, t.v[k]));
+        }
+        st_quad(a.x, q, xn);
+        st_quad(a.r, q, rn);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            acc(rn.v[k], rh.v[k]);
+    }
+    for (uint32_t i = 4 * n4 + tid; i < a.n; i += stride) {
         a.x[i] = __fadd_rn(a.x[i], __fadd_rn(__fmul_rn(al, a.p[i]), __fmul_rn(om, a.s[i])));
         const float rv = __fsub_rn(a.s[i], __fmul_rn(om, a.t[i]));
         a.r[i] = rv;
-        const double d = rv;
-        nr += a.l2 ? d * d : fabs(d);
-        rr += static_cast<double>(a.rhat[i]) * d;
+        acc(rv, a.rhat[i]);
     }
     nr = block_sum<kBiThreads>(nr, s_red);
     rr = block_sum<kBiThreads>(rr, s_red);
@@ -364,15 +457,30 @@ static __global__ void __launch_bounds__(kBiThreads) bi_start(BiArgs a) {
     __shared__ bool s_last;
     BiScalars *sc = a.sc;
     double nr = 0.0, rr = 0.0;
-    for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < a.n; i += gridDim.x * kBiThreads) {
+    auto acc = [&](float b) {
+        const double d = b;
+        nr += a.l2 ? d * d : fabs(d);
+        rr += d * d;
+    };
+    const Quad zero{{0.f, 0.f, 0.f, 0.f}};
+    const uint32_t n4 = a.n >> 2, stride = gridDim.x * kBiThreads, tid = blockIdx.x * kBiThreads + threadIdx.x;
+    for (uint32_t q = tid; q < n4; q += stride) {
+        const Quad b = ld_quad(a.r, q);
+        st_quad(a.rhat, q, b);
+        st_quad(a.x, q, zero);
+        st_quad(a.p, q, zero);
+        st_quad(a.v, q, zero);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            acc(b.v[k]);
+    }
+    for (uint32_t i = 4 * n4 + tid; i < a.n; i += stride) {
         const float b = a.r[i];
         a.rhat[i] = b;
         a.x[i] = 0.f;
         a.p[i] = 0.f;
         a.v[i] = 0.f;
-        const double d = b;
-        nr += a.l2 ? d * d : fabs(d);
-        rr += d * d;
+        acc(b);
     }
     if (a.g && blockIdx.x == 0 && threadIdx.x == 0)
         a.g[a.n] = 0.f;
@@ -420,15 +528,43 @@ __global__ void __launch_bounds__(kBiThreads)
     __shared__ double s_red[32];
     __shared__ bool s_last;
     double sk = 0.0;
-    for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < n; i += gridDim.x * kBiThreads) {
-        const double x = add ? x64[i] + static_cast<double>(x32[i]) : static_cast<double>(x32[i]);
-        x64[i] = x;
-        const uint32_t dc = degc[i];
-        const double d = WEIGHTED ? degw[i] : static_cast<double>(dc);
-        y64[i] = dc ? x / d : x;
+    auto entry = [&](double x32v, double x64v, uint32_t dc, double dw, double &xo, double &yo) {
+        const double x = add ? x64v + x32v : x32v;
+        xo = x;
+        const double d = WEIGHTED ? dw : static_cast<double>(dc);
+        yo = dc ? x / d : x;
         if (!dc)
             sk += x;
+    };
+    // Quads of entries: 16-byte loads of x32 and degc, 2 x 16 bytes of each
+    // FP64 vector (all separate allocations, so 16-byte aligned).
+    const uint32_t n4 = n >> 2, stride = gridDim.x * kBiThreads, tid = blockIdx.x * kBiThreads + threadIdx.x;
+    for (uint32_t q = tid; q < n4; q += stride) {
+        const Quad xs = ld_quad(x32, q);
+        const uint4 dc = reinterpret_cast<const uint4 *>(degc)[q];
+        const uint32_t c[4] = {dc.x, dc.y, dc.z, dc.w};
+        double xo[4], yo[4], xi[4] = {0.0, 0.0, 0.0, 0.0}, dw[4] = {0.0, 0.0, 0.0, 0.0};
+        if (add) {
+            const double2 a0 = reinterpret_cast<const double2 *>(x64)[2 * q];
+            const double2 a1 = reinterpret_cast<const double2 *>(x64)[2 * q + 1];
+            xi[0] = a0.x, xi[1] = a0.y, xi[2] = a1.x, xi[3] = a1.y;
+        }
+        if (WEIGHTED) {
+            const double2 w0 = reinterpret_cast<const double2 *>(degw)[2 * q];
+            const double2 w1 = reinterpret_cast<const double2 *>(degw)[2 * q + 1];
+            dw[0] = w0.x, dw[1] = w0.y, dw[2] = w1.x, dw[3] = w1.y;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            entry(static_cast<double>(xs.v[k]), xi[k], c[k], dw[k], xo[k], yo[k]);
+        reinterpret_cast<double2 *>(x64)[2 * q] = make_double2(xo[0], xo[1]);
+        reinterpret_cast<double2 *>(x64)[2 * q + 1] = make_double2(xo[2], xo[3]);
+        reinterpret_cast<double2 *>(y64)[2 * q] = make_double2(yo[0], yo[1]);
+        reinterpret_cast<double2 *>(y64)[2 * q + 1] = make_double2(yo[2], yo[3]);
     }
+    for (uint32_t i = 4 * n4 + tid; i < n; i += stride)
+        entry(static_cast<double>(x32[i]), add ? x64[i] : 0.0, degc[i], WEIGHTED ? degw[i] : 0.0,
+              x64[i], y64[i]);
     sk = block_sum<kBiThreads>(sk, s_red);
     if (threadIdx.x == 0)
         part[blockIdx.x] = sk;
@@ -478,6 +614,14 @@ struct BiLaunch {
 template <bool WEIGHTED, int OP>
 void bi_solve(const BiArgs &a, BiLaunch &L, double rel, double floor) {
     cudaStream_t s = L.stream;
+    for (const void *v : {static_cast<const void *>(a.x), static_cast<const void *>(a.r),
+                          static_cast<const void *>(a.rhat), static_cast<const void *>(a.p),
+                          static_cast<const void *>(a.v), static_cast<const void *>(a.s),
+                          static_cast<const void *>(a.t), static_cast<const void *>(a.g),
+                          static_cast<const void *>(a.degc), static_cast<const void *>(a.degw),
+                          static_cast<const void *>(a.tele)})
+        if (reinterpret_cast<uintptr_t>(v) % 16)
+            throw Error(NKG_ERR_INVALID_ARG, "BiCGSTAB vectors must be 16-byte aligned");
     bi_start<<<L.vec_ctas, kBiThreads, 0, s>>>(a);
     NKG_CUDA(cudaMemcpyAsync(L.h_sc, L.d_sc, sizeof(BiScalars), cudaMemcpyDeviceToHost, s));
     NKG_CUDA(cudaStreamSynchronize(s));
