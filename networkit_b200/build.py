@@ -5,6 +5,9 @@
 * ``_lib/libnkgen.so``  - host-side synthetic graph generators and the
   NetworkitBinaryGraph file decoder (C++/OpenMP), used by the benchmarks and
   tests to make their inputs and by :mod:`networkit_b200.graphio`.
+* ``_cypagerank*.so``   - the Cython ``PageRank`` class (``_cypagerank.pyx``
+  with the declarations of ``_nkgpu.pxd``), compiled against include/nkgpu.h
+  and linked to ``_lib/libnkgpu.so``.
 
 ``python -m networkit_b200.build`` rebuilds whatever is out of date.
 """
@@ -14,6 +17,7 @@ import os
 import shutil
 import subprocess
 import sys
+import sysconfig
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -79,9 +83,37 @@ def build_gen(force: bool = False) -> str:
     return GEN_LIB
 
 
+def cython_target() -> str:
+    suffix = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
+    return os.path.join(PKG, "_cypagerank" + suffix)
+
+
+def build_cython(force: bool = False) -> str:
+    """Cythonize ``_cypagerank.pyx`` and link it to libnkgpu.so (found at run
+    time through an ``$ORIGIN/_lib`` rpath)."""
+    pyx = os.path.join(PKG, "_cypagerank.pyx")
+    pxd = os.path.join(PKG, "_nkgpu.pxd")
+    target = cython_target()
+    if not force and not _stale(target, [pyx, pxd, GPU_LIB, os.path.join(INCLUDE, "nkgpu.h"),
+                                         __file__]):
+        return target
+    os.makedirs(LIBDIR, exist_ok=True)
+    c_file = os.path.join(LIBDIR, "_cypagerank.c")
+    subprocess.run([sys.executable, "-m", "cython", "-3", "-I", ROOT, "-o", c_file, pyx],
+                   check=True)
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else (shutil.which("gcc") or "gcc")
+    cmd = [cc, "-O2", "-fPIC", "-shared", "-I", sysconfig.get_paths()["include"], "-I", INCLUDE,
+           "-o", target + ".tmp", c_file, "-L", LIBDIR, "-l:libnkgpu.so",
+           "-Wl,-rpath,$ORIGIN/_lib"]
+    subprocess.run(cmd, check=True)
+    os.replace(target + ".tmp", target)
+    return target
+
+
 def build_all(force: bool = False, verbose: bool = False) -> None:
     build_gen(force)
     build_gpu(force, verbose)
+    build_cython(force)
 
 
 if __name__ == "__main__":
