@@ -224,22 +224,80 @@ __global__ void build_perm(const uint32_t *__restrict__ sorted_ids, uint64_t n,
         degw[r] = wdeg[o];
 }
 
-// Copy every row into its new place, mapping column ids; one warp per row.
+// Copy every row into its new place, mapping column ids. Rows longer than
+// kLaneRow arcs are a prefix [0, nb) of the new order (rows are sorted by
+// length, or by half-octave length bucket whose edges fall on 2^k + 1). Their
+// arcs are split into equal contiguous ranges, one per warp, so no warp holds
+// a hub row alone; each lane walks its arcs with the row found by binary search
+// once. The short rows go 32 consecutive rows per warp, one row per lane, so
+// the dependent loads of 32 rows overlap. Neither part relies on the prefix
+// order for correctness, only for speed.
+constexpr uint32_t kLaneRow = 32;
+
+__global__ void count_rows_over(const uint32_t *__restrict__ rowlen, uint64_t n, uint32_t thr,
+                                unsigned long long *__restrict__ cnt) {
+    const uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    const int a = __syncthreads_count(r < n && rowlen[r] > thr);
+    if (threadIdx.x == 0 && a)
+        atomicAdd(cnt, static_cast<unsigned long long>(a));
+}
+
 __global__ void relabel_rows(const uint32_t *__restrict__ perm, const uint64_t *__restrict__ in_ptr,
                              const uint32_t *__restrict__ in_col, const double *__restrict__ in_w,
                              const uint32_t *__restrict__ inv, const uint32_t *__restrict__ row_ptr,
-                             uint64_t n, uint32_t *__restrict__ col, double *__restrict__ w) {
+                             uint64_t n, const unsigned long long *__restrict__ n_long_rows,
+                             uint32_t *__restrict__ col, double *__restrict__ w) {
     const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
     const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
-    for (uint64_t r = warp; r < n; r += nwarps) {
-        const uint64_t src = in_ptr[perm[r]];
-        const uint32_t dst = row_ptr[r];
-        const uint32_t len = row_ptr[r + 1] - dst;
-        for (uint32_t j = lane; j < len; j += 32) {
-            col[dst + j] = inv[in_col[src + j]];
+    const uint64_t nb = *n_long_rows;
+    // Part 1: the arcs of rows [0, nb).
+    const uint64_t big = row_ptr[nb];
+    const uint64_t per = (big + nwarps - 1) / nwarps;
+    const uint64_t a = warp * per;
+    const uint64_t e = a + per < big ? a + per : big;
+    uint64_t k = a + lane;
+    if (k < e) {
+        // the last row r with row_ptr[r] <= k: row_ptr[lo] <= k < row_ptr[hi]
+        uint64_t lo = 0, hi = nb;
+        while (hi - lo > 1) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (row_ptr[mid] <= k)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        uint64_t r = lo;
+        uint64_t base = row_ptr[r], next = row_ptr[r + 1];
+        uint64_t src = in_ptr[perm[r]];
+        for (; k < e; k += 32) {
+            if (next <= k) {
+                do {
+                    ++r;
+                    base = next;
+                    next = row_ptr[r + 1];
+                } while (next <= k);
+                src = in_ptr[perm[r]];
+            }
+            const uint64_t sk = src + (k - base);
+            col[k] = inv[in_col[sk]];
             if (w)
-                w[dst + j] = in_w[src + j];
+                w[k] = in_w[sk];
+        }
+    }
+    // Part 2: rows [nb, n), one per lane.
+    for (uint64_t g0 = nb + warp * 32; g0 < n; g0 += nwarps * 32) {
+        const uint64_t rr = g0 + lane;
+        if (rr >= n)
+            continue;
+        const uint32_t dst = row_ptr[rr];
+        const uint32_t len = row_ptr[rr + 1] - dst;
+        const uint64_t sr = in_ptr[perm[rr]];
+#pragma unroll 4
+        for (uint32_t j = 0; j < len; ++j) {
+            col[dst + j] = inv[in_col[sr + j]];
+            if (w)
+                w[dst + j] = in_w[sr + j];
         }
     }
 }
@@ -930,10 +988,13 @@ static nkg_graph *build_graph(std::unique_ptr<nkg_graph> g, DeviceArray<uint64_t
     g->col.alloc(arcs, 4);
     if (g->weighted)
         g->w64src.alloc(arcs, 4);
-    if (arcs)
+    if (arcs) {
+        NKG_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(unsigned long long), s));
+        count_rows_over<<<ceil_div(n, 256), 256, 0, s>>>(rowlen.get(), n, kLaneRow, cnt.get());
         relabel_rows<<<sms * 16, 256, 0, s>>>(g->perm.get(), d_ptr.get(), d_col.get(), d_w.get(),
-                                              g->inv.get(), g->row_ptr.get(), n, g->col.get(),
-                                              g->w64src.get());
+                                              g->inv.get(), g->row_ptr.get(), n, cnt.get(),
+                                              g->col.get(), g->w64src.get());
+    }
     NKG_CUDA(cudaGetLastError());
     if (opt) {
         require(opt->sweep_shape >= -1 && opt->sweep_shape < kNumSweepShapes,
