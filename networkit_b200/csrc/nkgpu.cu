@@ -1226,7 +1226,8 @@ static void sweep_setup(nkg_graph *g) {
     unit_bounds<<<ceil_div(static_cast<uint64_t>(P.units) + 1, 256), 256, 0, s>>>(
         g->fw.slice_cost.get(), g->fw.slices, P.units, P.unit_start.get());
     NKG_CUDA(cudaGetLastError());
-    P.fix_ctas = g->fw.n_vlong + ceil_div(std::max<uint32_t>(g->fw.n_long - g->fw.n_vlong, 1), kFixThreads);
+    P.fix_ctas = fix_vlong_ctas(g->fw.n_vlong) +
+                 ceil_div(std::max<uint32_t>(g->fw.n_long - g->fw.n_vlong, 1), kFixThreads);
     require(P.sweep_ctas <= g->cta_res.size() && P.fix_ctas <= g->fix_res.size(),
             "partial-sum buffers too small");
     NKG_CUDA(cudaStreamSynchronize(s));

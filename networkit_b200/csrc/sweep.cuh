@@ -220,9 +220,14 @@ __global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs<T> a) {
 
 // Fix-up: finish the split rows from their chunk sums (in chunk order), then
 // (last CTA) reduce all partial sums in index order and close the iteration
-// (PageRank.cpp:68-70). CTAs [0, n_vlong) each finish one row with many
-// chunks; the others take one split row per thread.
+// (PageRank.cpp:68-70). The first fix_vlong_ctas() CTAs finish the rows with
+// many chunks, one row per warp; the others take one split row per thread.
 constexpr int kFixThreads = 256;
+constexpr uint32_t kFixWarps = kFixThreads / 32;
+
+__host__ __device__ inline uint32_t fix_vlong_ctas(uint32_t n_vlong) {
+    return (n_vlong + kFixWarps - 1) / kFixWarps;
+}
 
 template <typename T, bool WEIGHTED>
 __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
@@ -233,17 +238,22 @@ __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
     const RunParams rp = *a.rp;
     const T sink_coef = static_cast<T>(a.st->sink_coef);
     double res = 0.0, sink = 0.0;
-    if (blockIdx.x < a.n_vlong) {
-        const uint32_t r = blockIdx.x;
-        const uint32_t cb = a.chunk_begin[r], ce = a.chunk_begin[r + 1];
-        T part = T(0);
-        for (uint32_t k = cb + threadIdx.x; k < ce; k += kFixThreads)
-            part += a.chunk_val[k];
-        const double tot = block_sum<kFixThreads>(static_cast<double>(part), s_red);
-        if (threadIdx.x == 0)
-            finish_row<T, WEIGHTED>(a, rp, sink_coef, r, static_cast<T>(tot), res, sink);
+    const uint32_t vctas = fix_vlong_ctas(a.n_vlong);
+    if (blockIdx.x < vctas) {
+        const uint32_t r = blockIdx.x * kFixWarps + (threadIdx.x >> 5);
+        const int lane = threadIdx.x & 31;
+        if (r < a.n_vlong) {
+            const uint32_t cb = a.chunk_begin[r], ce = a.chunk_begin[r + 1];
+            T part = T(0);
+#pragma unroll 4
+            for (uint32_t k = cb + lane; k < ce; k += 32)
+                part += a.chunk_val[k];
+            const double tot = warp_sum(static_cast<double>(part));
+            if (lane == 0)
+                finish_row<T, WEIGHTED>(a, rp, sink_coef, r, static_cast<T>(tot), res, sink);
+        }
     } else {
-        const uint32_t r = a.n_vlong + (blockIdx.x - a.n_vlong) * kFixThreads + threadIdx.x;
+        const uint32_t r = a.n_vlong + (blockIdx.x - vctas) * kFixThreads + threadIdx.x;
         if (r < a.n_long) {
             const uint32_t cb = a.chunk_begin[r], ce = a.chunk_begin[r + 1];
             T parts[kShortChunks];
