@@ -125,6 +125,33 @@ __device__ __forceinline__ void finish_row(const SweepArgs<T> &a, const RunParam
     }
 }
 
+// Per-run constants read where a row is finished. The volatile asm keeps each
+// load at its use, so the values are not hoisted into registers held across
+// the gather loop.
+__device__ __forceinline__ double ld_keep(const double *p) {
+    double v;
+    asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ int ld_keep(const int *p) {
+    int v;
+    asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
+template <typename T, bool WEIGHTED>
+__device__ __forceinline__ void finish_row_sweep(const SweepArgs<T> &a, uint32_t r, T acc,
+                                                 double &res, double &sink) {
+    RunParams rp;
+    rp.damp = ld_keep(&a.rp->damp);
+    rp.tele_uniform = ld_keep(&a.rp->tele_uniform);
+    rp.one_minus_damp = ld_keep(&a.rp->one_minus_damp);
+    rp.distribute = ld_keep(&a.rp->distribute);
+    rp.personal = ld_keep(&a.rp->personal);
+    rp.l2 = ld_keep(&a.rp->l2);
+    const T sink_coef = static_cast<T>(ld_keep(&a.st->sink_coef));
+    finish_row<T, WEIGHTED>(a, rp, sink_coef, r, acc, res, sink);
+}
 
 // Gathers go through L1 with the default policy (__ldg); the kernel uses no
 // shared memory, so the whole L1 caches the hot scores. The sweep is bound by
@@ -155,13 +182,15 @@ inline void with_sweep_shape(int v, F &&f) {
 // The sweep: each warp walks its units; each lane accumulates one virtual
 // row of a slice in arc order. Chunk slices store partial sums; row slices
 // finish rows.
+// Registers are fitted to 48 warps per SM (more warps do not make the sweep
+// faster: it is bound by the rate of L1 miss requests), except for the
+// 16-step batches, which would spill at that budget.
 template <typename T, bool WEIGHTED, int THREADS, int UNROLL>
-__global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs<T> a) {
+__global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 1 : 1536 / THREADS)
+    sweep_kernel(SweepArgs<T> a) {
     __shared__ double s_red[32];
     if (*(volatile int *)&a.st->done)
         return;
-    const RunParams rp = *a.rp;
-    const T sink_coef = static_cast<T>(a.st->sink_coef);
     const int lane = threadIdx.x & 31;
     const uint32_t wpc = THREADS / 32;
     const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);
@@ -194,19 +223,35 @@ __global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs<T> a) {
                 for (int k = 0; k < UNROLL; ++k)
                     acc += v[k];
             }
-            for (; j < len; ++j) {
-                const uint32_t c = ld_stream(cp + static_cast<size_t>(j) * 32);
-                T v = __ldg(a.y_in + c);
-                if (WEIGHTED)
-                    v = t_mul(v, ld_stream(a.w_sell + base + static_cast<size_t>(j) * 32));
-                acc += v;
+            if (j < len) {
+                // The last len - j < UNROLL steps as one predicated batch, so
+                // their gathers are in flight together; the sum keeps the same
+                // order (absent steps add nothing).
+                uint32_t c[UNROLL];
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    c[k] = j + k < len ? ld_stream(cp + static_cast<size_t>(j + k) * 32) : 0u;
+                T v[UNROLL];
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    v[k] = j + k < len ? __ldg(a.y_in + c[k]) : T(0);
+                if (WEIGHTED) {
+#pragma unroll
+                    for (int k = 0; k < UNROLL; ++k)
+                        if (j + k < len)
+                            v[k] = t_mul(v[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
+                }
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    if (j + k < len)
+                        acc += v[k];
             }
             if (s < a.s_chunk) {
                 a.chunk_val[static_cast<size_t>(s) * 32 + lane] = acc;
             } else {
                 const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
                 if (r < a.n)
-                    finish_row<T, WEIGHTED>(a, rp, sink_coef, r, acc, res, sink);
+                    finish_row_sweep<T, WEIGHTED>(a, r, acc, res, sink);
             }
         }
     }
