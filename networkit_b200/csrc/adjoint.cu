@@ -292,7 +292,8 @@ __device__ __forceinline__ void adj_row(const AdjArgs &a, uint32_t v, double acc
 }
 
 template <bool WEIGHTED, int THREADS, int UNROLL>
-__global__ void __launch_bounds__(THREADS) adj_sweep(AdjArgs a) {
+__global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 512 / THREADS : WEIGHTED ? 1024 / THREADS : 1536 / THREADS)
+    adj_sweep(AdjArgs a) {
     __shared__ double s_red[32];
     if (*(volatile int *)&a.st->done)
         return;
@@ -329,11 +330,26 @@ __global__ void __launch_bounds__(THREADS) adj_sweep(AdjArgs a) {
                 for (int k = 0; k < UNROLL; ++k)
                     acc += v[k];
             }
-            for (; j < len; ++j) {
-                double v = __ldg(a.lam_in + ld_stream(cp + static_cast<size_t>(j) * 32));
-                if (WEIGHTED)
-                    v *= ld_stream(a.w_sell + base + static_cast<size_t>(j) * 32);
-                acc += v;
+            if (j < len) {
+                // the last len - j < UNROLL steps as one predicated batch (same order)
+                uint32_t c[UNROLL];
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    c[k] = j + k < len ? ld_stream(cp + static_cast<size_t>(j + k) * 32) : 0u;
+                double v[UNROLL];
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    v[k] = j + k < len ? __ldg(a.lam_in + c[k]) : 0.0;
+                if (WEIGHTED) {
+#pragma unroll
+                    for (int k = 0; k < UNROLL; ++k)
+                        if (j + k < len)
+                            v[k] *= ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32);
+                }
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    if (j + k < len)
+                        acc += v[k];
             }
             if (s < a.s_chunk) {
                 a.chunk_val[static_cast<size_t>(s) * 32 + lane] = acc;

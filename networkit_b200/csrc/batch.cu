@@ -154,7 +154,8 @@ __device__ __forceinline__ void batch_finish(const BatchArgs<T> &a, const T *yin
 }
 
 template <typename T, int THREADS, int UNROLL, bool CG>
-__global__ void __launch_bounds__(THREADS) batch_kernel(BatchArgs<T> a) {
+__global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 512 / THREADS : sizeof(T) > 4 ? 1024 / THREADS : 1280 / THREADS)
+    batch_kernel(BatchArgs<T> a) {
     __shared__ ClusterShared sh;
     cg::cluster_group cluster = cg::this_cluster();
     const unsigned crank = cluster.block_rank();
@@ -246,8 +247,21 @@ __global__ void __launch_bounds__(THREADS) batch_kernel(BatchArgs<T> a) {
                         for (int u = 0; u < UNROLL; ++u)
                             acc += v[u];
                     }
-                    for (; j < len; ++j)
-                        acc += ld_iter<CG>(yin + __ldg(cp + static_cast<size_t>(j) * 32));
+                    if (j < len) {
+                        // the last len - j < UNROLL steps as one predicated batch (same order)
+                        uint32_t c[UNROLL];
+#pragma unroll
+                        for (int u = 0; u < UNROLL; ++u)
+                            c[u] = j + u < len ? __ldg(cp + static_cast<size_t>(j + u) * 32) : 0u;
+                        T v[UNROLL];
+#pragma unroll
+                        for (int u = 0; u < UNROLL; ++u)
+                            v[u] = j + u < len ? ld_iter<CG>(yin + c[u]) : T(0);
+#pragma unroll
+                        for (int u = 0; u < UNROLL; ++u)
+                            if (j + u < len)
+                                acc += v[u];
+                    }
                     const uint32_t i = m.n_long + (item - m.n_long) * 32 + lane;
                     if (i < m.n)
                         batch_finish<T, CG>(a, yin, yout, m.base + i, acc, damp, tele, sink_coef,

@@ -78,7 +78,8 @@ __device__ __forceinline__ void cent_row(const CentArgs &a, uint32_t r, double a
 }
 
 template <int MODE, bool WEIGHTED, int THREADS, int UNROLL>
-__global__ void __launch_bounds__(THREADS) cent_sweep(CentArgs a) {
+__global__ void __launch_bounds__(THREADS, WEIGHTED || UNROLL > 8 ? 1024 / THREADS : 1536 / THREADS)
+    cent_sweep(CentArgs a) {
     __shared__ double s_red[32];
     if (*(volatile int *)&a.st->done)
         return;
@@ -112,11 +113,24 @@ __global__ void __launch_bounds__(THREADS) cent_sweep(CentArgs a) {
                 for (int k = 0; k < UNROLL; ++k)
                     acc = __dadd_rn(acc, cent_term<MODE, WEIGHTED>(a, x[k], w[k]));
             }
-            for (; j < len; ++j) {
-                const double x = __ldg(a.x_in + ld_stream(cp + static_cast<size_t>(j) * 32));
-                const double w =
-                    WEIGHTED ? ld_stream(a.w_sell + base + static_cast<size_t>(j) * 32) : 1.0;
-                acc = __dadd_rn(acc, cent_term<MODE, WEIGHTED>(a, x, w));
+            if (j < len) {
+                // the last len - j < UNROLL steps as one predicated batch (same order)
+                uint32_t c[UNROLL];
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    c[k] = j + k < len ? ld_stream(cp + static_cast<size_t>(j + k) * 32) : 0u;
+                double x[UNROLL], w[UNROLL];
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k) {
+                    x[k] = j + k < len ? __ldg(a.x_in + c[k]) : 0.0;
+                    w[k] = WEIGHTED && j + k < len
+                               ? ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32)
+                               : 1.0;
+                }
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    if (j + k < len)
+                        acc = __dadd_rn(acc, cent_term<MODE, WEIGHTED>(a, x[k], w[k]));
             }
             if (s < a.s_chunk) {
                 a.chunk_val[static_cast<size_t>(s) * 32 + lane] = acc;

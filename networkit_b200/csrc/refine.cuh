@@ -112,7 +112,7 @@ __device__ __forceinline__ void bi_mv_row(const BiArgs &a, uint32_t r, float acc
 
 // The SpMV of one slice per warp (the loop of sweep_kernel in FP32).
 template <bool WEIGHTED, int MODE, int OP, int THREADS, int UNROLL>
-__global__ void __launch_bounds__(THREADS) bi_mv(BiArgs a) {
+__global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 1024 / THREADS : 1536 / THREADS) bi_mv(BiArgs a) {
     __shared__ double s_red[32];
     if (a.sc->breakdown)
         return;
@@ -151,11 +151,26 @@ __global__ void __launch_bounds__(THREADS) bi_mv(BiArgs a) {
                 for (int k = 0; k < UNROLL; ++k)
                     acc += vv[k];
             }
-            for (; j < len; ++j) {
-                float vv = __ldg(gsrc + ld_stream(cp + static_cast<size_t>(j) * 32));
-                if (WEIGHTED)
-                    vv = __fmul_rn(vv, ld_stream(a.w_sell + base + static_cast<size_t>(j) * 32));
-                acc += vv;
+            if (j < len) {
+                // the last len - j < UNROLL steps as one predicated batch (same order)
+                uint32_t c[UNROLL];
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    c[k] = j + k < len ? ld_stream(cp + static_cast<size_t>(j + k) * 32) : 0u;
+                float vv[UNROLL];
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    vv[k] = j + k < len ? __ldg(gsrc + c[k]) : 0.f;
+                if (WEIGHTED) {
+#pragma unroll
+                    for (int k = 0; k < UNROLL; ++k)
+                        if (j + k < len)
+                            vv[k] = __fmul_rn(vv[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
+                }
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    if (j + k < len)
+                        acc += vv[k];
             }
             if (s < a.s_chunk) {
                 a.chunk_val[static_cast<size_t>(s) * 32 + lane] = acc;

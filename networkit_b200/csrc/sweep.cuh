@@ -183,10 +183,10 @@ inline void with_sweep_shape(int v, F &&f) {
 // row of a slice in arc order. Chunk slices store partial sums; row slices
 // finish rows.
 // Registers are fitted to 48 warps per SM (more warps do not make the sweep
-// faster: it is bound by the rate of L1 miss requests), except for the
-// 16-step batches, which would spill at that budget.
+// faster: it is bound by the rate of L1 miss requests), and to 32 for the
+// other batch depths, which would spill at 48.
 template <typename T, bool WEIGHTED, int THREADS, int UNROLL>
-__global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 1 : 1536 / THREADS)
+__global__ void __launch_bounds__(THREADS, UNROLL != 8 ? 1024 / THREADS : 1536 / THREADS)
     sweep_kernel(SweepArgs<T> a) {
     __shared__ double s_red[32];
     if (*(volatile int *)&a.st->done)
