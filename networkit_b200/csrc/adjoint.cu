@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 512 / THREADS : WEIGHTED
                 double v[UNROLL];
 #pragma unroll
                 for (int k = 0; k < UNROLL; ++k)
-                    v[k] = __ldg(a.lam_in + c[k]);
+                    v[k] = c[k] != a.n ? __ldg(a.lam_in + c[k]) : 0.0;
                 if (WEIGHTED) {
 #pragma unroll
                     for (int k = 0; k < UNROLL; ++k)
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 512 / THREADS : WEIGHTED
                 double v[UNROLL];
 #pragma unroll
                 for (int k = 0; k < UNROLL; ++k)
-                    v[k] = j + k < len ? __ldg(a.lam_in + c[k]) : 0.0;
+                    v[k] = j + k < len && c[k] != a.n ? __ldg(a.lam_in + c[k]) : 0.0;
                 if (WEIGHTED) {
 #pragma unroll
                     for (int k = 0; k < UNROLL; ++k)

@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 1024 / THREADS : 1536 / 
                 float vv[UNROLL];
 #pragma unroll
                 for (int k = 0; k < UNROLL; ++k)
-                    vv[k] = __ldg(gsrc + c[k]);
+                    vv[k] = c[k] != a.n ? __ldg(gsrc + c[k]) : 0.f;
                 if (WEIGHTED) {
 #pragma unroll
                     for (int k = 0; k < UNROLL; ++k)
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 1024 / THREADS : 1536 / 
                 float vv[UNROLL];
 #pragma unroll
                 for (int k = 0; k < UNROLL; ++k)
-                    vv[k] = j + k < len ? __ldg(gsrc + c[k]) : 0.f;
+                    vv[k] = j + k < len && c[k] != a.n ? __ldg(gsrc + c[k]) : 0.f;
                 if (WEIGHTED) {
 #pragma unroll
                     for (int k = 0; k < UNROLL; ++k)

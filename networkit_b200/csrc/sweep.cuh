@@ -153,6 +153,8 @@ __device__ __forceinline__ void finish_row_sweep(const SweepArgs<T> &a, uint32_t
     finish_row<T, WEIGHTED>(a, rp, sink_coef, r, acc, res, sink);
 }
 
+// Padding slots (column n, whose gathered value is the zero entry y[n]) skip
+// the load and add zero, the same sum bit for bit without the L1 lookup.
 // Gathers go through L1 with the default policy (__ldg); the kernel uses no
 // shared memory, so the whole L1 caches the hot scores. The sweep is bound by
 // L1 miss requests to L2 (one sector per scattered lane). Measured
@@ -184,9 +186,9 @@ inline void with_sweep_shape(int v, F &&f) {
 // finish rows.
 // Registers are fitted to 48 warps per SM (more warps do not make the sweep
 // faster: it is bound by the rate of L1 miss requests), and to 32 for the
-// other batch depths, which would spill at 48.
+// other batch depths and the weighted FP64 sweep, which would spill at 48.
 template <typename T, bool WEIGHTED, int THREADS, int UNROLL>
-__global__ void __launch_bounds__(THREADS, UNROLL != 8 ? 1024 / THREADS : 1536 / THREADS)
+__global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T) > 4) ? 1024 / THREADS : 1536 / THREADS)
     sweep_kernel(SweepArgs<T> a) {
     __shared__ double s_red[32];
     if (*(volatile int *)&a.st->done)
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(THREADS, UNROLL != 8 ? 1024 / THREADS : 1536 /
                 T v[UNROLL];
 #pragma unroll
                 for (int k = 0; k < UNROLL; ++k)
-                    v[k] = __ldg(a.y_in + c[k]);
+                    v[k] = c[k] != a.n ? __ldg(a.y_in + c[k]) : T(0);
                 if (WEIGHTED) {
 #pragma unroll
                     for (int k = 0; k < UNROLL; ++k)
@@ -234,7 +236,7 @@ __global__ void __launch_bounds__(THREADS, UNROLL != 8 ? 1024 / THREADS : 1536 /
                 T v[UNROLL];
 #pragma unroll
                 for (int k = 0; k < UNROLL; ++k)
-                    v[k] = j + k < len ? __ldg(a.y_in + c[k]) : T(0);
+                    v[k] = j + k < len && c[k] != a.n ? __ldg(a.y_in + c[k]) : T(0);
                 if (WEIGHTED) {
 #pragma unroll
                     for (int k = 0; k < UNROLL; ++k)
