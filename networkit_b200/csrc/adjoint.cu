@@ -271,7 +271,7 @@ struct AdjArgs {
     AdjState *st;
     double damp, inv_n, tol;
     unsigned long long max_iter;
-    uint32_t n, n_long, s_chunk, units, sweep_ctas;
+    uint32_t n, n_long, n_vlong, s_chunk, units, sweep_ctas;
     int distribute, personal;
 };
 
@@ -378,13 +378,10 @@ __global__ void __launch_bounds__(kAdjThreads) adj_fix(AdjArgs a) {
         return;
     const double tdot = a.st->tdot;
     double res = 0.0, td = 0.0;
-    const uint32_t r = blockIdx.x * kAdjThreads + threadIdx.x;
-    if (r < a.n_long) {
-        double acc = 0.0;
-        for (uint32_t k = a.chunk_begin[r]; k < a.chunk_begin[r + 1]; ++k)
-            acc += a.chunk_val[k];
+    uint32_t r;
+    double acc;
+    if (split_row_sum<kAdjThreads>(a.chunk_begin, a.chunk_val, a.n_long, a.n_vlong, r, acc))
         adj_row<WEIGHTED>(a, r, acc, tdot, res, td);
-    }
     res = block_sum<kAdjThreads>(res, s_red);
     td = block_sum<kAdjThreads>(td, s_red);
     if (threadIdx.x == 0) {
@@ -936,7 +933,7 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
     const int distribute = p.distribute_sinks ? 1 : 0;
     const double inv_n = 1.0 / static_cast<double>(n);
     const unsigned vec_ctas = std::max<unsigned>(1, std::min<unsigned>(sms * 4, ceil_div(n, kBiThreads)));
-    const unsigned fix_ctas = std::max<unsigned>(1, ceil_div(A.tl.n_long, kBiThreads));
+    const unsigned fix_ctas = split_fix_ctas<kBiThreads>(A.tl.n_long, A.tl.n_vlong);
     ensure_work(g, A, vec_ctas, fix_ctas);
     AdjWork &W = A.work;
     AdjResult R;
@@ -990,12 +987,13 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
     aa.tol = tol_abs;
     aa.n = n;
     aa.n_long = A.tl.n_long;
+    aa.n_vlong = A.tl.n_vlong;
     aa.s_chunk = A.tl.s_chunk;
     aa.units = A.n_units64;
     aa.sweep_ctas = A.ctas64;
     aa.distribute = distribute;
     aa.personal = personal;
-    const unsigned adj_fix_ctas = std::max<unsigned>(1, ceil_div(A.tl.n_long, kAdjThreads));
+    const unsigned adj_fix_ctas = split_fix_ctas<kAdjThreads>(A.tl.n_long, A.tl.n_vlong);
     auto sweep64 = [&](const double *in, double *out, double *cout, unsigned long long max_it) {
         aa.lam_in = in;
         aa.lam_out = out;

@@ -58,7 +58,7 @@ struct CentArgs {
     CentState *st;
     double alpha, beta, tol;
     unsigned long long max_iter;
-    uint32_t n, n_long, s_chunk, units, sweep_ctas;
+    uint32_t n, n_long, n_vlong, s_chunk, units, sweep_ctas;
 };
 
 // One arc's term: w * x (eigenvector) or (w * alpha) * (1 + x) (Katz).
@@ -146,7 +146,8 @@ __global__ void __launch_bounds__(THREADS, WEIGHTED || UNROLL > 8 ? 1024 / THREA
         a.part[blockIdx.x] = sq;
 }
 
-// Split rows (one thread each, chunk sums in order), then the last CTA sums
+// Split rows (a warp for each row of many chunks, one thread for each other
+// row; split_row_sum), then the last CTA sums
 // the squares in a fixed order and takes NumericTools::equal(length, old, tol).
 template <int MODE>
 __global__ void __launch_bounds__(kCentFix) cent_fix(CentArgs a) {
@@ -155,13 +156,10 @@ __global__ void __launch_bounds__(kCentFix) cent_fix(CentArgs a) {
     if (*(volatile int *)&a.st->done)
         return;
     double sq = 0.0;
-    const uint32_t r = blockIdx.x * kCentFix + threadIdx.x;
-    if (r < a.n_long) {
-        double acc = 0.0;
-        for (uint32_t k = a.chunk_begin[r]; k < a.chunk_begin[r + 1]; ++k)
-            acc = __dadd_rn(acc, a.chunk_val[k]);
+    uint32_t r;
+    double acc;
+    if (split_row_sum<kCentFix>(a.chunk_begin, a.chunk_val, a.n_long, a.n_vlong, r, acc))
         cent_row<MODE>(a, r, acc, sq);
-    }
     sq = block_sum<kCentFix>(sq, s_red);
     if (threadIdx.x == 0) {
         a.fix_part[blockIdx.x] = sq;
@@ -273,7 +271,7 @@ CentResult cent_run(nkg_graph *g, const SellLayout &L, const double *w_sell, dou
     const uint32_t units = static_cast<uint32_t>(std::max<uint64_t>(
         1, std::min<uint64_t>(static_cast<uint64_t>(ctas) * (kCentThreads / 32) * kUnitsPerWarp,
                               std::max<uint64_t>(slices, 1))));
-    const unsigned fix_ctas = std::max<unsigned>(1, ceil_div(L.n_long, kCentFix));
+    const unsigned fix_ctas = split_fix_ctas<kCentFix>(L.n_long, L.n_vlong);
     DeviceArray<uint32_t> unit_start(static_cast<size_t>(units) + 1);
     sell_units(L, units, unit_start.get(), s);
     DeviceArray<double> x[2] = {DeviceArray<double>(n + 1), DeviceArray<double>(n + 1)};
@@ -302,6 +300,7 @@ CentResult cent_run(nkg_graph *g, const SellLayout &L, const double *w_sell, dou
     a.max_iter = max_iter;
     a.n = n;
     a.n_long = L.n_long;
+    a.n_vlong = L.n_vlong;
     a.s_chunk = L.s_chunk;
     a.units = units;
     a.sweep_ctas = ctas;

@@ -1470,7 +1470,7 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
     DeviceArray<float> &bx = W.x, &br = W.r, &brhat = W.rhat, &bp = W.p, &bv = W.v, &bs = W.s,
                        &bt = W.t, &bg = W.g;
     DeviceArray<double> &x64 = W.x64, &part = W.part;
-    const unsigned fix_ctas = std::max<unsigned>(1, ceil_div(g->fw.n_long, kBiThreads));
+    const unsigned fix_ctas = split_fix_ctas<kBiThreads>(g->fw.n_long, g->fw.n_vlong);
     if (W.fix_part.size() < 2 * static_cast<size_t>(fix_ctas))
         W.fix_part.alloc(2 * static_cast<size_t>(fix_ctas));
     DeviceArray<double> &fix_part = W.fix_part;

@@ -200,13 +200,10 @@ __global__ void __launch_bounds__(kBiThreads) bi_mv_fix(BiArgs a) {
     const float *px = MODE == 0 ? a.p : a.s;
     float *out = MODE == 0 ? a.v : a.t;
     double d1 = 0.0, d2 = 0.0;
-    const uint32_t r = blockIdx.x * kBiThreads + threadIdx.x;
-    if (r < a.n_long) {
-        float acc = 0.f;
-        for (uint32_t k = a.chunk_begin[r]; k < a.chunk_begin[r + 1]; ++k)
-            acc += a.chunk_val[k];
+    uint32_t r;
+    float acc;
+    if (split_row_sum<kBiThreads>(a.chunk_begin, a.chunk_val, a.n_long, a.n_vlong, r, acc))
         bi_mv_row<WEIGHTED, MODE, OP>(a, r, acc, px, out, d1, d2);
-    }
     d1 = block_sum<kBiThreads>(d1, s_red);
     d2 = block_sum<kBiThreads>(d2, s_red);
     if (threadIdx.x == 0) {

@@ -22,6 +22,8 @@
 // set-up), so every sum has a fixed order and a run is bit-reproducible.
 #pragma once
 
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace nkg {
@@ -274,6 +276,51 @@ constexpr uint32_t kFixWarps = kFixThreads / 32;
 
 __host__ __device__ inline uint32_t fix_vlong_ctas(uint32_t n_vlong) {
     return (n_vlong + kFixWarps - 1) / kFixWarps;
+}
+
+// The same layout for the other fix-ups of split rows (FP32 product, adjoint,
+// centrality), with THREADS threads per CTA: the first CTAs give each row of
+// more than kShortChunks chunks a warp, the rest one thread per split row.
+template <int THREADS>
+inline unsigned split_fix_ctas(uint32_t n_long, uint32_t n_vlong) {
+    constexpr uint32_t w = THREADS / 32;
+    const uint64_t short_rows = n_long > n_vlong ? n_long - n_vlong : 0;
+    return static_cast<unsigned>(std::max<uint64_t>(
+        1, (n_vlong + w - 1) / w + (short_rows + THREADS - 1) / THREADS));
+}
+
+// Split row r of this thread in that layout and its chunk sum. Returns true
+// for the thread that finishes r (lane 0 of a row's warp, or the row's own
+// thread). A warp sums lane-strided partials in V, then across lanes in double
+// in a fixed tree; a thread sums the chunks in order. Every thread of a warp
+// given a row must call it (the lane sum is warp-wide).
+template <int THREADS, typename V>
+__device__ __forceinline__ bool split_row_sum(const uint32_t *__restrict__ chunk_begin,
+                                              const V *__restrict__ chunk_val, uint32_t n_long,
+                                              uint32_t n_vlong, uint32_t &r, V &acc) {
+    constexpr uint32_t w = THREADS / 32;
+    const uint32_t vctas = (n_vlong + w - 1) / w;
+    if (blockIdx.x < vctas) {
+        r = blockIdx.x * w + (threadIdx.x >> 5);
+        if (r >= n_vlong)
+            return false;
+        const int lane = threadIdx.x & 31;
+        const uint32_t cb = chunk_begin[r], ce = chunk_begin[r + 1];
+        V part = V(0);
+#pragma unroll 4
+        for (uint32_t k = cb + lane; k < ce; k += 32)
+            part += chunk_val[k];
+        acc = static_cast<V>(warp_sum(static_cast<double>(part)));
+        return lane == 0;
+    }
+    r = n_vlong + (blockIdx.x - vctas) * THREADS + threadIdx.x;
+    if (r >= n_long)
+        return false;
+    V sum = V(0);
+    for (uint32_t k = chunk_begin[r]; k < chunk_begin[r + 1]; ++k)
+        sum += chunk_val[k];
+    acc = sum;
+    return true;
 }
 
 template <typename T, bool WEIGHTED>
