@@ -15,8 +15,11 @@
 // Per iteration: one sweep over the slices (each lane sums its row in arc
 // order, products rounded separately like the reference, no FMA
 // contraction), one fix-up for rows split into chunks whose last CTA reduces
-// sum(values^2) in a fixed order and takes the stopping test, and for the
-// eigenvector one scaling pass. Padding slots gather the extra entry x[n],
+// sum(values^2) in a fixed order and takes the stopping test. The eigenvector's
+// division by the length is folded into the next sweep: x holds the values
+// before scaling, every row divides its sum by the previous length once (the
+// first sweep reads the initial 1s and divides by nothing), and the output
+// pass divides by the last length. Padding slots gather the extra entry x[n],
 // set to 0 (eigenvector) or -1 (Katz: alpha * (1 + -1) = 0), so they add 0.
 // KatzCentrality with EdgeDirection::OutEdges runs over the out-layout of the
 // adjoint (rows = nodes by out-degree).
@@ -70,9 +73,16 @@ __device__ __forceinline__ double cent_term(const CentArgs &a, double x, double 
     return __dmul_rn(wa, __dadd_rn(1.0, x));
 }
 
+// The previous iteration's length that eigenvector rows divide their sums by
+// (0: the first iteration, whose input is the unscaled initial vector).
+__device__ __forceinline__ double cent_prev_length(const CentArgs &a) {
+    return a.st->iteration ? a.st->length : 0.0;
+}
+
 template <int MODE>
-__device__ __forceinline__ void cent_row(const CentArgs &a, uint32_t r, double acc, double &sq) {
-    const double v = MODE == 0 ? acc : __dadd_rn(acc, a.beta);
+__device__ __forceinline__ void cent_row(const CentArgs &a, uint32_t r, double acc, double len_prev,
+                                         double &sq) {
+    const double v = MODE == 0 ? (len_prev > 0.0 ? acc / len_prev : acc) : __dadd_rn(acc, a.beta);
     a.x_out[r] = v;
     sq += v * v;
 }
@@ -83,6 +93,7 @@ __global__ void __launch_bounds__(THREADS, WEIGHTED || UNROLL > 8 ? 1024 / THREA
     __shared__ double s_red[32];
     if (*(volatile int *)&a.st->done)
         return;
+    const double len_prev = MODE == 0 ? cent_prev_length(a) : 0.0;
     const int lane = threadIdx.x & 31;
     const uint32_t wpc = THREADS / 32;
     const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);
@@ -137,7 +148,7 @@ __global__ void __launch_bounds__(THREADS, WEIGHTED || UNROLL > 8 ? 1024 / THREA
             } else {
                 const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
                 if (r < a.n)
-                    cent_row<MODE>(a, r, acc, sq);
+                    cent_row<MODE>(a, r, acc, len_prev, sq);
             }
         }
     }
@@ -155,11 +166,12 @@ __global__ void __launch_bounds__(kCentFix) cent_fix(CentArgs a) {
     __shared__ bool s_last;
     if (*(volatile int *)&a.st->done)
         return;
+    const double len_prev = MODE == 0 ? cent_prev_length(a) : 0.0;
     double sq = 0.0;
     uint32_t r;
     double acc;
     if (split_row_sum<kCentFix>(a.chunk_begin, a.chunk_val, a.n_long, a.n_vlong, r, acc))
-        cent_row<MODE>(a, r, acc, sq);
+        cent_row<MODE>(a, r, acc, len_prev, sq);
     sq = block_sum<kCentFix>(sq, s_red);
     if (threadIdx.x == 0) {
         a.fix_part[blockIdx.x] = sq;
@@ -189,20 +201,9 @@ __global__ void __launch_bounds__(kCentFix) cent_fix(CentArgs a) {
     }
 }
 
-// Eigenvector: x /= length after iteration `expected` (the launch does
-// nothing when the run stopped before that iteration and no sweep wrote x).
-__global__ void cent_scale(double *__restrict__ x, uint32_t n, const CentState *st,
-                           unsigned long long expected) {
-    if (st->iteration != expected)
-        return;
-    const double len = st->length;
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < n)
-        x[r] = x[r] / len;
-}
-
 // Scores in the caller's ids: row of caller id o (via map, kNone = deleted)
-// divided by `len` (1 for the eigenvector), deleted ids 1; sign_fix makes
+// divided by the last length (both measures: the eigenvector's values are
+// kept unscaled between sweeps), deleted ids 1; sign_fix makes
 // every score |x| when x of caller id 0 is negative (EigenvectorCentrality.cpp:53-57).
 __global__ void cent_output(const double *__restrict__ x, const uint32_t *__restrict__ row_of,
                             uint64_t z, const CentState *st, int divide, int sign_fix,
@@ -306,24 +307,19 @@ CentResult cent_run(nkg_graph *g, const SellLayout &L, const double *w_sell, dou
     a.sweep_ctas = ctas;
     CentState *hst = reinterpret_cast<CentState *>(g->scalars_host.get());
     static_assert(sizeof(CentState) <= 16 * sizeof(double), "CentState fits the pinned buffer");
-    unsigned long long it0 = 0;  // iterations done before this batch
     for (;;) {
         for (int k = 0; k < kSweepsPerGraph; ++k) {
             a.x_in = x[k & 1].get();
             a.x_out = x[(k + 1) & 1].get();
             kfn<<<ctas, kCentThreads, 0, s>>>(a);
             cent_fix<MODE><<<fix_ctas, kCentFix, 0, s>>>(a);
-            if (MODE == 0)
-                cent_scale<<<ceil_div(n, 256), 256, 0, s>>>(a.x_out, n, st.get(),
-                                                            it0 + k + 1);
         }
         NKG_CUDA(cudaGetLastError());
-        R.launches += kSweepsPerGraph * (MODE == 0 ? 3 : 2);
+        R.launches += kSweepsPerGraph * 2;
         NKG_CUDA(cudaMemcpyAsync(hst, st.get(), sizeof(CentState), cudaMemcpyDeviceToHost, s));
         NKG_CUDA(cudaStreamSynchronize(s));
         if (hst->done)
             break;
-        it0 = hst->iteration;
         if (g->cancel.load()) {
             g->cancel.store(0);
             throw Error(NKG_ERR_CANCELLED, "centrality run cancelled");
@@ -332,8 +328,8 @@ CentResult cent_run(nkg_graph *g, const SellLayout &L, const double *w_sell, dou
     R.iterations = hst->iteration;
     R.length = hst->length;
     const double *xfin = x[R.iterations & 1].get();
-    cent_output<<<ceil_div(g->z, 256), 256, 0, s>>>(xfin, row_of, g->z, st.get(),
-                                                    MODE == 1 ? 1 : 0, MODE == 0 ? 1 : 0, d_out);
+    cent_output<<<ceil_div(g->z, 256), 256, 0, s>>>(xfin, row_of, g->z, st.get(), 1,
+                                                    MODE == 0 ? 1 : 0, d_out);
     NKG_CUDA(cudaGetLastError());
     R.launches += 2;
     NKG_CUDA(cudaEventRecord(g->ev1, s));
