@@ -75,7 +75,7 @@ def oracle_lib():
         lib.nko_pagerank_adjoint.restype = C.c_int64
         lib.nko_pagerank_adjoint.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _f64p, _u32p, _f64p,
                                              C.c_double, C.c_int, _f64p, _f64p, C.c_double,
-                                             C.c_uint64, _f64p, _f64p, _f64p]
+                                             C.c_uint64, _f64p, _f64p, _f64p, C.c_int]
         lib.nko_eigenvector.restype = C.c_int64
         lib.nko_eigenvector.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _u8p, C.c_double,
                                         C.c_uint64, _f64p]
@@ -87,6 +87,13 @@ def oracle_lib():
         lib.nko_apr.restype = C.c_int64
         lib.nko_apr.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _f64p, C.c_double, C.c_double,
                                 _u32p, C.c_uint64, C.c_uint64, _u32p, _f64p, _u64p]
+        lib.nko_finish.restype = None
+        lib.nko_finish.argtypes = [C.c_uint64, _u8p, _u32p, C.c_double, C.c_int, C.c_uint64,
+                                   _f64p, _f64p]
+        lib.nko_sweep_rows.restype = C.c_int
+        lib.nko_sweep_rows.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _f64p, _f64p, _u32p,
+                                       C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_int,
+                                       C.c_int, _f64p, _f64p, _f64p]
         lib.nko_sweep_set.restype = C.c_int64
         lib.nko_sweep_set.argtypes = [C.c_uint64, _u64p, _u32p, _f64p, _f64p, C.c_double,
                                       C.c_uint64, C.c_uint64, _u32p, _f64p, _u32p]
@@ -175,6 +182,34 @@ def pagerank(csr, damp=0.85, tol=1e-8, norm=1, normalized=False, distribute_sink
     return OracleResult(scores, it, float(mx.value), trace[:min(it, trace_cap)].copy())
 
 
+def finish(scores, outdeg, damp, normalized, n=None, exists=None):
+    """PageRank.cpp:75-102 on a final iterate (a copy): (scores, maximum)."""
+    lib = oracle_lib()
+    x = np.array(scores, np.float64, copy=True)
+    z = x.shape[0]
+    n = z if n is None else int(n)
+    mx = C.c_double(0.0)
+    lib.nko_finish(z, _ptr(exists, _u8p), _ptr(np.ascontiguousarray(outdeg, np.uint32), _u32p),
+                   float(damp), int(bool(normalized)), n, _ptr(x, _f64p), C.byref(mx))
+    return x, float(mx.value)
+
+
+def sweep_rows(ptr, col, w, x, wdeg, outdeg_rows, base, damp, teleport_prob, share, distribute,
+               l2, x_out):
+    """One sweep of a row slice (nko_sweep_rows): writes x_out, returns
+    (residual partial sum, sink-mass partial sum)."""
+    lib = oracle_lib()
+    res, sink = C.c_double(0.0), C.c_double(0.0)
+    rows = int(np.asarray(ptr).shape[0]) - 1
+    rc = lib.nko_sweep_rows(rows, _ptr(ptr, _u64p), _ptr(col, _u32p), _ptr(w, _f64p),
+                            _ptr(x, _f64p), _ptr(wdeg, _f64p), _ptr(outdeg_rows, _u32p), int(base),
+                            float(damp), float(teleport_prob), float(share), int(bool(distribute)),
+                            int(bool(l2)), _ptr(x_out, _f64p), C.byref(res), C.byref(sink))
+    if rc != 0:
+        raise RuntimeError("oracle nko_sweep_rows failed")
+    return float(res.value), float(sink.value)
+
+
 def ranking(scores, exists=None):
     lib = oracle_lib()
     z = scores.shape[0]
@@ -222,8 +257,9 @@ def katz(z, ptr, col, w=None, exists=None, alpha=0.0, beta=0.1, tol=1e-8, max_de
 
 
 def adjoint(csr, x, g, damp=0.85, distribute_sinks=True, teleport=None, tol=1e-14,
-            max_iter=100000):
-    """FP64 host adjoint solve; returns (lam, grad_w, grad_t, sweeps)."""
+            max_iter=100000, nthreads=1):
+    """FP64 host adjoint solve; returns (lam, grad_w, grad_t, sweeps). The
+    result does not depend on nthreads."""
     lib = oracle_lib()
     z = int(csr.z)
     lam = np.empty(z, np.float64)
@@ -237,7 +273,7 @@ def adjoint(csr, x, g, damp=0.85, distribute_sinks=True, teleport=None, tol=1e-1
                                       _ptr(csr.outdeg, _u32p), _ptr(tele, _f64p), damp,
                                       int(bool(distribute_sinks)), _ptr(x, _f64p),
                                       _ptr(g, _f64p), tol, max_iter, _ptr(lam, _f64p),
-                                      _ptr(gw, _f64p), _ptr(gt, _f64p))
+                                      _ptr(gw, _f64p), _ptr(gt, _f64p), int(nthreads))
     if sweeps < 0:
         raise RuntimeError("oracle adjoint failed")
     return lam, gw, gt, int(sweeps)

@@ -55,6 +55,80 @@ static double sink_mass(uint64_t z, const uint8_t *exists, const uint32_t *outde
     return s;
 }
 
+/* PageRank.cpp:75-102 on the final iterate `scores` (in place): the
+ * normalisation of both modes and maximum(). */
+void nko_finish(uint64_t z, const uint8_t *exists, const uint32_t *outdeg, double damp,
+                int normalized, uint64_t n, double *scores, double *max_out) {
+    /* PageRank.cpp:75-92 */
+    if (!normalized) {
+        double sum = 0.0;
+        for (uint64_t u = 0; u < z; ++u)
+            if (exists_at(exists, u))
+                sum += scores[u];
+        for (uint64_t u = 0; u < z; ++u)
+            if (exists_at(exists, u))
+                scores[u] /= sum;
+    } else {
+        double sum = 0.0;
+        for (uint64_t u = 0; u < z; ++u)
+            if (exists_at(exists, u) && outdeg[u] == 0)
+                sum += scores[u];
+        const double normFactor = (1.0 / (double)n) * ((1 - damp) + (damp * sum));
+        for (uint64_t u = 0; u < z; ++u)
+            if (exists_at(exists, u))
+                scores[u] /= normFactor;
+    }
+    /* PageRank.cpp:95-102 */
+    if (max_out) {
+        if (!normalized) {
+            *max_out = 1.0;
+        } else {
+            double m = scores[0];
+            for (uint64_t u = 0; u < z; ++u)
+                if (exists_at(exists, u) && scores[u] > m)
+                    m = scores[u];
+            *max_out = m;
+        }
+    }
+}
+
+/* One Jacobi sweep (PageRank.cpp:56-66) of a slice of rows, the step each
+ * rank of a row-partitioned run takes: row r < rows has the in-arcs
+ * ptr[r]..ptr[r+1] whose sources are positions col[e] in the shared vectors x
+ * (the previous iterate, x itself) and wdeg (weighted degrees); the new value
+ * goes to x_out[r]. The sink term adds `share` to the row sum before the
+ * damping when distribute is set. Returns the slice's residual sum against
+ * x[base + r] (|d| or d^2, PageRank.cpp:34-39) and its sink mass (new x over
+ * rows with outdeg_rows[r] == 0), rows in order. */
+int nko_sweep_rows(uint64_t rows, const uint64_t *ptr, const uint32_t *col, const double *w,
+                   const double *x, const double *wdeg, const uint32_t *outdeg_rows,
+                   uint64_t base, double damp, double teleport_prob, double share, int distribute,
+                   int l2, double *x_out, double *res_out, double *sink_out) {
+    if (!ptr || !x || !wdeg || !outdeg_rows || !x_out || !res_out || !sink_out)
+        return -1;
+    double res = 0.0, sink = 0.0;
+    for (uint64_t r = 0; r < rows; ++r) {
+        double acc = 0.0;
+        for (uint64_t e = ptr[r]; e < ptr[r + 1]; ++e) {
+            const uint32_t v = col[e];
+            const double we = w ? w[e] : 1.0;
+            acc += x[v] * we / wdeg[v];
+        }
+        if (distribute)
+            acc += share;
+        acc *= damp;
+        acc += teleport_prob;
+        x_out[r] = acc;
+        const double d = x[base + r] - acc;
+        res += l2 ? d * d : fabs(d);
+        if (outdeg_rows[r] == 0)
+            sink += acc;
+    }
+    *res_out = res;
+    *sink_out = sink;
+    return 0;
+}
+
 int nko_pagerank(uint64_t z, const uint64_t *in_ptr, const uint32_t *in_col, const double *in_w,
                  const double *wdeg, const uint32_t *outdeg, const uint8_t *exists,
                  const double *teleport, const nko_params *p, double *scores, uint64_t *iterations,
@@ -126,37 +200,7 @@ int nko_pagerank(uint64_t z, const uint64_t *in_ptr, const uint32_t *in_col, con
         memcpy(scores, scoreData, z * sizeof(double));
         pr = scoreData; /* the malloc'd buffer, freed below */
     }
-    /* PageRank.cpp:75-92 */
-    if (!p->normalized) {
-        double sum = 0.0;
-        for (uint64_t u = 0; u < z; ++u)
-            if (exists_at(exists, u))
-                sum += scores[u];
-        for (uint64_t u = 0; u < z; ++u)
-            if (exists_at(exists, u))
-                scores[u] /= sum;
-    } else {
-        double sum = 0.0;
-        for (uint64_t u = 0; u < z; ++u)
-            if (exists_at(exists, u) && outdeg[u] == 0)
-                sum += scores[u];
-        const double normFactor = (1.0 / (double)n) * ((1 - damp) + (damp * sum));
-        for (uint64_t u = 0; u < z; ++u)
-            if (exists_at(exists, u))
-                scores[u] /= normFactor;
-    }
-    /* PageRank.cpp:95-102 */
-    if (max_out) {
-        if (!p->normalized) {
-            *max_out = 1.0;
-        } else {
-            double m = scores[0];
-            for (uint64_t u = 0; u < z; ++u)
-                if (exists_at(exists, u) && scores[u] > m)
-                    m = scores[u];
-            *max_out = m;
-        }
-    }
+    nko_finish(z, exists, outdeg, damp, p->normalized, n, scores, max_out);
     if (iterations)
         *iterations = iters;
     free(pr);
@@ -199,14 +243,34 @@ int nko_ranking(uint64_t z, const double *scores, const uint8_t *exists, uint64_
     return 0;
 }
 
+/* c = A^T lam over the out-lists built from the in-CSR (pull form, rows in
+ * parallel): c[v] = sum over the in-arcs (u <- v), u ascending and then in
+ * arc order, of (w / wdeg[v]) * lam[u]. That is the order in which a scatter
+ * over the in-CSR (u ascending, arcs in order) adds to c[v], so the result is
+ * the same bit for bit for any thread count. */
+static void adjoint_pull(uint64_t z, const uint64_t *optr, const uint32_t *orow,
+                         const uint64_t *oarc, const double *in_w, const double *wdeg,
+                         const double *lam, double *c, int nthreads) {
+#pragma omp parallel for schedule(guided) num_threads(nthreads > 1 ? nthreads : 1)
+    for (int64_t v = 0; v < (int64_t)z; ++v) {
+        double acc = 0.0;
+        for (uint64_t k = optr[v]; k < optr[v + 1]; ++k) {
+            const double w = in_w ? in_w[oarc[k]] : 1.0;
+            acc += w / wdeg[v] * lam[orow[k]];
+        }
+        c[v] = acc;
+    }
+}
+
 int64_t nko_pagerank_adjoint(uint64_t z, const uint64_t *in_ptr, const uint32_t *in_col,
                              const double *in_w, const double *wdeg, const uint32_t *outdeg,
                              const double *teleport, double damp, int distribute_sinks,
                              const double *x, const double *g, double tol, uint64_t max_iter,
-                             double *lam, double *grad_w, double *grad_t) {
+                             double *lam, double *grad_w, double *grad_t, int nthreads) {
     if (!in_ptr || !wdeg || !outdeg || !x || !g || !lam || z == 0)
         return -1;
     const double n = (double)z;
+    const uint64_t m = in_ptr[z];
     double sumx = 0.0, S = 0.0;
     for (uint64_t u = 0; u < z; ++u) {
         sumx += x[u];
@@ -219,26 +283,40 @@ int64_t nko_pagerank_adjoint(uint64_t z, const uint64_t *in_ptr, const uint32_t 
     double *gbar = (double *)malloc(z * sizeof(double));
     double *c = (double *)malloc(z * sizeof(double));
     double *lam2 = (double *)malloc(z * sizeof(double));
-    if (!gbar || !c || !lam2) {
+    /* Out-lists of the in-CSR: for source v, (target u, arc index e) with u
+     * ascending and e ascending within u (a stable counting sort). */
+    uint64_t *optr = (uint64_t *)calloc(z + 1, sizeof(uint64_t));
+    uint32_t *orow = (uint32_t *)malloc((m ? m : 1) * sizeof(uint32_t));
+    uint64_t *oarc = (uint64_t *)malloc((m ? m : 1) * sizeof(uint64_t));
+    uint64_t *fill = (uint64_t *)malloc((z + 1) * sizeof(uint64_t));
+    if (!gbar || !c || !lam2 || !optr || !orow || !oarc || !fill) {
         free(gbar);
         free(c);
         free(lam2);
+        free(optr);
+        free(orow);
+        free(oarc);
+        free(fill);
         return -1;
     }
+    for (uint64_t e = 0; e < m; ++e)
+        optr[in_col[e] + 1]++;
+    for (uint64_t v = 0; v < z; ++v)
+        optr[v + 1] += optr[v];
+    memcpy(fill, optr, (z + 1) * sizeof(uint64_t));
+    for (uint64_t u = 0; u < z; ++u)
+        for (uint64_t e = in_ptr[u]; e < in_ptr[u + 1]; ++e) {
+            const uint64_t k = fill[in_col[e]]++;
+            orow[k] = (uint32_t)u;
+            oarc[k] = e;
+        }
     for (uint64_t u = 0; u < z; ++u) {
         gbar[u] = (g[u] - gp) / sumx;
         lam[u] = gbar[u];
     }
     int64_t sweeps = 0;
     for (;;) {
-        /* c = A^T lam: scatter over the in-arcs (u <- v). */
-        memset(c, 0, z * sizeof(double));
-        for (uint64_t u = 0; u < z; ++u)
-            for (uint64_t e = in_ptr[u]; e < in_ptr[u + 1]; ++e) {
-                const uint32_t v = in_col[e];
-                const double w = in_w ? in_w[e] : 1.0;
-                c[v] += w / wdeg[v] * lam[u];
-            }
+        adjoint_pull(z, optr, orow, oarc, in_w, wdeg, lam, c, nthreads);
         double tl = 0.0;
         if (distribute_sinks)
             for (uint64_t u = 0; u < z; ++u)
@@ -257,13 +335,7 @@ int64_t nko_pagerank_adjoint(uint64_t z, const uint64_t *in_ptr, const uint32_t 
             break;
     }
     /* c for the final lam */
-    memset(c, 0, z * sizeof(double));
-    for (uint64_t u = 0; u < z; ++u)
-        for (uint64_t e = in_ptr[u]; e < in_ptr[u + 1]; ++e) {
-            const uint32_t v = in_col[e];
-            const double w = in_w ? in_w[e] : 1.0;
-            c[v] += w / wdeg[v] * lam[u];
-        }
+    adjoint_pull(z, optr, orow, oarc, in_w, wdeg, lam, c, nthreads);
     if (grad_w)
         for (uint64_t u = 0; u < z; ++u)
             for (uint64_t e = in_ptr[u]; e < in_ptr[u + 1]; ++e) {
@@ -278,6 +350,10 @@ int64_t nko_pagerank_adjoint(uint64_t z, const uint64_t *in_ptr, const uint32_t 
     free(gbar);
     free(c);
     free(lam2);
+    free(optr);
+    free(orow);
+    free(oarc);
+    free(fill);
     return sweeps;
 }
 

@@ -66,7 +66,19 @@ int64_t nko_pagerank_adjoint(uint64_t z, const uint64_t *in_ptr, const uint32_t 
                              const double *in_w, const double *wdeg, const uint32_t *outdeg,
                              const double *teleport, double damp, int distribute_sinks,
                              const double *x, const double *g, double tol, uint64_t max_iter,
-                             double *lam, double *grad_w, double *grad_t);
+                             double *lam, double *grad_w, double *grad_t, int nthreads);
+
+/* PageRank.cpp:75-102 on a final iterate (in place): normalisation and
+ * maximum(); n = numberOfNodes(). */
+void nko_finish(uint64_t z, const uint8_t *exists, const uint32_t *outdeg, double damp,
+                int normalized, uint64_t n, double *scores, double *max_out);
+
+/* One sweep of a slice of rows of a row-partitioned run (PageRank.cpp:56-66
+ * restricted to the slice); see pagerank_oracle.c. */
+int nko_sweep_rows(uint64_t rows, const uint64_t *ptr, const uint32_t *col, const double *w,
+                   const double *x, const double *wdeg, const uint32_t *outdeg_rows,
+                   uint64_t base, double damp, double teleport_prob, double share, int distribute,
+                   int l2, double *x_out, double *res_out, double *sink_out);
 
 /* EigenvectorCentrality::run() (EigenvectorCentrality.cpp:20-60): x = 1 for
  * all z ids; repeat values[u] = sum over in-arcs of w * x[v] (arc order),

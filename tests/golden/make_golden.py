@@ -2,7 +2,7 @@
 
 Run from the repository root, where the reference sources are available:
 
-    python tests/golden/make_golden.py [--ref /path/to/networkit]
+    python tests/golden/make_golden.py [--ref /path/to/networkit]  (default $NK_REFERENCE)
 
 It builds the reference subset (oracle/Makefile -> oracle/_ref/libnkref.so),
 reads the reference's own test inputs with the reference's own readers
@@ -91,7 +91,10 @@ def run_all(g, arrays, tag, damp=0.85, tol=1e-8):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("NK_REFERENCE")
+                    or os.path.join(os.path.dirname(ROOT), "reference"),
+                    help="the reference checkout (default: $NK_REFERENCE, else `reference` "
+                         "beside this repository)")
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={args.ref}", "all"],
                    check=True)
