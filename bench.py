@@ -61,6 +61,12 @@ def parse_args():
                     help="sweep launch shape (nkg_graph_options.sweep_shape; -1 default)")
     ap.add_argument("--arc-order", type=int, default=0, choices=[0, 1],
                     help="nkg_graph_options.arc_order (0 keep the reference order, 1 sorted)")
+    ap.add_argument("--hot-tier-kb", type=int, default=-1,
+                    help="nkg_graph_options.hot_tier_kb: shared-memory tier of the sweep "
+                         "(-1 library default, 0 none, 1..224 KB)")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the parity check of the timed run against the reference's own "
+                         "PageRank on the same graph")
     ap.add_argument("--form", default="",
                     choices=["", "ppr", "refine", "adjoint", "batch", "centrality", "local",
                              "reader", "locality"],
@@ -256,10 +262,14 @@ def cpu_baseline_port(csr, nthreads, target_s=4.0, runs=3):
                       f"{min(secs):.1f}-{max(secs):.1f} s each)"}
 
 
-def form_ppr(local, n=4_000_000, m=8, k=256, steps=2):
+def form_ppr(local, n=4_000_000, m=8, k=256, steps=2, oracle_columns=2):
     """Batched personalised PageRank: Barabasi-Albert n=4M, m=8 (undirected),
     256 one-hot seeds (uniform, seed 42), one FP32 SpMM with k = 256 columns,
-    FP64 residual per column, damp 0.85, tol 1e-7 (L1)."""
+    FP64 residual per column, damp 0.85, tol 1e-7 (L1). Errors: every 32nd
+    column against the GPU's FP64 personalised run to tol 1e-12, and
+    `oracle_columns` columns against the oracle (the CPU restatement of
+    PageRank.cpp with the personalised teleport, tol 1e-10, all host
+    cores)."""
     import torch
 
     from networkit_b200 import _capi, generators
@@ -300,10 +310,32 @@ def form_ppr(local, n=4_000_000, m=8, k=256, steps=2):
         errs.append(float(np.abs(scores[j].astype(np.float64) - d_o.cpu().numpy()).sum()))
     plain_ms *= k / len(sample)
     dg.close()
+    o_rows = []
+    if oracle_columns:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        for j in sample[:oracle_columns]:
+            t = np.zeros(csr.z)
+            t[int(seeds[j])] = 1.0
+            o = oracle.pagerank(csr, damp=0.85, tol=1e-10, norm=NORM_L1, teleport=t,
+                                nthreads=cores)
+            d = np.abs(scores[j].astype(np.float64) - o.scores)
+            big = o.scores >= 1.0 / csr.z
+            o_rows.append({"column": j, "seed": int(seeds[j]), "l1_err": float(d.sum()),
+                           "max_abs_err": float(d.max()),
+                           "max_rel_err_at_or_above_1_over_n": float(
+                               (d[big] / o.scores[big]).max()),
+                           "oracle_iterations": o.iterations})
+        o_secs = time.perf_counter() - t0
     return {"workload": f"ppr_ba{n}_m{m}_k{k}_fp32", "n": csr.z, "arcs": csr.arcs, "k": k,
             "plain_fp64_per_seed_ms": plain_ms, "plain_seeds_timed": len(sample),
             "speedup_vs_plain_fp64": plain_ms / (ms / steps),
             "l1_err_max_vs_fp64": max(errs),
+            "vs_oracle": ({"kind": "port", "tol": 1e-10, "seconds": o_secs, "columns": o_rows,
+                           "l1_err_max": max(r["l1_err"] for r in o_rows)} if o_rows else None),
             "sweeps": sweeps // steps, "column_sweeps": col_sweeps, "ms_per_run": ms / steps,
             "ms_per_sweep": per_sweep_ms,
             "gteps_per_iter": csr.arcs * k / (per_sweep_ms / 1e3) / 1e9,
@@ -311,11 +343,19 @@ def form_ppr(local, n=4_000_000, m=8, k=256, steps=2):
             "alg_gbs": bytes_sweep / (per_sweep_ms / 1e3) / 1e9, "gpu_launches": launches}
 
 
-def form_refine(local, csr, steps=2):
+def err_vs(s, ref):
+    d = np.abs(np.asarray(s, np.float64) - ref)
+    return float(d.sum()), float((d / np.maximum(np.abs(ref), 1e-300)).max())
+
+
+def form_refine(local, csr, steps=2, checker=None, checker_kind=None):
     """Plain FP64 vs FP32+FP64-refinement on the R-MAT scale-24 graph: time to
     the FP64 stopping test at tol 1e-10 (L1), and at tol 1.5e-7, the point
-    where both reach ~1e-6 L1 error. Errors are against an FP64 solve to tol
-    1e-14 on the same GPU (the FP64 path is parity-tested against the oracle)."""
+    where both reach ~1e-6 L1 error. Errors: against the FP64 oracle's scores
+    of the headline parity check (`checker`: the reference's own PageRank, or
+    the oracle's restatement, at tol 1e-10 L1, whose own distance to the
+    fixed point is at most about 6e-10), and against an FP64 solve to tol
+    1e-14 on the same GPU."""
     import torch
 
     from networkit_b200 import _capi
@@ -338,18 +378,23 @@ def form_refine(local, csr, steps=2):
                 ms += st["ms_total"]
             s = out.cpu().numpy()
             diff = np.abs(s - ref)
-            res[f"{name}_tol{tol:g}"] = {
+            row = {
                 "ms": ms / steps, "fp64_sweeps": st["fp64_sweeps"], "fp32_sweeps": st["fp32_sweeps"],
                 "l1_err": float(diff.sum()),
                 "max_rel_err": float((diff / np.maximum(np.abs(ref), 1e-300)).max()),
                 "gpu_launches": st["kernel_launches"]}
+            if checker is not None:
+                row["l1_err_vs_oracle"], row["max_rel_err_vs_oracle"] = err_vs(s, checker)
+            res[f"{name}_tol{tol:g}"] = row
     dg.close()
     for tol in ("1e-10", "1.5e-07"):
         res[f"speedup_tol{tol}"] = res[f"fp64_tol{tol}"]["ms"] / res[f"fp32_refine_tol{tol}"]["ms"]
+    res["oracle"] = ({"kind": checker_kind, "tol": TOL, "norm": "L1"} if checker is not None
+                     else None)
     return res
 
 
-def form_adjoint(local, scale=22, steps=3, fd_edges=64, only_step=False):
+def form_adjoint(local, scale=22, steps=3, fd_edges=64, only_step=False, oracle_check=True):
     """Differentiable weighted PageRank: directed R-MAT scale 22, edgefactor
     16, weights uniform in (0.1, 1] (seed 43), loss L = sum_v g_v p_v with
     g ~ N(0, 1) (seed 42), damp 0.85, reference sink semantics. One step is
@@ -360,7 +405,10 @@ def form_adjoint(local, scale=22, steps=3, fd_edges=64, only_step=False):
     1e-13 (both parity-tested against the oracle); the FP64 gradient is also
     checked by central differences (h = 1e-4) of the FP64 forward on
     `fd_edges` random arcs. only_step: the reference solves and the
-    time breakdown only (a short launch sequence for profiling)."""
+    time breakdown only (a short launch sequence for profiling).
+    oracle_check: the forward scores and dL/dw of each timed form also
+    against the oracle's FP64 forward and host adjoint solve (tol 1e-13, all
+    host cores; the oracle's restatement of PageRank.cpp and its adjoint)."""
     import torch
 
     from networkit_b200 import _capi, autograd, generators
@@ -433,6 +481,21 @@ def form_adjoint(local, scale=22, steps=3, fd_edges=64, only_step=False):
         G.graph.close()
         return res
     gwn = float(gw_ref.abs().max())
+    o_scores = o_gw = None
+    if oracle_check:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        o = oracle.pagerank(csr, damp=DAMP, tol=1e-13, norm=NORM_L1, nthreads=cores)
+        _, o_gw, _, o_sweeps = oracle.adjoint(csr, o.scores, g_np, damp=DAMP,
+                                              distribute_sinks=False, tol=1e-13, nthreads=cores)
+        o_scores = o.scores
+        res["oracle"] = {"kind": "port", "cores": cores, "seconds": time.perf_counter() - t0,
+                         "forward_iterations": o.iterations, "adjoint_sweeps": o_sweeps,
+                         "tol": 1e-13}
+        o_gwn = float(np.abs(o_gw).max())
     for tol, btol in ((1e-10, 1e-10), (1.5e-7, 1e-6)):
         ms_p, s_p = timed(plain(tol))
         row = {"plain_fp64_fwd_ms": ms_p, "plain_l1_err": float((s_p - p_ref).abs().sum())}
@@ -442,6 +505,15 @@ def form_adjoint(local, scale=22, steps=3, fd_edges=64, only_step=False):
             row[f"{prec}_l1_err"] = float((s - p_ref).abs().sum())
             row[f"{prec}_max_rel_err"] = float(((s - p_ref).abs() / p_ref.abs()).max())
             row[f"{prec}_grad_w_err"] = float((gw - gw_ref).abs().max()) / gwn
+            if o_scores is not None:
+                sh = s.cpu().numpy()
+                row[f"{prec}_l1_err_vs_oracle"], row[f"{prec}_max_rel_err_vs_oracle"] = err_vs(
+                    sh, o_scores)
+                row[f"{prec}_grad_w_err_vs_oracle"] = float(
+                    np.abs(gw.cpu().numpy() - o_gw).max()) / o_gwn
+        if o_scores is not None:
+            row["plain_l1_err_vs_oracle"], row["plain_max_rel_err_vs_oracle"] = err_vs(
+                s_p.cpu().numpy(), o_scores)
         row["fwd_bwd_vs_plain_fwd"] = ms_p / row["fp32_refine_fwd_bwd_ms"]
         res[f"tol{tol:g}"] = row
     if fd_edges:
@@ -530,6 +602,23 @@ def form_batch(local, count=1024, steps=3, plain_graphs=None, step_only=False):
     s_ref = out.cpu().numpy()
     errs = np.array([np.abs(s32[int(offs[i]):int(offs[i + 1])] -
                             s_ref[int(offs[i]):int(offs[i + 1])]).sum() for i in range(count)])
+    # Every 32nd graph against the oracle (CPU restatement of PageRank.cpp,
+    # FP64, tol 1e-13, all host cores).
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    o_errs, o_rel = [], []
+    t0 = time.perf_counter()
+    for i in range(0, count, 32):
+        a, b = int(offs[i]), int(offs[i + 1])
+        ptr = (csr.in_ptr[a:b + 1] - csr.in_ptr[a]).astype(np.uint64)
+        col = (csr.in_col[int(csr.in_ptr[a]):int(csr.in_ptr[b])] - np.uint32(a)).astype(np.uint32)
+        gi = InCSR(b - a, b - a, ptr, col, None, csr.wdeg[a:b], csr.outdeg[a:b], None, False)
+        o = oracle.pagerank(gi, damp=DAMP, tol=1e-13, norm=NORM_L1, nthreads=os.cpu_count() or 1)
+        l1, rel = err_vs(s32[a:b], o.scores)
+        o_errs.append(l1)
+        o_rel.append(rel)
+    o_secs = time.perf_counter() - t0
     sweeps = its.astype(np.float64)
     arc_it = float((arcs_g * sweeps).sum())
     alg_bytes = float(((4 * arcs_g + 20 * n_g + 4) * sweeps).sum())
@@ -564,6 +653,8 @@ def form_batch(local, count=1024, steps=3, plain_graphs=None, step_only=False):
             "alg_gbs": alg_bytes / (ms32 / 1e3) / 1e9, "alg_frac_of_hbm": alg_bytes / (ms32 / 1e3) / 1e9 / peak,
             "peak_source": peak_kind,
             "fp32_l1_err_max": float(errs.max()), "fp32_l1_err_median": float(np.median(errs)),
+            "vs_oracle": {"kind": "port", "tol": 1e-13, "graphs": len(o_errs), "seconds": o_secs,
+                          "fp32_l1_err_max": max(o_errs), "fp32_max_rel_err_max": max(o_rel)},
             "e2e_ms_host_scores": e2e_ms,
             "fp64_batch_ms": ms64_batch, "plain_fp64_per_graph_ms": plain_ms,
             "plain_graphs_timed": len(idx),
@@ -798,6 +889,50 @@ def form_reader(local, csr, chunks=32, runs=3):
     return res
 
 
+def headline_parity(csr, scores, iterations, gpu_rank_ids, rank_scores):
+    """Parity of the benchmarked run with the reference's own PageRank::run()
+    (oracle/_ref, compiled from the reference sources) on the same graph and
+    parameters, on all host cores; the oracle's C restatement when the
+    reference library is absent. Reports the L1 and largest relative
+    difference of the scores, both iteration counts, and the ranking
+    positions where the two orders differ on nodes whose scores differ by
+    more than 1e-12 relative (anything else is an exact or rounding tie)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    if oracle.ref_available():
+        rows = np.repeat(np.arange(csr.z, dtype=np.uint32), np.diff(csr.in_ptr).astype(np.int64))
+        g = oracle.RefGraph.from_edges(csr.z, csr.in_col, rows, directed=True)
+        del rows
+        r = g.pagerank(damp=DAMP, tol=TOL, norm=NORM_L1, nthreads=cores, want_ranking=True)
+        del g
+        ref_scores, ref_it, ref_ids = r["scores"], r["iterations"], r["ranking_ids"]
+        kind = "reference"
+    else:
+        o = oracle.pagerank(csr, damp=DAMP, tol=TOL, norm=NORM_L1, nthreads=cores)
+        ref_scores, ref_it = o.scores, o.iterations
+        ref_ids = oracle.ranking(o.scores)[0]
+        kind = "port"
+    secs = time.perf_counter() - t0
+    diff = np.abs(scores - ref_scores)
+    ids_g = np.asarray(gpu_rank_ids, np.int64)
+    ids_r = np.asarray(ref_ids, np.int64)
+    pos = np.flatnonzero(ids_g != ids_r)
+    a, b = rank_scores[ids_g[pos]], rank_scores[ids_r[pos]]
+    outside = int(np.count_nonzero(np.abs(a - b) > 1e-12 * np.maximum(np.abs(a), np.abs(b))))
+    return {"checker": kind, "cores": cores, "seconds": secs, "tol": TOL, "norm": "L1",
+            "l1": float(diff.sum()),
+            "max_rel": float((diff / np.maximum(np.abs(ref_scores), 1e-300)).max()),
+            "iterations": int(iterations), "checker_iterations": int(ref_it),
+            "ranking_positions_differing": int(pos.shape[0]),
+            "ranking_mismatches_outside_ties": outside,
+            "bar": {"l1": 1e-10, "iterations": 1, "ranking_mismatches_outside_ties": 0},
+            "pass": bool(diff.sum() <= 1e-10 and abs(int(iterations) - int(ref_it)) <= 1
+                         and outside == 0)}, ref_scores
+
+
 def run_reference_arm(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -817,18 +952,26 @@ def run_reference_arm(args):
     # order (unweighted graph: out-list order does not enter the result).
     g = oracle.RefGraph.from_edges(csr.z, csr.in_col, rows, directed=True)
     del rows
-    probe = g.pagerank(damp=DAMP, tol=TOL, norm=NORM_L1, max_iterations=1, nthreads=cores,
-                       want_ranking=False)
-    iters = int(max(2, min(20, 3.0 / max(probe["seconds"], 1e-3))))
+    # Warm-up steps run one iteration each (page-in and thread start-up);
+    # every timed step is PageRank::run() with maxIterations = iters, so the
+    # run's fixed work (PageRank.cpp:22-30 set-up, :75-104 normalisation) is
+    # paid once per `iters` sweeps. `fixed_s` estimates that fixed part from
+    # the one-iteration runs, for reference.
+    one = []
+    for i in range(max(args.warmup, 2)):
+        one.append(g.pagerank(damp=DAMP, tol=TOL, norm=NORM_L1, max_iterations=1, nthreads=cores,
+                              want_ranking=False)["seconds"])
+    iters = int(max(4, min(12, 8.0 / max(min(one), 1e-3))))
     times, its = [], []
-    for i in range(args.warmup + args.steps):
+    for i in range(args.steps):
         r = g.pagerank(damp=DAMP, tol=TOL, norm=NORM_L1, max_iterations=iters, nthreads=cores,
                        want_ranking=False)
-        if i >= args.warmup:
-            times.append(r["seconds"])
-            its.append(r["iterations"])
+        times.append(r["seconds"])
+        its.append(r["iterations"])
     total = sum(times)
     value = csr.arcs * sum(its) / total / 1e9
+    per_iter = total / sum(its)
+    fixed_s = max(0.0, statistics.median(one[1:] or one) - per_iter)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -839,8 +982,13 @@ def run_reference_arm(args):
                    "tol": TOL, "norm": "L1", "iterations_per_step": iters},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                          "cpu_model": host_cpu()["model"], "physical_cores": host_cpu()["physical"],
+                         "build": "reference sources, C++14 -O3 -DNDEBUG "
+                                  "-DNETWORKIT_RELEASE_LOGGING -fopenmp (its CMake Release "
+                                  "defaults)",
+                         "fixed_s_per_run": fixed_s, "s_per_iteration": per_iter,
                          "sample": f"{iters} iterations of NetworKit::PageRank::run() per step "
-                                   f"(maxIterations={iters}) on the same graph"},
+                                   f"(maxIterations={iters}) on the same graph; warm-up steps "
+                                   f"of one iteration"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -900,13 +1048,15 @@ def main():
         print(json.dumps(form_reader(local, csr)))
         return
     arcs, n = csr.arcs, csr.z
-    dg = _capi.DeviceGraph(csr, device=local, sweep_shape=args.shape, arc_order=args.arc_order)
+    dg = _capi.DeviceGraph(csr, device=local, sweep_shape=args.shape, arc_order=args.arc_order,
+                           hot_tier_kb=args.hot_tier_kb)
     info = dg.info()
     if args.profile_only:
         prec = _capi.NKG_PREC_FP64 if args.precision == "fp64" else _capi.NKG_PREC_FP32
         ms_k, ms_i = dg.profile_sweeps(prec, args.profile_only)
         print(json.dumps({"profile_only": args.profile_only, "precision": args.precision,
                           "shape": args.shape, "arc_order": args.arc_order,
+                          "hot_tier_kb": args.hot_tier_kb,
                           "scale": args.scale, "n": n, "arcs": arcs,
                           "slots": info["slots"], "split_rows": info["split_rows"],
                           "ms_sweep_kernel": ms_k, "ms_iteration": ms_i}))
@@ -986,6 +1136,14 @@ def main():
     h2d = 8 * (n + 1) + 4 * arcs
     d2h = 8 * n
 
+    # Parity of the benchmarked run (the last timed step's scores) with the
+    # reference on the same graph, after the timed region.
+    parity, checker_scores = None, None
+    if rank == 0 and not args.no_parity:
+        gpu_scores = d_out.cpu().numpy()
+        rank_ids, _ = dg.ranking(gpu_scores)
+        parity, checker_scores = headline_parity(csr, gpu_scores, iters[-1], rank_ids, gpu_scores)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(csr, host_cpu()["physical"] or os.cpu_count() or 1)
@@ -995,7 +1153,10 @@ def main():
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
         forms = {}
-        for name, fn in (("fp32_refine", lambda: form_refine(local, csr, steps=1)),
+        for name, fn in (("fp32_refine", lambda: form_refine(local, csr, steps=1,
+                                                             checker=checker_scores,
+                                                             checker_kind=parity and
+                                                             parity["checker"])),
                          ("ppr", lambda: form_ppr(local, steps=1)),
                          ("fwd_bwd", lambda: form_adjoint(local, steps=2, fd_edges=0)),
                          ("eigenvector_katz", lambda: form_centrality(local, csr)),
@@ -1019,6 +1180,7 @@ def main():
                        "edgefactor": EDGEFACTOR, "abcd": [*RMAT, round(1 - sum(RMAT), 6)],
                        "n": n, "arcs": arcs, "sinks": info["sinks"], "damp": DAMP, "tol": TOL,
                        "norm": "L1", "iterations": iters[0], "parallelism": f"replicas{world}",
+                       "hot_tier_kb": args.hot_tier_kb,
                        "l2": "inputs larger than L2 (CSR 1.1 GB)",
                        "wall_s": wall, "ms_create": info["ms_create"]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -1036,6 +1198,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "parity": parity,
         }
         if forms is not None:
             line["forms"] = forms
