@@ -11,8 +11,11 @@ read-back inside the timed region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-N > 1 (under torchrun) runs N replicas of the same workload, one per GPU: the
-plain single-graph path has no partitioned form here, so scaling is weak.
+N > 1 (under torchrun) runs the same PageRank run with its rows cut into N
+slices, one per GPU (networkit_b200.distributed.RowPartitionedPageRank: per
+iteration an all-gather of the iterate and an all-reduce of two sums over
+NCCL), so the total work is fixed and scaling is strong; --multi replicas
+runs N independent copies of the single-GPU run instead (weak scaling).
 """
 from __future__ import annotations
 
@@ -80,11 +83,18 @@ def parse_args():
     ap.add_argument("--batch-step-only", action="store_true",
                     help="--form batch: no tuning and no comparison, two runs with the default "
                          "launch shape (the short launch sequence used for ncu captures)")
+    ap.add_argument("--ppr-n", type=int, default=4_000_000, help="graph nodes of --form ppr")
+    ap.add_argument("--ppr-step-only", action="store_true",
+                    help="--form ppr: one warm-up and one timed run only (the short launch "
+                         "sequence used for ncu captures)")
     ap.add_argument("--local-n", type=int, default=1_000_000, help="graph nodes of --form local")
     ap.add_argument("--local-seeds", type=int, default=16384, help="seeds of --form local")
     ap.add_argument("--local-ref-sample", type=int, default=48,
                     help="seeds the reference runs in --form local (0: none)")
     ap.add_argument("--local-runs", type=int, default=2, help="timed calls of --form local")
+    ap.add_argument("--multi", default="rows", choices=["rows", "replicas"],
+                    help="N > 1: the row-partitioned run (rows, strong scaling) or N independent "
+                         "replicas (weak scaling)")
     ap.add_argument("--cache", default=os.path.join(tempfile.gettempdir(), "nk_b200_graphs"))
     return ap.parse_args()
 
@@ -262,7 +272,7 @@ def cpu_baseline_port(csr, nthreads, target_s=4.0, runs=3):
                       f"{min(secs):.1f}-{max(secs):.1f} s each)"}
 
 
-def form_ppr(local, n=4_000_000, m=8, k=256, steps=2, oracle_columns=2):
+def form_ppr(local, n=4_000_000, m=8, k=256, steps=2, oracle_columns=2, step_only=False):
     """Batched personalised PageRank: Barabasi-Albert n=4M, m=8 (undirected),
     256 one-hot seeds (uniform, seed 42), one FP32 SpMM with k = 256 columns,
     FP64 residual per column, damp 0.85, tol 1e-7 (L1). Errors: every 32nd
@@ -280,6 +290,13 @@ def form_ppr(local, n=4_000_000, m=8, k=256, steps=2, oracle_columns=2):
     p = dg.params(0.85, 1e-7, NORM_L1, False, False, _capi.NKG_PREC_FP32, 1000)
     out = torch.empty((k, csr.z), dtype=torch.float32, device=f"cuda:{local}")
     dg.ppr(seeds, p, out.data_ptr())  # warm-up
+    if step_only:
+        _, its, st = dg.ppr(seeds, p, out.data_ptr())
+        dg.close()
+        return {"workload": f"ppr_ba{n}_m{m}_k{k}_fp32", "n": csr.z, "arcs": csr.arcs, "k": k,
+                "ms_per_run": st["ms_total"], "sweeps": st["fp32_sweeps"],
+                "column_sweeps": int(its.sum()), "ms_per_sweep": st["ms_total"] / st["fp32_sweeps"],
+                "alg_bytes_per_sweep": st["bytes_per_sweep_fp32"]}
     ms, sweeps, launches = 0.0, 0, 0
     for _ in range(steps):
         _, its, st = dg.ppr(seeds, p, out.data_ptr())
@@ -933,6 +950,97 @@ def headline_parity(csr, scores, iterations, gpu_rank_ids, rank_scores):
                          and outside == 0)}, ref_scores
 
 
+def run_row_partitioned(args, csr, local, rank, world, barrier):
+    """bench.py --gpus N (N > 1): one PageRank run on the R-MAT graph with its
+    rows cut into N slices of about equal arc counts, one per rank. A step is
+    one run to convergence; every rank times its steps with CUDA events and
+    the job's time is the slowest rank's. value = arcs x iterations / that
+    time (the whole job's rate: strong scaling)."""
+    import torch
+
+    from networkit_b200 import distributed
+
+    comm = distributed.Comm()
+    kw = dict(damp=DAMP, tol=TOL, norm=NORM_L1)
+    t0 = time.perf_counter()
+    pr = distributed.RowPartitionedPageRank(csr, device=local, comm=comm)
+    create_s = time.perf_counter() - t0
+    for _ in range(max(args.warmup, 3)):
+        pr.run(**kw)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        ev[0].record()
+        iters = []
+        for _ in range(args.steps):
+            scores, it, _, _ = pr.run(**kw)
+            iters.append(it)
+        ev[1].record()
+        torch.cuda.synchronize()
+        barrier()
+    clocks = clk.summary()
+    total_ms = max_over_ranks(ev[0].elapsed_time(ev[1]), f"cuda:{local}")
+    value = csr.arcs * sum(iters) / (total_ms / 1e3) / 1e9
+    # Where an iteration goes on this rank: its slice's sweeps, and the
+    # all-reduce + all-gather (one timed run).
+    _, it_b, _, stb = pr.run(timing=True, **kw)
+    ms_sweep = max_over_ranks(stb["ms_sweeps"] / it_b, f"cuda:{local}")
+    ms_exch = max_over_ranks(stb["ms_exchange"] / it_b, f"cuda:{local}")
+    slice_bytes = 4 * pr.slice_arcs[rank] + 32 * int(pr.plan.rows[rank]) + 4
+    peak, peak_kind = measured_peak_hbm()
+    slice_arcs, body = pr.slice_arcs, pr.body
+    pr.close()
+    # End to end through the same API: slices uploaded from host arrays,
+    # run, scores gathered to the host, per step.
+    e2e_t, e2e_it = [], []
+    for i in range(2):
+        barrier()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        p2 = distributed.RowPartitionedPageRank(csr, device=local, comm=comm)
+        _, it2, _, _ = p2.run(**kw)
+        p2.close()
+        torch.cuda.synchronize()
+        dt = max_over_ranks(time.perf_counter() - t1, f"cuda:{local}")
+        if i > 0:
+            e2e_t.append(dt)
+            e2e_it.append(it2)
+    parity = None
+    if rank == 0 and not args.no_parity:
+        rank_ids = np.argsort(-scores, kind="stable")
+        parity, _ = headline_parity(csr, scores, iters[-1], rank_ids, scores)
+    barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"pagerank_rmat{args.scale}_fp64", "scale": args.scale,
+                       "edgefactor": EDGEFACTOR, "abcd": [*RMAT, round(1 - sum(RMAT), 6)],
+                       "n": csr.z, "arcs": csr.arcs, "damp": DAMP, "tol": TOL, "norm": "L1",
+                       "iterations": iters[0], "parallelism": f"rows{world}",
+                       "slice_arcs": slice_arcs, "create_s": create_s,
+                       "l2": "inputs larger than L2 (CSR 1.1 GB)"},
+            "roofline": {"bound": "hbm", "achieved": slice_bytes / (ms_sweep / 1e3) / 1e9,
+                         "peak": peak, "unit": "GB/s",
+                         "frac": slice_bytes / (ms_sweep / 1e3) / 1e9 / peak, "traffic": None,
+                         "kernel": "sweep_kernel<double, PART> (rank 0's slice)",
+                         "bytes_per_launch": slice_bytes, "ms_per_sweep": ms_sweep,
+                         "ms_exchange_per_iteration": ms_exch,
+                         "exchange_bytes_per_iteration": 8 * body + 16,
+                         "peak_source": peak_kind},
+            "e2e": {"value": csr.arcs * sum(e2e_it) / sum(e2e_t) / 1e9, "unit": UNIT,
+                    "h2d_bytes_per_step": 8 * (csr.z + world) + 4 * csr.arcs + 4 * csr.z,
+                    "d2h_bytes_per_step": 8 * body * world,
+                    "ms_per_step": 1e3 * sum(e2e_t) / len(e2e_t)},
+            "gpu_launches": sum(iters) * 2 * world,
+            "clocks": clocks, "cpu_baseline": None, "parity": parity,
+        }
+        print(json.dumps(line))
+
+
 def run_reference_arm(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -1004,7 +1112,7 @@ def main():
 
     torch.cuda.set_device(local)
     if args.form == "ppr":
-        print(json.dumps(form_ppr(local)))
+        print(json.dumps(form_ppr(local, n=args.ppr_n, step_only=args.ppr_step_only)))
         return
     if args.form == "batch":
         print(json.dumps(form_batch(local, count=args.batch_graphs,
@@ -1038,6 +1146,10 @@ def main():
     from networkit_b200 import _capi
 
     csr = make_graph(args.scale, args.cache, rank, barrier)
+    if world > 1 and args.multi == "rows":
+        run_row_partitioned(args, csr, local, rank, world, barrier)
+        dist.destroy_process_group()
+        return
     if args.form == "refine":
         print(json.dumps(form_refine(local, csr)))
         return

@@ -3,9 +3,9 @@
  *
  * Drop-in boundary for NetworKit's PageRank path. The reference reaches its
  * C++ through Cython (networkit/centrality.pyx:1989-2037 -> PageRank.hpp:28-75);
- * a Cython class replacing it binds the functions below (INTEGRATION.md shows
- * the binding). Plain pointers and sizes only; host arrays are caller-owned and
- * copied; device buffers are owned by the opaque handle.
+ * a Cython class replacing it binds the functions below. Plain pointers and
+ * sizes only; host arrays are caller-owned and copied; device buffers are
+ * owned by the opaque handle.
  *
  * Return codes: 0 on success, a negative NKG_ERR_* otherwise; the message of
  * the last failure on the calling thread is nkg_last_error(). The Python layer
@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define NKG_ABI_VERSION 1
+#define NKG_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define NKG_API __attribute__((visibility("default")))
@@ -70,7 +70,18 @@ typedef struct {
     uint64_t max_iterations; /* UINT64_MAX = unbounded (the reference default) */
 } nkg_pr_params;
 
-/* Per-run statistics (device timings from CUDA events on the handle's stream). */
+/* Per-run statistics (device timings from CUDA events on the handle's stream).
+ * Residual trace: before the call the caller may point residual_trace at an
+ * array of trace_capacity doubles (NULL / 0: no trace). A PageRank run
+ * (nkg_pagerank_run*) then stores there the stopping-test residual of every
+ * sweep that the test is applied to, in order (the values `converged()` of
+ * PageRank.cpp:41-51 compares with tol): every sweep of the FP64 and FP32
+ * power iterations, every FP64 sweep of FP32_REFINE. trace_length receives
+ * the number of such sweeps, which may exceed what was stored (at most
+ * trace_capacity entries, and at most the first 65,536 sweeps). Every call
+ * that fills an nkg_stats keeps residual_trace and trace_capacity as given;
+ * the other calls report trace_length 0. A caller that does not use the trace
+ * zero-initialises the struct (nkg_stats st = {0};). */
 typedef struct {
     uint64_t iterations;       /* numberOfIterations() */
     double residual;           /* last residual norm (L1 sum or L2 sqrt) */
@@ -82,6 +93,9 @@ typedef struct {
     uint64_t fp32_sweeps;      /* SpMV sweeps in FP32 */
     uint64_t bytes_per_sweep_fp64; /* algorithmic bytes of one FP64 sweep */
     uint64_t bytes_per_sweep_fp32; /* algorithmic bytes of one FP32 sweep */
+    double *residual_trace;    /* in: caller's array, or NULL */
+    uint64_t trace_capacity;   /* in: entries of residual_trace */
+    uint64_t trace_length;     /* out: sweeps with a stopping test */
 } nkg_stats;
 
 /* Graph shape after upload. */
@@ -102,9 +116,9 @@ typedef struct {
 /* Options of nkg_graph_create_ex. */
 typedef struct {
     int32_t device;      /* CUDA device ordinal (-1: current device) */
-    int32_t sweep_shape; /* launch shape of the sweep kernel (-1 default; 0: 256
-                            threads, L1-cached gathers; 1: 256 threads, L2-only
-                            gathers; 2: 512 threads; 3: 128 threads) */
+    int32_t sweep_shape; /* launch shape of the sweep kernels: threads per CTA and
+                            gathers in flight per lane (-1 default = 0: 512
+                            threads, 8; 1: 256, 8; 2: 256, 4; 3: 256, 16) */
     int32_t arc_order;   /* 0 (default): keep every in-row in the caller's order,
                             which is the reference's summation order; 1: sort
                             each in-row by source after relabelling (faster
@@ -119,6 +133,15 @@ typedef struct {
                             ids closer than max(64, z/1024), else 0; nkg_graph_create
                             (no options) uses -1. Results do not depend on it beyond
                             the order of the reductions */
+    int32_t hot_tier_kb; /* shared-memory tier of the PageRank sweep: the iterate
+                            of the first ids (the most-gathered sources after
+                            the relabelling) is copied into this many KB of
+                            shared memory per CTA every sweep, and gathers of
+                            those ids read it there (1..224 KB; 0: no tier, the
+                            whole L1 for the gathers; -1: the library's choice,
+                            no tier). Every row sum is the same either way; the
+                            residual and sink mass are summed over a different
+                            number of CTAs */
 } nkg_graph_options;
 
 /* Upload a graph given as its in-adjacency CSR.
@@ -298,10 +321,22 @@ NKG_API int nkg_katz_run(nkg_graph *g, double alpha, double beta, double tol, in
  * scores, e.g. from nkg_pagerank_run); ids_out / vals_out: n entries each. */
 NKG_API int nkg_ranking(nkg_graph *g, const double *scores, uint64_t *ids_out, double *vals_out);
 
-/* Ask a running nkg_pagerank_run* on this handle to stop (the reference's
- * SIGINT check, PageRank.cpp:55 / SignalHandling.cpp:62-66). Safe from any
- * thread or a signal handler; the run returns NKG_ERR_CANCELLED. */
+/* Ask the run on this handle to stop (the reference's SIGINT check,
+ * PageRank.cpp:55 / SignalHandling.cpp:62-66): the running nkg_pagerank_run*
+ * (or eigenvector, Katz, personalised or adjoint run), or, if none is running,
+ * the next one, returns NKG_ERR_CANCELLED at its next check (between
+ * CUDA-graph chunks of sweeps). A request is cleared when the run it stopped,
+ * or any other run on the handle, ends. Safe from any thread or a signal
+ * handler (one atomic store). */
 NKG_API void nkg_cancel(nkg_graph *g);
+
+/* Aux::SignalHandler (SignalHandling.cpp:29-60) for the runs on g: while
+ * enabled, SIGINT calls nkg_cancel(g) instead of reaching the handler that
+ * was installed before, which disabling puts back. One handle at a time per
+ * process, like the reference's root handler: enabling for a second handle
+ * while one holds SIGINT fails with NKG_ERR_INVALID_ARG. *got_sigint_out
+ * (nullable, on disable) tells whether a SIGINT arrived while enabled. */
+NKG_API int nkg_sigint_cancels(nkg_graph *g, int enable, int *got_sigint_out);
 
 /* Diagnostic, no reference counterpart: run `sweeps` iterations (precision
  * NKG_PREC_FP64 or NKG_PREC_FP32, the stopping test disabled) on the
@@ -320,6 +355,56 @@ NKG_API int nkg_profile_sweeps(nkg_graph *g, int precision, int sweeps, double *
  * graph on this GPU, the floor under nkg_profile_sweeps' sweep time. */
 NKG_API int nkg_profile_gathers(nkg_graph *g, int precision, int reps, double *ms_gather_kernel);
 
+/* Row partition of the PageRank iteration over several GPUs; no counterpart
+ * in the reference (whose run is one shared-memory process). The rows of the
+ * in-CSR are cut into contiguous slices of about equal arc counts, one slice
+ * per GPU (or several). Each slice computes its rows of the next iterate from
+ * the whole previous one (PageRank.cpp:56-66 restricted to its rows); between
+ * sweeps the caller all-gathers the slices into the shared iterate and
+ * all-reduces the residual and sink-mass partial sums, then applies the
+ * stopping test (PageRank.cpp:41-51) and the sink term to the reduced sums.
+ *
+ * The shared iterate (vec_len doubles, device memory of each GPU) holds the
+ * slices in gather form (x / deg, or x for out-degree-0 nodes): slice q at
+ * [q * stride, q * stride + rows_q) for a stride >= every rows_q, so that an
+ * all-gather of equal blocks assembles it, and a last entry (vec_len - 1) that
+ * is 0. The caller numbers the in-arc sources of its slice in that layout.
+ *
+ * nkg_part_create: row_base = the slice's offset in the shared iterate; rows,
+ *   arcs, row_ptr (rows + 1, from 0) and col (arcs, positions < vec_len - 1)
+ *   its in-CSR (host arrays, each row in the reference's arc order); w
+ *   (nullable) the arc weights; out_deg / out_wdeg (rows) the out-degree count
+ *   and, for weighted graphs, the weighted out-degree (Graph.cpp:426-452) of
+ *   the slice's nodes in the whole graph. device -1: the current device.
+ * nkg_part_begin: x = 1 / n_global (PageRank.cpp:26) into d_y_out (rows, the
+ *   slice's block of the shared iterate); p gives damp, norm and
+ *   distribute_sinks (FP64 only; tol and max_iterations are the caller's).
+ * nkg_part_sweep: one sweep of the slice from the shared iterate d_y_in into
+ *   d_y_out (rows), with sink_coef added to every row sum before the damping
+ *   (distribute_sinks: the previous iterate's sink mass / n_global). Returns
+ *   the slice's residual sum (sum of |x' - x|, or of (x' - x)^2 for L2, before
+ *   any square root) and its sink mass (sum of x' over out-degree-0 nodes).
+ * nkg_part_sums: sum of x, sum of x over out-degree-0 nodes, and max of x over
+ *   the slice, for PageRank.cpp:75-102 after reduction across slices.
+ * nkg_part_scores: x / factor for the slice rows into d_out (rows).
+ * All d_* pointers are device memory on the slice's device; work runs on
+ * `stream` (a cudaStream_t, NULL: the handle's own) and every call returns
+ * once it has finished. */
+typedef struct nkg_part nkg_part;
+NKG_API int nkg_part_create(nkg_part **out, uint64_t vec_len, uint64_t row_base, uint64_t rows,
+                            uint64_t arcs, const uint64_t *row_ptr, const uint32_t *col,
+                            const double *w, const uint32_t *out_deg, const double *out_wdeg,
+                            int device);
+NKG_API void nkg_part_destroy(nkg_part *p);
+NKG_API int nkg_part_begin(nkg_part *p, const nkg_pr_params *prm, uint64_t n_global,
+                           double *d_y_out, void *stream);
+NKG_API int nkg_part_sweep(nkg_part *p, const double *d_y_in, double sink_coef, double *d_y_out,
+                           double *residual_sum_out, double *sink_sum_out, void *stream);
+NKG_API int nkg_part_sums(nkg_part *p, const double *d_y, double *sum_out, double *sink_sum_out,
+                          double *max_out, void *stream);
+NKG_API int nkg_part_scores(nkg_part *p, const double *d_y, double factor, double *d_out,
+                            void *stream);
+
 /* PageRank without any device allocation; no counterpart in the reference.
  * For callers that cannot allocate device memory when they call in: a
  * framework whose caching allocator owns the device memory, a service with
@@ -328,15 +413,21 @@ NKG_API int nkg_profile_gathers(nkg_graph *g, int precision, int reps, double *m
  * graph and the output in device memory:
  *   d_in_row_ptr  n+1 in-CSR offsets (device), d_in_col  arcs sources (device)
  *   d_scores_out  n doubles (device)
- * FP64 only, n <= 524288 nodes; larger graphs are rejected with
- * NKG_ERR_INVALID_ARG. All working storage is one 12.1 MB file-scope
- * __device__ array of the library, held by every GPU that loads the library
- * until the process exits. The first call on a device looks up that array's
- * address (cudaGetSymbolAddress, with the device current); make that first
- * call before any stream capture. Calls share the array: calls that overlap
- * on the GPU (other threads, other streams) race and must be serialised by
- * the caller. Work runs on `stream` (a cudaStream_t; NULL = default stream)
- * and the call returns when it has finished. */
+ * FP64 only and unweighted: every arc counts with weight 1.0 and a node's
+ * degree is its number of out-arcs in d_in_col, so weighted graphs must use
+ * nkg_pagerank_run. n <= 524288 nodes; larger graphs are rejected with
+ * NKG_ERR_INVALID_ARG, as are offsets that are not a CSR (row_ptr[0] != 0,
+ * decreasing, or row_ptr[n] != arcs) and column ids >= n; both are checked on
+ * the device before any sweep reads the graph. All working storage is one
+ * 12.1 MB file-scope __device__ array of the library, held by every GPU that
+ * loads the library until the process exits. The first call on a device looks
+ * up that array's address (cudaGetSymbolAddress, with the device current) and
+ * keeps it; make that first call before any stream capture, and make no call
+ * on a device after a cudaDeviceReset of it (the kept address is then stale).
+ * Calls share the array: calls that overlap on the GPU (other threads, other
+ * streams) race and must be serialised by the caller. Work runs on `stream`
+ * (a cudaStream_t; NULL = default stream) and the call returns when it has
+ * finished. */
 NKG_API int nkg_pagerank_csr_noalloc(uint64_t n, uint64_t arcs, const uint64_t *d_in_row_ptr,
                                      const uint32_t *d_in_col, const nkg_pr_params *p,
                                      double *d_scores_out, uint64_t *iterations_out,

@@ -1,9 +1,10 @@
 """ctypes binding of libnkgpu.so (include/nkgpu.h).
 
 This plays the role of the Cython declarations a NetworKit build would use
-(``cdef extern from "nkgpu.h"``); INTEGRATION.md shows that Cython form. The
-library is loaded from the package's ``_lib`` directory; if it is missing the
-import fails loudly - there is no CPU fallback.
+(``cdef extern from "nkgpu.h"``; the compiled form of those is
+``_nkgpu.pxd`` / ``_cypagerank.pyx``). The library is loaded from the
+package's ``_lib`` directory; if it is missing, or was built for another ABI
+version, loading fails loudly - there is no CPU fallback.
 """
 from __future__ import annotations
 
@@ -29,6 +30,8 @@ NKG_PREC_FP32 = 2
 
 UINT64_MAX = 2**64 - 1
 NKG_DEVICE_PTRS = 1
+# include/nkgpu.h NKG_ABI_VERSION this binding's structures follow.
+ABI_VERSION = 2
 
 
 class PRParams(C.Structure):
@@ -55,10 +58,24 @@ class Stats(C.Structure):
         ("fp32_sweeps", C.c_uint64),
         ("bytes_per_sweep_fp64", C.c_uint64),
         ("bytes_per_sweep_fp32", C.c_uint64),
+        ("residual_trace", C.POINTER(C.c_double)),
+        ("trace_capacity", C.c_uint64),
+        ("trace_length", C.c_uint64),
     ]
 
     def as_dict(self):
-        return {f: getattr(self, f) for f, _ in self._fields_}
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "residual_trace"}
+
+    @classmethod
+    def with_trace(cls, capacity: int):
+        """Stats whose residual trace goes to a new float64 array of
+        `capacity` entries (returned beside it)."""
+        st = cls()
+        buf = np.zeros(max(int(capacity), 0), np.float64)
+        if capacity > 0:
+            st.residual_trace = buf.ctypes.data_as(C.POINTER(C.c_double))
+            st.trace_capacity = int(capacity)
+        return st, buf
 
 
 class GraphInfo(C.Structure):
@@ -82,7 +99,12 @@ class GraphInfo(C.Structure):
 
 class GraphOptions(C.Structure):
     _fields_ = [("device", C.c_int32), ("sweep_shape", C.c_int32), ("arc_order", C.c_int32),
-                ("row_order", C.c_int32)]
+                ("row_order", C.c_int32), ("hot_tier_kb", C.c_int32)]
+
+    def __init__(self, *a, **kw):
+        super().__init__(*a, **kw)
+        if "hot_tier_kb" not in kw and len(a) < 5:
+            self.hot_tier_kb = -1
 
 
 class BatchTuning(C.Structure):
@@ -133,6 +155,7 @@ SIGNATURES = {
                                             _f64p, C.POINTER(Stats)]),
     "nkg_ranking": (C.c_int, [_vp, _f64p, _u64p, _f64p]),
     "nkg_cancel": (None, [_vp]),
+    "nkg_sigint_cancels": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
     "nkg_profile_sweeps": (C.c_int, [_vp, C.c_int, C.c_int, _f64p, _f64p]),
     "nkg_profile_gathers": (C.c_int, [_vp, C.c_int, C.c_int, _f64p]),
     "nkg_pagerank_csr_noalloc": (C.c_int, [C.c_uint64, C.c_uint64, _vp, _vp, C.POINTER(PRParams),
@@ -165,6 +188,13 @@ SIGNATURES = {
                                 C.c_uint64, _u64p, _u64p, C.POINTER(LocalStats)]),
     "nkg_local_support": (C.c_int, [_vp, _u32p, _f64p]),
     "nkg_local_sets": (C.c_int, [_vp, _u32p]),
+    "nkg_part_create": (C.c_int, [C.POINTER(_vp), C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
+                                  _u64p, _u32p, _f64p, _u32p, _f64p, C.c_int]),
+    "nkg_part_destroy": (None, [_vp]),
+    "nkg_part_begin": (C.c_int, [_vp, C.POINTER(PRParams), C.c_uint64, _vp, _vp]),
+    "nkg_part_sweep": (C.c_int, [_vp, _vp, C.c_double, _vp, _f64p, _f64p, _vp]),
+    "nkg_part_sums": (C.c_int, [_vp, _vp, _f64p, _f64p, _f64p, _vp]),
+    "nkg_part_scores": (C.c_int, [_vp, _vp, C.c_double, _vp, _vp]),
 }
 
 _lib = None
@@ -183,6 +213,9 @@ def lib():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
+        if L.nkg_abi_version() != ABI_VERSION:
+            raise RuntimeError(f"{LIB_PATH} has ABI version {L.nkg_abi_version()}, this binding "
+                               f"expects {ABI_VERSION}: rebuild with `python -m networkit_b200.build`")
         _lib = L
     return _lib
 
@@ -211,7 +244,7 @@ class DeviceGraph:
     """Owning wrapper of an nkg_graph handle."""
 
     def __init__(self, csr, device: int = -1, sweep_shape: int = -1, arc_order: int = 0,
-                 row_order: int = -1):
+                 row_order: int = -1, hot_tier_kb: int = -1):
         L = lib()
         h = _vp()
         in_ptr = np.ascontiguousarray(csr.in_ptr, np.uint64)
@@ -224,6 +257,7 @@ class DeviceGraph:
         opts.sweep_shape = int(sweep_shape)
         opts.arc_order = int(arc_order)
         opts.row_order = int(row_order)
+        opts.hot_tier_kb = int(hot_tier_kb)
         check(L.nkg_graph_create_ex(C.byref(h), int(csr.z), int(in_col.shape[0]),
                                     ptr(in_ptr, _u64p), ptr(in_col, _u32p), ptr(in_w, _f64p),
                                     ptr(wdeg, _f64p), ptr(ex, _u8p), int(bool(csr.directed)),
@@ -294,10 +328,12 @@ class DeviceGraph:
         return PRParams(float(damp), float(tol), int(norm), int(bool(normalized)),
                         int(bool(distribute_sinks)), int(precision), int(max_iterations))
 
-    def run(self, p: PRParams, teleport=None, out=None):
+    def run(self, p: PRParams, teleport=None, out=None, trace: int = 0):
         """Run to convergence; returns (scores[z], iterations, maximum, stats).
         `out`: optional float64[z] host array to receive the scores (pinned
-        memory makes the read-back a direct DMA)."""
+        memory makes the read-back a direct DMA). trace > 0: stats also holds
+        "residual_trace", the residual of every sweep with a stopping test
+        (at most `trace` of them)."""
         L = lib()
         if out is not None:
             if out.dtype != np.float64 or out.shape != (self.z,) or not out.flags.c_contiguous:
@@ -307,7 +343,7 @@ class DeviceGraph:
             scores = np.empty(self.z, np.float64)
         it = C.c_uint64(0)
         mx = C.c_double(0.0)
-        st = Stats()
+        st, tbuf = Stats.with_trace(trace)
         if teleport is None:
             check(L.nkg_pagerank_run(self.h, C.byref(p), ptr(scores, _f64p), C.byref(it),
                                      C.byref(mx), C.byref(st)))
@@ -318,7 +354,10 @@ class DeviceGraph:
             check(L.nkg_pagerank_run_teleport(self.h, C.byref(p), ptr(t, _f64p),
                                               ptr(scores, _f64p), C.byref(it), C.byref(mx),
                                               C.byref(st)))
-        return scores, int(it.value), float(mx.value), st.as_dict()
+        d = st.as_dict()
+        if trace > 0:
+            d["residual_trace"] = tbuf[:min(int(st.trace_length), int(trace))].copy()
+        return scores, int(it.value), float(mx.value), d
 
     def run_device(self, p: PRParams, d_out_ptr: int):
         """Run with the scores written to device memory at d_out_ptr."""
@@ -426,6 +465,13 @@ class DeviceGraph:
 
     def cancel(self):
         lib().nkg_cancel(self.h)
+
+    def sigint_cancels(self, enable: bool) -> bool:
+        """Route SIGINT to cancel() (enable) or give it back to the handler
+        it had; on disable, returns whether a SIGINT arrived meanwhile."""
+        got = C.c_int(0)
+        check(lib().nkg_sigint_cancels(self.h, int(bool(enable)), C.byref(got)))
+        return bool(got.value)
 
     def profile_sweeps(self, precision: int, sweeps: int):
         """(ms per sweep-kernel launch, ms per iteration) from CUDA events."""

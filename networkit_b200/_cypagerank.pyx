@@ -18,7 +18,9 @@ from libc.stdint cimport uint8_t, uint32_t, uint64_t, UINT64_MAX
 
 from networkit_b200._nkgpu cimport (
     nkg_graph, nkg_pr_params, nkg_stats, nkg_graph_create, nkg_graph_destroy, nkg_pagerank_run,
-    nkg_ranking, nkg_cancel, nkg_last_error, NKG_PREC_FP64, NKG_NORM_L2)
+    nkg_ranking, nkg_cancel, nkg_sigint_cancels, nkg_last_error, NKG_PREC_FP64, NKG_NORM_L2,
+    NKG_ERR_CANCELLED)
+from libc.string cimport memset
 
 import numpy as np
 
@@ -109,12 +111,23 @@ cdef class PageRank:
         scores = np.empty(csr.z, np.float64)
         cdef double[::1] s = scores
         cdef nkg_stats st
+        memset(&st, 0, sizeof(st))           # no residual trace
         cdef uint64_t it = 0
         cdef double mx = 0.0
         cdef int rc
+        cdef int got_sigint = 0
+        # SIGINT cancels the run while it is in the library, as the
+        # reference's SignalHandler does (PageRank.cpp:55); if another handle
+        # already holds SIGINT, this run goes without.
+        cdef bint routed = nkg_sigint_cancels(self._g, 1, NULL) == 0
         with nogil:                           # base.pyx:28
             rc = nkg_pagerank_run(self._g, &self._p, &s[0], &it, &mx, &st)
+        if routed:
+            nkg_sigint_cancels(self._g, 0, &got_sigint)
         if rc != 0:
+            if rc == NKG_ERR_CANCELLED and got_sigint:
+                # Aux::SignalHandling::InterruptException (SignalHandling.hpp:26-30)
+                raise RuntimeError("Received CTRL+C/SIGINT")
             _raise_last()
         self._scores = scores
         self._iters = it

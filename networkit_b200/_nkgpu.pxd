@@ -28,9 +28,13 @@ cdef extern from "nkgpu.h" nogil:
         uint64_t fp32_sweeps
         uint64_t bytes_per_sweep_fp64
         uint64_t bytes_per_sweep_fp32
+        double *residual_trace
+        uint64_t trace_capacity
+        uint64_t trace_length
 
     enum:
         NKG_OK
+        NKG_ERR_CANCELLED
         NKG_PREC_FP64
         NKG_PREC_FP32_REFINE
         NKG_PREC_FP32
@@ -45,4 +49,5 @@ cdef extern from "nkgpu.h" nogil:
                          uint64_t *iterations_out, double *max_out, nkg_stats *stats)
     int nkg_ranking(nkg_graph *g, const double *scores, uint64_t *ids_out, double *vals_out)
     void nkg_cancel(nkg_graph *g)
+    int nkg_sigint_cancels(nkg_graph *g, int enable, int *got_sigint_out)
     const char *nkg_last_error()

@@ -17,6 +17,31 @@ from . import _capi
 from .graph import Graph
 
 
+def _run_interruptible(dg, call):
+    """Run `call` (a library run on the handle dg) with SIGINT routed to
+    dg's cancel flag, as the reference's SignalHandler routes it for the
+    length of a run (SignalHandling.cpp:29-60): Ctrl-C ends the run at its
+    next check with RuntimeError("Received CTRL+C/SIGINT"), the message of
+    Aux::SignalHandling::InterruptException. If another handle holds SIGINT
+    already, the run goes without."""
+    try:
+        dg.sigint_cancels(True)
+        routed = True
+    except _capi.NkgError:
+        routed = False
+    try:
+        return call()
+    except _capi.NkgError as e:
+        got = dg.sigint_cancels(False) if routed else False
+        routed = False
+        if e.code == _capi.NKG_ERR_CANCELLED and got:
+            raise RuntimeError("Received CTRL+C/SIGINT") from None
+        raise
+    finally:
+        if routed:
+            dg.sigint_cancels(False)
+
+
 class Algorithm:
     """Abstract base class for algorithms (networkit/base.pyx:3-69)."""
 
@@ -200,13 +225,19 @@ class PageRank(Centrality):
         dg = self._device_graph()
         p = dg.params(self._damp, self._tol, self._norm, self._normalized, self._distribute,
                       _PRECISIONS[self._precision], self._maxIterations)
-        scores, it, mx, st = dg.run(p, teleport)
+        scores, it, mx, st = _run_interruptible(dg, lambda: dg.run(p, teleport))
         self._scores = scores
         self._iterations = it
         self._max = mx
         self.lastStats = st
         self._hasRun = True
         return self
+
+    def cancel(self):
+        """Stop a run in progress (or the next run) with RuntimeError: the
+        SIGINT check of PageRank.cpp:55, callable from another thread."""
+        if self._dg is not None:
+            self._dg.cancel()
 
     def numberOfIterations(self) -> int:
         """Number of iterations performed (PageRank.hpp:58-61)."""

@@ -1011,10 +1011,7 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
     auto read_state = [&] {
         NKG_CUDA(cudaMemcpyAsync(hst, st, sizeof(AdjState), cudaMemcpyDeviceToHost, s));
         NKG_CUDA(cudaStreamSynchronize(s));
-        if (g->cancel.load()) {
-            g->cancel.store(0);
-            throw Error(NKG_ERR_CANCELLED, "PageRank adjoint cancelled");
-        }
+        check_cancel(g, "PageRank adjoint cancelled");
     };
 
     int fin = 0;  // W.lam[fin] holds the solution
@@ -1198,7 +1195,7 @@ int nkg_pagerank_adjoint(nkg_graph *g, const nkg_pr_params *p, const double *tel
                 "damp must be in [0, 1)");
         require(p->tol >= 0.0, "tol must be >= 0");
         DeviceGuard guard(g->device);
-        g->cancel.store(0);
+        RunScope scope(g);
         const bool dev = (flags & NKG_DEVICE_PTRS) != 0;
         cudaStream_t s = g->stream;
         DeviceArray<double> t_tmp, s_tmp, g_tmp, gw_tmp, gt_tmp;
@@ -1232,7 +1229,7 @@ int nkg_pagerank_adjoint(nkg_graph *g, const nkg_pr_params *p, const double *tel
         if (iterations_out)
             *iterations_out = R.fp64_sweeps + R.fp32_matvecs;
         if (stats) {
-            std::memset(stats, 0, sizeof(*stats));
+            clear_stats(stats);
             stats->iterations = R.fp64_sweeps + R.fp32_matvecs;
             stats->residual = R.residual;
             stats->ms_total = R.ms;

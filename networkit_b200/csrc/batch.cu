@@ -1084,7 +1084,7 @@ int nkg_batch_run(nkg_batch *b, const nkg_pr_params *p, double *scores_out, int 
         if (floor_stops_out)
             *floor_stops_out = counters[1];
         if (stats) {
-            std::memset(stats, 0, sizeof(*stats));
+            clear_stats(stats);
             stats->iterations = sweeps;
             stats->residual = maxres;
             stats->ms_total = ms;

@@ -320,10 +320,7 @@ CentResult cent_run(nkg_graph *g, const SellLayout &L, const double *w_sell, dou
         NKG_CUDA(cudaStreamSynchronize(s));
         if (hst->done)
             break;
-        if (g->cancel.load()) {
-            g->cancel.store(0);
-            throw Error(NKG_ERR_CANCELLED, "centrality run cancelled");
-        }
+        check_cancel(g, "centrality run cancelled");
     }
     R.iterations = hst->iteration;
     R.length = hst->length;
@@ -363,7 +360,7 @@ void fill_stats(const CentResult &R, uint64_t *iterations_out, nkg_stats *stats)
     if (iterations_out)
         *iterations_out = R.iterations;
     if (stats) {
-        std::memset(stats, 0, sizeof(*stats));
+        clear_stats(stats);
         stats->iterations = R.iterations;
         stats->residual = R.length;
         stats->ms_total = R.ms;
@@ -387,7 +384,7 @@ int nkg_eigenvector_run(nkg_graph *g, double tol, uint64_t max_iterations, doubl
         require((flags & ~NKG_DEVICE_PTRS) == 0, "unknown flags");
         require(!std::isnan(tol), "tol must not be NaN");
         DeviceGuard guard(g->device);
-        g->cancel.store(0);
+        RunScope scope(g);
         const bool dev = (flags & NKG_DEVICE_PTRS) != 0;
         DeviceArray<double> tmp;
         double *d_out = scores_out;
@@ -416,7 +413,7 @@ int nkg_katz_run(nkg_graph *g, double alpha, double beta, double tol, int edge_d
         require(!(alpha < 0), "Alpha must be non negative.");
         require(!std::isnan(tol) && std::isfinite(beta), "tol / beta must be numbers");
         DeviceGuard guard(g->device);
-        g->cancel.store(0);
+        RunScope scope(g);
         cudaStream_t s = g->stream;
         if (alpha == 0) {
             // KatzCentrality::defaultAlpha: 1 / (1 + maxDegree(G)), maxDegree = out-degree count

@@ -42,6 +42,16 @@ inline void require(bool ok, const std::string &msg) {
         throw Error(NKG_ERR_INVALID_ARG, msg);
 }
 
+// Zero the statistics a call reports, keeping the caller's residual-trace
+// array and its capacity (inputs of the struct).
+inline void clear_stats(nkg_stats *st) {
+    double *trace = st->residual_trace;
+    const uint64_t cap = st->trace_capacity;
+    *st = nkg_stats{};
+    st->residual_trace = trace;
+    st->trace_capacity = cap;
+}
+
 // Device memory of the library: cudaMalloc'ed blocks that are kept, once
 // freed, in a per-device cache keyed by size, so that graph create / destroy
 // cycles do not map and unmap gigabytes each time. device_free first waits

@@ -39,10 +39,11 @@ struct SellLayout {
 
 // Build the sliced layout of a CSR whose n rows are sorted by length,
 // descending; the weight of entry k is w[w_index[k]] (w[k] without an index,
-// no weights when w is null).
+// no weights when w is null). Padding slots hold pad_col (kNone: n, the zero
+// entry of an iterate of n + 1).
 void build_sell(SellLayout &L, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                 const double *w, const uint32_t *w_index, const uint32_t *rowlen, int device,
-                cudaStream_t s);
+                cudaStream_t s, uint32_t pad_col = kNone);
 // map[slot] = index[k] for the CSR entry k each slot of L holds (kNone for
 // padding slots).
 void build_slot_map(const SellLayout &L, uint32_t n, const uint32_t *row_ptr, const uint32_t *index,
@@ -70,6 +71,14 @@ struct Plane {
     cudaGraphExec_t exec[2] = {nullptr, nullptr};  // [personal]
     unsigned sweep_ctas = 0;
     unsigned fix_ctas = 0;
+    uint32_t hot = 0;            // ids in the shared-memory tier (0: none)
+    // The tier kernel's own grid and work units; the fields above stay those
+    // of the regular shape, which the FP32 product of the refinement solve
+    // also uses.
+    DeviceArray<uint32_t> hot_unit_start;
+    uint32_t hot_units = 0;
+    unsigned hot_ctas = 0;
+    int hot_threads = 0;         // kHotThreads or kHotThreadsPair
 };
 
 } // namespace nkg
@@ -114,12 +123,34 @@ struct nkg_graph {
     nkg::PinnedHost<nkg::IterState> st_host;
     nkg::PinnedHost<double> scalars_host;
 
+    nkg::DeviceArray<double> trace;      // residual of sweep i at [i] (kTraceCapacity)
+    int hot_tier_kb = -1;                // nkg_graph_options.hot_tier_kb
+
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     std::atomic<int> cancel{0};
     bool has_run = false;
 };
 
 namespace nkg {
+// Cancellation (nkg_cancel): a request stays set until a run on the handle
+// ends, so one issued just before a run starts stops that run. Every run
+// holds a RunScope, which clears the request when the run ends (normally or
+// by an error); the checks between chunks of sweeps only read it.
+struct RunScope {
+    nkg_graph *g;
+    explicit RunScope(nkg_graph *h) : g(h) {}
+    RunScope(const RunScope &) = delete;
+    RunScope &operator=(const RunScope &) = delete;
+    ~RunScope() { g->cancel.store(0); }
+};
+inline void check_cancel(const nkg_graph *g, const char *what) {
+    if (g->cancel.load())
+        throw Error(NKG_ERR_CANCELLED, what);
+}
+
+// Most sweeps whose residual a run records for nkg_stats.residual_trace.
+constexpr uint32_t kTraceCapacity = 65536;
+
 // The out-adjacency layout of the adjoint (adjoint.cu), built on first use.
 AdjointState &adjoint_ensure(nkg_graph *g);
 // Read-only view of that layout for other kernels: rows are the nodes in

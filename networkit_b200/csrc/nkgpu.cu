@@ -6,6 +6,8 @@
 // are mapped back to the caller's ids on the way out.
 #include <cub/cub.cuh>
 
+#include <signal.h>
+
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -401,7 +403,8 @@ __global__ void fill_slices(uint32_t slices, uint32_t s_chunk, uint32_t n_chunks
                             const uint32_t *__restrict__ row_ptr, const uint32_t *__restrict__ col,
                             const double *__restrict__ w, const uint32_t *__restrict__ w_index,
                             const uint32_t *__restrict__ slice_off,
-                            uint32_t *__restrict__ col_sell, double *__restrict__ w_sell) {
+                            uint32_t *__restrict__ col_sell, double *__restrict__ w_sell,
+                            uint32_t pad_col) {
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -413,7 +416,7 @@ __global__ void fill_slices(uint32_t slices, uint32_t s_chunk, uint32_t n_chunks
             const size_t slot = (static_cast<size_t>(off) + j) * 32 + lane;
             const bool real = j < v.len;
             if (col_sell)
-                col_sell[slot] = real ? col[v.start + j] : n;
+                col_sell[slot] = real ? col[v.start + j] : pad_col;
             if (w_sell)
                 w_sell[slot] = real ? w[w_index ? w_index[v.start + j] : v.start + j] : 0.0;
         }
@@ -697,7 +700,9 @@ static void sort_rows(nkg_graph *g, cudaStream_t s) {
 // descending (row_ptr, col, optional weights w through w_index, rowlen).
 void build_sell(SellLayout &L, uint32_t n, const uint32_t *row_ptr, const uint32_t *col,
                 const double *w, const uint32_t *w_index, const uint32_t *rowlen, int device,
-                cudaStream_t s) {
+                cudaStream_t s, uint32_t pad_col) {
+    if (pad_col == kNone)
+        pad_col = n;
     const unsigned sms = num_sms(device);
     DeviceArray<unsigned long long> cnt(2);
     NKG_CUDA(cudaMemsetAsync(cnt.get(), 0, 2 * sizeof(unsigned long long), s));
@@ -769,7 +774,7 @@ void build_sell(SellLayout &L, uint32_t n, const uint32_t *row_ptr, const uint32
         fill_slices<<<sms * 16, 256, 0, s>>>(L.slices, L.s_chunk, L.n_chunks, L.n_long, n,
                                              chunk_row.get(), chunk_idx.get(), row_ptr, col, w,
                                              w_index, L.slice_off.get(), L.col_sell.get(),
-                                             L.w_sell64.get());
+                                             L.w_sell64.get(), pad_col);
         NKG_CUDA(cudaGetLastError());
     }
     NKG_CUDA(cudaStreamSynchronize(s));
@@ -1000,6 +1005,9 @@ static nkg_graph *build_graph(std::unique_ptr<nkg_graph> g, DeviceArray<uint64_t
         require(opt->sweep_shape >= -1 && opt->sweep_shape < kNumSweepShapes,
                 "unknown sweep shape");
         require(opt->arc_order == 0 || opt->arc_order == 1, "arc_order must be 0 or 1");
+        require(opt->hot_tier_kb >= -1 && opt->hot_tier_kb <= static_cast<int>(kHotMaxBytes / 1024),
+                "hot_tier_kb must be in [-1, 224]");
+        g->hot_tier_kb = opt->hot_tier_kb;
         if (opt->sweep_shape >= 0)
             g->sweep_shape = opt->sweep_shape;
         if (opt->arc_order == 1 && arcs > 1 && arcs < 0x7fffffffull)
@@ -1023,6 +1031,7 @@ static nkg_graph *build_graph(std::unique_ptr<nkg_graph> g, DeviceArray<uint64_t
     g->fix_sink.alloc(fix);
     g->rp.alloc(1);
     g->st.alloc(1);
+    g->trace.alloc(kTraceCapacity);
     g->red.alloc(4 + 3 * 4096);
     g->red_ticket.alloc(1);
     NKG_CUDA(cudaMemsetAsync(g->red_ticket.get(), 0, sizeof(unsigned int), s));
@@ -1185,6 +1194,25 @@ Plane<double> &plane<double>(nkg_graph *g) { return g->p64; }
 template <>
 Plane<float> &plane<float>(nkg_graph *g) { return g->p32; }
 
+// Tier size used when the options leave it to the library (KB per SM): none,
+// the measured best (the tier costs L1 that the gathers need).
+constexpr int kDefaultHotTierKB = 0;
+
+// Ids held by the shared-memory tier of the PageRank sweep: the requested KB
+// in ids, at most the n + 1 entries of the iterate rounded up to 16 bytes
+// (the iterate buffers carry 4 elements of zero padding past n + 1, so the
+// rounded copy stays inside them and the extra ids read zero).
+template <typename T>
+static uint32_t hot_tier_ids(const nkg_graph *g) {
+    const int kb = g->hot_tier_kb < 0 ? kDefaultHotTierKB : g->hot_tier_kb;
+    if (kb <= 0)
+        return 0;
+    constexpr uint64_t per16 = 16 / sizeof(T);
+    const uint64_t want = static_cast<uint64_t>(kb) * 1024 / sizeof(T);
+    const uint64_t all = (g->n + 1 + per16 - 1) / per16 * per16;
+    return static_cast<uint32_t>(std::min(want, all) / per16 * per16);
+}
+
 template <typename T, bool WEIGHTED>
 static void sweep_setup(nkg_graph *g) {
     Plane<T> &P = plane<T>(g);
@@ -1228,6 +1256,41 @@ static void sweep_setup(nkg_graph *g) {
     NKG_CUDA(cudaGetLastError());
     P.fix_ctas = fix_vlong_ctas(g->fw.n_vlong) +
                  ceil_div(std::max<uint32_t>(g->fw.n_long - g->fw.n_vlong, 1), kFixThreads);
+    P.hot = hot_tier_ids<T>(g);
+    if (P.hot) {
+        const int bytes = static_cast<int>(P.hot * sizeof(T));
+        int sm_smem = 0;
+        NKG_CUDA(cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor,
+                                        g->device));
+        require(sm_smem > 0, "device reports no shared memory");
+        // Two CTAs of 768 threads per SM where two copies of the tier fit
+        // (with the static scratch and the per-CTA reserve), else one of 1024.
+        const int per_cta = bytes + 2048;
+        const int copies = 2 * per_cta <= sm_smem ? 2 : 1;
+        P.hot_threads = copies == 2 ? kHotThreadsPair : kHotThreads;
+        auto kfn = copies == 2 ? sweep_kernel<T, WEIGHTED, kHotThreadsPair, kHotUnroll, true>
+                               : sweep_kernel<T, WEIGHTED, kHotThreads, kHotUnroll, true>;
+        // Carve out only what the CTAs need, leaving the rest of the SM's L1
+        // to the gathers.
+        const int carve = std::min(100, (copies * per_cta) * 100 / sm_smem + 1);
+        NKG_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        NKG_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        int hocc = 0;
+        NKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&hocc, kfn, P.hot_threads, bytes));
+        require(hocc >= 1, "shared-memory tier does not fit on an SM");
+        P.hot_ctas = static_cast<unsigned>(std::max<uint64_t>(
+            1, std::min<uint64_t>(static_cast<uint64_t>(hocc) * sms,
+                                  (static_cast<uint64_t>(g->fw.slices) * 32 + P.hot_threads - 1) /
+                                      P.hot_threads)));
+        const uint64_t hwarps = static_cast<uint64_t>(P.hot_ctas) * (P.hot_threads / 32);
+        P.hot_units = static_cast<uint32_t>(
+            std::max<uint64_t>(1, std::min<uint64_t>(hwarps * kUnitsPerWarp, g->fw.slices)));
+        P.hot_unit_start.alloc(static_cast<size_t>(P.hot_units) + 1);
+        unit_bounds<<<ceil_div(static_cast<uint64_t>(P.hot_units) + 1, 256), 256, 0, s>>>(
+            g->fw.slice_cost.get(), g->fw.slices, P.hot_units, P.hot_unit_start.get());
+        NKG_CUDA(cudaGetLastError());
+        require(P.hot_ctas <= g->cta_res.size(), "partial-sum buffers too small");
+    }
     require(P.sweep_ctas <= g->cta_res.size() && P.fix_ctas <= g->fix_res.size(),
             "partial-sum buffers too small");
     NKG_CUDA(cudaStreamSynchronize(s));
@@ -1263,14 +1326,28 @@ static SweepArgs<T> sweep_args(nkg_graph *g, int in_buf) {
     a.n_long = g->fw.n_long;
     a.n_vlong = g->fw.n_vlong;
     a.s_chunk = g->fw.s_chunk;
-    a.units = P.units;
-    a.sweep_ctas = P.sweep_ctas;
+    a.units = P.hot ? P.hot_units : P.units;
+    a.sweep_ctas = P.hot ? P.hot_ctas : P.sweep_ctas;
+    if (P.hot)
+        a.unit_start = P.hot_unit_start.get();
+    a.hot = P.hot;
+    a.trace = g->trace.get();
+    a.trace_cap = kTraceCapacity;
     return a;
 }
 
 template <typename T, bool WEIGHTED>
 static void launch_sweep_kernel(nkg_graph *g, const SweepArgs<T> &a, cudaStream_t s) {
     Plane<T> &P = plane<T>(g);
+    if (P.hot) {
+        if (P.hot_threads == kHotThreadsPair)
+            sweep_kernel<T, WEIGHTED, kHotThreadsPair, kHotUnroll, true>
+                <<<P.hot_ctas, kHotThreadsPair, P.hot * sizeof(T), s>>>(a);
+        else
+            sweep_kernel<T, WEIGHTED, kHotThreads, kHotUnroll, true>
+                <<<P.hot_ctas, kHotThreads, P.hot * sizeof(T), s>>>(a);
+        return;
+    }
     with_sweep_shape(g->sweep_shape, [&](auto S) {
         using Sh = decltype(S);
         sweep_kernel<T, WEIGHTED, Sh::threads, Sh::unroll><<<P.sweep_ctas, Sh::threads, 0, s>>>(a);
@@ -1311,6 +1388,12 @@ struct RunResult {
     double ms_total = 0.0, ms_iter = 0.0;
     uint64_t launches = 0;
     uint64_t fp64_sweeps = 0, fp32_sweeps = 0;
+    // Residuals of the sweeps with a stopping test: trace_length of them, in
+    // g->trace on the device (power iterations, written by the fix-up) or in
+    // host_trace (the FP64 sweeps of the refinement, read by the host).
+    uint64_t trace_length = 0;
+    bool device_trace = false;
+    std::vector<double> host_trace;
 };
 
 // PageRank.cpp:75-102 on the final iterate yfin (gather form, this plane's
@@ -1414,16 +1497,15 @@ static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *d
         NKG_CUDA(cudaStreamSynchronize(s));
         if (sh->done)
             break;
-        if (g->cancel.load()) {
-            g->cancel.store(0);
-            throw Error(NKG_ERR_CANCELLED, "PageRank run cancelled");
-        }
+        check_cancel(g, "PageRank run cancelled");
         batch = std::min(batch * 2, 8);
     }
     NKG_CUDA(cudaEventRecord(g->ev1, s));
     R.iterations = sh->iteration;
     R.residual = sh->residual;
     R.sink_mass = sh->sink_mass;
+    R.trace_length = R.iterations;
+    R.device_trace = true;
     const int fin = static_cast<int>(R.iterations & 1ull);
     finalize<T, WEIGHTED>(g, p, P.y[fin].get(), d_out, R);
     return R;
@@ -1542,6 +1624,8 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
         ++fp64;
         NKG_CUDA(cudaMemcpyAsync(sh, g->st.get(), sizeof(IterState), cudaMemcpyDeviceToHost, s));
         NKG_CUDA(cudaStreamSynchronize(s));
+        if (R.host_trace.size() < kTraceCapacity)
+            R.host_trace.push_back(sh->residual);
         if (sh->residual <= p.tol)
             break;
         bi_residual_rhs<WEIGHTED><<<ceil_div(n, 256), 256, 0, s>>>(
@@ -1555,6 +1639,7 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
     R.sink_mass = sh->sink_mass;
     R.fp64_sweeps = fp64;
     R.fp32_sweeps = bl.matvecs;
+    R.trace_length = fp64;
     R.launches += bl.launches;
     finalize<double, WEIGHTED>(g, p, P64.y[1].get(), d_out, R);
     return R;
@@ -1573,7 +1658,7 @@ static RunResult run_dispatch(nkg_graph *g, const nkg_pr_params *p, const double
                               double *d_out) {
     check_params(p);
     DeviceGuard guard(g->device);
-    g->cancel.store(0);
+    RunScope scope(g);
     RunResult R;
     if (p->precision == NKG_PREC_FP64) {
         R = g->weighted ? run_power<double, true>(g, *p, teleport, d_out)
@@ -1592,7 +1677,8 @@ static RunResult run_dispatch(nkg_graph *g, const nkg_pr_params *p, const double
 static void fill_stats(const nkg_graph *g, const RunResult &R, int precision, nkg_stats *st) {
     if (!st)
         return;
-    std::memset(st, 0, sizeof(*st));
+    clear_stats(st);
+    st->trace_length = R.trace_length;
     st->iterations = R.iterations;
     st->residual = R.residual;
     st->sink_mass = R.sink_mass;
@@ -1736,12 +1822,41 @@ static int run_to(nkg_graph *g, const nkg_pr_params *p, const double *teleport, 
                                      g->stream));
             NKG_CUDA(cudaStreamSynchronize(g->stream));
         }
+        if (stats && stats->residual_trace && stats->trace_capacity) {
+            const uint64_t k = std::min<uint64_t>(
+                std::min<uint64_t>(R.trace_length, stats->trace_capacity), kTraceCapacity);
+            if (R.device_trace) {
+                NKG_CUDA(cudaMemcpyAsync(stats->residual_trace, g->trace.get(), k * sizeof(double),
+                                         cudaMemcpyDeviceToHost, g->stream));
+                NKG_CUDA(cudaStreamSynchronize(g->stream));
+            } else {
+                std::copy(R.host_trace.begin(),
+                          R.host_trace.begin() + std::min<uint64_t>(k, R.host_trace.size()),
+                          stats->residual_trace);
+            }
+        }
         if (iters)
             *iters = R.iterations;
         if (max_out)
             *max_out = R.maximum;
         fill_stats(g, R, p->precision, stats);
     });
+}
+
+// The process's SIGINT route of nkg_sigint_cancels: the handle whose runs a
+// SIGINT cancels (the reference's root SignalHandler), the handler it
+// replaced, and whether a SIGINT arrived. The handler only does lock-free
+// atomic loads and stores, which are async-signal-safe.
+static std::mutex g_sigint_mutex;
+static std::atomic<nkg_graph *> g_sigint_owner{nullptr};
+static std::atomic<int> g_sigint_seen{0};
+static struct sigaction g_sigint_prev;
+
+static void on_sigint(int) {
+    g_sigint_seen.store(1);
+    nkg_graph *g = g_sigint_owner.load();
+    if (g)
+        g->cancel.store(1);
 }
 
 static void ranking_prepare(double *keys, uint32_t *ids, const uint32_t *inv, uint64_t z,
@@ -1909,6 +2024,36 @@ int nkg_ranking(nkg_graph *g, const double *scores, uint64_t *ids_out, double *v
 void nkg_cancel(nkg_graph *g) {
     if (g)
         g->cancel.store(1);
+}
+
+int nkg_sigint_cancels(nkg_graph *g, int enable, int *got_sigint_out) {
+    return guarded([&] {
+        require(g != nullptr, "graph handle is NULL");
+        std::lock_guard<std::mutex> lock(nkg::g_sigint_mutex);
+        if (enable) {
+            nkg_graph *owner = nkg::g_sigint_owner.load();
+            require(owner == nullptr || owner == g,
+                    "SIGINT is already routed to another graph handle");
+            if (owner == g)
+                return;
+            nkg::g_sigint_seen.store(0);
+            nkg::g_sigint_owner.store(g);
+            struct sigaction sa {};
+            sa.sa_handler = nkg::on_sigint;
+            sigemptyset(&sa.sa_mask);
+            if (sigaction(SIGINT, &sa, &nkg::g_sigint_prev) != 0) {
+                nkg::g_sigint_owner.store(nullptr);
+                throw nkg::Error(NKG_ERR_INVALID_ARG, "sigaction(SIGINT) failed");
+            }
+        } else {
+            if (nkg::g_sigint_owner.load() == g) {
+                sigaction(SIGINT, &nkg::g_sigint_prev, nullptr);
+                nkg::g_sigint_owner.store(nullptr);
+            }
+            if (got_sigint_out)
+                *got_sigint_out = nkg::g_sigint_seen.load();
+        }
+    });
 }
 
 int nkg_profile_sweeps(nkg_graph *g, int precision, int sweeps, double *ms_sweep_kernel,

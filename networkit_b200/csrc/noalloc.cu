@@ -109,6 +109,20 @@ __global__ void na_count(NaLayout L, const uint32_t *__restrict__ col, uint64_t 
     }
 }
 
+// The caller's in-CSR offsets, checked before any sweep walks them (the
+// checks of the regular path's graph upload): row_ptr[0] = 0, non-decreasing,
+// row_ptr[n] = arcs. A bad offset sets *err to 2, so no sweep is launched.
+__global__ void na_check_rows(const uint64_t *__restrict__ row_ptr, uint64_t arcs, uint32_t n,
+                              int *err) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        const uint64_t a = row_ptr[i], b = row_ptr[i + 1];
+        if (b < a || b > arcs || (i == 0 && a != 0) || (i + 1 == n && b != arcs))
+            atomicExch(err, 2);
+    }
+}
+
 __global__ void na_start(NaLayout L, uint32_t n, double x0, double sink_coef0) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < n) {
@@ -254,7 +268,9 @@ __global__ void na_scale(NaLayout L, uint32_t n, int fin_buf, int normalized, do
     out[r] = x / factor;
 }
 
-// Scratch address per device, looked up once with that device current.
+// Scratch address per device, looked up once with that device current (the
+// first call on the device). A cudaDeviceReset of the device gives the
+// module a new context, so the cached address is not valid after one.
 std::mutex g_na_mutex;
 unsigned char *g_na_addr[64] = {};
 
@@ -297,11 +313,16 @@ extern "C" int nkg_pagerank_csr_noalloc(uint64_t n, uint64_t arcs, const uint64_
         // The error word lives in the partials block (zeroed here).
         int *err = reinterpret_cast<int *>(L.part_max);
         NKG_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+        na_check_rows<<<std::min<unsigned>(blocks_n, 1024), kNaThreads, 0, s>>>(d_in_row_ptr,
+                                                                                 arcs, nn, err);
         if (arcs)
             na_count<<<256, kNaThreads, 0, s>>>(L, d_in_col, arcs, nn, err);
+        NKG_CUDA(cudaGetLastError());
         int h_err = 0;
         NKG_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s));
         NKG_CUDA(cudaStreamSynchronize(s));
+        require(h_err != 2, "d_in_row_ptr is not a valid CSR offset array (row_ptr[0] must be 0, "
+                            "the offsets non-decreasing and row_ptr[n] = arcs)");
         require(h_err == 0, "d_in_col holds a node id >= n");
         const double x0 = 1.0 / static_cast<double>(n);
         NaParams np{};

@@ -590,10 +590,7 @@ void run_ppr(nkg_graph *g, const nkg_pr_params &p, uint32_t k, const uint32_t *s
         h = read_scalar(st.get(), s);
         if (h.all_done)
             break;
-        if (g->cancel.load()) {
-            g->cancel.store(0);
-            throw Error(NKG_ERR_CANCELLED, "personalised PageRank run cancelled");
-        }
+        check_cancel(g, "personalised PageRank run cancelled");
     }
     NKG_CUDA(cudaEventRecord(g->ev1, s));
     const float *yfin = (h.iteration & 1) ? y1.get() : y0.get();
@@ -650,7 +647,7 @@ void run_ppr(nkg_graph *g, const nkg_pr_params &p, uint32_t k, const uint32_t *s
         for (uint32_t j = 0; j < k; ++j)
             iters_out[j] = hit[j];
     if (stats) {
-        std::memset(stats, 0, sizeof(*stats));
+        clear_stats(stats);
         float ms = 0.f;
         NKG_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev2));
         stats->ms_total = ms;
@@ -687,6 +684,7 @@ extern "C" int nkg_ppr_run(nkg_graph *g, const nkg_pr_params *p, uint32_t k, con
         for (uint32_t j = 0; j < k; ++j)
             require(seeds[j] < g->z, "seed id out of range");
         DeviceGuard guard(g->device);
+        RunScope scope(g);
         // CPL columns per lane (float4 loads): 128 or 256 columns per sweep.
         if (k <= 128)
             run_ppr<4>(g, *p, k, seeds, scores_out, out_on_device != 0, iterations_out, stats);

@@ -660,10 +660,8 @@ void bi_solve(const BiArgs &a, BiLaunch &L, double rel, double floor) {
         L.matvecs += 8;
         NKG_CUDA(cudaMemcpyAsync(L.h_sc, L.d_sc, sizeof(BiScalars), cudaMemcpyDeviceToHost, s));
         NKG_CUDA(cudaStreamSynchronize(s));
-        if (L.cancel && L.cancel->load()) {
-            L.cancel->store(0);
+        if (L.cancel && L.cancel->load())
             throw Error(NKG_ERR_CANCELLED, "PageRank run cancelled");
-        }
     }
 }
 

@@ -52,6 +52,7 @@ struct RunParams {
 struct IterState {
     unsigned long long iteration;  // completed sweeps
     double residual;               // norm of the last sweep
+    double residual_sum;           // its sum before the square root (L2)
     double sink_mass;              // sum of x over sinks of the last iterate
     double sink_coef;              // sink term applied by the next sweep
     int done;                      // converged / max reached
@@ -85,6 +86,17 @@ struct SweepArgs {
     uint32_t s_chunk;       // slices [0, s_chunk) hold chunks, the rest rows
     uint32_t units;
     uint32_t sweep_ctas;
+    uint32_t hot;           // ids [0, hot) are read from the shared-memory tier
+    uint32_t trace_cap;     // entries of trace
+    double *trace;          // residual of completed sweep i at [i] (i < trace_cap)
+    // Row slice of a partitioned run (PART kernels): local row r (in the
+    // slice's own relabelled order) is slice row row_map[r]; the slice's
+    // iterate entries, degrees, teleport and output are in slice row order,
+    // and its previous iterate value sits at y_in[row_base + row_map[r]] of
+    // the shared iterate, whose entry `pad` is the zero of padding slots.
+    const uint32_t *__restrict__ row_map;
+    uint32_t row_base;
+    uint32_t pad;
 };
 
 template <typename T>
@@ -104,12 +116,13 @@ __device__ __forceinline__ float t_add<float>(float a, float b) { return __fadd_
 // term of distributeSinks), the residual term of PageRank.cpp:34-39 and the
 // new gather-form value. No FMA contraction: the reference rounds the
 // multiply and the add separately.
-template <typename T, bool WEIGHTED>
+template <typename T, bool WEIGHTED, bool PART = false>
 __device__ __forceinline__ void finish_row(const SweepArgs<T> &a, const RunParams &rp, T sink_coef,
-                                           uint32_t r, T acc, double &res, double &sink) {
+                                           uint32_t r0, T acc, double &res, double &sink) {
+    const uint32_t r = PART ? a.row_map[r0] : r0;
     const uint32_t dc = ld_stream(a.degc + r);
     const T deg = WEIGHTED ? ld_stream(a.degw + r) : static_cast<T>(dc);
-    const T yo = a.y_in[r];
+    const T yo = a.y_in[(PART ? a.row_base : 0u) + r];
     if (rp.distribute)
         acc = t_add(acc, rp.personal ? t_mul(sink_coef, a.tele[r]) : sink_coef);
     T x = t_mul(acc, static_cast<T>(rp.damp));
@@ -141,7 +154,7 @@ __device__ __forceinline__ int ld_keep(const int *p) {
     return v;
 }
 
-template <typename T, bool WEIGHTED>
+template <typename T, bool WEIGHTED, bool PART = false>
 __device__ __forceinline__ void finish_row_sweep(const SweepArgs<T> &a, uint32_t r, T acc,
                                                  double &res, double &sink) {
     RunParams rp;
@@ -152,7 +165,7 @@ __device__ __forceinline__ void finish_row_sweep(const SweepArgs<T> &a, uint32_t
     rp.personal = ld_keep(&a.rp->personal);
     rp.l2 = ld_keep(&a.rp->l2);
     const T sink_coef = static_cast<T>(ld_keep(&a.st->sink_coef));
-    finish_row<T, WEIGHTED>(a, rp, sink_coef, r, acc, res, sink);
+    finish_row<T, WEIGHTED, PART>(a, rp, sink_coef, r, acc, res, sink);
 }
 
 // Padding slots (column n, whose gathered value is the zero entry y[n]) skip
@@ -183,18 +196,65 @@ inline void with_sweep_shape(int v, F &&f) {
     }
 }
 
+// Hot-source tier. The rows are relabelled by in-degree, and on power-law
+// graphs in- and out-degree go together, so the first ids are also the
+// sources that most arcs gather from (on directed R-MAT scale 24 the first
+// 28,672 ids are the sources of 34% of the arcs, the first 57,344 of 46%).
+// The tier copies y_in[0, hot) into shared memory at the start of every
+// sweep, and a gather of such an id is a shared-memory load instead of a
+// request through L1. Every other gather goes through L1 as before. Each CTA
+// holds its own copy of the tier: two CTAs of 768 threads per SM (48 warps,
+// as the regular sweep) where two copies fit, else one CTA of 1024 threads.
+// Measured on B200 it is not faster than the whole L1 for the gathers (the
+// shared memory it takes is L1 the gathers lose), so it is off by default.
+constexpr int kHotThreads = 1024;
+constexpr int kHotThreadsPair = 768;
+constexpr int kHotUnroll = 8;
+// Largest tier: 224 KB of the 227 KB a CTA may opt into (the rest holds the
+// block reduction's scratch).
+constexpr uint32_t kHotMaxBytes = 224u * 1024u;
+
+template <typename T, bool HOT, bool PART = false>
+__device__ __forceinline__ T gather_y(const SweepArgs<T> &a, const T *s_y, uint32_t c) {
+    if (HOT && c < a.hot)
+        return s_y[c];
+    return c != (PART ? a.pad : a.n) ? __ldg(a.y_in + c) : T(0);
+}
+
+// 16-byte read-only load that does not allocate in L1 (the tier copy).
+__device__ __forceinline__ uint4 ld_na_v4(const uint4 *p) {
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+
 // The sweep: each warp walks its units; each lane accumulates one virtual
 // row of a slice in arc order. Chunk slices store partial sums; row slices
 // finish rows.
 // Registers are fitted to 48 warps per SM (more warps do not make the sweep
 // faster: it is bound by the rate of L1 miss requests), and to 32 for the
 // other batch depths and the weighted FP64 sweep, which would spill at 48.
-template <typename T, bool WEIGHTED, int THREADS, int UNROLL>
+// HOT: the variant with the shared-memory tier (a.hot * sizeof(T) bytes of
+// dynamic shared memory, a multiple of 16). PART: the row slice of a
+// partitioned run (see SweepArgs.row_map).
+template <typename T, bool WEIGHTED, int THREADS, int UNROLL, bool HOT = false, bool PART = false>
 __global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T) > 4) ? 1024 / THREADS : 1536 / THREADS)
     sweep_kernel(SweepArgs<T> a) {
     __shared__ double s_red[32];
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    T *s_y = reinterpret_cast<T *>(s_dyn);
     if (*(volatile int *)&a.st->done)
         return;
+    if (HOT) {
+        const uint32_t vecs = a.hot * static_cast<uint32_t>(sizeof(T)) / 16u;
+        const uint4 *src = reinterpret_cast<const uint4 *>(a.y_in);
+        uint4 *dst = reinterpret_cast<uint4 *>(s_dyn);
+        for (uint32_t i = threadIdx.x; i < vecs; i += THREADS)
+            dst[i] = ld_na_v4(src + i);
+        __syncthreads();
+    }
     const int lane = threadIdx.x & 31;
     const uint32_t wpc = THREADS / 32;
     const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);
@@ -217,7 +277,7 @@ __global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T)
                 T v[UNROLL];
 #pragma unroll
                 for (int k = 0; k < UNROLL; ++k)
-                    v[k] = c[k] != a.n ? __ldg(a.y_in + c[k]) : T(0);
+                    v[k] = gather_y<T, HOT, PART>(a, s_y, c[k]);
                 if (WEIGHTED) {
 #pragma unroll
                     for (int k = 0; k < UNROLL; ++k)
@@ -238,7 +298,7 @@ __global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T)
                 T v[UNROLL];
 #pragma unroll
                 for (int k = 0; k < UNROLL; ++k)
-                    v[k] = j + k < len && c[k] != a.n ? __ldg(a.y_in + c[k]) : T(0);
+                    v[k] = j + k < len ? gather_y<T, HOT, PART>(a, s_y, c[k]) : T(0);
                 if (WEIGHTED) {
 #pragma unroll
                     for (int k = 0; k < UNROLL; ++k)
@@ -255,7 +315,7 @@ __global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T)
             } else {
                 const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
                 if (r < a.n)
-                    finish_row_sweep<T, WEIGHTED>(a, r, acc, res, sink);
+                    finish_row_sweep<T, WEIGHTED, PART>(a, r, acc, res, sink);
             }
         }
     }
@@ -323,7 +383,7 @@ __device__ __forceinline__ bool split_row_sum(const uint32_t *__restrict__ chunk
     return true;
 }
 
-template <typename T, bool WEIGHTED>
+template <typename T, bool WEIGHTED, bool PART = false>
 __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
     __shared__ double s_red[32];
     __shared__ bool s_last;
@@ -344,7 +404,7 @@ __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
                 part += a.chunk_val[k];
             const double tot = warp_sum(static_cast<double>(part));
             if (lane == 0)
-                finish_row<T, WEIGHTED>(a, rp, sink_coef, r, static_cast<T>(tot), res, sink);
+                finish_row<T, WEIGHTED, PART>(a, rp, sink_coef, r, static_cast<T>(tot), res, sink);
         }
     } else {
         const uint32_t r = a.n_vlong + (blockIdx.x - vctas) * kFixThreads + threadIdx.x;
@@ -358,7 +418,7 @@ __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
 #pragma unroll
             for (uint32_t k = 0; k < kShortChunks; ++k)
                 sum += parts[k];
-            finish_row<T, WEIGHTED>(a, rp, sink_coef, r, sum, res, sink);
+            finish_row<T, WEIGHTED, PART>(a, rp, sink_coef, r, sum, res, sink);
         }
     }
     const double bres = block_sum<kFixThreads>(res, s_red);
@@ -392,6 +452,9 @@ __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
         const double norm = rp.l2 ? sqrt(r) : r;
         st->iteration = it;
         st->residual = norm;
+        st->residual_sum = r;
+        if (it - 1 < a.trace_cap)
+            a.trace[it - 1] = norm;
         st->sink_mass = s;
         st->sink_coef = rp.distribute ? (rp.personal ? s : s / static_cast<double>(a.n)) : 0.0;
         st->ticket = 0;

@@ -119,7 +119,39 @@ def test_capi_library_exports_every_header_symbol():
         assert hasattr(lib, s), s
     assert set(syms) <= set(_capi.SIGNATURES), "every header symbol has a ctypes signature"
     L = _capi.lib()
-    assert L.nkg_abi_version() == 1
+    assert L.nkg_abi_version() == _capi.ABI_VERSION
+
+
+def test_capi_structures_match_the_header(tmp_path):
+    """The ctypes structures have the size and field offsets of the C
+    structures of include/nkgpu.h (compiled here with gcc)."""
+    import ctypes as C
+    import shutil
+    import subprocess
+
+    from networkit_b200 import _capi
+    cc = shutil.which("gcc") or "/usr/bin/gcc"
+    checks = {"nkg_stats": (_capi.Stats, ["iterations", "bytes_per_sweep_fp32", "residual_trace",
+                                         "trace_capacity", "trace_length"]),
+              "nkg_graph_options": (_capi.GraphOptions, ["row_order", "hot_tier_kb"]),
+              "nkg_pr_params": (_capi.PRParams, ["precision", "max_iterations"]),
+              "nkg_graph_info": (_capi.GraphInfo, ["row_order", "ms_create"])}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "nkgpu.h"', 'int main(void) {']
+    for name, (_, fields) in checks.items():
+        lines.append(f'printf("{name} %zu\\n", sizeof({name}));')
+        for f in fields:
+            lines.append(f'printf("{name}.{f} %zu\\n", offsetof({name}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "sizes.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "sizes"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    got = dict(l.split() for l in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                 text=True).stdout.splitlines())
+    for name, (cls, fields) in checks.items():
+        assert int(got[name]) == C.sizeof(cls), name
+        for f in fields:
+            assert int(got[f"{name}.{f}"]) == getattr(cls, f).offset, (name, f)
 
 
 def test_hyperbolic_generator_shape():
