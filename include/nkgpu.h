@@ -179,6 +179,31 @@ NKG_API int nkg_graph_create_from_edges(nkg_graph **out, uint64_t z, uint64_t m,
                                         const uint32_t *src, const uint32_t *dst, const double *w,
                                         const uint8_t *exists, int directed, int flags,
                                         const nkg_graph_options *opts);
+/* NetworkitBinaryReader::read (NetworkitBinaryReader.cpp:19-235) on the GPU:
+ * a NetworkitBinaryGraph file (its `size` bytes, host memory or, with flags =
+ * NKG_DEVICE_PTRS, device memory) decoded on the device straight into the
+ * graph, with the adjacency the reference reader stores (directed: row v = v's
+ * transpose list, weighted degree = the sum of v's out-list weights in list
+ * order; undirected: row v = v's adjacency list, then its transpose list
+ * without self-loops; weighted degree = the row's sum in row order; node flag
+ * bit 0 = the node exists). Every weight encoding (none, varint, zigzag,
+ * double, float). The decode is fully parallel: a scan finds every varint,
+ * one CTA per file chunk walks the list lengths. Malformed files (magic,
+ * sections outside the file, chunks not starting at a list length, truncated
+ * lists, neighbour ids >= the node count) fail with NKG_ERR_INVALID_ARG.
+ * ms_decode_out (nullable): device time of the decode, after the copy of a
+ * host file.
+ * nkg_nkbg_decode: the same decode into caller-owned HOST arrays (any may be
+ * NULL; sizes from a first call with all of them NULL: z_out, arcs_out):
+ * in_ptr z+1, in_col / in_w arcs, wdeg / outdeg / exists z. */
+NKG_API int nkg_graph_create_from_nkbg(nkg_graph **out, const void *file, uint64_t size,
+                                       int flags, const nkg_graph_options *opts,
+                                       double *ms_decode_out);
+NKG_API int nkg_nkbg_decode(const void *file, uint64_t size, int flags, int device,
+                            uint64_t *z_out, uint64_t *arcs_out, int *directed_out,
+                            int *weighted_out, uint64_t *in_ptr, uint32_t *in_col, double *in_w,
+                            double *wdeg, uint32_t *outdeg, uint8_t *exists,
+                            double *ms_decode_out);
 NKG_API void nkg_graph_destroy(nkg_graph *g);
 NKG_API int nkg_graph_get_info(const nkg_graph *g, nkg_graph_info *info);
 

@@ -188,6 +188,11 @@ SIGNATURES = {
                                 C.c_uint64, _u64p, _u64p, C.POINTER(LocalStats)]),
     "nkg_local_support": (C.c_int, [_vp, _u32p, _f64p]),
     "nkg_local_sets": (C.c_int, [_vp, _u32p]),
+    "nkg_graph_create_from_nkbg": (C.c_int, [C.POINTER(_vp), _vp, C.c_uint64, C.c_int,
+                                             C.POINTER(GraphOptions), _f64p]),
+    "nkg_nkbg_decode": (C.c_int, [_vp, C.c_uint64, C.c_int, C.c_int, _u64p, _u64p,
+                                  C.POINTER(C.c_int), C.POINTER(C.c_int), _u64p, _u32p, _f64p,
+                                  _f64p, _u32p, _u8p, _f64p]),
     "nkg_part_create": (C.c_int, [C.POINTER(_vp), C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
                                   _u64p, _u32p, _f64p, _u32p, _f64p, C.c_int]),
     "nkg_part_destroy": (None, [_vp]),
@@ -280,6 +285,34 @@ class DeviceGraph:
         return cls._from_edge_pointers(
             z, int(s.shape[0]), s.ctypes.data, d.ctypes.data, 0 if ww is None else ww.ctypes.data,
             0 if ex is None else ex.ctypes.data, directed, False, device, sweep_shape, row_order)
+
+    @classmethod
+    def from_nkbg(cls, data, device: int = -1, row_order: int = -1, on_device: bool = False,
+                  size: int = 0):
+        """Build the graph from a NetworkitBinaryGraph file's bytes, decoded on
+        the device (nkg_graph_create_from_nkbg): `data` is a bytes-like host
+        buffer, or with on_device a device pointer of `size` bytes. The decode's
+        device time is in .ms_decode."""
+        self = cls.__new__(cls)
+        h = _vp()
+        opts = GraphOptions()
+        opts.device = int(device)
+        opts.row_order = int(row_order)
+        ms = C.c_double(0.0)
+        if on_device:
+            buf, nbytes, flags = _vp(int(data)), int(size), NKG_DEVICE_PTRS
+        else:
+            arr = np.frombuffer(data, np.uint8) if not isinstance(data, np.ndarray) else data
+            arr = np.ascontiguousarray(arr, np.uint8)
+            buf, nbytes, flags = _vp(arr.ctypes.data), int(arr.shape[0]), 0
+        check(lib().nkg_graph_create_from_nkbg(C.byref(h), buf, nbytes, flags, C.byref(opts),
+                                               C.byref(ms)))
+        self.h = h
+        info = self.info()
+        self.z = int(info["z"])
+        self.n = int(info["n"])
+        self.ms_decode = float(ms.value)
+        return self
 
     @classmethod
     def from_device_edges(cls, z, m, src_ptr, dst_ptr, w_ptr=0, exists_ptr=0, directed=False,

@@ -29,7 +29,7 @@ GPU_LIB = os.path.join(LIBDIR, "libnkgpu.so")
 GEN_LIB = os.path.join(LIBDIR, "libnkgen.so")
 
 GPU_SOURCES = ["nkgpu.cu", "noalloc.cu", "ppr.cu", "adjoint.cu", "batch.cu", "centrality.cu",
-               "local.cu", "part.cu"]
+               "local.cu", "part.cu", "nkbg.cu"]
 GPU_HEADERS = ["common.cuh", "sweep.cuh", "refine.cuh", "graph.hpp", "host.hpp"]
 GEN_SOURCES = ["graphgen.cpp", "graphio.cpp"]
 

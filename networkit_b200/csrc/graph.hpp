@@ -148,6 +148,17 @@ inline void check_cancel(const nkg_graph *g, const char *what) {
         throw Error(NKG_ERR_CANCELLED, what);
 }
 
+// A graph from an in-CSR already in device memory (nkgpu.cu): the shell on the
+// options' device (its stream is the one to build on), then the regular upload
+// steps from the device arrays (host copy of the existence mask, nullable).
+std::unique_ptr<nkg_graph> device_graph_shell(const nkg_graph_options *opt, uint64_t z,
+                                              bool weighted, int directed);
+nkg_graph *device_graph_build(std::unique_ptr<nkg_graph> g, uint64_t arcs,
+                              DeviceArray<uint64_t> &d_ptr, DeviceArray<uint32_t> &d_col,
+                              DeviceArray<double> &d_w, DeviceArray<double> &d_wdeg,
+                              DeviceArray<uint8_t> &d_ex, const uint8_t *exists_host,
+                              const nkg_graph_options *opt);
+
 // Most sweeps whose residual a run records for nkg_stats.residual_trace.
 constexpr uint32_t kTraceCapacity = 65536;
 

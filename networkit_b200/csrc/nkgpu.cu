@@ -1177,6 +1177,27 @@ static nkg_graph *create_from_edges(uint64_t z, uint64_t m, const uint32_t *src,
     return build_graph(std::move(g0), d_ptr, d_col, d_w, d_wdeg, d_ex, exh, opt);
 }
 
+// Graph creation from an in-CSR another translation unit built on the device
+// (the NetworkitBinaryGraph decoder, nkbg.cu): a shell on `device` whose
+// stream the builder uses, then the regular validation, relabelling and
+// layout of build_graph once z and arcs are known.
+std::unique_ptr<nkg_graph> device_graph_shell(const nkg_graph_options *opt, uint64_t z,
+                                              bool weighted, int directed) {
+    DeviceGuard guard(option_device(opt));
+    return graph_shell(option_device(opt), z, 0, weighted, directed);
+}
+
+nkg_graph *device_graph_build(std::unique_ptr<nkg_graph> g, uint64_t arcs,
+                              DeviceArray<uint64_t> &d_ptr, DeviceArray<uint32_t> &d_col,
+                              DeviceArray<double> &d_w, DeviceArray<double> &d_wdeg,
+                              DeviceArray<uint8_t> &d_ex, const uint8_t *exists_host,
+                              const nkg_graph_options *opt) {
+    DeviceGuard guard(g->device);
+    g->arcs = arcs;
+    NKG_CUDA(cudaEventRecord(g->ev0, g->stream));
+    return build_graph(std::move(g), d_ptr, d_col, d_w, d_wdeg, d_ex, exists_host, opt);
+}
+
 static void destroy_plane_graphs(nkg_graph *g) {
     for (int i = 0; i < 2; ++i) {
         if (g->p64.exec[i])

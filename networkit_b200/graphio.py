@@ -65,6 +65,41 @@ def _array(ptr, n, dtype):
     return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
 
 
+def decode_nkbg_device(data, device: int = -1):
+    """Decode a NetworkitBinaryGraph file's bytes on the GPU (nkg_nkbg_decode)
+    into an :class:`InCSR` on the host: the same arrays :func:`read_nkbg`
+    returns, from the device decoder (used to check one against the other).
+    Returns (csr, device milliseconds of the decode)."""
+    from . import _capi
+
+    arr = np.ascontiguousarray(np.frombuffer(data, np.uint8) if not isinstance(data, np.ndarray)
+                               else data, np.uint8)
+    L = _capi.lib()
+    z, m = C.c_uint64(0), C.c_uint64(0)
+    d, wt = C.c_int(0), C.c_int(0)
+    ms = C.c_double(0.0)
+    buf = C.c_void_p(arr.ctypes.data)
+    _capi.check(L.nkg_nkbg_decode(buf, arr.shape[0], 0, int(device), C.byref(z), C.byref(m),
+                                  C.byref(d), C.byref(wt), None, None, None, None, None, None,
+                                  None))
+    z, m = int(z.value), int(m.value)
+    in_ptr = np.empty(z + 1, np.uint64)
+    in_col = np.empty(max(m, 1), np.uint32)
+    w = np.empty(max(m, 1), np.float64) if wt.value else None
+    wdeg = np.empty(z, np.float64)
+    outdeg = np.empty(z, np.uint32)
+    ex = np.empty(z, np.uint8)
+    p = lambda a, t: None if a is None else a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    _capi.check(L.nkg_nkbg_decode(buf, arr.shape[0], 0, int(device), None, None, None, None,
+                                  p(in_ptr, C.c_uint64), p(in_col, C.c_uint32),
+                                  p(w, C.c_double), p(wdeg, C.c_double), p(outdeg, C.c_uint32),
+                                  p(ex, C.c_uint8), C.byref(ms)))
+    exists = None if ex.all() else ex
+    csr = InCSR(z, int(ex.sum()), in_ptr, in_col[:m], None if w is None else w[:m], wdeg,
+                outdeg, exists, bool(d.value))
+    return csr, float(ms.value)
+
+
 def read_nkbg(path: str, nthreads: int = 0) -> InCSR:
     """Decode a NetworkitBinaryGraph file into an :class:`InCSR`.
 
