@@ -83,6 +83,70 @@ __host__ __device__ inline SegMap identity_map() {
     return r;
 }
 
+__host__ __device__ inline SegMap compose(const SegMap &a, const SegMap &b) {
+    return ComposeMaps()(a, b);
+}
+
+// Exclusive scan of n segment maps (composition: earlier then later), in
+// three launches: every block scans kScanItems consecutive maps (each thread
+// composes kScanPer of them in order, the block combines the thread totals in
+// shared memory), one thread scans the block totals, every map then takes its
+// block's prefix. Reads and writes stay below n and below the block count.
+constexpr int kScanThreads = 256;
+constexpr int kScanPer = 8;
+constexpr uint64_t kScanItems = static_cast<uint64_t>(kScanThreads) * kScanPer;
+
+__global__ void __launch_bounds__(kScanThreads)
+    maps_block_scan(const SegMap *__restrict__ in, uint64_t n, SegMap *__restrict__ out,
+                    SegMap *__restrict__ block_total) {
+    __shared__ SegMap sm[kScanThreads];
+    const uint64_t b0 = static_cast<uint64_t>(blockIdx.x) * kScanItems;
+    const uint64_t t0 = b0 + static_cast<uint64_t>(threadIdx.x) * kScanPer;
+    SegMap acc = identity_map();
+    for (int i = 0; i < kScanPer; ++i)
+        if (t0 + i < n)
+            acc = compose(acc, in[t0 + i]);
+    sm[threadIdx.x] = acc;
+    __syncthreads();
+    for (int off = 1; off < kScanThreads; off <<= 1) {
+        const SegMap mine = sm[threadIdx.x];
+        SegMap v = mine;
+        if (threadIdx.x >= off)
+            v = compose(sm[threadIdx.x - off], mine);
+        __syncthreads();
+        sm[threadIdx.x] = v;
+        __syncthreads();
+    }
+    // sm[t] is now the inclusive total of threads 0..t.
+    SegMap run = threadIdx.x ? sm[threadIdx.x - 1] : identity_map();
+    for (int i = 0; i < kScanPer; ++i)
+        if (t0 + i < n) {
+            out[t0 + i] = run;
+            run = compose(run, in[t0 + i]);
+        }
+    if (threadIdx.x == kScanThreads - 1)
+        block_total[blockIdx.x] = sm[kScanThreads - 1];
+}
+
+// Exclusive prefix of the block totals, in place (one thread).
+__global__ void maps_total_scan(SegMap *__restrict__ total, uint64_t blocks) {
+    if (blockIdx.x != 0 || threadIdx.x != 0)
+        return;
+    SegMap run = identity_map();
+    for (uint64_t b = 0; b < blocks; ++b) {
+        const SegMap t = total[b];
+        total[b] = run;
+        run = compose(run, t);
+    }
+}
+
+__global__ void maps_apply(SegMap *__restrict__ out, uint64_t n,
+                           const SegMap *__restrict__ block_prefix) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i < n)
+        out[i] = compose(block_prefix[i / kScanItems], out[i]);
+}
+
 __device__ __forceinline__ uint32_t varint_bytes(uint8_t first) {
     return first == 0 ? 9u : static_cast<uint32_t>(__ffs(first));
 }
@@ -509,13 +573,13 @@ void decode_stream(const uint8_t *d_file, uint64_t begin, uint64_t end,
     S.prefix.alloc(S.segs);
     seg_maps<<<ceil_div(S.segs, 256), 256, 0, s>>>(d_file, begin, end, S.segs, maps.get());
     NKG_CUDA(cudaGetLastError());
-    size_t tb = 0;
-    NKG_CUDA(cub::DeviceScan::ExclusiveScan(nullptr, tb, maps.get(), S.prefix.get(), ComposeMaps(),
-                                            identity_map(), static_cast<int64_t>(S.segs), s));
-    DeviceArray<unsigned char> tmp(std::max<size_t>(tb, 1));
-    NKG_CUDA(cub::DeviceScan::ExclusiveScan(tmp.get(), tb, maps.get(), S.prefix.get(),
-                                            ComposeMaps(), identity_map(),
-                                            static_cast<int64_t>(S.segs), s));
+    const uint64_t blocks = (S.segs + kScanItems - 1) / kScanItems;
+    DeviceArray<SegMap> totals(blocks);
+    maps_block_scan<<<static_cast<unsigned>(blocks), kScanThreads, 0, s>>>(
+        maps.get(), S.segs, S.prefix.get(), totals.get());
+    maps_total_scan<<<1, 32, 0, s>>>(totals.get(), blocks);
+    maps_apply<<<ceil_div(S.segs, 256), 256, 0, s>>>(S.prefix.get(), S.segs, totals.get());
+    NKG_CUDA(cudaGetLastError());
     SegMap last, lastp;
     NKG_CUDA(cudaMemcpyAsync(&last, maps.get() + S.segs - 1, sizeof(SegMap),
                              cudaMemcpyDeviceToHost, s));
