@@ -48,7 +48,7 @@ def check(oracle_mod, gs, offs, scores, its, prec, norm, tol, distribute, normal
             assert err <= 1e-10 * scale, (i, err)
             assert abs(int(its[i]) - o.iterations) <= 1, (i, its[i], o.iterations)
         else:
-            assert err <= 2e-6 * scale, (i, err)
+            assert err <= 1e-6 * scale, (i, err)  # the companion forms' bar
 
 
 @pytest.mark.parametrize("shape", [(1, 128, 4, 0), (2, 256, 32, 1), (4, 512, 128, 2), (8, 256, 1024, 3),

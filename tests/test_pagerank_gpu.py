@@ -295,3 +295,24 @@ def test_row_order_relabelling(oracle_mod, row_order):
         s32, _, _, _ = dg.run(p32)
         assert np.abs(s32 - o.scores).sum() <= 1e-9
         dg.close()
+
+
+def test_rmat20_matches_the_reference_library(oracle_mod):
+    """The benchmark's kind of graph at scale 20 against the reference's own
+    PageRank::run() (oracle/_ref, all host cores), not only the C
+    restatement: L1 <= 1e-10, iterations within 1, ranking identical apart
+    from ties (the reference's ranking comes from its Centrality::ranking)."""
+    import os
+
+    if not oracle_mod.ref_available():
+        pytest.skip("the reference library (oracle/_ref) is not built")
+    csr = generators.rmat_directed(20, 16, seed=42)
+    rows = np.repeat(np.arange(csr.z, dtype=np.uint32), np.diff(csr.in_ptr).astype(np.int64))
+    rg = oracle_mod.RefGraph.from_edges(csr.z, csr.in_col, rows, directed=True)
+    r = rg.pagerank(damp=0.85, tol=1e-10, norm=0, nthreads=os.cpu_count() or 1,
+                    want_ranking=True)
+    dg, s, it, _, _ = gpu_run(csr, tol=1e-10, norm=0)
+    assert np.abs(s - r["scores"]).sum() <= L1_FP64
+    assert abs(it - r["iterations"]) <= 1
+    ids, _ = dg.ranking(s)
+    assert_ranking_equal(ids, r["ranking_ids"], s)

@@ -1,12 +1,14 @@
 """Batched personalised PageRank (FP32 SpMM, one column per seed) against the
 oracle's FP64 PageRank with the matching one-hot teleport. FP32 bar: L1 per
-column <= 2e-5 at tol 1e-7 (the FP32 rounding floor of a unit-mass vector)."""
+column <= 1e-6 at tol 1e-7, the companion forms' bar."""
 import numpy as np
 import pytest
 
 from networkit_b200 import _capi, generators
 
 pytestmark = pytest.mark.gpu
+
+L1_FP32 = 1e-6
 
 
 def one_hot(z, s):
@@ -32,7 +34,7 @@ def test_ppr_columns_match_oracle(oracle_mod, graph):
     for j in range(0, k, 7):
         o = oracle_mod.pagerank(csr, tol=1e-12, norm=0, distribute_sinks=distribute,
                                 teleport=one_hot(csr.z, seeds[j]))
-        assert np.abs(scores[j].astype(np.float64) - o.scores).sum() <= 2e-5, j
+        assert np.abs(scores[j].astype(np.float64) - o.scores).sum() <= L1_FP32, j
         assert 1 <= its[j] <= 300
     assert st["kernel_launches"] > 0 and st["fp32_sweeps"] >= its.max()
 
@@ -53,7 +55,7 @@ def test_ppr_256_columns_and_device_output(oracle_mod):
     np.testing.assert_array_equal(its, its2)
     for j in (0, 100, 255):
         o = oracle_mod.pagerank(csr, tol=1e-12, norm=0, teleport=one_hot(csr.z, seeds[j]))
-        assert np.abs(host[j].astype(np.float64) - o.scores).sum() <= 2e-5
+        assert np.abs(host[j].astype(np.float64) - o.scores).sum() <= L1_FP32
 
 
 def test_ppr_rejects_bad_input():
