@@ -357,12 +357,30 @@ def form_ppr(local, n=4_000_000, m=8, k=256, steps=2, oracle_columns=2, step_onl
             "ms_per_sweep": per_sweep_ms,
             "gteps_per_iter": csr.arcs * k / (per_sweep_ms / 1e3) / 1e9,
             "alg_bytes_per_sweep": bytes_sweep,
-            "alg_gbs": bytes_sweep / (per_sweep_ms / 1e3) / 1e9, "gpu_launches": launches}
+            "alg_gbs": bytes_sweep / (per_sweep_ms / 1e3) / 1e9, "gpu_launches": launches,
+            "roofline": ppr_roofline(csr, k, per_sweep_ms)}
 
 
 def err_vs(s, ref):
     d = np.abs(np.asarray(s, np.float64) - ref)
     return float(d.sum()), float((d / np.maximum(np.abs(ref), 1e-300)).max())
+
+
+def ppr_roofline(csr, k, ms_per_sweep):
+    """Roofline of the PPR SpMM on its real traffic. The iterate (n x k FP32)
+    is far larger than L2, so every arc gathers its source's k-column row:
+    per sweep 4 arcs (columns) + 4 k arcs (gathered rows) + 8 n k (own row
+    read, new row written) bytes. `traffic` is the ncu DRAM figure of the
+    committed BA 1M capture (profiles/ppr_sweep_ba1m_k256.txt) scaled by the
+    arc count (the traffic grows with the arcs: about 1 KB per arc there)."""
+    peak, kind = measured_peak_hbm()
+    model = 4 * csr.arcs + 4 * k * csr.arcs + 8 * csr.z * k
+    achieved = model / (ms_per_sweep / 1e3) / 1e9
+    t1m = profiled_traffic("ppr_sweep_ba1m_k256")
+    traffic = t1m * csr.arcs / 15_999_888 if t1m else None
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "model_bytes_per_sweep": model,
+            "peak_source": kind}
 
 
 def form_refine(local, csr, steps=2, checker=None, checker_kind=None):
