@@ -1,6 +1,7 @@
 """Batched personalised PageRank (FP32 SpMM, one column per seed) against the
 oracle's FP64 PageRank with the matching one-hot teleport. FP32 bar: L1 per
-column <= 1e-6 at tol 1e-7, the companion forms' bar."""
+column <= 1e-6, the companion forms' bar (tol 1e-7 per column, 1e-8 where
+the graph leaks mass into sinks)."""
 import numpy as np
 import pytest
 
@@ -28,7 +29,12 @@ def test_ppr_columns_match_oracle(oracle_mod, graph):
     k = 40
     seeds = rng.choice(csr.z, k, replace=False).astype(np.uint32)
     dg = _capi.DeviceGraph(csr)
-    p = dg.params(0.85, 1e-7, 0, False, distribute, _capi.NKG_PREC_FP32, 300)
+    # With the reference's sink semantics a directed graph's column leaks mass
+    # into its sinks, and the final division by the column's sum magnifies
+    # the truncation error the stopping test leaves (about tol / ((1 - d) x
+    # the mass kept)): that case stops at a tighter per-column tol.
+    tol = 1e-8 if graph == "rmat" else 1e-7
+    p = dg.params(0.85, tol, 0, False, distribute, _capi.NKG_PREC_FP32, 300)
     scores, its, st = dg.ppr(seeds, p)
     assert scores.shape == (k, csr.z)
     for j in range(0, k, 7):
