@@ -1375,46 +1375,12 @@ static void launch_sweep_kernel(nkg_graph *g, const SweepArgs<T> &a, cudaStream_
     });
 }
 
-// A launch with programmatic dependent launch allowed: in a captured run the
-// kernel may be scheduled while the previous one finishes (both sides use
-// pdl_wait_and_release, sweep.cuh).
-template <typename... KArgs, typename... Args>
-static void launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem,
-                       cudaStream_t s, Args... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    NKG_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
-}
-
-// One Jacobi sweep of a captured run: sweep + fix-up, chained by programmatic
-// dependent launch.
 template <typename T, bool WEIGHTED>
 static void launch_sweep(nkg_graph *g, int in_buf, cudaStream_t s) {
     Plane<T> &P = plane<T>(g);
     const SweepArgs<T> a = sweep_args<T, WEIGHTED>(g, in_buf);
-    if (P.hot) {
-        if (P.hot_threads == kHotThreadsPair)
-            launch_pdl(sweep_kernel<T, WEIGHTED, kHotThreadsPair, kHotUnroll, true>, P.hot_ctas,
-                       kHotThreadsPair, P.hot * sizeof(T), s, a);
-        else
-            launch_pdl(sweep_kernel<T, WEIGHTED, kHotThreads, kHotUnroll, true>, P.hot_ctas,
-                       kHotThreads, P.hot * sizeof(T), s, a);
-    } else {
-        with_sweep_shape(g->sweep_shape, [&](auto S) {
-            using Sh = decltype(S);
-            launch_pdl(sweep_kernel<T, WEIGHTED, Sh::threads, Sh::unroll>, P.sweep_ctas,
-                       Sh::threads, 0, s, a);
-        });
-    }
-    launch_pdl(fixup_kernel<T, WEIGHTED>, P.fix_ctas, kFixThreads, 0, s, a);
+    launch_sweep_kernel<T, WEIGHTED>(g, a, s);
+    fixup_kernel<T, WEIGHTED><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
 }
 
 // Capture kSweepsPerGraph sweeps (sweep + fix-up each) as one CUDA graph.

@@ -140,19 +140,6 @@ __device__ __forceinline__ void finish_row(const SweepArgs<T> &a, const RunParam
     }
 }
 
-// Programmatic dependent launch (the sweep and fix-up launches of a captured
-// run): wait until the grid this one depends on has finished and its writes
-// are visible, then let the next grid be scheduled while this one runs (it
-// waits in turn). Both are no-ops for a grid launched without the attribute.
-// Every grid of the chain fits on the GPU at once (the sweep is one wave of
-// persistent CTAs, the fix-up at most one wave), and a dependent grid starts
-// only once every CTA of its predecessor has issued launch_dependents, so an
-// early-scheduled grid cannot hold back the one it waits for.
-__device__ __forceinline__ void pdl_wait_and_release() {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 // Per-run constants read where a row is finished. The volatile asm keeps each
 // load at its use, so the values are not hoisted into registers held across
 // the gather loop.
@@ -258,7 +245,6 @@ __global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T)
     __shared__ double s_red[32];
     extern __shared__ __align__(16) unsigned char s_dyn[];
     T *s_y = reinterpret_cast<T *>(s_dyn);
-    pdl_wait_and_release();
     if (*(volatile int *)&a.st->done)
         return;
     if (HOT) {
@@ -401,7 +387,6 @@ template <typename T, bool WEIGHTED, bool PART = false>
 __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
     __shared__ double s_red[32];
     __shared__ bool s_last;
-    pdl_wait_and_release();
     if (*(volatile int *)&a.st->done)
         return;
     const RunParams rp = *a.rp;
