@@ -128,15 +128,29 @@ __global__ void __launch_bounds__(kScanThreads)
         block_total[blockIdx.x] = sm[kScanThreads - 1];
 }
 
-// Exclusive prefix of the block totals, in place (one thread).
-__global__ void maps_total_scan(SegMap *__restrict__ total, uint64_t blocks) {
-    if (blockIdx.x != 0 || threadIdx.x != 0)
-        return;
-    SegMap run = identity_map();
-    for (uint64_t b = 0; b < blocks; ++b) {
-        const SegMap t = total[b];
-        total[b] = run;
-        run = compose(run, t);
+// Exclusive prefix of the block totals, in place: one block stages tiles of
+// kScanThreads totals in shared memory, its first thread composes them in order.
+__global__ void __launch_bounds__(kScanThreads) maps_total_scan(SegMap *__restrict__ total,
+                                                               uint64_t blocks) {
+    __shared__ SegMap tile[kScanThreads];
+    SegMap run = identity_map();  // meaningful in thread 0
+    for (uint64_t t0 = 0; t0 < blocks; t0 += kScanThreads) {
+        const uint64_t b = t0 + threadIdx.x;
+        if (b < blocks)
+            tile[threadIdx.x] = total[b];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const uint64_t m = blocks - t0 < kScanThreads ? blocks - t0 : kScanThreads;
+            for (uint64_t i = 0; i < m; ++i) {
+                const SegMap t = tile[i];
+                tile[i] = run;
+                run = compose(run, t);
+            }
+        }
+        __syncthreads();
+        if (b < blocks)
+            total[b] = tile[threadIdx.x];
+        __syncthreads();
     }
 }
 
@@ -248,60 +262,103 @@ __global__ void chunk_index(const uint8_t *__restrict__ file, uint64_t begin,
     chunk_base[c] = k;
 }
 
-// One CTA per chunk walks the chunk's list lengths: node first_c + j has its
-// length at index hdr[first_c + j] of vals, the next length follows its
-// entries. The walking thread reads vals through a shared-memory window that
-// the whole CTA fills. Marks every length in is_hdr; err = 2 when a walk
+// One CTA per chunk and list stream walks the chunk's list lengths: node
+// first_c + j has its length at index hdr[first_c + j] of vals, the next length
+// follows its entries. The walk reads vals through a shared-memory window that
+// the whole CTA fills with 16-byte loads, and records the lengths' indices in a
+// shared list that the whole CTA then writes out (hdr, and the is_hdr marks),
+// so the walking thread's steps touch shared memory only. CTAs
+// [0, chunks) walk stream 0, [chunks, 2 chunks) stream 1. err = 2 when a walk
 // leaves the stream or a length does not fit.
-constexpr uint32_t kWin = 24576;  // 96 KB of dynamic shared memory
+constexpr uint32_t kWin = 24576;  // window and list: 2 x 96 KB of dynamic shared memory
 constexpr int kWalkThreads = 256;
 
+struct WalkStream {
+    const uint32_t *vals;  // K values
+    uint64_t K;
+    const uint64_t *chunk_base;
+    uint32_t *hdr;
+    uint8_t *is_hdr;
+    uint64_t *chunk_end;
+};
+
 __global__ void __launch_bounds__(kWalkThreads)
-    walk_headers(const uint32_t *__restrict__ vals, uint64_t K,
-                 const uint64_t *__restrict__ chunk_base, const uint64_t *__restrict__ first,
-                 uint32_t *__restrict__ hdr, uint8_t *__restrict__ is_hdr,
-                 uint64_t *__restrict__ chunk_end, int *err) {
-    extern __shared__ uint32_t win[];
+    walk_headers(WalkStream s0, WalkStream s1, uint32_t chunks, const uint64_t *__restrict__ first,
+                 int *err) {
+    extern __shared__ uint4 s_dyn4[];
+    uint32_t *win = reinterpret_cast<uint32_t *>(s_dyn4);
+    uint32_t *hl = win + kWin;
     __shared__ uint64_t s_h, s_j;
+    __shared__ uint32_t s_cnt;
     __shared__ int s_bad;
-    const uint32_t c = blockIdx.x;
+    const WalkStream &S = blockIdx.x < chunks ? s0 : s1;
+    const uint32_t c = blockIdx.x < chunks ? blockIdx.x : blockIdx.x - chunks;
     const uint64_t nodes = first[c + 1] - first[c];
-    uint64_t h = chunk_base[c], j = 0;
+    const uint64_t K = S.K;
+    uint64_t h = S.chunk_base[c], j = 0;
     if (threadIdx.x == 0)
         s_bad = 0;
     __syncthreads();
     while (j < nodes) {
-        const uint64_t ws = h;
-        for (uint32_t i = threadIdx.x; i < kWin; i += kWalkThreads)
-            win[i] = ws + i < K ? vals[ws + i] : kBad;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint64_t hh = h, jj = j;
-            while (jj < nodes && hh < ws + kWin) {
-                if (hh >= K) {
-                    s_bad = 1;
-                    break;
+        const uint64_t ws = h & ~3ull;  // 16-byte aligned start (vals is 256-byte aligned)
+        const uint4 *src = reinterpret_cast<const uint4 *>(S.vals + ws);
+        uint4 *dst = reinterpret_cast<uint4 *>(win);
+        if (ws + kWin <= K) {  // asynchronous 16-byte copies, all in flight at once
+            const uint32_t d0 = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+            for (uint32_t i = threadIdx.x; i < kWin / 4; i += kWalkThreads)
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d0 + 16 * i),
+                             "l"(src + i)
+                             : "memory");
+            asm volatile("cp.async.wait_all;\n" ::: "memory");
+        } else {
+            for (uint32_t i = threadIdx.x; i < kWin / 4; i += kWalkThreads) {
+                const uint64_t idx = ws + 4ull * i;  // entries at K and beyond read as kBad
+                if (idx + 4 <= K) {
+                    dst[i] = src[i];
+                } else {
+                    uint32_t *d = win + 4 * i;
+                    for (uint32_t e = 0; e < 4; ++e)
+                        d[e] = idx + e < K ? S.vals[idx + e] : kBad;
                 }
-                const uint32_t len = win[hh - ws];
-                if (len == kBad || hh + 1 + static_cast<uint64_t>(len) > K) {
-                    s_bad = 1;
-                    break;
-                }
-                hdr[first[c] + jj] = static_cast<uint32_t>(hh);
-                is_hdr[hh] = 1;
-                hh += 1 + static_cast<uint64_t>(len);
-                ++jj;
             }
-            s_h = hh;
-            s_j = s_bad ? nodes : jj;
         }
         __syncthreads();
+        if (threadIdx.x == 0) {
+            // The walk keeps 32-bit offsets into the window; a step is clamped
+            // to 2^31, which leaves the window, and the exact position after
+            // the last list is worked out once from that list's length. A
+            // length of kBad (an entry at K or beyond) puts it past K, so one
+            // test catches that and any list that ends past K.
+            const uint32_t lim = nodes - j < kWin ? static_cast<uint32_t>(nodes - j) : kWin;
+            uint32_t p = static_cast<uint32_t>(h - ws), cnt = 0;
+            while (cnt < lim && p < kWin) {
+                const uint32_t len = win[p];
+                hl[cnt++] = p;
+                p += 1u + (len < 0x7fffffffu ? len : 0x7fffffffu);
+            }
+            const uint32_t last = hl[cnt - 1];  // cnt >= 1: the first step starts inside
+            const uint64_t hh = ws + last + 1 + static_cast<uint64_t>(win[last]);
+            const bool bad = hh > K;
+            if (bad)
+                s_bad = 1;
+            s_h = hh;
+            s_j = bad ? nodes : j + cnt;
+            s_cnt = bad ? 0 : cnt;  // a failed walk writes nothing
+        }
+        __syncthreads();
+        const uint32_t cnt = s_cnt;
+        const uint64_t out0 = first[c] + j;
+        for (uint32_t i = threadIdx.x; i < cnt; i += kWalkThreads) {
+            const uint32_t hi = static_cast<uint32_t>(ws + hl[i]);
+            S.hdr[out0 + i] = hi;
+            S.is_hdr[hi] = 1;
+        }
         h = s_h;
         j = s_j;
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        chunk_end[c] = h;
+        S.chunk_end[c] = h;
         if (s_bad)
             atomicExch(err, 2);
     }
@@ -577,7 +634,7 @@ void decode_stream(const uint8_t *d_file, uint64_t begin, uint64_t end,
     DeviceArray<SegMap> totals(blocks);
     maps_block_scan<<<static_cast<unsigned>(blocks), kScanThreads, 0, s>>>(
         maps.get(), S.segs, S.prefix.get(), totals.get());
-    maps_total_scan<<<1, 32, 0, s>>>(totals.get(), blocks);
+    maps_total_scan<<<1, kScanThreads, 0, s>>>(totals.get(), blocks);
     maps_apply<<<ceil_div(S.segs, 256), 256, 0, s>>>(S.prefix.get(), S.segs, totals.get());
     NKG_CUDA(cudaGetLastError());
     SegMap last, lastp;
@@ -726,14 +783,17 @@ void decode_nkbg(const uint8_t *file_any, uint64_t size, bool on_device, int dev
     DeviceArray<uint8_t> ia(std::max<uint64_t>(A.K, 1)), it(std::max<uint64_t>(T.K, 1));
     NKG_CUDA(cudaMemsetAsync(ia.get(), 0, std::max<uint64_t>(A.K, 1), s));
     NKG_CUDA(cudaMemsetAsync(it.get(), 0, std::max<uint64_t>(T.K, 1), s));
-    NKG_CUDA(cudaFuncSetAttribute(walk_headers, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(kWin * sizeof(uint32_t))));
-    walk_headers<<<static_cast<unsigned>(chunks), kWalkThreads, kWin * sizeof(uint32_t), s>>>(
-        A.vals.get(), A.K, A.chunk_base.get(), d_first.get(), ha.get(), ia.get(), cend_a.get(),
-        d_err.get());
-    walk_headers<<<static_cast<unsigned>(chunks), kWalkThreads, kWin * sizeof(uint32_t), s>>>(
-        T.vals.get(), T.K, T.chunk_base.get(), d_first.get(), ht.get(), it.get(), cend_t.get(),
-        d_err.get());
+    {
+        const size_t smem = 2 * kWin * sizeof(uint32_t);
+        NKG_CUDA(cudaFuncSetAttribute(walk_headers, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(smem)));
+        const WalkStream wa{A.vals.get(), A.K, A.chunk_base.get(), ha.get(), ia.get(),
+                            cend_a.get()};
+        const WalkStream wt{T.vals.get(), T.K, T.chunk_base.get(), ht.get(), it.get(),
+                            cend_t.get()};
+        walk_headers<<<2 * static_cast<unsigned>(chunks), kWalkThreads, smem, s>>>(
+            wa, wt, static_cast<uint32_t>(chunks), d_first.get(), d_err.get());
+    }
     NKG_CUDA(cudaGetLastError());
     require(read_scalar(d_err.get(), s) == 0, "truncated or inconsistent list data");
     // Inclusive prefixes of the length flags (as 32-bit counts).
