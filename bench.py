@@ -72,7 +72,7 @@ def parse_args():
                          "PageRank on the same graph")
     ap.add_argument("--form", default="",
                     choices=["", "ppr", "refine", "adjoint", "batch", "centrality", "local",
-                             "reader", "locality"],
+                             "reader", "locality", "er"],
                     help="run only one companion form and print its figures")
     ap.add_argument("--fd-edges", type=int, default=64,
                     help="arcs checked by finite differences in --form adjoint")
@@ -770,6 +770,68 @@ def centrality_vs_reference(local, scale=21):
     return out
 
 
+def form_er(local, n=100_000, avg_deg=10, seed=42, runs=5):
+    """PageRank FP64 on G(n = 1e5, average degree 10), undirected, the graph
+    the reference's ErdosRenyiGenerator draws from seed 42 (one thread,
+    setSeed(42, False); `generators.erdos_renyi_stream` draws the same
+    graph), damp 0.85, tol 1e-8, L2, not normalized. With distributeSinks,
+    as the workload asks: device time per run, iterations and L1 against the
+    oracle. Without (this reference has no sink redistribution): the same,
+    plus the reference's own PageRank::run() on the reference's own graph,
+    on all host cores, and the L1 between the two. Device runs are timed with
+    CUDA events (graph resident); `e2e_ms` is upload of the host in-CSR,
+    run and scores back, by the host clock."""
+    import torch
+
+    from networkit_b200 import _capi, generators
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    p = avg_deg / (n - 1)
+    csr = generators.erdos_renyi_stream(n, p, seed)
+    res = {"workload": "pagerank_er1e5_deg10_l2_fp64", "n": n, "arcs": int(csr.arcs),
+           "graph": "the reference generator's draw (seed 42, one thread)"}
+    for distribute in (True, False):
+        dg = _capi.DeviceGraph(csr, device=local)
+        prm = dg.params(0.85, 1e-8, 1, False, distribute, _capi.NKG_PREC_FP64, _capi.UINT64_MAX)
+        dg.run(prm)
+        best, s, it, st = float("inf"), None, 0, None
+        for _ in range(runs):
+            s, it, _, st = dg.run(prm)
+            best = min(best, st["ms_total"])
+        dg.close()
+        e2e = float("inf")
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            g2 = _capi.DeviceGraph(csr, device=local)
+            g2.run(g2.params(0.85, 1e-8, 1, False, distribute, _capi.NKG_PREC_FP64,
+                             _capi.UINT64_MAX))
+            e2e = min(e2e, (time.perf_counter() - t0) * 1e3)
+            g2.close()
+        o = oracle.pagerank(csr, tol=1e-8, norm=1, distribute_sinks=distribute,
+                            nthreads=os.cpu_count() or 1)
+        r = {"ms": best, "iterations": it, "e2e_ms": e2e, "gpu_launches": st["kernel_launches"],
+             "gteps_per_iter": csr.arcs * it / (best / 1e3) / 1e9,
+             "oracle_iterations": o.iterations,
+             "l1_vs_oracle": float(np.abs(s - o.scores).sum())}
+        if not distribute and oracle.ref_available():
+            cores = os.cpu_count() or 1
+            rg = oracle.RefGraph.erdos_renyi(n, p, seed, directed=False, threads=1)
+            ref = min((rg.pagerank(damp=0.85, tol=1e-8, normalized=False, norm=1,
+                                   nthreads=cores, want_ranking=False) for _ in range(3)),
+                      key=lambda x: x["seconds"])
+            r.update({"reference_ms": ref["seconds"] * 1e3, "reference_cores": cores,
+                      "reference_iterations": ref["iterations"],
+                      "l1_vs_reference": float(np.abs(s - ref["scores"]).sum()),
+                      "speedup_device": ref["seconds"] * 1e3 / best,
+                      "speedup_e2e": ref["seconds"] * 1e3 / e2e})
+            del rg
+        res["distribute_sinks" if distribute else "no_sink_redistribution"] = r
+    return res
+
+
 def form_locality(local, n=4_000_000, deg=16):
     """PageRank FP64 (tol 1e-10, L1) on an undirected threshold hyperbolic graph
     numbered by angle (as HyperbolicGenerator numbers its nodes): the sliced
@@ -1175,6 +1237,9 @@ def main():
     if args.form == "locality":
         print(json.dumps(form_locality(local)))
         return
+    if args.form == "er":
+        print(json.dumps(form_er(local)))
+        return
     if args.form == "local":
         print(json.dumps(form_local(local, n=args.local_n, seeds=args.local_seeds,
                                     ref_sample=args.local_ref_sample, runs=args.local_runs)))
@@ -1323,6 +1388,7 @@ def main():
                                                              checker=checker_scores,
                                                              checker_kind=parity and
                                                              parity["checker"])),
+                         ("er_config", lambda: form_er(local)),
                          ("ppr", lambda: form_ppr(local, steps=1)),
                          ("fwd_bwd", lambda: form_adjoint(local, steps=2, fd_edges=0)),
                          ("eigenvector_katz", lambda: form_centrality(local, csr)),

@@ -50,6 +50,8 @@ def _load():
                                  C.c_uint64, C.c_int, C.POINTER(_Csr)]
         L.nkgen_erdos_renyi.argtypes = [C.c_uint64, C.c_double, C.c_uint64, C.c_int,
                                         C.POINTER(_Csr)]
+        L.nkgen_erdos_renyi_stream.argtypes = [C.c_uint64, C.c_double, C.c_uint64, C.c_int,
+                                               C.POINTER(_Csr)]
         L.nkgen_barabasi_albert.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(_Csr)]
         L.nkgen_hyperbolic.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_uint64,
                                        C.POINTER(_Csr)]
@@ -90,6 +92,17 @@ def erdos_renyi(n: int, p: float, seed: int = 42, nthreads: int = 0) -> InCSR:
     out = _Csr()
     _check(_load().nkgen_erdos_renyi(int(n), float(p), int(seed), int(nthreads), C.byref(out)))
     return _take(out, False)
+
+
+def erdos_renyi_stream(n: int, p: float, seed: int = 42, directed: bool = False) -> InCSR:
+    """G(n, p) drawn as NetworKit's ErdosRenyiGenerator(n, p, directed) draws
+    it on one OpenMP thread after ``setSeed(seed, False)``: the same graph,
+    with the adjacency order of the Graph it builds (a single
+    std::mt19937_64 stream, so the result is sequential)."""
+    out = _Csr()
+    _check(_load().nkgen_erdos_renyi_stream(int(n), float(p), int(seed), int(bool(directed)),
+                                            C.byref(out)))
+    return _take(out, bool(directed))
 
 
 def barabasi_albert(k: int, n: int, seed: int = 42) -> InCSR:

@@ -131,6 +131,9 @@ def ref_lib():
         lib.nkref_write_nkbg.argtypes = [C.c_void_p, C.c_char_p, C.c_uint64, C.c_int]
         lib.nkref_read_nkbg.restype = C.c_int
         lib.nkref_read_nkbg.argtypes = [C.POINTER(C.c_void_p), C.c_char_p]
+        lib.nkref_erdos_renyi.restype = C.c_int
+        lib.nkref_erdos_renyi.argtypes = [C.POINTER(C.c_void_p), C.c_uint64, C.c_double,
+                                          C.c_uint64, C.c_int, C.c_int]
         lib.nkref_eigenvector.restype = C.c_int
         lib.nkref_eigenvector.argtypes = [C.c_void_p, C.c_double, C.c_int, _f64p, _f64p]
         lib.nkref_katz.restype = C.c_int
@@ -433,6 +436,17 @@ class RefGraph:
         lib = ref_lib()
         h = C.c_void_p()
         if lib.nkref_read_nkbg(C.byref(h), path.encode()) != 0:
+            raise RuntimeError(lib.nkref_last_error().decode())
+        return cls(h)
+
+    @classmethod
+    def erdos_renyi(cls, n, p, seed=42, directed=False, threads=1):
+        """The reference's ErdosRenyiGenerator(n, p, directed).generate() on
+        `threads` OpenMP threads after Aux::Random::setSeed(seed, False)."""
+        lib = ref_lib()
+        h = C.c_void_p()
+        if lib.nkref_erdos_renyi(C.byref(h), int(n), float(p), int(seed), int(bool(directed)),
+                                 int(threads)) != 0:
             raise RuntimeError(lib.nkref_last_error().decode())
         return cls(h)
 

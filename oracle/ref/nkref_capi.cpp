@@ -26,6 +26,8 @@
 #include <networkit/centrality/EigenvectorCentrality.hpp>
 #include <networkit/centrality/KatzCentrality.hpp>
 #include <networkit/centrality/PageRank.hpp>
+#include <networkit/auxiliary/Random.hpp>
+#include <networkit/generators/ErdosRenyiGenerator.hpp>
 #include <networkit/graph/Graph.hpp>
 #include <networkit/io/GMLGraphReader.hpp>
 #include <networkit/io/NetworkitBinaryReader.hpp>
@@ -71,6 +73,27 @@ int nkref_graph_create(void **out, uint64_t n, int weighted, int directed, uint6
         *out = h;
         return 0;
     } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// NetworKit::ErdosRenyiGenerator(n, p, directed).generate() run with
+// `threads` OpenMP threads after Aux::Random::setSeed(seed, false); the
+// previous thread count is restored afterwards.
+int nkref_erdos_renyi(void **out, uint64_t n, double p, uint64_t seed, int directed,
+                      int threads) {
+    const int prev = omp_get_max_threads();
+    try {
+        Aux::Random::setSeed(seed, false);
+        omp_set_num_threads(threads);
+        auto *rg = new RefGraph;
+        rg->G.reset(new NetworKit::Graph(
+            NetworKit::ErdosRenyiGenerator(n, p, directed != 0).generate()));
+        omp_set_num_threads(prev);
+        *out = rg;
+        return 0;
+    } catch (const std::exception &e) {
+        omp_set_num_threads(prev);
         return fail(e);
     }
 }

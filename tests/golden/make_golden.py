@@ -17,7 +17,9 @@ It also writes every graph with the reference's NetworkitBinaryWriter
 that file (keys ``nkbg_*``), plus one file per weight encoding of the format
 (``nkbg_<case>.nkbg``, ``nkbg_formats.npz``), and the reference's
 ApproximatePageRank and PageRankNibble results on the reference's SCD test
-graphs (``local_ppr.npz``). The GPU box has no
+graphs (``local_ppr.npz``), and the reference's Erdos-Renyi graph of the
+G(1e5, average degree 10) workload with the reference's PageRank on it
+(``er_config.npz``). The GPU box has no
 reference checkout: the tests read only these files.
 """
 from __future__ import annotations
@@ -127,6 +129,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **arrays, **res)
     nkbg_formats(O)
     local_ppr(O, inp)
+    er_config(O)
 
 
 # (alpha, epsilon, seeds) of the local PageRank fixtures. SelectiveCDGTest.cpp
@@ -232,6 +235,37 @@ def nkbg_formats(O):
         out.update({f"{name}_{k}": back[k] for k in NKBG_KEYS})
         print(f"nkbg_{name}: z={z} m={src.shape[0]} {os.path.getsize(path)} bytes")
     np.savez_compressed(os.path.join(HERE, "nkbg_formats.npz"), **out)
+
+
+# The Erdos-Renyi workload: G(n = 100000, average degree 10), undirected,
+# edges drawn from seed 42.
+ER_N, ER_P, ER_SEED = 100000, 10.0 / 99999.0, 42
+ER_SAMPLE = 97  # every 97th score is stored
+
+
+def er_config(O):
+    """The reference's ErdosRenyiGenerator(100000, 10 / 99999) graph, drawn
+    on one OpenMP thread after setSeed(42, False), and the reference's
+    PageRank on it (damp 0.85, tol 1e-8, L2, not normalized; this reference
+    has no sink redistribution) in ``er_config.npz``: SHA-256 digests of the
+    in-adjacency (row offsets as uint64, ids as uint32), the arc count, the
+    iteration count, maximum(), every ER_SAMPLE-th score and the first 100
+    ranking ids."""
+    import hashlib
+
+    g = O.RefGraph.erdos_renyi(ER_N, ER_P, ER_SEED, directed=False, threads=1)
+    a = export_to_arrays(g)
+    r = g.pagerank(damp=0.85, tol=1e-8, normalized=False, norm=1, nthreads=1)
+    out = dict(
+        n=np.int64(ER_N), p=np.float64(ER_P), seed=np.int64(ER_SEED),
+        arcs=np.int64(a["in_ptr"][-1]),
+        in_ptr_sha256=np.bytes_(hashlib.sha256(a["in_ptr"].tobytes()).hexdigest()),
+        in_col_sha256=np.bytes_(hashlib.sha256(a["in_col"].tobytes()).hexdigest()),
+        iterations=np.int64(r["iterations"]), maximum=np.float64(r["maximum"]),
+        sample_every=np.int64(ER_SAMPLE), scores_sample=r["scores"][::ER_SAMPLE].copy(),
+        rank_ids_top100=r["ranking_ids"][:100].astype(np.uint32))
+    np.savez_compressed(os.path.join(HERE, "er_config.npz"), **out)
+    print(f"er_config: arcs={int(out['arcs'])} it={r['iterations']} max={r['maximum']:.6g}")
 
 
 if __name__ == "__main__":

@@ -79,13 +79,28 @@ def test_rmat_parity_l1(oracle_mod, distribute, scale, arc_order, shape):
 
 
 def test_er_config_parity(oracle_mod):
-    """G(n=1e5, avg degree 10) undirected, L2 1e-8, distributeSinks."""
-    csr = generators.erdos_renyi(100000, 10 / 99999, seed=42)
+    """G(n=1e5, avg degree 10) undirected as the reference's generator draws
+    it from seed 42, L2 1e-8, with and without distributeSinks: against the
+    oracle, and (without, as this reference has no sink redistribution)
+    against the reference's own stored run on that graph
+    (tests/golden/er_config.npz): iterations within 1, every stored score
+    and the stored top-100 ranking."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "er_config.npz"))
+    csr = generators.erdos_renyi_stream(int(g["n"]), float(g["p"]), int(g["seed"]))
+    assert csr.in_ptr[-1] == int(g["arcs"])
     for distribute in (False, True):
         o = oracle_mod.pagerank(csr, tol=1e-8, norm=1, distribute_sinks=distribute)
         dg, s, it, mx, st = gpu_run(csr, tol=1e-8, norm=1, distribute=distribute)
         assert np.abs(s - o.scores).sum() <= L1_FP64
         assert abs(it - o.iterations) <= 1
+        if not distribute:
+            k = int(g["sample_every"])
+            assert abs(it - int(g["iterations"])) <= 1
+            assert np.abs(s[::k] - g["scores_sample"]).sum() <= L1_FP64
+            ids, _ = dg.ranking(s)
+            assert_ranking_equal(ids[:100], g["rank_ids_top100"], s)
 
 
 def test_weighted_parity(oracle_mod):
