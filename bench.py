@@ -273,8 +273,9 @@ def cpu_baseline_port(csr, nthreads, target_s=4.0, runs=3):
 
 
 def form_ppr(local, n=4_000_000, m=8, k=256, steps=2, oracle_columns=2, step_only=False):
-    """Batched personalised PageRank: Barabasi-Albert n=4M, m=8 (undirected),
-    256 one-hot seeds (uniform, seed 42), one FP32 SpMM with k = 256 columns,
+    """Batched personalised PageRank: Barabasi-Albert n=4M, m=8 (undirected;
+    the graph the reference's BarabasiAlbertGenerator draws after
+    setSeed(42, False), `generators.barabasi_albert_stream`), 256 one-hot seeds (uniform, seed 42), one FP32 SpMM with k = 256 columns,
     FP64 residual per column, damp 0.85, tol 1e-7 (L1). Errors: every 32nd
     column against the GPU's FP64 personalised run to tol 1e-12, and
     `oracle_columns` columns against the oracle (the CPU restatement of
@@ -284,7 +285,7 @@ def form_ppr(local, n=4_000_000, m=8, k=256, steps=2, oracle_columns=2, step_onl
 
     from networkit_b200 import _capi, generators
 
-    csr = generators.barabasi_albert(m, n, seed=42)
+    csr = generators.barabasi_albert_stream(m, n, seed=42)
     seeds = np.random.default_rng(42).choice(csr.z, k, replace=False).astype(np.uint32)
     dg = _capi.DeviceGraph(csr, device=local)
     p = dg.params(0.85, 1e-7, NORM_L1, False, False, _capi.NKG_PREC_FP32, 1000)
@@ -578,8 +579,9 @@ def form_adjoint(local, scale=22, steps=3, fd_edges=64, only_step=False, oracle_
 
 def form_batch(local, count=1024, steps=3, plain_graphs=None, step_only=False):
     """Many-graph batch: 1024 random hyperbolic graphs, n_i log-uniform in
-    [1e3, 2e5] (numpy seed 42), average degree 16, exponent 3, graph i from
-    seed 42 + i; FP32, damp 0.85, tol 1e-8 (L1), one persistent launch in a
+    [1e3, 2e5] (numpy seed 42), average degree 16, exponent 3, graph i the
+    one the reference's HyperbolicGenerator draws after setSeed(42 + i,
+    False) (`generators.hyperbolic_stream_batch`); FP32, damp 0.85, tol 1e-8 (L1), one persistent launch in a
     CUDA graph with the autotuned launch shape. Against it: the plain FP64
     path run graph by graph (nkg_pagerank_run_device on every graph, the
     graphs already resident), and the FP64 batch for the error figures (the
@@ -592,7 +594,7 @@ def form_batch(local, count=1024, steps=3, plain_graphs=None, step_only=False):
     rng = np.random.default_rng(42)
     ns = np.round(np.exp(rng.uniform(np.log(1e3), np.log(2e5), count))).astype(np.uint64)
     t0 = time.perf_counter()
-    csr, offs = generators.hyperbolic_batch(ns, 16.0, 3.0, seed=42)
+    csr, offs = generators.hyperbolic_stream_batch(ns, 16.0, 3.0, seed=42)
     t_gen = time.perf_counter() - t0
     t0 = time.perf_counter()
     db = _capi.DeviceBatch(csr, offs, device=local)
@@ -834,13 +836,14 @@ def form_er(local, n=100_000, avg_deg=10, seed=42, runs=5):
 
 def form_locality(local, n=4_000_000, deg=16):
     """PageRank FP64 (tol 1e-10, L1) on an undirected threshold hyperbolic graph
-    numbered by angle (as HyperbolicGenerator numbers its nodes): the sliced
+    numbered by angle (the graph the reference's HyperbolicGenerator draws
+    after setSeed(21, False), `generators.hyperbolic_stream`): the sliced
     layout with in-degree relabelling (row_order 0) against half-octave
     in-degree buckets that keep the id order inside a bucket (row_order 1,
     the automatic choice for this graph). Device time per run, graph resident."""
     from networkit_b200 import _capi, generators
 
-    g = generators.hyperbolic(n, deg, 3, seed=21)
+    g = generators.hyperbolic_stream(n, deg, 3, seed=21)
     res = {"workload": f"pagerank_hyperbolic{n}_deg{deg}_fp64", "n": g.z, "arcs": g.arcs}
     for ro in (0, 1, -1):
         dg = _capi.DeviceGraph(g, device=local, row_order=ro)
@@ -862,13 +865,14 @@ def form_local(local, n=1_000_000, deg=16, seeds=16384, alpha=0.1, eps=1e-5, ref
     """PageRankNibble(G, 0.1, 1e-5) (the SelectiveCDGTest.cpp parameters),
     one community per seed (SelectiveCommunityDetector::run) for `seeds`
     random seeds of an undirected threshold hyperbolic graph (n nodes,
-    average degree `deg`, exponent 3): device time, end-to-end time through
+    average degree `deg`, exponent 3; the reference HyperbolicGenerator's
+    draw after setSeed(11, False)): device time, end-to-end time through
     the C ABI (host seeds in, host communities out), pushes per second, and
     the reference's own PageRankNibble on a sample of the seeds (one core: the
     reference runs the seeds one after another)."""
     from networkit_b200 import _capi, generators
 
-    g = generators.hyperbolic(n, deg, 3, seed=11)
+    g = generators.hyperbolic_stream(n, deg, 3, seed=11)
     dl = _capi.DeviceLocal(g.z, g.in_ptr, g.in_col, None, None, False, device=local)
     rng = np.random.default_rng(5)
     sd = np.sort(rng.choice(g.z, seeds, replace=False))

@@ -32,6 +32,10 @@ GPU_SOURCES = ["nkgpu.cu", "noalloc.cu", "ppr.cu", "adjoint.cu", "batch.cu", "ce
                "local.cu", "part.cu", "nkbg.cu"]
 GPU_HEADERS = ["common.cuh", "sweep.cuh", "refine.cuh", "graph.hpp", "host.hpp"]
 GEN_SOURCES = ["graphgen.cpp", "graphio.cpp"]
+# Restatements of the reference's generators: compiled as the reference is
+# (baseline x86-64, no floating-point contraction) so that they round alike.
+GEN_EXACT_SOURCES = ["refgen.cpp"]
+GEN_HEADERS = ["nkgen.hpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -72,12 +76,21 @@ def build_gpu(force: bool = False, verbose: bool = False) -> str:
 
 def build_gen(force: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in GEN_SOURCES]
-    if not force and not _stale(GEN_LIB, srcs + [os.path.join(INCLUDE, "nkgio.h"), __file__]):
+    exact = [os.path.join(CSRC, s) for s in GEN_EXACT_SOURCES]
+    deps = srcs + exact + [os.path.join(CSRC, h) for h in GEN_HEADERS] + [
+        os.path.join(INCLUDE, "nkgio.h"), __file__]
+    if not force and not _stale(GEN_LIB, deps):
         return GEN_LIB
     os.makedirs(LIBDIR, exist_ok=True)
+    objs = []
+    for src in exact:
+        obj = os.path.join(LIBDIR, os.path.basename(src) + ".o")
+        subprocess.run([_host_cxx(), "-std=c++17", "-O3", "-ffp-contract=off", "-fopenmp", "-fPIC",
+                        "-c", "-o", obj, src], check=True)
+        objs.append(obj)
     cmd = [_host_cxx(), "-std=c++17", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared",
            "-I", INCLUDE,
-           "-o", GEN_LIB + ".tmp", *srcs]
+           "-o", GEN_LIB + ".tmp", *srcs, *objs]
     subprocess.run(cmd, check=True)
     os.replace(GEN_LIB + ".tmp", GEN_LIB)
     return GEN_LIB

@@ -25,12 +25,12 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
-#include <limits>
 #include <numeric>
-#include <random>
 #include <stdexcept>
 #include <string>
 #include <vector>
+
+#include "nkgen.hpp"
 
 namespace {
 
@@ -353,16 +353,9 @@ void rhg_rows(uint64_t n, double avg_deg, double exponent, uint64_t seed,
 
 } // namespace
 
-extern "C" {
+void nkgen_set_error(const char *msg) { g_err = msg; }
 
-struct nkgen_csr {
-    uint64_t z;
-    uint64_t arcs;
-    uint64_t *in_ptr;
-    uint32_t *in_col;
-    uint32_t *outdeg;
-    double *w;
-};
+extern "C" {
 
 const char *nkgen_last_error(void) { return g_err.c_str(); }
 
@@ -383,124 +376,6 @@ static void export_csr(const Csr &c, nkgen_csr *out) {
     out->in_col = c.in_col;
     out->outdeg = c.outdeg;
     out->w = c.w;
-}
-
-// G(n, p) as NetworKit's ErdosRenyiGenerator(n, p, directed) draws it with
-// one OpenMP thread after Aux::Random::setSeed(seed, false)
-// (ErdosRenyiGenerator.cpp:21-33, ErdosRenyiEnumerator.hpp, Random.cpp): one
-// std::mt19937_64 seeded with `seed`, 64-bit fixed-point uniforms X in
-// [1, 2^64 - 1] (std::uniform_int_distribution), and geometric skips
-// 1 + floor((log2 X - 64) / log2(1 - q)) over the cells of the adjacency matrix
-// in row order (Batagelj & Brandes): rows u = 0..n-1 with columns 0..n-1
-// (directed) or rows u = 1..n-1 with columns 0..u-1 (undirected). q = p; for
-// p > 0.9 the draw runs with q = 1 - p and the cells are emitted in order from
-// a cursor that stops at each drawn cell and goes on from it, as the
-// reference's complement pass does. No draws when q < n^-3. Self-loops of the
-// directed draw are dropped. The adjacency is GraphBuilder::toGraph's
-// (GraphBuilder.cpp:282-362): row u keeps its own draws in draw order, then
-// every other endpoint's draws to u appended in ascending endpoint order
-// (undirected: the neighbour list; directed: the in-list, sources ascending).
-int nkgen_erdos_renyi_stream(uint64_t n, double p, uint64_t seed, int directed,
-                             nkgen_csr *out) {
-    try {
-        if (n < 1 || n >= 0xffffffffull)
-            throw std::runtime_error("n out of range");
-        if (!(p >= 0.0 && p <= 1.0))
-            throw std::runtime_error("p must be in [0, 1]");
-        const bool dir = directed != 0;
-        std::vector<std::vector<uint32_t>> own(n);
-        auto emit = [&](uint64_t u, uint64_t v) {
-            if (u != v)
-                own[u].push_back(static_cast<uint32_t>(v));
-        };
-        const bool complement = p > 0.9;
-        const double q = complement ? 1.0 - p : p;
-        uint64_t cu = dir ? 0 : 1, cv = 0;  // complement cursor
-        auto cover_to = [&](uint64_t u, uint64_t v) {
-            while (!(cu == u && cv == v)) {
-                emit(cu, cv);
-                if (++cv == (dir ? n : cu)) {
-                    cv = 0;
-                    ++cu;
-                }
-            }
-        };
-        auto take = [&](uint64_t u, uint64_t v) {
-            if (complement)
-                cover_to(u, v);
-            else
-                emit(u, v);
-        };
-        if (!(q < std::pow(static_cast<double>(n), -3.0))) {
-            const double inv_log2 = 1.0 / std::log2(1.0 - q);
-            std::mt19937_64 urng(seed);
-            std::uniform_int_distribution<unsigned long long> uni{
-                1, std::numeric_limits<unsigned long long>::max()};
-            uint64_t cur = dir ? 0 : 1;
-            uint64_t nxt = ~0ull;
-            while (cur < n) {
-                const double x = static_cast<double>(uni(urng));
-                nxt += 1 + static_cast<uint64_t>(std::floor((std::log2(x) - 64.0) * inv_log2));
-                while (nxt >= (dir ? n : cur)) {
-                    nxt -= dir ? n : cur;
-                    ++cur;
-                }
-                if (cur < n)
-                    take(cur, nxt);
-            }
-        }
-        if (complement)
-            cover_to(n, 0);
-        // Completion: row u = own[u], then the other half edges into u.
-        std::vector<uint64_t> deg(n, 0);
-        for (uint64_t v = 0; v < n; ++v) {
-            deg[v] += own[v].size();
-            for (uint32_t u : own[v])
-                deg[u] += 1;
-        }
-        Csr cs;
-        cs.z = n;
-        cs.in_ptr = static_cast<uint64_t *>(calloc(n + 1, sizeof(uint64_t)));
-        std::vector<uint64_t> fill(n);
-        if (dir) {
-            // In-CSR: row u = the sources v of draws (v, u), v ascending.
-            std::vector<uint64_t> indeg(n, 0);
-            for (uint64_t v = 0; v < n; ++v)
-                for (uint32_t u : own[v])
-                    ++indeg[u];
-            for (uint64_t u = 0; u < n; ++u)
-                cs.in_ptr[u + 1] = cs.in_ptr[u] + indeg[u];
-            cs.arcs = cs.in_ptr[n];
-            cs.in_col = static_cast<uint32_t *>(malloc(std::max<uint64_t>(cs.arcs, 1) * 4));
-            std::copy(cs.in_ptr, cs.in_ptr + n, fill.begin());
-            for (uint64_t v = 0; v < n; ++v)
-                for (uint32_t u : own[v])
-                    cs.in_col[fill[u]++] = static_cast<uint32_t>(v);
-            cs.outdeg = static_cast<uint32_t *>(malloc(n * sizeof(uint32_t)));
-            for (uint64_t v = 0; v < n; ++v)
-                cs.outdeg[v] = static_cast<uint32_t>(own[v].size());
-        } else {
-            for (uint64_t u = 0; u < n; ++u)
-                cs.in_ptr[u + 1] = cs.in_ptr[u] + deg[u];
-            cs.arcs = cs.in_ptr[n];
-            cs.in_col = static_cast<uint32_t *>(malloc(std::max<uint64_t>(cs.arcs, 1) * 4));
-            std::copy(cs.in_ptr, cs.in_ptr + n, fill.begin());
-            for (uint64_t u = 0; u < n; ++u)
-                for (uint32_t v : own[u])
-                    cs.in_col[fill[u]++] = v;
-            for (uint64_t v = 0; v < n; ++v)
-                for (uint32_t u : own[v])
-                    cs.in_col[fill[u]++] = static_cast<uint32_t>(v);
-            cs.outdeg = static_cast<uint32_t *>(malloc(n * sizeof(uint32_t)));
-            for (uint64_t v = 0; v < n; ++v)
-                cs.outdeg[v] = static_cast<uint32_t>(deg[v]);
-        }
-        export_csr(cs, out);
-        return 0;
-    } catch (const std::exception &e) {
-        g_err = e.what();
-        return -1;
-    }
 }
 
 // Directed R-MAT: edgefactor * 2^scale draws, then duplicates and self-loops

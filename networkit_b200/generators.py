@@ -52,6 +52,13 @@ def _load():
                                         C.POINTER(_Csr)]
         L.nkgen_erdos_renyi_stream.argtypes = [C.c_uint64, C.c_double, C.c_uint64, C.c_int,
                                                C.POINTER(_Csr)]
+        L.nkgen_barabasi_albert_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64,
+                                                   C.c_uint64, C.POINTER(_Csr)]
+        L.nkgen_hyperbolic_stream.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_uint64,
+                                              C.POINTER(_Csr)]
+        L.nkgen_hyperbolic_stream_batch.argtypes = [C.c_uint64, C.POINTER(C.c_uint64),
+                                                    C.c_double, C.c_double, C.c_uint64,
+                                                    C.POINTER(_Csr), C.POINTER(C.c_uint64)]
         L.nkgen_barabasi_albert.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(_Csr)]
         L.nkgen_hyperbolic.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_uint64,
                                        C.POINTER(_Csr)]
@@ -113,6 +120,17 @@ def barabasi_albert(k: int, n: int, seed: int = 42) -> InCSR:
     return _take(out, False)
 
 
+def barabasi_albert_stream(k: int, n: int, seed: int = 42, n0: int = 0) -> InCSR:
+    """Undirected Barabasi-Albert graph as NetworKit's
+    BarabasiAlbertGenerator(k, n, n0) draws it (its default Batagelj-Brandes
+    method) after ``setSeed(seed, False)``: the same graph, with the
+    adjacency order of the Graph it builds."""
+    out = _Csr()
+    _check(_load().nkgen_barabasi_albert_stream(int(k), int(n), int(n0), int(seed),
+                                                C.byref(out)))
+    return _take(out, False)
+
+
 def hyperbolic(n: int, avg_deg: float = 16.0, exponent: float = 3.0, seed: int = 42) -> InCSR:
     """Undirected random hyperbolic graph, threshold model: n points in a
     hyperbolic disc whose radius gives expected average degree avg_deg,
@@ -122,6 +140,30 @@ def hyperbolic(n: int, avg_deg: float = 16.0, exponent: float = 3.0, seed: int =
     _check(_load().nkgen_hyperbolic(int(n), float(avg_deg), float(exponent), int(seed),
                                     C.byref(out)))
     return _take(out, False)
+
+
+def hyperbolic_stream(n: int, avg_deg: float = 16.0, exponent: float = 3.0,
+                      seed: int = 42) -> InCSR:
+    """Undirected threshold random hyperbolic graph as NetworKit's
+    HyperbolicGenerator(n, avg_deg, exponent).generate() draws it after
+    ``setSeed(seed, False)``: the same graph (nodes numbered by angle), with
+    the adjacency order of the Graph it builds on one thread."""
+    out = _Csr()
+    _check(_load().nkgen_hyperbolic_stream(int(n), float(avg_deg), float(exponent), int(seed),
+                                           C.byref(out)))
+    return _take(out, False)
+
+
+def hyperbolic_stream_batch(ns, avg_deg: float = 16.0, exponent: float = 3.0, seed: int = 42):
+    """len(ns) graphs of `hyperbolic_stream` (graph i with ns[i] nodes and
+    seed + i) as one block-diagonal InCSR plus node_offsets."""
+    ns = np.ascontiguousarray(ns, np.uint64)
+    offs = np.zeros(ns.shape[0] + 1, np.uint64)
+    out = _Csr()
+    _check(_load().nkgen_hyperbolic_stream_batch(
+        int(ns.shape[0]), ns.ctypes.data_as(C.POINTER(C.c_uint64)), float(avg_deg),
+        float(exponent), int(seed), C.byref(out), offs.ctypes.data_as(C.POINTER(C.c_uint64))))
+    return _take(out, False), offs
 
 
 def hyperbolic_batch(ns, avg_deg: float = 16.0, exponent: float = 3.0, seed: int = 42,

@@ -131,6 +131,12 @@ def ref_lib():
         lib.nkref_write_nkbg.argtypes = [C.c_void_p, C.c_char_p, C.c_uint64, C.c_int]
         lib.nkref_read_nkbg.restype = C.c_int
         lib.nkref_read_nkbg.argtypes = [C.POINTER(C.c_void_p), C.c_char_p]
+        lib.nkref_barabasi_albert.restype = C.c_int
+        lib.nkref_barabasi_albert.argtypes = [C.POINTER(C.c_void_p), C.c_uint64, C.c_uint64,
+                                              C.c_uint64, C.c_uint64]
+        lib.nkref_hyperbolic.restype = C.c_int
+        lib.nkref_hyperbolic.argtypes = [C.POINTER(C.c_void_p), C.c_uint64, C.c_double,
+                                         C.c_double, C.c_uint64, C.c_int]
         lib.nkref_erdos_renyi.restype = C.c_int
         lib.nkref_erdos_renyi.argtypes = [C.POINTER(C.c_void_p), C.c_uint64, C.c_double,
                                           C.c_uint64, C.c_int, C.c_int]
@@ -447,6 +453,27 @@ class RefGraph:
         h = C.c_void_p()
         if lib.nkref_erdos_renyi(C.byref(h), int(n), float(p), int(seed), int(bool(directed)),
                                  int(threads)) != 0:
+            raise RuntimeError(lib.nkref_last_error().decode())
+        return cls(h)
+
+    @classmethod
+    def barabasi_albert(cls, k, n, seed=42, n0=0):
+        """The reference's BarabasiAlbertGenerator(k, n, n0).generate() after
+        Aux::Random::setSeed(seed, False)."""
+        lib = ref_lib()
+        h = C.c_void_p()
+        if lib.nkref_barabasi_albert(C.byref(h), int(k), int(n), int(n0), int(seed)) != 0:
+            raise RuntimeError(lib.nkref_last_error().decode())
+        return cls(h)
+
+    @classmethod
+    def hyperbolic(cls, n, avg_deg=16.0, exponent=3.0, seed=42, threads=1):
+        """The reference's HyperbolicGenerator(n, avg_deg, exponent).generate()
+        on `threads` OpenMP threads after Aux::Random::setSeed(seed, False)."""
+        lib = ref_lib()
+        h = C.c_void_p()
+        if lib.nkref_hyperbolic(C.byref(h), int(n), float(avg_deg), float(exponent), int(seed),
+                                int(threads)) != 0:
             raise RuntimeError(lib.nkref_last_error().decode())
         return cls(h)
 

@@ -27,7 +27,9 @@
 #include <networkit/centrality/KatzCentrality.hpp>
 #include <networkit/centrality/PageRank.hpp>
 #include <networkit/auxiliary/Random.hpp>
+#include <networkit/generators/BarabasiAlbertGenerator.hpp>
 #include <networkit/generators/ErdosRenyiGenerator.hpp>
+#include <networkit/generators/HyperbolicGenerator.hpp>
 #include <networkit/graph/Graph.hpp>
 #include <networkit/io/GMLGraphReader.hpp>
 #include <networkit/io/NetworkitBinaryReader.hpp>
@@ -89,6 +91,40 @@ int nkref_erdos_renyi(void **out, uint64_t n, double p, uint64_t seed, int direc
         auto *rg = new RefGraph;
         rg->G.reset(new NetworKit::Graph(
             NetworKit::ErdosRenyiGenerator(n, p, directed != 0).generate()));
+        omp_set_num_threads(prev);
+        *out = rg;
+        return 0;
+    } catch (const std::exception &e) {
+        omp_set_num_threads(prev);
+        return fail(e);
+    }
+}
+
+// NetworKit::BarabasiAlbertGenerator(k, n, n0).generate() (Batagelj-Brandes,
+// sequential) after Aux::Random::setSeed(seed, false).
+int nkref_barabasi_albert(void **out, uint64_t k, uint64_t n, uint64_t n0, uint64_t seed) {
+    try {
+        Aux::Random::setSeed(seed, false);
+        auto *rg = new RefGraph;
+        rg->G.reset(new NetworKit::Graph(NetworKit::BarabasiAlbertGenerator(k, n, n0).generate()));
+        *out = rg;
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// NetworKit::HyperbolicGenerator(n, avg_deg, exponent).generate() run with
+// `threads` OpenMP threads after Aux::Random::setSeed(seed, false).
+int nkref_hyperbolic(void **out, uint64_t n, double avg_deg, double exponent, uint64_t seed,
+                     int threads) {
+    const int prev = omp_get_max_threads();
+    try {
+        Aux::Random::setSeed(seed, false);
+        omp_set_num_threads(threads);
+        auto *rg = new RefGraph;
+        rg->G.reset(new NetworKit::Graph(
+            NetworKit::HyperbolicGenerator(n, avg_deg, exponent).generate()));
         omp_set_num_threads(prev);
         *out = rg;
         return 0;

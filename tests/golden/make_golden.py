@@ -19,7 +19,9 @@ that file (keys ``nkbg_*``), plus one file per weight encoding of the format
 ApproximatePageRank and PageRankNibble results on the reference's SCD test
 graphs (``local_ppr.npz``), and the reference's Erdos-Renyi graph of the
 G(1e5, average degree 10) workload with the reference's PageRank on it
-(``er_config.npz``). The GPU box has no
+(``er_config.npz``), and digests of the reference's Barabasi-Albert graph of
+the batched-PPR workload (``ba_config.npz``) and of the reference's random
+hyperbolic graphs (``rhg_config.npz``). The GPU box has no
 reference checkout: the tests read only these files.
 """
 from __future__ import annotations
@@ -130,6 +132,8 @@ def main():
     nkbg_formats(O)
     local_ppr(O, inp)
     er_config(O)
+    ba_config(O)
+    rhg_config(O)
 
 
 # (alpha, epsilon, seeds) of the local PageRank fixtures. SelectiveCDGTest.cpp
@@ -266,6 +270,50 @@ def er_config(O):
         rank_ids_top100=r["ranking_ids"][:100].astype(np.uint32))
     np.savez_compressed(os.path.join(HERE, "er_config.npz"), **out)
     print(f"er_config: arcs={int(out['arcs'])} it={r['iterations']} max={r['maximum']:.6g}")
+
+
+# The batched-PPR workload: Barabasi-Albert, n = 4M, k = 8 attachments per
+# new node, seed 42.
+BA_K, BA_N, BA_SEED = 8, 4_000_000, 42
+
+
+def ba_config(O):
+    """The reference's BarabasiAlbertGenerator(8, 4000000) graph after
+    setSeed(42, False), as SHA-256 digests of its in-adjacency (row offsets as
+    uint64, ids as uint32) and its arc count, in ``ba_config.npz``."""
+    import hashlib
+
+    a = export_to_arrays(O.RefGraph.barabasi_albert(BA_K, BA_N, BA_SEED))
+    out = dict(k=np.int64(BA_K), n=np.int64(BA_N), seed=np.int64(BA_SEED),
+               arcs=np.int64(a["in_ptr"][-1]),
+               in_ptr_sha256=np.bytes_(hashlib.sha256(a["in_ptr"].tobytes()).hexdigest()),
+               in_col_sha256=np.bytes_(hashlib.sha256(a["in_col"].tobytes()).hexdigest()))
+    np.savez_compressed(os.path.join(HERE, "ba_config.npz"), **out)
+    print(f"ba_config: arcs={int(out['arcs'])}")
+
+
+# Random hyperbolic graphs (average degree 16, exponent 3): a small one, the
+# largest size of the many-graph batch, and the 4M graph of the locality
+# workload.
+RHG_CASES = [(1000, 42), (200_000, 42), (4_000_000, 21)]
+
+
+def rhg_config(O):
+    """The reference's HyperbolicGenerator(n, 16, 3) graphs of RHG_CASES,
+    drawn on one OpenMP thread after setSeed(seed, False), as SHA-256
+    digests of their in-adjacency and their arc counts (``rhg_config.npz``,
+    keys ``<n>_<seed>_<field>``)."""
+    import hashlib
+
+    out = {}
+    for n, seed in RHG_CASES:
+        a = export_to_arrays(O.RefGraph.hyperbolic(n, 16.0, 3.0, seed, threads=1))
+        key = f"{n}_{seed}_"
+        out[key + "arcs"] = np.int64(a["in_ptr"][-1])
+        out[key + "in_ptr_sha256"] = np.bytes_(hashlib.sha256(a["in_ptr"].tobytes()).hexdigest())
+        out[key + "in_col_sha256"] = np.bytes_(hashlib.sha256(a["in_col"].tobytes()).hexdigest())
+        print(f"rhg_config: n={n} seed={seed} arcs={int(out[key + 'arcs'])}")
+    np.savez_compressed(os.path.join(HERE, "rhg_config.npz"), **out)
 
 
 if __name__ == "__main__":

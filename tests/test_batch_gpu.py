@@ -19,7 +19,7 @@ def mixed_graphs():
     """Uneven shapes: hyperbolic graphs of several sizes (hubs above any
     split threshold), a directed R-MAT with sinks, an Erdos-Renyi graph with
     isolated nodes, a single node and a two-node path."""
-    gs = [generators.hyperbolic(n, 16, 3, seed=42 + i)
+    gs = [generators.hyperbolic_stream(n, 16, 3, seed=42 + i)
           for i, n in enumerate((200, 1500, 7000, 30000))]
     gs.append(generators.rmat_directed(12, 8, seed=3))
     gs.append(generators.erdos_renyi(3000, 1.5 / 2999, seed=5))

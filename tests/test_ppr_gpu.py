@@ -21,7 +21,7 @@ def one_hot(z, s):
 @pytest.mark.parametrize("graph", ["ba", "rmat", "rmat_distribute"])
 def test_ppr_columns_match_oracle(oracle_mod, graph):
     if graph == "ba":
-        csr = generators.barabasi_albert(8, 20000, seed=42)
+        csr = generators.barabasi_albert_stream(8, 20000, seed=42)
     else:
         csr = generators.rmat_directed(13, 8, seed=3)
     distribute = graph.endswith("distribute")
