@@ -719,7 +719,7 @@ nkg_batch *batch_create(uint32_t count, const uint64_t *node_off, const uint64_t
     b->total = static_cast<uint32_t>(total);
     b->arcs = arcs;
     b->node_off.assign(node_off, node_off + count + 1);
-    NKG_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    b->stream = stream_acquire(dev);
     NKG_CUDA(cudaEventCreate(&b->ev0));
     NKG_CUDA(cudaEventCreate(&b->ev1));
     cudaStream_t s = b->stream;
@@ -919,9 +919,9 @@ void nkg_batch_destroy(nkg_batch *b) {
     if (b->ev1)
         cudaEventDestroy(b->ev1);
     cudaStream_t s = b->stream;
+    const int dev = b->device;
     delete b;
-    if (s)
-        cudaStreamDestroy(s);
+    nkg::stream_release(dev, s);
     if (prev >= 0)
         cudaSetDevice(prev);
 }

@@ -60,6 +60,20 @@ inline void clear_stats(nkg_stats *st) {
 void *device_alloc(size_t bytes, int &device);
 void device_free(void *p, int device);
 
+// Page-locked host memory of the library: cudaHostAlloc'ed blocks kept, once
+// freed, in a process-wide cache keyed by size (allocating and freeing
+// page-locked memory costs milliseconds, more than a small graph's whole
+// build). pinned_free files the block; the caller has waited for every copy
+// that uses it. nkg_release_cached_memory hands the cached blocks back.
+void *pinned_alloc(size_t bytes);
+void pinned_free(void *p, size_t bytes);
+
+// Streams of the library's handles: kept per device once a handle is
+// destroyed (creating and destroying a stream costs about 0.1 ms). The
+// stream returned is non-blocking and idle.
+cudaStream_t stream_acquire(int device);
+void stream_release(int device, cudaStream_t s);
+
 // Owning device allocation (device_alloc/device_free). Sizes are in elements;
 // the allocation is padded by `pad` elements so that vectorised or bulk copies
 // that round an end offset up stay inside it.
@@ -117,21 +131,24 @@ class PinnedHost {
     PinnedHost() = default;
     explicit PinnedHost(size_t n) { alloc(n); }
     void alloc(size_t n) {
+        reset();
+        p_ = static_cast<T *>(pinned_alloc(n * sizeof(T)));
+        bytes_ = n * sizeof(T);
+    }
+    void reset() {
         if (p_)
-            cudaFreeHost(p_);
+            pinned_free(p_, bytes_);
         p_ = nullptr;
-        NKG_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&p_), n * sizeof(T), cudaHostAllocDefault));
+        bytes_ = 0;
     }
     PinnedHost(const PinnedHost &) = delete;
     PinnedHost &operator=(const PinnedHost &) = delete;
-    ~PinnedHost() {
-        if (p_)
-            cudaFreeHost(p_);
-    }
+    ~PinnedHost() { reset(); }
     T *get() const { return p_; }
 
   private:
     T *p_ = nullptr;
+    size_t bytes_ = 0;
 };
 
 constexpr uint32_t kNone = 0xffffffffu;

@@ -84,6 +84,10 @@ struct Plane {
 } // namespace nkg
 
 struct nkg_graph {
+    nkg_graph() = default;
+    nkg_graph(const nkg_graph &) = delete;
+    nkg_graph &operator=(const nkg_graph &) = delete;
+    ~nkg_graph();
     int device = 0;
     cudaStream_t stream = nullptr;
     uint64_t z = 0, n = 0, arcs = 0, sinks = 0;

@@ -930,7 +930,7 @@ int nkg_local_create(nkg_local **out, uint64_t z, const uint64_t *row_ptr, const
         h->total_volume = (w ? wsum_edges : edges) * 2;
         if (exists)
             h->exists.assign(exists, exists + z);
-        NKG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->stream = stream_acquire(h->device);
         NKG_CUDA(cudaEventCreate(&h->ev0));
         NKG_CUDA(cudaEventCreate(&h->ev1));
         NKG_CUDA(cudaEventCreate(&h->ev2));
@@ -981,9 +981,9 @@ void nkg_local_destroy(nkg_local *h) {
     if (h->ev3)
         cudaEventDestroy(h->ev3);
     cudaStream_t s = h->stream;
+    const int dev = h->device;
     delete h;
-    if (s)
-        cudaStreamDestroy(s);
+    nkg::stream_release(dev, s);
     if (prev >= 0)
         cudaSetDevice(prev);
 }

@@ -1029,12 +1029,12 @@ int nkg_nkbg_decode(const void *file, uint64_t size, int flags, int device, uint
         if (dev < 0)
             NKG_CUDA(cudaGetDevice(&dev));
         DeviceGuard guard(dev);
-        cudaStream_t s = nullptr;
-        NKG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        cudaStream_t s = stream_acquire(dev);
         struct StreamGuard {
+            int dev;
             cudaStream_t s;
-            ~StreamGuard() { cudaStreamDestroy(s); }
-        } sg{s};
+            ~StreamGuard() { stream_release(dev, s); }
+        } sg{dev, s};
         DeviceCsr G;
         decode_nkbg(static_cast<const uint8_t *>(file), size, (flags & NKG_DEVICE_PTRS) != 0, dev,
                     s, G);

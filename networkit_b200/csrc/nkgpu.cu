@@ -110,6 +110,63 @@ void device_free(void *p, int device) {
         cudaSetDevice(prev);
 }
 
+namespace {
+std::mutex g_pinned_mutex;
+std::multimap<size_t, void *> g_pinned_free;  // cached page-locked blocks by size
+std::mutex g_stream_mutex;
+std::vector<cudaStream_t> g_streams[kMaxDevices];  // idle streams per device
+}  // namespace
+
+void *pinned_alloc(size_t bytes) {
+    bytes = std::max<size_t>(bytes, 1);
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mutex);
+        auto it = g_pinned_free.lower_bound(bytes);
+        if (it != g_pinned_free.end() && it->first <= 2 * bytes) {
+            void *p = it->second;
+            g_pinned_free.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    NKG_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocDefault));
+    return p;
+}
+
+void pinned_free(void *p, size_t bytes) {
+    if (!p)
+        return;
+    std::lock_guard<std::mutex> lock(g_pinned_mutex);
+    g_pinned_free.emplace(std::max<size_t>(bytes, 1), p);
+}
+
+cudaStream_t stream_acquire(int device) {
+    require(device >= 0 && device < kMaxDevices, "device ordinal out of range");
+    {
+        std::lock_guard<std::mutex> lock(g_stream_mutex);
+        if (!g_streams[device].empty()) {
+            cudaStream_t s = g_streams[device].back();
+            g_streams[device].pop_back();
+            return s;
+        }
+    }
+    cudaStream_t s = nullptr;
+    NKG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return s;
+}
+
+void stream_release(int device, cudaStream_t s) {
+    if (!s)
+        return;
+    if (cudaStreamSynchronize(s) != cudaSuccess) {  // a stream in a failed state is not kept
+        cudaGetLastError();
+        cudaStreamDestroy(s);
+        return;
+    }
+    std::lock_guard<std::mutex> lock(g_stream_mutex);
+    g_streams[device].push_back(s);
+}
+
 // ---------------------------------------------------------------------------
 // Graph build kernels
 
@@ -849,7 +906,7 @@ static std::unique_ptr<nkg_graph> graph_shell(int dev, uint64_t z, uint64_t arcs
     g->arcs = arcs;
     g->weighted = weighted;
     g->directed = directed != 0;
-    NKG_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    g->stream = stream_acquire(dev);
     NKG_CUDA(cudaEventCreate(&g->ev0));
     NKG_CUDA(cudaEventCreate(&g->ev1));
     NKG_CUDA(cudaEventCreate(&g->ev2));
@@ -1207,6 +1264,25 @@ static void destroy_plane_graphs(nkg_graph *g) {
         g->p64.exec[i] = g->p32.exec[i] = nullptr;
     }
 }
+
+}  // namespace nkg
+
+// Waits for the handle's stream, then releases its CUDA objects (the stream
+// goes back to the per-device pool); the device arrays free themselves after.
+nkg_graph::~nkg_graph() {
+    if (stream)
+        cudaStreamSynchronize(stream);
+    nkg::destroy_plane_graphs(this);
+    if (ev0)
+        cudaEventDestroy(ev0);
+    if (ev1)
+        cudaEventDestroy(ev1);
+    if (ev2)
+        cudaEventDestroy(ev2);
+    nkg::stream_release(device, stream);
+}
+
+namespace nkg {
 
 template <typename T>
 Plane<T> &plane(nkg_graph *g);
@@ -1905,8 +1981,14 @@ int nkg_release_cached_memory(int device) {
         require(dev >= 0 && dev < kMaxDevices, "device ordinal out of range");
         DeviceGuard guard(dev);
         NKG_CUDA(cudaDeviceSynchronize());
-        std::lock_guard<std::mutex> lock(g_cache_mutex);
-        release_blocks(g_cache[dev]);
+        {
+            std::lock_guard<std::mutex> lock(g_cache_mutex);
+            release_blocks(g_cache[dev]);
+        }
+        std::lock_guard<std::mutex> lock(g_pinned_mutex);
+        for (auto &kv : g_pinned_free)
+            cudaFreeHost(kv.second);
+        g_pinned_free.clear();
     });
 }
 
@@ -1945,18 +2027,7 @@ void nkg_graph_destroy(nkg_graph *g) {
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(g->device);
-    cudaStreamSynchronize(g->stream);
-    destroy_plane_graphs(g);
-    if (g->ev0)
-        cudaEventDestroy(g->ev0);
-    if (g->ev1)
-        cudaEventDestroy(g->ev1);
-    if (g->ev2)
-        cudaEventDestroy(g->ev2);
-    cudaStream_t s = g->stream;
     delete g;
-    if (s)
-        cudaStreamDestroy(s);
     if (prev >= 0)
         cudaSetDevice(prev);
 }

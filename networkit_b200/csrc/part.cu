@@ -201,7 +201,7 @@ nkg_part *create_part(uint64_t vec_len, uint64_t row_base, uint64_t rows, uint64
     p->pad = pad;
     p->arcs = arcs;
     p->weighted = w != nullptr;
-    NKG_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    p->stream = stream_acquire(dev);
     cudaStream_t s = p->stream;
     const unsigned sms = num_sms(dev);
     const uint32_t n = p->rows;
@@ -346,9 +346,9 @@ void nkg_part_destroy(nkg_part *p) {
     cudaSetDevice(p->device);
     cudaStreamSynchronize(p->stream);
     cudaStream_t s = p->stream;
+    const int dev = p->device;
     delete p;
-    if (s)
-        cudaStreamDestroy(s);
+    nkg::stream_release(dev, s);
     if (prev >= 0)
         cudaSetDevice(prev);
 }
