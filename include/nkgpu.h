@@ -193,12 +193,23 @@ NKG_API int nkg_graph_create_from_edges(nkg_graph **out, uint64_t z, uint64_t m,
  * lists, neighbour ids >= the node count) fail with NKG_ERR_INVALID_ARG.
  * ms_decode_out (nullable): device time of the decode, after the copy of a
  * host file.
+ * nkg_graph_create_from_nkbg_file: the same from the file at `path` (what
+ * NetworkitBinaryReader::read(path) takes): reader threads read it in pieces
+ * of staging_bytes (0: 16 MiB) into page-locked staging blocks and copy each
+ * piece to the device as soon as it is read, so reading and copying overlap;
+ * s_load_out (nullable): host seconds from opening the file to all of it on
+ * the device. A file that cannot be opened or read fails with
+ * NKG_ERR_INVALID_ARG.
  * nkg_nkbg_decode: the same decode into caller-owned HOST arrays (any may be
  * NULL; sizes from a first call with all of them NULL: z_out, arcs_out):
  * in_ptr z+1, in_col / in_w arcs, wdeg / outdeg / exists z. */
 NKG_API int nkg_graph_create_from_nkbg(nkg_graph **out, const void *file, uint64_t size,
                                        int flags, const nkg_graph_options *opts,
                                        double *ms_decode_out);
+NKG_API int nkg_graph_create_from_nkbg_file(nkg_graph **out, const char *path,
+                                            uint64_t staging_bytes,
+                                            const nkg_graph_options *opts,
+                                            double *ms_decode_out, double *s_load_out);
 NKG_API int nkg_nkbg_decode(const void *file, uint64_t size, int flags, int device,
                             uint64_t *z_out, uint64_t *arcs_out, int *directed_out,
                             int *weighted_out, uint64_t *in_ptr, uint32_t *in_col, double *in_w,

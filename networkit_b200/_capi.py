@@ -190,6 +190,8 @@ SIGNATURES = {
     "nkg_local_sets": (C.c_int, [_vp, _u32p]),
     "nkg_graph_create_from_nkbg": (C.c_int, [C.POINTER(_vp), _vp, C.c_uint64, C.c_int,
                                              C.POINTER(GraphOptions), _f64p]),
+    "nkg_graph_create_from_nkbg_file": (C.c_int, [C.POINTER(_vp), C.c_char_p, C.c_uint64,
+                                                  C.POINTER(GraphOptions), _f64p, _f64p]),
     "nkg_nkbg_decode": (C.c_int, [_vp, C.c_uint64, C.c_int, C.c_int, _u64p, _u64p,
                                   C.POINTER(C.c_int), C.POINTER(C.c_int), _u64p, _u32p, _f64p,
                                   _f64p, _u32p, _u8p, _f64p]),
@@ -312,6 +314,30 @@ class DeviceGraph:
         self.z = int(info["z"])
         self.n = int(info["n"])
         self.ms_decode = float(ms.value)
+        return self
+
+    @classmethod
+    def from_nkbg_file(cls, path, device: int = -1, row_order: int = -1, staging_bytes: int = 0):
+        """Build the graph from a NetworkitBinaryGraph file on disk
+        (nkg_graph_create_from_nkbg_file): read in pieces by reader threads,
+        each piece copied to the device as it arrives, then decoded there.
+        .ms_decode: device time of the decode; .s_load: host seconds to get
+        the whole file onto the device."""
+        self = cls.__new__(cls)
+        h = _vp()
+        opts = GraphOptions()
+        opts.device = int(device)
+        opts.row_order = int(row_order)
+        ms, sl = C.c_double(0.0), C.c_double(0.0)
+        check(lib().nkg_graph_create_from_nkbg_file(C.byref(h), os.fsencode(path),
+                                                    int(staging_bytes), C.byref(opts),
+                                                    C.byref(ms), C.byref(sl)))
+        self.h = h
+        info = self.info()
+        self.z = int(info["z"])
+        self.n = int(info["n"])
+        self.ms_decode = float(ms.value)
+        self.s_load = float(sl.value)
         return self
 
     @classmethod

@@ -34,9 +34,18 @@
 // the rows, weights, degrees) is scans and scatter/gather passes.
 #include <cub/cub.cuh>
 
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <atomic>
+#include <cerrno>
+#include <chrono>
 #include <cstring>
 #include <memory>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "graph.hpp"
@@ -975,10 +984,145 @@ int option_device_of(const nkg_graph_options *opt) {
     return dev;
 }
 
+// A graph handle from the file's bytes (host, or device with on_device):
+// the decode, then the build nkg_graph_create does, on the handle's stream.
+nkg_graph *create_from_nkbg(const void *file, uint64_t size, bool on_device,
+                            const nkg_graph_options *opts, double *ms_decode_out) {
+    DeviceGuard guard(option_device_of(opts));
+    // Read the header first for the shell's z / kind.
+    uint8_t hdr[80];
+    require(file != nullptr && size >= 80, "not a NetworkitBinaryGraph file");
+    NKG_CUDA(cudaMemcpy(hdr, file, 80,
+                        on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost));
+    const uint64_t features = load_u64(hdr + 16), nodes = load_u64(hdr + 24);
+    require(std::memcmp(hdr, "nkbg002", 8) == 0, "not a NetworkitBinaryGraph file (magic nkbg002)");
+    std::unique_ptr<nkg_graph> g = device_graph_shell(
+        opts, nodes, ((features & 0xEu) >> 1) != 0, static_cast<int>(features & 1u));
+    DeviceCsr G;
+    decode_nkbg(static_cast<const uint8_t *>(file), size, on_device, g->device, g->stream, G);
+    if (ms_decode_out)
+        *ms_decode_out = G.ms_decode;
+    // As nkg_graph_create takes them: weights and weighted degrees for
+    // weighted graphs only, the existence mask only when a node is absent.
+    DeviceArray<uint8_t> ex;
+    if (!G.ex_host.empty())
+        ex = std::move(G.ex);
+    DeviceArray<double> w, wdeg;
+    if (G.weighted) {
+        w = std::move(G.w);
+        wdeg = std::move(G.wdeg);
+    }
+    return device_graph_build(std::move(g), G.arcs, G.ptr, G.col, w, wdeg, ex,
+                              G.ex_host.empty() ? nullptr : G.ex_host.data(), opts);
+}
+
+// The file at `path` into device memory (d_file, size bytes plus 16 of
+// padding): reader threads pread it in pieces of `piece` bytes into their own
+// two page-locked staging blocks, each thread on its own stream, so that the
+// reads, the copies over PCIe and the other threads' work overlap; a staging
+// block is refilled once the copy out of it has finished. Returns the size.
+uint64_t load_file_to_device(const char *path, uint64_t piece, int dev,
+                             DeviceArray<uint8_t> &d_file) {
+    require(path != nullptr, "path is NULL");
+    const int fd = open(path, O_RDONLY);
+    if (fd < 0)
+        throw Error(NKG_ERR_INVALID_ARG, std::string("cannot open ") + path + ": " +
+                                             std::strerror(errno));
+    struct FdGuard {
+        int fd;
+        ~FdGuard() { close(fd); }
+    } fg{fd};
+    struct stat st;
+    require(fstat(fd, &st) == 0 && S_ISREG(st.st_mode), "not a regular file");
+    const uint64_t size = static_cast<uint64_t>(st.st_size);
+    require(size >= 80, "not a NetworkitBinaryGraph file");
+    if (piece == 0)
+        piece = 16ull << 20;
+    const uint64_t pieces = (size + piece - 1) / piece;
+    d_file.alloc(size, 16);
+    uint8_t *dst = d_file.get();
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int threads =
+        static_cast<int>(std::min<uint64_t>(pieces, std::min<unsigned>(8u, std::max(1u, hw / 2))));
+    std::vector<std::string> errs(threads);
+    auto reader = [&](int t) {
+        cudaStream_t s = nullptr;
+        void *slot[2] = {nullptr, nullptr};
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        try {
+            NKG_CUDA(cudaSetDevice(dev));
+            s = stream_acquire(dev);
+            for (int k = 0; k < 2; ++k) {
+                slot[k] = pinned_alloc(piece);
+                NKG_CUDA(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+            }
+            bool used[2] = {false, false};
+            int k = 0;
+            for (uint64_t c = t; c < pieces; c += threads, k ^= 1) {
+                if (used[k])
+                    NKG_CUDA(cudaEventSynchronize(ev[k]));
+                const uint64_t off = c * piece, len = std::min(piece, size - off);
+                uint64_t got = 0;
+                while (got < len) {
+                    const ssize_t r = pread(fd, static_cast<uint8_t *>(slot[k]) + got, len - got,
+                                            static_cast<off_t>(off + got));
+                    if (r < 0 && errno == EINTR)
+                        continue;
+                    require(r > 0, "the file could not be read to its end");
+                    got += static_cast<uint64_t>(r);
+                }
+                NKG_CUDA(cudaMemcpyAsync(dst + off, slot[k], len, cudaMemcpyHostToDevice, s));
+                NKG_CUDA(cudaEventRecord(ev[k], s));
+                used[k] = true;
+            }
+            NKG_CUDA(cudaStreamSynchronize(s));
+        } catch (const std::exception &e) {
+            errs[t] = e.what();
+            if (s)
+                cudaStreamSynchronize(s);
+        }
+        for (int k = 0; k < 2; ++k) {
+            if (ev[k])
+                cudaEventDestroy(ev[k]);
+            pinned_free(slot[k], piece);
+        }
+        stream_release(dev, s);
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t)
+        pool.emplace_back(reader, t);
+    reader(0);
+    for (auto &th : pool)
+        th.join();
+    for (const std::string &e : errs)
+        if (!e.empty())
+            throw Error(NKG_ERR_INVALID_ARG, e);
+    return size;
+}
+
 } // namespace
 } // namespace nkg
 
 extern "C" {
+
+int nkg_graph_create_from_nkbg_file(nkg_graph **out, const char *path, uint64_t staging_bytes,
+                                    const nkg_graph_options *opts, double *ms_decode_out,
+                                    double *s_load_out) {
+    using namespace nkg;
+    return guarded([&] {
+        require(out != nullptr, "out is NULL");
+        *out = nullptr;
+        const int dev = option_device_of(opts);
+        DeviceGuard guard(dev);
+        const auto t0 = std::chrono::steady_clock::now();
+        DeviceArray<uint8_t> d_file;
+        const uint64_t size = load_file_to_device(path, staging_bytes, dev, d_file);
+        if (s_load_out)
+            *s_load_out =
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        *out = create_from_nkbg(d_file.get(), size, true, opts, ms_decode_out);
+    });
+}
 
 int nkg_graph_create_from_nkbg(nkg_graph **out, const void *file, uint64_t size, int flags,
                                const nkg_graph_options *opts, double *ms_decode_out) {
@@ -987,34 +1131,7 @@ int nkg_graph_create_from_nkbg(nkg_graph **out, const void *file, uint64_t size,
         require(out != nullptr, "out is NULL");
         require((flags & ~NKG_DEVICE_PTRS) == 0, "unknown flags");
         *out = nullptr;
-        DeviceGuard guard(option_device_of(opts));
-        // Read the header first for the shell's z / kind.
-        uint8_t hdr[80];
-        require(file != nullptr && size >= 80, "not a NetworkitBinaryGraph file");
-        NKG_CUDA(cudaMemcpy(hdr, file, 80, (flags & NKG_DEVICE_PTRS) ? cudaMemcpyDeviceToHost
-                                                                      : cudaMemcpyHostToHost));
-        const uint64_t features = load_u64(hdr + 16), nodes = load_u64(hdr + 24);
-        require(std::memcmp(hdr, "nkbg002", 8) == 0,
-                "not a NetworkitBinaryGraph file (magic nkbg002)");
-        std::unique_ptr<nkg_graph> g = device_graph_shell(
-            opts, nodes, ((features & 0xEu) >> 1) != 0, static_cast<int>(features & 1u));
-        DeviceCsr G;
-        decode_nkbg(static_cast<const uint8_t *>(file), size, (flags & NKG_DEVICE_PTRS) != 0,
-                    g->device, g->stream, G);
-        if (ms_decode_out)
-            *ms_decode_out = G.ms_decode;
-        // As nkg_graph_create takes them: weights and weighted degrees for
-        // weighted graphs only, the existence mask only when a node is absent.
-        DeviceArray<uint8_t> ex;
-        if (!G.ex_host.empty())
-            ex = std::move(G.ex);
-        DeviceArray<double> w, wdeg;
-        if (G.weighted) {
-            w = std::move(G.w);
-            wdeg = std::move(G.wdeg);
-        }
-        *out = device_graph_build(std::move(g), G.arcs, G.ptr, G.col, w, wdeg, ex,
-                                  G.ex_host.empty() ? nullptr : G.ex_host.data(), opts);
+        *out = create_from_nkbg(file, size, (flags & NKG_DEVICE_PTRS) != 0, opts, ms_decode_out);
     });
 }
 

@@ -141,3 +141,49 @@ def test_malformed_files_are_refused(tmp_path):
     # The next, valid file decodes normally.
     dev, _ = graphio.decode_nkbg_device(good)
     same(dev, graphio.read_nkbg(os.path.join(HERE, "nkbg_signed_undir.nkbg")))
+
+
+@pytest.mark.parametrize("staging", [0, 4096, 4096 * 3 + 16, 100_000])
+@pytest.mark.parametrize("name", ["wikivote_directed", "nkbg_double_undir", "nkbg_none_undir"])
+def test_graph_from_file_path_equals_graph_from_bytes(name, staging):
+    """nkg_graph_create_from_nkbg_file: reader threads, pieces of `staging`
+    bytes (odd sizes: pieces that split varints and chunks), then the same
+    decode: the same graph, the same PageRank bit for bit."""
+    path = os.path.join(HERE, name + ".nkbg")
+    a = _capi.DeviceGraph.from_nkbg(open(path, "rb").read())
+    b = _capi.DeviceGraph.from_nkbg_file(path, staging_bytes=staging)
+    assert b.info() == {**a.info(), "ms_create": b.info()["ms_create"]}
+    assert b.s_load > 0 and b.ms_decode > 0
+    p = a.params(0.85, 1e-10, 0, False, False, _capi.NKG_PREC_FP64, SWEEPS)
+    sa, ia, _, _ = a.run(p)
+    sb, ib, _, _ = b.run(p)
+    assert ia == ib
+    np.testing.assert_array_equal(sa.view(np.uint64), sb.view(np.uint64))
+
+
+def test_generated_file_path_many_pieces(tmp_path):
+    csr = generators.rmat_directed(15, 16, seed=5)
+    p = _write(tmp_path, csr, 13)
+    a = _capi.DeviceGraph(graphio.read_nkbg(p))
+    b = _capi.DeviceGraph.from_nkbg_file(p, staging_bytes=65536 + 8)  # dozens of pieces
+    prm = a.params(0.85, 1e-10, 0, False, False, _capi.NKG_PREC_FP64, SWEEPS)
+    sa, ia, _, _ = a.run(prm)
+    sb, ib, _, _ = b.run(prm)
+    assert ia == ib
+    np.testing.assert_array_equal(sa.view(np.uint64), sb.view(np.uint64))
+
+
+def test_file_path_errors(tmp_path):
+    with pytest.raises(_capi.NkgError, match="cannot open"):
+        _capi.DeviceGraph.from_nkbg_file(str(tmp_path / "missing.nkbg"))
+    with pytest.raises(_capi.NkgError, match="regular file"):
+        _capi.DeviceGraph.from_nkbg_file(str(tmp_path))
+    short = tmp_path / "short.nkbg"
+    short.write_bytes(b"nkbg002" + b"\0" * 20)
+    with pytest.raises(_capi.NkgError, match="NetworkitBinaryGraph"):
+        _capi.DeviceGraph.from_nkbg_file(str(short))
+    bad = tmp_path / "bad.nkbg"
+    good = open(os.path.join(HERE, "nkbg_signed_undir.nkbg"), "rb").read()
+    bad.write_bytes(good[: len(good) // 2])
+    with pytest.raises(_capi.NkgError):
+        _capi.DeviceGraph.from_nkbg_file(str(bad), staging_bytes=4096)
