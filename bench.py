@@ -902,11 +902,10 @@ def form_local(local, n=1_000_000, deg=16, seeds=16384, alpha=0.1, eps=1e-5, ref
     import oracle
 
     if oracle.ref_available() and ref_sample:
-        # Insert the edges (u < v, lexicographic: the generator's order) so
-        # that every reference row lists its neighbours in the same order.
-        rows = np.repeat(np.arange(g.z, dtype=np.uint32), np.diff(g.in_ptr).astype(np.int64))
-        keep = rows < g.in_col
-        rg = oracle.RefGraph.from_edges(g.z, rows[keep], g.in_col[keep], directed=False)
+        # The reference generator's own Graph: the same graph with the same
+        # neighbour order in every row (generators.hyperbolic_stream restates
+        # it; tests/test_reference_generators.py pins the two together).
+        rg = oracle.RefGraph.hyperbolic(n, deg, 3, seed=11, threads=1)
         sample = sd[:: max(1, seeds // ref_sample)][:ref_sample]
         ref_sets, secs = rg.prn(alpha, eps, sample)
         idx = np.searchsorted(sd, sample)

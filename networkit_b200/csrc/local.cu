@@ -241,6 +241,10 @@ __device__ int map_grow(const PushArgs &a, WarpMap &m, uint64_t need_cap, uint32
     return 0;
 }
 
+// Rows longer than this have their nibble cut change counted by the whole
+// warp (unweighted graphs).
+constexpr uint64_t kCutWarpRow = 64;
+
 // One warp runs one problem at a time, taking problems from a global counter
 // until none are left.
 template <bool WEIGHTED>
@@ -434,8 +438,12 @@ __global__ void __launch_bounds__(kLocalThreads) local_push(PushArgs a) {
                 a.out_key[off + i] = kv;
                 // Cut change of v: +w for a neighbour outside the prefix that
                 // ends before v (v itself included), -w inside; row order.
+                // Unweighted rows longer than kCutWarpRow are counted by the
+                // whole warp below.
                 double acc = 0.0;
                 const uint64_t eb = ptr[v], ee = ptr[v + 1];
+                if (!WEIGHTED && ee - eb > kCutWarpRow)
+                    continue;
                 for (uint64_t qq = eb; qq < ee; ++qq) {
                     const uint32_t x = col[qq];
                     const double wq = WEIGHTED ? a.w[qq] : 1.0;
@@ -455,6 +463,48 @@ __global__ void __launch_bounds__(kLocalThreads) local_push(PushArgs a) {
             }
         }
         __syncwarp();
+        if (a.nibble && !WEIGHTED) {
+            // The long rows' cut changes, one row at a time across the warp:
+            // with unit weights the row-order sum of +-1 is the exact integer
+            // (neighbours) - 2 (neighbours before v), whatever the order.
+            for (uint64_t base = 0; base < T; base += 32) {
+                const uint64_t i = base + lane;
+                uint32_t v = 0;
+                bool longrow = false;
+                if (i < T) {
+                    v = static_cast<uint32_t>(m.tab[m.tl[i]].tag);
+                    longrow = ptr[v + 1] - ptr[v] > kCutWarpRow;
+                }
+                unsigned lm = __ballot_sync(kFull, longrow);
+                while (lm) {
+                    const int src = __ffs(lm) - 1;
+                    lm &= lm - 1;
+                    const uint32_t vv = __shfl_sync(kFull, v, src);
+                    const uint64_t ii = base + static_cast<uint64_t>(src);
+                    const uint64_t kv = order_bits(__ddiv_rn(m.tab[m.tl[ii]].p, vol[vv]));
+                    const uint64_t eb = ptr[vv], ee = ptr[vv + 1];
+                    uint32_t before_cnt = 0;
+                    for (uint64_t qq = eb + lane; qq < ee; qq += 32) {
+                        const uint32_t x = col[qq];
+                        if (x == vv)
+                            continue;
+                        bool fr;
+                        double rx;
+                        const uint32_t hx = map_find(m.tab, m.cap, m.bits, epoch, x, false, fr, rx);
+                        if (hx < kNone - 1) {
+                            const uint64_t kx = order_bits(__ddiv_rn(m.tab[hx].p, vol[x]));
+                            before_cnt += (kx > kv || (kx == kv && x < vv)) ? 1u : 0u;
+                        }
+                    }
+                    for (int o = 16; o > 0; o >>= 1)
+                        before_cnt += __shfl_xor_sync(kFull, before_cnt, o);
+                    if (lane == 0)
+                        a.out_dcut[off + ii] =
+                            static_cast<double>(ee - eb) - 2.0 * static_cast<double>(before_cnt);
+                }
+            }
+            __syncwarp();
+        }
     }
 }
 
