@@ -772,11 +772,11 @@ def centrality_vs_reference(local, scale=21):
     return out
 
 
-def form_er(local, n=100_000, avg_deg=10, seed=42, runs=5):
+def form_er(local, n=100_000, avg_deg=10, seed=42, threads=8, runs=5):
     """PageRank FP64 on G(n = 1e5, average degree 10), undirected, the graph
-    the reference's ErdosRenyiGenerator draws from seed 42 (one thread,
-    setSeed(42, False); `generators.erdos_renyi_stream` draws the same
-    graph), damp 0.85, tol 1e-8, L2, not normalized. With distributeSinks,
+    the reference's ErdosRenyiGenerator draws from seed 42 on 8 OpenMP
+    threads (setSeed(42, False); `generators.erdos_renyi_stream` draws the
+    same graph), damp 0.85, tol 1e-8, L2, not normalized. With distributeSinks,
     as the workload asks: device time per run, iterations and L1 against the
     oracle. Without (this reference has no sink redistribution): the same,
     plus the reference's own PageRank::run() on the reference's own graph,
@@ -791,9 +791,9 @@ def form_er(local, n=100_000, avg_deg=10, seed=42, runs=5):
     import oracle
 
     p = avg_deg / (n - 1)
-    csr = generators.erdos_renyi_stream(n, p, seed)
+    csr = generators.erdos_renyi_stream(n, p, seed, threads=threads)
     res = {"workload": "pagerank_er1e5_deg10_l2_fp64", "n": n, "arcs": int(csr.arcs),
-           "graph": "the reference generator's draw (seed 42, one thread)"}
+           "graph": f"the reference generator's draw (seed {seed}, {threads} threads)"}
     for distribute in (True, False):
         dg = _capi.DeviceGraph(csr, device=local)
         prm = dg.params(0.85, 1e-8, 1, False, distribute, _capi.NKG_PREC_FP64, _capi.UINT64_MAX)
@@ -820,7 +820,7 @@ def form_er(local, n=100_000, avg_deg=10, seed=42, runs=5):
              "l1_vs_oracle": float(np.abs(s - o.scores).sum())}
         if not distribute and oracle.ref_available():
             cores = os.cpu_count() or 1
-            rg = oracle.RefGraph.erdos_renyi(n, p, seed, directed=False, threads=1)
+            rg = oracle.RefGraph.erdos_renyi(n, p, seed, directed=False, threads=threads)
             ref = min((rg.pagerank(damp=0.85, tol=1e-8, normalized=False, norm=1,
                                    nthreads=cores, want_ranking=False) for _ in range(3)),
                       key=lambda x: x["seconds"])

@@ -244,24 +244,31 @@ void hyperbolic_one(uint64_t n, double avg_deg, double exponent, std::mt19937_64
 
 extern "C" {
 
-// G(n, p) as NetworKit's ErdosRenyiGenerator(n, p, directed) draws it
-// (ErdosRenyiGenerator.cpp:21-33, ErdosRenyiEnumerator.hpp): 64-bit
-// fixed-point uniforms X in [1, 2^64 - 1] (std::uniform_int_distribution) and
-// geometric skips 1 + floor((log2 X - 64) / log2(1 - q)) over the cells of the
-// adjacency matrix in row order (Batagelj & Brandes): rows u = 0..n-1 with
-// columns 0..n-1 (directed) or rows u = 1..n-1 with columns 0..u-1
-// (undirected). q = p; for p > 0.9 the draw runs with q = 1 - p and the cells
-// are emitted in order from a cursor that stops at each drawn cell and goes
-// on from it, as the reference's complement pass does (so every cell is
+// G(n, p) as NetworKit's ErdosRenyiGenerator(n, p, directed) draws it with
+// `threads` OpenMP threads (ErdosRenyiGenerator.cpp:21-33,
+// ErdosRenyiEnumerator.hpp). Thread t takes a range of rows: ceil(n / T) rows
+// each (directed), or, undirected, rows whose lower-triangle cells add up to
+// about 1/T of all cells (the reference's sqrt-based boundaries), the last
+// thread to n. Every thread's generator is seeded with the same `seed`
+// (setSeed(seed, false)), so every range restarts the same stream. Within a
+// range: 64-bit fixed-point uniforms X in [1, 2^64 - 1]
+// (std::uniform_int_distribution) and geometric skips
+// 1 + floor((log2 X - 64) / log2(1 - q)) over the range's cells in row order
+// (Batagelj & Brandes): columns 0..n-1 (directed) or 0..u-1 (undirected, rows
+// from 1). q = p; for p > 0.9 the draw runs with q = 1 - p and the range's
+// cells are emitted in order from a cursor that stops at each drawn cell and
+// goes on from it, as the reference's complement pass does (so every cell is
 // emitted). No draws when q < n^-3. Self-loops of the directed draw are
 // dropped. Rows as GraphBuilder::toGraph(true, false) builds them.
-int nkgen_erdos_renyi_stream(uint64_t n, double p, uint64_t seed, int directed,
+int nkgen_erdos_renyi_stream(uint64_t n, double p, uint64_t seed, int directed, int threads,
                              nkgen_csr *out) {
     try {
         if (n < 1 || n >= 0xffffffffull)
             throw std::runtime_error("n out of range");
         if (!(p >= 0.0 && p <= 1.0))
             throw std::runtime_error("p must be in [0, 1]");
+        if (threads < 1)
+            throw std::runtime_error("threads must be at least 1");
         const bool dir = directed != 0;
         std::vector<std::vector<uint32_t>> own(n);
         auto emit = [&](uint64_t u, uint64_t v) {
@@ -270,40 +277,72 @@ int nkgen_erdos_renyi_stream(uint64_t n, double p, uint64_t seed, int directed,
         };
         const bool complement = p > 0.9;
         const double q = complement ? 1.0 - p : p;
-        uint64_t cu = dir ? 0 : 1, cv = 0;  // complement cursor
-        auto cover_to = [&](uint64_t u, uint64_t v) {
-            while (!(cu == u && cv == v)) {
-                emit(cu, cv);
-                if (++cv == (dir ? n : cu)) {
-                    cv = 0;
-                    ++cu;
+        // One thread's range [begin, end) of rows, drawn as the reference does.
+        auto draw_range = [&](uint64_t begin, uint64_t end) {
+            uint64_t cu = begin, cv = 0;  // complement cursor
+            if (!dir && cu == 0)
+                cu = 1;
+            auto cover_to = [&](uint64_t u, uint64_t v) {
+                while (!(cu == u && cv == v)) {
+                    emit(cu, cv);
+                    if (++cv == (dir ? n : cu)) {
+                        cv = 0;
+                        ++cu;
+                    }
+                }
+            };
+            if (!(q < std::pow(static_cast<double>(n), -3.0))) {
+                const double inv_log2 = 1.0 / std::log2(1.0 - q);
+                std::mt19937_64 urng(seed);
+                std::uniform_int_distribution<unsigned long long> uni{
+                    1, std::numeric_limits<unsigned long long>::max()};
+                uint64_t cur = begin;
+                if (!dir && cur == 0)
+                    cur = 1;
+                uint64_t nxt = ~0ull;
+                while (cur < end) {
+                    const double x = static_cast<double>(uni(urng));
+                    nxt += 1 + static_cast<uint64_t>(std::floor((std::log2(x) - 64.0) * inv_log2));
+                    while (nxt >= (dir ? n : cur)) {
+                        nxt -= dir ? n : cur;
+                        ++cur;
+                    }
+                    if (cur < end) {
+                        if (complement)
+                            cover_to(cur, nxt);
+                        else
+                            emit(cur, nxt);
+                    }
                 }
             }
+            if (complement)
+                cover_to(end, 0);
         };
-        if (!(q < std::pow(static_cast<double>(n), -3.0))) {
-            const double inv_log2 = 1.0 / std::log2(1.0 - q);
-            std::mt19937_64 urng(seed);
-            std::uniform_int_distribution<unsigned long long> uni{
-                1, std::numeric_limits<unsigned long long>::max()};
-            uint64_t cur = dir ? 0 : 1;
-            uint64_t nxt = ~0ull;
-            while (cur < n) {
-                const double x = static_cast<double>(uni(urng));
-                nxt += 1 + static_cast<uint64_t>(std::floor((std::log2(x) - 64.0) * inv_log2));
-                while (nxt >= (dir ? n : cur)) {
-                    nxt -= dir ? n : cur;
-                    ++cur;
-                }
-                if (cur < n) {
-                    if (complement)
-                        cover_to(cur, nxt);
-                    else
-                        emit(cur, nxt);
-                }
+        const uint64_t T = static_cast<uint64_t>(threads);
+        if (dir) {
+            const uint64_t chunk = (n + T - 1) / T;
+            for (uint64_t t = 0; t < T; ++t) {
+                const uint64_t b = std::min(n, t * chunk), e = std::min(n, (t + 1) * chunk);
+                if (b < e)
+                    draw_range(b, e);
+            }
+        } else {
+            // ErdosRenyiEnumerator::forEdgesParallel, undirected: boundaries in
+            // double arithmetic as the reference computes them.
+            const uint64_t chunk = (n * (n - 1) / 2 + T - 1) / T;
+            double last = 0.0;
+            for (uint64_t t = 0; t < T; ++t) {
+                const double first = last;
+                const uint64_t upper = static_cast<uint64_t>(
+                    std::ceil(std::sqrt(0.25 + first * first + first + 2 * chunk)));
+                last = static_cast<double>(std::min<uint64_t>(n, upper));
+                double end = last;
+                if (t + 1 == T)
+                    end = static_cast<double>(n);
+                if (first < end)
+                    draw_range(static_cast<uint64_t>(first), static_cast<uint64_t>(end));
             }
         }
-        if (complement)
-            cover_to(n, 0);
         half_edges_to_csr(own, dir, out);
         return 0;
     } catch (const std::exception &e) {

@@ -51,7 +51,7 @@ def _load():
         L.nkgen_erdos_renyi.argtypes = [C.c_uint64, C.c_double, C.c_uint64, C.c_int,
                                         C.POINTER(_Csr)]
         L.nkgen_erdos_renyi_stream.argtypes = [C.c_uint64, C.c_double, C.c_uint64, C.c_int,
-                                               C.POINTER(_Csr)]
+                                               C.c_int, C.POINTER(_Csr)]
         L.nkgen_barabasi_albert_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64,
                                                    C.c_uint64, C.POINTER(_Csr)]
         L.nkgen_hyperbolic_stream.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_uint64,
@@ -101,14 +101,16 @@ def erdos_renyi(n: int, p: float, seed: int = 42, nthreads: int = 0) -> InCSR:
     return _take(out, False)
 
 
-def erdos_renyi_stream(n: int, p: float, seed: int = 42, directed: bool = False) -> InCSR:
+def erdos_renyi_stream(n: int, p: float, seed: int = 42, directed: bool = False,
+                       threads: int = 1) -> InCSR:
     """G(n, p) drawn as NetworKit's ErdosRenyiGenerator(n, p, directed) draws
-    it on one OpenMP thread after ``setSeed(seed, False)``: the same graph,
-    with the adjacency order of the Graph it builds (a single
-    std::mt19937_64 stream, so the result is sequential)."""
+    it with `threads` OpenMP threads after ``setSeed(seed, False)``: the same
+    graph, with the adjacency order of the Graph it builds. The reference's
+    graph depends on its thread count (every thread restarts the seed's
+    stream on its own range of rows), so the count is part of the input."""
     out = _Csr()
     _check(_load().nkgen_erdos_renyi_stream(int(n), float(p), int(seed), int(bool(directed)),
-                                            C.byref(out)))
+                                            int(threads), C.byref(out)))
     return _take(out, bool(directed))
 
 

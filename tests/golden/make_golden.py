@@ -242,14 +242,15 @@ def nkbg_formats(O):
 
 
 # The Erdos-Renyi workload: G(n = 100000, average degree 10), undirected,
-# edges drawn from seed 42.
-ER_N, ER_P, ER_SEED = 100000, 10.0 / 99999.0, 42
+# edges drawn from seed 42 on 8 OpenMP threads (the reference's graph depends
+# on the thread count).
+ER_N, ER_P, ER_SEED, ER_THREADS = 100000, 10.0 / 99999.0, 42, 8
 ER_SAMPLE = 97  # every 97th score is stored
 
 
 def er_config(O):
     """The reference's ErdosRenyiGenerator(100000, 10 / 99999) graph, drawn
-    on one OpenMP thread after setSeed(42, False), and the reference's
+    on 8 OpenMP threads after setSeed(42, False), and the reference's
     PageRank on it (damp 0.85, tol 1e-8, L2, not normalized; this reference
     has no sink redistribution) in ``er_config.npz``: SHA-256 digests of the
     in-adjacency (row offsets as uint64, ids as uint32), the arc count, the
@@ -257,11 +258,12 @@ def er_config(O):
     ranking ids."""
     import hashlib
 
-    g = O.RefGraph.erdos_renyi(ER_N, ER_P, ER_SEED, directed=False, threads=1)
+    g = O.RefGraph.erdos_renyi(ER_N, ER_P, ER_SEED, directed=False, threads=ER_THREADS)
     a = export_to_arrays(g)
     r = g.pagerank(damp=0.85, tol=1e-8, normalized=False, norm=1, nthreads=1)
     out = dict(
         n=np.int64(ER_N), p=np.float64(ER_P), seed=np.int64(ER_SEED),
+        threads=np.int64(ER_THREADS),
         arcs=np.int64(a["in_ptr"][-1]),
         in_ptr_sha256=np.bytes_(hashlib.sha256(a["in_ptr"].tobytes()).hexdigest()),
         in_col_sha256=np.bytes_(hashlib.sha256(a["in_col"].tobytes()).hexdigest()),

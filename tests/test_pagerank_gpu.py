@@ -80,7 +80,7 @@ def test_rmat_parity_l1(oracle_mod, distribute, scale, arc_order, shape):
 
 def test_er_config_parity(oracle_mod):
     """G(n=1e5, avg degree 10) undirected as the reference's generator draws
-    it from seed 42, L2 1e-8, with and without distributeSinks: against the
+    it from seed 42 on 8 threads, L2 1e-8, with and without distributeSinks: against the
     oracle, and (without, as this reference has no sink redistribution)
     against the reference's own stored run on that graph
     (tests/golden/er_config.npz): iterations within 1, every stored score
@@ -88,7 +88,8 @@ def test_er_config_parity(oracle_mod):
     import os
 
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", "er_config.npz"))
-    csr = generators.erdos_renyi_stream(int(g["n"]), float(g["p"]), int(g["seed"]))
+    csr = generators.erdos_renyi_stream(int(g["n"]), float(g["p"]), int(g["seed"]),
+                                        threads=int(g["threads"]))
     assert csr.in_ptr[-1] == int(g["arcs"])
     for distribute in (False, True):
         o = oracle_mod.pagerank(csr, tol=1e-8, norm=1, distribute_sinks=distribute)

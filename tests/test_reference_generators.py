@@ -2,13 +2,13 @@
 are the reference generators' own draws.
 
 `generators.erdos_renyi_stream` restates NetworKit's ErdosRenyiGenerator on
-one OpenMP thread after setSeed(seed, False) (ErdosRenyiGenerator.cpp:21-33,
-ErdosRenyiEnumerator.hpp). Pinned two ways: the SHA-256 digests of the
-G(1e5, average degree 10) graph that the reference itself drew
-(tests/golden/er_config.npz, made by tests/golden/make_golden.py), and, where
-the reference library is built (oracle/_ref), array equality with the
-reference's Graph on directed, undirected, sparse and dense (complement-pass)
-cases. The oracle's PageRank on that graph then meets the reference's stored
+a given number of OpenMP threads after setSeed(seed, False)
+(ErdosRenyiGenerator.cpp:21-33, ErdosRenyiEnumerator.hpp). Pinned two ways:
+the SHA-256 digests of the G(1e5, average degree 10) graph that the reference
+itself drew on 8 threads (tests/golden/er_config.npz, made by
+tests/golden/make_golden.py), and, where the reference library is built
+(oracle/_ref), array equality with the reference's Graph on directed,
+undirected, sparse and dense (complement-pass) cases and 1 to 16 threads. The oracle's PageRank on that graph then meets the reference's stored
 run. `generators.barabasi_albert_stream` restates BarabasiAlbertGenerator's
 default (Batagelj-Brandes) draw, pinned the same two ways: the digests of the
 n = 4M, k = 8 graph of the batched-PPR workload (tests/golden/ba_config.npz)
@@ -35,7 +35,8 @@ def golden():
 
 def er_graph():
     g = golden()
-    return generators.erdos_renyi_stream(int(g["n"]), float(g["p"]), int(g["seed"]))
+    return generators.erdos_renyi_stream(int(g["n"]), float(g["p"]), int(g["seed"]),
+                                         threads=int(g["threads"]))
 
 
 def test_stream_graph_matches_the_reference_digests():
@@ -49,14 +50,16 @@ def test_stream_graph_matches_the_reference_digests():
     np.testing.assert_array_equal(csr.outdeg, np.diff(csr.in_ptr))
 
 
-@pytest.mark.parametrize("n,p,directed", [(3000, 0.004, False), (2500, 0.003, True),
-                                          (400, 0.95, False), (300, 0.92, True),
-                                          (60, 0.0, False), (50, 1.0, True), (1, 0.5, False)])
-def test_stream_graph_matches_the_reference_generator(oracle_mod, n, p, directed):
+@pytest.mark.parametrize("n,p,directed,threads", [
+    (3000, 0.004, False, 1), (3000, 0.004, False, 3), (2500, 0.003, True, 1),
+    (2500, 0.003, True, 8), (400, 0.95, False, 1), (400, 0.95, False, 4), (300, 0.92, True, 5),
+    (60, 0.0, False, 2), (50, 1.0, True, 1), (1, 0.5, False, 1), (7, 0.5, False, 16),
+    (20000, 5e-4, False, 8)])
+def test_stream_graph_matches_the_reference_generator(oracle_mod, n, p, directed, threads):
     if not oracle_mod.ref_available():
         pytest.skip("the reference library (oracle/_ref) is not built")
-    ours = generators.erdos_renyi_stream(n, p, 42, directed)
-    e = oracle_mod.RefGraph.erdos_renyi(n, p, 42, directed, threads=1).export()
+    ours = generators.erdos_renyi_stream(n, p, 42, directed, threads=threads)
+    e = oracle_mod.RefGraph.erdos_renyi(n, p, 42, directed, threads=threads).export()
     ptr, adj = (e["in_ptr"], e["in_adj"]) if directed else (e["out_ptr"], e["out_adj"])
     np.testing.assert_array_equal(ours.in_ptr, ptr)
     np.testing.assert_array_equal(ours.in_col, adj)
@@ -76,6 +79,8 @@ def test_stream_generator_rejects_bad_arguments():
         generators.erdos_renyi_stream(10, 1.5)
     with pytest.raises(RuntimeError, match="n out of range"):
         generators.erdos_renyi_stream(0, 0.5)
+    with pytest.raises(RuntimeError, match="threads"):
+        generators.erdos_renyi_stream(10, 0.5, threads=0)
 
 
 BA_GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "ba_config.npz")
