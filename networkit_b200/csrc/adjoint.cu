@@ -266,9 +266,10 @@ struct AdjArgs {
     double *__restrict__ lam_out;         // n+1 or null (c only)
     double *__restrict__ c_out;           // n or null
     double *__restrict__ chunk_val;
-    double *__restrict__ part;            // 2 per sweep CTA
+    double *__restrict__ part;            // 2 per work unit of the sweep
     double *__restrict__ fix_part;        // 2 per fix-up CTA
     AdjState *st;
+    unsigned int *queue;                  // next work unit of the sweep (reset by adj_fix)
     double damp, inv_n, tol;
     unsigned long long max_iter;
     uint32_t n, n_long, n_vlong, s_chunk, units, sweep_ctas;
@@ -294,16 +295,20 @@ __device__ __forceinline__ void adj_row(const AdjArgs &a, uint32_t v, double acc
 template <bool WEIGHTED, int THREADS, int UNROLL>
 __global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 512 / THREADS : WEIGHTED ? 1024 / THREADS : 1536 / THREADS)
     adj_sweep(AdjArgs a) {
-    __shared__ double s_red[32];
     if (*(volatile int *)&a.st->done)
         return;
     const double tdot = a.st->tdot;
     const int lane = threadIdx.x & 31;
-    const uint32_t wpc = THREADS / 32;
-    const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);
-    const uint32_t nw = gridDim.x * wpc;
-    double res = 0.0, td = 0.0;
-    for (uint32_t u = gw; u < a.units; u += nw) {
+    // Warps take units from a device counter in order (as the queued
+    // PageRank sweep); every unit's two partial sums go to their own slots.
+    for (;;) {
+        uint32_t u = 0;
+        if (lane == 0)
+            u = atomicAdd(a.queue, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= a.units)
+            return;
+        double res = 0.0, td = 0.0;
         const uint32_t s_end = a.unit_start[u + 1];
         for (uint32_t s = a.unit_start[u]; s < s_end; ++s) {
             const uint32_t off = a.slice_off[s];
@@ -359,12 +364,12 @@ __global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 512 / THREADS : WEIGHTED
                     adj_row<WEIGHTED>(a, r, acc, tdot, res, td);
             }
         }
-    }
-    res = block_sum<THREADS>(res, s_red);
-    td = block_sum<THREADS>(td, s_red);
-    if (threadIdx.x == 0) {
-        a.part[2 * blockIdx.x] = res;
-        a.part[2 * blockIdx.x + 1] = td;
+        res = warp_sum(res);
+        td = warp_sum(td);
+        if (lane == 0) {
+            a.part[2 * static_cast<size_t>(u)] = res;
+            a.part[2 * static_cast<size_t>(u) + 1] = td;
+        }
     }
 }
 
@@ -378,6 +383,12 @@ __global__ void __launch_bounds__(kAdjThreads) adj_fix(AdjArgs a) {
         return;
     const double tdot = a.st->tdot;
     double res = 0.0, td = 0.0;
+    // The sweep's unit partials: a fixed share of the units per thread.
+    for (uint32_t i = blockIdx.x * kAdjThreads + threadIdx.x; i < a.units;
+         i += gridDim.x * kAdjThreads) {
+        res += a.part[2 * static_cast<size_t>(i)];
+        td += a.part[2 * static_cast<size_t>(i) + 1];
+    }
     uint32_t r;
     double acc;
     if (split_row_sum<kAdjThreads>(a.chunk_begin, a.chunk_val, a.n_long, a.n_vlong, r, acc))
@@ -391,10 +402,6 @@ __global__ void __launch_bounds__(kAdjThreads) adj_fix(AdjArgs a) {
     if (!bi_last_block(&a.st->ticket, &s_last))
         return;
     double t1 = 0.0, t2 = 0.0;
-    for (uint32_t i = threadIdx.x; i < a.sweep_ctas; i += kAdjThreads) {
-        t1 += ((volatile double *)a.part)[2 * i];
-        t2 += ((volatile double *)a.part)[2 * i + 1];
-    }
     for (uint32_t i = threadIdx.x; i < gridDim.x; i += kAdjThreads) {
         t1 += ((volatile double *)a.fix_part)[2 * i];
         t2 += ((volatile double *)a.fix_part)[2 * i + 1];
@@ -410,6 +417,7 @@ __global__ void __launch_bounds__(kAdjThreads) adj_fix(AdjArgs a) {
             st->tdot = a.personal ? t2 : t2 * a.inv_n;
         }
         st->ticket = 0;
+        *a.queue = 0;
         __threadfence();
         st->done = (it >= a.max_iter || t1 <= a.tol) ? 1 : 0;
     }
@@ -833,8 +841,8 @@ void adjoint_launch_setup(nkg_graph *g, AdjointState &A) {
     int occ32 = 0, occ64 = 0, threads = 0;
     with_sweep_shape(g->sweep_shape, [&](auto S) {
         using Sh = decltype(S);
-        auto k32 = bi_mv<WEIGHTED, 0, 1, Sh::threads, Sh::unroll>;
-        auto k32b = bi_mv<WEIGHTED, 1, 1, Sh::threads, Sh::unroll>;
+        auto k32 = bi_mv<WEIGHTED, 0, 1, Sh::threads, Sh::unroll, true>;
+        auto k32b = bi_mv<WEIGHTED, 1, 1, Sh::threads, Sh::unroll, true>;
         auto k64 = adj_sweep<WEIGHTED, Sh::threads, Sh::unroll>;
         NKG_CUDA(cudaFuncSetAttribute(k32, cudaFuncAttributePreferredSharedMemoryCarveout, 0));
         NKG_CUDA(cudaFuncSetAttribute(k32b, cudaFuncAttributePreferredSharedMemoryCarveout, 0));
@@ -856,7 +864,7 @@ void adjoint_launch_setup(nkg_graph *g, AdjointState &A) {
     auto units = [&](unsigned c) {
         const uint64_t warps = static_cast<uint64_t>(c) * (threads / 32);
         return static_cast<uint32_t>(std::max<uint64_t>(
-            1, std::min<uint64_t>(warps * kUnitsPerWarp, std::max<uint64_t>(slices, 1))));
+            1, std::min<uint64_t>(warps * kQueueUnitsPerWarp, std::max<uint64_t>(slices, 1))));
     };
     A.ctas32 = ctas(occ32);
     A.ctas64 = ctas(occ64);
@@ -876,7 +884,9 @@ void adjoint_launch_setup(nkg_graph *g, AdjointState &A) {
     A.work.ready = false;  // partial-sum buffers depend on the grids
 }
 
-constexpr size_t kScalOffBi = 0, kScalOffAdj = 128, kScalOffSt = 256, kScalBytes = 384;
+constexpr size_t kScalOffBi = 0, kScalOffAdj = 128, kScalOffSt = 256, kScalOffQueue = 320,
+                 kScalBytes = 384;
+static_assert(sizeof(AdjState) <= kScalOffQueue - kScalOffSt, "the queue counter follows the state");
 
 void ensure_work(nkg_graph *g, AdjointState &A, unsigned vec_ctas, unsigned fix_ctas) {
     AdjWork &W = A.work;
@@ -889,7 +899,8 @@ void ensure_work(nkg_graph *g, AdjointState &A, unsigned vec_ctas, unsigned fix_
         a->alloc(n);
     W.lam[0].alloc(n + 1);
     W.lam[1].alloc(n + 1);
-    W.part.alloc(3 * part_n);
+    W.part.alloc(std::max<size_t>(3 * part_n, 2 * static_cast<size_t>(
+                                                   std::max(A.n_units32, A.n_units64))));
     W.fix_part.alloc(2 * static_cast<size_t>(fix_ctas));
     W.chunk64.alloc(chunks);
     W.chunk32.alloc(chunks);
@@ -982,6 +993,8 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
     aa.part = W.part.get();
     aa.fix_part = W.fix_part.get();
     aa.st = st;
+    // The sweep's unit counter sits after the state in the zeroed scalars.
+    aa.queue = reinterpret_cast<unsigned int *>(W.scal.get() + kScalOffQueue);
     aa.damp = p.damp;
     aa.inv_n = inv_n;
     aa.tol = tol_abs;
@@ -1063,6 +1076,9 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
         a.s_chunk = A.tl.s_chunk;
         a.units = A.n_units32;
         a.sweep_ctas = A.ctas32;
+        // Queued products (the units of units32); their partials share W.part
+        // with the vector kernels', which never run at the same time.
+        a.unit_part = W.part.get();
         a.distribute = distribute;
         a.personal = personal;
         a.l2 = 0;

@@ -14,7 +14,9 @@
 //
 // Per iteration: one sweep over the slices (each lane sums its row in arc
 // order, products rounded separately like the reference, no FMA
-// contraction), one fix-up for rows split into chunks whose last CTA reduces
+// contraction; warps take cost-balanced units of slices from a device
+// counter and store each unit's sum of squares in a slot of its own), one
+// fix-up for rows split into chunks whose last CTA reduces
 // sum(values^2) in a fixed order and takes the stopping test. The eigenvector's
 // division by the length is folded into the next sweep: x holds the values
 // before scaling, every row divides its sum by the previous length once (the
@@ -45,6 +47,7 @@ struct CentState {
     unsigned long long iteration;
     int done;
     unsigned int ticket;
+    unsigned int queue;   // next work unit of the sweep (reset by cent_fix)
 };
 
 struct CentArgs {
@@ -56,7 +59,7 @@ struct CentArgs {
     const double *__restrict__ x_in;         // n+1 (x_in[n] = pad)
     double *__restrict__ x_out;              // n+1 (rows < n written)
     double *__restrict__ chunk_val;
-    double *__restrict__ part;               // per sweep CTA
+    double *__restrict__ part;               // per work unit of the sweep
     double *__restrict__ fix_part;           // per fix-up CTA
     CentState *st;
     double alpha, beta, tol;
@@ -90,16 +93,20 @@ __device__ __forceinline__ void cent_row(const CentArgs &a, uint32_t r, double a
 template <int MODE, bool WEIGHTED, int THREADS, int UNROLL>
 __global__ void __launch_bounds__(THREADS, WEIGHTED || UNROLL > 8 ? 1024 / THREADS : 1536 / THREADS)
     cent_sweep(CentArgs a) {
-    __shared__ double s_red[32];
     if (*(volatile int *)&a.st->done)
         return;
     const double len_prev = MODE == 0 ? cent_prev_length(a) : 0.0;
     const int lane = threadIdx.x & 31;
-    const uint32_t wpc = THREADS / 32;
-    const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);
-    const uint32_t nw = gridDim.x * wpc;
-    double sq = 0.0;
-    for (uint32_t u = gw; u < a.units; u += nw) {
+    // Warps take units from a device counter in order (as the queued
+    // PageRank sweep); every unit's sum of squares goes to its own slot.
+    for (;;) {
+        uint32_t u = 0;
+        if (lane == 0)
+            u = atomicAdd(&a.st->queue, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= a.units)
+            return;
+        double sq = 0.0;
         const uint32_t s_end = a.unit_start[u + 1];
         for (uint32_t s = a.unit_start[u]; s < s_end; ++s) {
             const uint32_t off = a.slice_off[s];
@@ -151,10 +158,10 @@ __global__ void __launch_bounds__(THREADS, WEIGHTED || UNROLL > 8 ? 1024 / THREA
                     cent_row<MODE>(a, r, acc, len_prev, sq);
             }
         }
+        sq = warp_sum(sq);
+        if (lane == 0)
+            a.part[u] = sq;
     }
-    sq = block_sum<THREADS>(sq, s_red);
-    if (threadIdx.x == 0)
-        a.part[blockIdx.x] = sq;
 }
 
 // Split rows (a warp for each row of many chunks, one thread for each other
@@ -168,6 +175,9 @@ __global__ void __launch_bounds__(kCentFix) cent_fix(CentArgs a) {
         return;
     const double len_prev = MODE == 0 ? cent_prev_length(a) : 0.0;
     double sq = 0.0;
+    // The sweep's unit partials: a fixed share of the units per thread.
+    for (uint32_t i = blockIdx.x * kCentFix + threadIdx.x; i < a.units; i += gridDim.x * kCentFix)
+        sq += a.part[i];
     uint32_t r;
     double acc;
     if (split_row_sum<kCentFix>(a.chunk_begin, a.chunk_val, a.n_long, a.n_vlong, r, acc))
@@ -183,8 +193,6 @@ __global__ void __launch_bounds__(kCentFix) cent_fix(CentArgs a) {
         return;
     __threadfence();
     double t = 0.0;
-    for (uint32_t i = threadIdx.x; i < a.sweep_ctas; i += kCentFix)
-        t += ((volatile double *)a.part)[i];
     for (uint32_t i = threadIdx.x; i < gridDim.x; i += kCentFix)
         t += ((volatile double *)a.fix_part)[i];
     t = block_sum<kCentFix>(t, s_red);
@@ -196,6 +204,7 @@ __global__ void __launch_bounds__(kCentFix) cent_fix(CentArgs a) {
         st->length = length;
         st->iteration = it;
         st->ticket = 0;
+        st->queue = 0;
         __threadfence();
         st->done = ((length <= old + a.tol && length >= old - a.tol) || it >= a.max_iter) ? 1 : 0;
     }
@@ -270,13 +279,13 @@ CentResult cent_run(nkg_graph *g, const SellLayout &L, const double *w_sell, dou
         1, std::min<uint64_t>(static_cast<uint64_t>(occ) * sms,
                               (slices * 32 + kCentThreads - 1) / kCentThreads)));
     const uint32_t units = static_cast<uint32_t>(std::max<uint64_t>(
-        1, std::min<uint64_t>(static_cast<uint64_t>(ctas) * (kCentThreads / 32) * kUnitsPerWarp,
+        1, std::min<uint64_t>(static_cast<uint64_t>(ctas) * (kCentThreads / 32) * kQueueUnitsPerWarp,
                               std::max<uint64_t>(slices, 1))));
     const unsigned fix_ctas = split_fix_ctas<kCentFix>(L.n_long, L.n_vlong);
     DeviceArray<uint32_t> unit_start(static_cast<size_t>(units) + 1);
     sell_units(L, units, unit_start.get(), s);
     DeviceArray<double> x[2] = {DeviceArray<double>(n + 1), DeviceArray<double>(n + 1)};
-    DeviceArray<double> chunk_val(static_cast<size_t>(L.s_chunk) * 32 + 1), part(ctas),
+    DeviceArray<double> chunk_val(static_cast<size_t>(L.s_chunk) * 32 + 1), part(units),
         fix_part(fix_ctas);
     DeviceArray<CentState> st(1);
     CentResult R;

@@ -13,6 +13,12 @@ namespace nkg {
 constexpr int kSweepsPerGraph = 8;
 // Work units per resident warp of the sweep kernel.
 constexpr uint32_t kUnitsPerWarp = 8;
+// Work units per resident warp of the queued PageRank sweep. Measured on
+// R-MAT scale 24 (FP64 sweep, B200): 4 / 8 / 12 / 16 / 24 / 32 / 64 units per
+// warp ran 0.941 / 0.880 / 0.876 / 0.875 / 0.889 / 0.900 / 0.975 ms, against
+// 0.956 ms for 8 static units per warp. Fewer units leave a longer tail;
+// more units pay the ticket round trip and a cold start more often.
+constexpr uint32_t kQueueUnitsPerWarp = 16;
 // Cost of a slice in units of one slot step, besides its length (the
 // epilogue of its 32 rows).
 constexpr uint32_t kSliceOverhead = 3;
@@ -21,6 +27,7 @@ constexpr uint32_t kSliceOverhead = 3;
 struct RefineWork {
     DeviceArray<float> x, r, rhat, p, v, s, t, g;  // g: n+1 (gather form, g[n] = 0)
     DeviceArray<double> x64, part, fix_part;
+    DeviceArray<double> unit_part;                  // queued product: 2 per unit
     DeviceArray<unsigned char> sc;                  // BiScalars
 };
 
@@ -79,6 +86,12 @@ struct Plane {
     uint32_t hot_units = 0;
     unsigned hot_ctas = 0;
     int hot_threads = 0;         // kHotThreads or kHotThreadsPair
+    // Queued sweep (warps take units from a device counter): its units and
+    // their residual / sink partials (2 x q_units). q_units 0: the static
+    // assignment of unit_start (the shared-memory tier).
+    DeviceArray<uint32_t> q_unit_start;
+    DeviceArray<double> q_part;
+    uint32_t q_units = 0;
 };
 
 } // namespace nkg

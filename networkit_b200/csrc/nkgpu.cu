@@ -1334,7 +1334,7 @@ static void sweep_setup(nkg_graph *g) {
     int occ = 0, threads = 0;
     with_sweep_shape(g->sweep_shape, [&](auto S) {
         using Sh = decltype(S);
-        auto kfn = sweep_kernel<T, WEIGHTED, Sh::threads, Sh::unroll>;
+        auto kfn = sweep_kernel<T, WEIGHTED, Sh::threads, Sh::unroll, false, false, true>;
         // The kernel needs almost no shared memory: give the L1 the most room.
         NKG_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, 0));
         NKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, Sh::threads, 0));
@@ -1354,6 +1354,16 @@ static void sweep_setup(nkg_graph *g) {
     P.fix_ctas = fix_vlong_ctas(g->fw.n_vlong) +
                  ceil_div(std::max<uint32_t>(g->fw.n_long - g->fw.n_vlong, 1), kFixThreads);
     P.hot = hot_tier_ids<T>(g);
+    if (!P.hot) {
+        // The queued sweep's units (the tier kernel keeps the static ones).
+        P.q_units = static_cast<uint32_t>(std::max<uint64_t>(
+            1, std::min<uint64_t>(warps * kQueueUnitsPerWarp, g->fw.slices)));
+        P.q_unit_start.alloc(static_cast<size_t>(P.q_units) + 1);
+        P.q_part.alloc(2 * static_cast<size_t>(P.q_units));
+        unit_bounds<<<ceil_div(static_cast<uint64_t>(P.q_units) + 1, 256), 256, 0, s>>>(
+            g->fw.slice_cost.get(), g->fw.slices, P.q_units, P.q_unit_start.get());
+        NKG_CUDA(cudaGetLastError());
+    }
     if (P.hot) {
         const int bytes = static_cast<int>(P.hot * sizeof(T));
         int sm_smem = 0;
@@ -1427,6 +1437,12 @@ static SweepArgs<T> sweep_args(nkg_graph *g, int in_buf) {
     a.sweep_ctas = P.hot ? P.hot_ctas : P.sweep_ctas;
     if (P.hot)
         a.unit_start = P.hot_unit_start.get();
+    if (P.q_units) {
+        a.units = P.q_units;
+        a.unit_start = P.q_unit_start.get();
+        a.unit_res = P.q_part.get();
+        a.unit_sink = P.q_part.get() + P.q_units;
+    }
     a.hot = P.hot;
     a.trace = g->trace.get();
     a.trace_cap = kTraceCapacity;
@@ -1447,7 +1463,8 @@ static void launch_sweep_kernel(nkg_graph *g, const SweepArgs<T> &a, cudaStream_
     }
     with_sweep_shape(g->sweep_shape, [&](auto S) {
         using Sh = decltype(S);
-        sweep_kernel<T, WEIGHTED, Sh::threads, Sh::unroll><<<P.sweep_ctas, Sh::threads, 0, s>>>(a);
+        sweep_kernel<T, WEIGHTED, Sh::threads, Sh::unroll, false, false, true>
+            <<<P.sweep_ctas, Sh::threads, 0, s>>>(a);
     });
 }
 
@@ -1684,6 +1701,14 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
     a.s_chunk = g->fw.s_chunk;
     a.units = P32.units;
     a.sweep_ctas = P32.sweep_ctas;
+    if (P32.q_units) {
+        // The queued cut of the FP32 sweep (bi_mv QUEUED).
+        if (W.unit_part.size() < 2 * static_cast<size_t>(P32.q_units))
+            W.unit_part.alloc(2 * static_cast<size_t>(P32.q_units));
+        a.units = P32.q_units;
+        a.unit_start = P32.q_unit_start.get();
+        a.unit_part = W.unit_part.get();
+    }
     a.distribute = p.distribute_sinks ? 1 : 0;
     a.personal = personal;
     a.l2 = p.norm == NKG_NORM_L2;

@@ -34,6 +34,7 @@ struct BiScalars {
     double sink_vec;  // m.q (OP 0) or tel.q (OP 1), q the next product's input
     int breakdown;
     unsigned int ticket;
+    unsigned int queue;  // next work unit of a queued product (reset by bi_mv_fix)
 };
 
 struct BiArgs {
@@ -56,6 +57,11 @@ struct BiArgs {
     double damp, inv_n;
     uint32_t n, n_long, n_vlong, s_chunk, units, sweep_ctas;
     int distribute, personal, l2;
+    // Queued product (unit_part non-null): warps take units from sc->queue
+    // and store each unit's two partial sums at unit_part[2u], [2u+1], which
+    // bi_mv_fix adds in a fixed order; `units` / `unit_start` are then the
+    // queued cut. Null: round-robin units with per-CTA partials in `part`.
+    double *__restrict__ unit_part;
 };
 
 __device__ __forceinline__ float bi_tel(const BiArgs &a, uint32_t r) {
@@ -110,8 +116,72 @@ __device__ __forceinline__ void bi_mv_row(const BiArgs &a, uint32_t r, float acc
     }
 }
 
-// The SpMV of one slice per warp (the loop of sweep_kernel in FP32).
-template <bool WEIGHTED, int MODE, int OP, int THREADS, int UNROLL>
+// The SpMV of one work unit per warp (the loop of sweep_unit in FP32):
+// slices [s_begin, s_end), each lane one virtual row.
+template <bool WEIGHTED, int MODE, int OP, int UNROLL>
+__device__ __forceinline__ void bi_mv_unit(const BiArgs &a, const float *px, float *out,
+                                           const float *gsrc, uint32_t s_begin, uint32_t s_end,
+                                           int lane, double &d1, double &d2) {
+    for (uint32_t s = s_begin; s < s_end; ++s) {
+        const uint32_t off = a.slice_off[s];
+        const uint32_t len = a.slice_off[s + 1] - off;
+        const size_t base = static_cast<size_t>(off) * 32 + lane;
+        const uint32_t *cp = a.col_sell + base;
+        float acc = 0.f;
+        uint32_t j = 0;
+        for (; j + UNROLL <= len; j += UNROLL) {
+            uint32_t c[UNROLL];
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                c[k] = ld_stream(cp + static_cast<size_t>(j + k) * 32);
+            float vv[UNROLL];
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                vv[k] = c[k] != a.n ? __ldg(gsrc + c[k]) : 0.f;
+            if (WEIGHTED) {
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    vv[k] = __fmul_rn(vv[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
+            }
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                acc += vv[k];
+        }
+        if (j < len) {
+            // the last len - j < UNROLL steps as one predicated batch (same order)
+            uint32_t c[UNROLL];
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                c[k] = j + k < len ? ld_stream(cp + static_cast<size_t>(j + k) * 32) : 0u;
+            float vv[UNROLL];
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                vv[k] = j + k < len && c[k] != a.n ? __ldg(gsrc + c[k]) : 0.f;
+            if (WEIGHTED) {
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    if (j + k < len)
+                        vv[k] = __fmul_rn(vv[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
+            }
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                if (j + k < len)
+                    acc += vv[k];
+        }
+        if (s < a.s_chunk) {
+            a.chunk_val[static_cast<size_t>(s) * 32 + lane] = acc;
+        } else {
+            const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
+            if (r < a.n)
+                bi_mv_row<WEIGHTED, MODE, OP>(a, r, acc, px, out, d1, d2);
+        }
+    }
+}
+
+// The product. QUEUED: warps take units from sc->queue in order (as the
+// queued PageRank sweep) and every unit's partials go to unit_part; else
+// round-robin units with per-CTA partials.
+template <bool WEIGHTED, int MODE, int OP, int THREADS, int UNROLL, bool QUEUED = false>
 __global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 1024 / THREADS : 1536 / THREADS) bi_mv(BiArgs a) {
     __shared__ double s_red[32];
     if (a.sc->breakdown)
@@ -120,67 +190,32 @@ __global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 1024 / THREADS : 1536 / 
     float *out = MODE == 0 ? a.v : a.t;
     const float *gsrc = OP == 0 ? a.g : px;
     const int lane = threadIdx.x & 31;
+    if (QUEUED) {
+        for (;;) {
+            uint32_t u = 0;
+            if (lane == 0)
+                u = atomicAdd(&a.sc->queue, 1u);
+            u = __shfl_sync(0xffffffffu, u, 0);
+            if (u >= a.units)
+                return;
+            double d1 = 0.0, d2 = 0.0;
+            bi_mv_unit<WEIGHTED, MODE, OP, UNROLL>(a, px, out, gsrc, a.unit_start[u],
+                                                   a.unit_start[u + 1], lane, d1, d2);
+            d1 = warp_sum(d1);
+            d2 = warp_sum(d2);
+            if (lane == 0) {
+                a.unit_part[2 * static_cast<size_t>(u)] = d1;
+                a.unit_part[2 * static_cast<size_t>(u) + 1] = d2;
+            }
+        }
+    }
     const uint32_t wpc = THREADS / 32;
     const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);
     const uint32_t nw = gridDim.x * wpc;
     double d1 = 0.0, d2 = 0.0;
-    for (uint32_t u = gw; u < a.units; u += nw) {
-        const uint32_t s_end = a.unit_start[u + 1];
-        for (uint32_t s = a.unit_start[u]; s < s_end; ++s) {
-            const uint32_t off = a.slice_off[s];
-            const uint32_t len = a.slice_off[s + 1] - off;
-            const size_t base = static_cast<size_t>(off) * 32 + lane;
-            const uint32_t *cp = a.col_sell + base;
-            float acc = 0.f;
-            uint32_t j = 0;
-            for (; j + UNROLL <= len; j += UNROLL) {
-                uint32_t c[UNROLL];
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    c[k] = ld_stream(cp + static_cast<size_t>(j + k) * 32);
-                float vv[UNROLL];
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    vv[k] = c[k] != a.n ? __ldg(gsrc + c[k]) : 0.f;
-                if (WEIGHTED) {
-#pragma unroll
-                    for (int k = 0; k < UNROLL; ++k)
-                        vv[k] = __fmul_rn(vv[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
-                }
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    acc += vv[k];
-            }
-            if (j < len) {
-                // the last len - j < UNROLL steps as one predicated batch (same order)
-                uint32_t c[UNROLL];
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    c[k] = j + k < len ? ld_stream(cp + static_cast<size_t>(j + k) * 32) : 0u;
-                float vv[UNROLL];
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    vv[k] = j + k < len && c[k] != a.n ? __ldg(gsrc + c[k]) : 0.f;
-                if (WEIGHTED) {
-#pragma unroll
-                    for (int k = 0; k < UNROLL; ++k)
-                        if (j + k < len)
-                            vv[k] = __fmul_rn(vv[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
-                }
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    if (j + k < len)
-                        acc += vv[k];
-            }
-            if (s < a.s_chunk) {
-                a.chunk_val[static_cast<size_t>(s) * 32 + lane] = acc;
-            } else {
-                const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
-                if (r < a.n)
-                    bi_mv_row<WEIGHTED, MODE, OP>(a, r, acc, px, out, d1, d2);
-            }
-        }
-    }
+    for (uint32_t u = gw; u < a.units; u += nw)
+        bi_mv_unit<WEIGHTED, MODE, OP, UNROLL>(a, px, out, gsrc, a.unit_start[u], a.unit_start[u + 1],
+                                               lane, d1, d2);
     d1 = block_sum<THREADS>(d1, s_red);
     d2 = block_sum<THREADS>(d2, s_red);
     if (threadIdx.x == 0) {
@@ -200,6 +235,14 @@ __global__ void __launch_bounds__(kBiThreads) bi_mv_fix(BiArgs a) {
     const float *px = MODE == 0 ? a.p : a.s;
     float *out = MODE == 0 ? a.v : a.t;
     double d1 = 0.0, d2 = 0.0;
+    if (a.unit_part) {
+        // Partials of a queued product: a fixed share of the units per thread.
+        for (uint32_t i = blockIdx.x * kBiThreads + threadIdx.x; i < a.units;
+             i += gridDim.x * kBiThreads) {
+            d1 += a.unit_part[2 * static_cast<size_t>(i)];
+            d2 += a.unit_part[2 * static_cast<size_t>(i) + 1];
+        }
+    }
     uint32_t r;
     float acc;
     if (split_row_sum<kBiThreads>(a.chunk_begin, a.chunk_val, a.n_long, a.n_vlong, r, acc))
@@ -213,7 +256,8 @@ __global__ void __launch_bounds__(kBiThreads) bi_mv_fix(BiArgs a) {
     if (!bi_last_block(&a.sc->ticket, &s_last))
         return;
     double t1 = 0.0, t2 = 0.0;
-    for (uint32_t i = threadIdx.x; i < a.sweep_ctas; i += kBiThreads) {
+    const uint32_t sweep_parts = a.unit_part ? 0u : a.sweep_ctas;
+    for (uint32_t i = threadIdx.x; i < sweep_parts; i += kBiThreads) {
         t1 += ((volatile double *)a.part)[2 * i];
         t2 += ((volatile double *)a.part)[2 * i + 1];
     }
@@ -239,6 +283,7 @@ __global__ void __launch_bounds__(kBiThreads) bi_mv_fix(BiArgs a) {
                 sc->breakdown = 1;
         }
         sc->ticket = 0;
+        sc->queue = 0;
     }
 }
 
@@ -644,13 +689,21 @@ void bi_solve(const BiArgs &a, BiLaunch &L, double rel, double floor) {
             bi_vec_p<WEIGHTED, OP><<<L.vec_ctas, kBiThreads, 0, s>>>(a);
             with_sweep_shape(L.sweep_shape, [&](auto S) {
                 using Sh = decltype(S);
-                bi_mv<WEIGHTED, 0, OP, Sh::threads, Sh::unroll><<<L.sweep_ctas, Sh::threads, 0, s>>>(a);
+                if (a.unit_part)
+                    bi_mv<WEIGHTED, 0, OP, Sh::threads, Sh::unroll, true>
+                        <<<L.sweep_ctas, Sh::threads, 0, s>>>(a);
+                else
+                    bi_mv<WEIGHTED, 0, OP, Sh::threads, Sh::unroll><<<L.sweep_ctas, Sh::threads, 0, s>>>(a);
             });
             bi_mv_fix<WEIGHTED, 0, OP><<<L.fix_ctas, kBiThreads, 0, s>>>(a);
             bi_vec_s<WEIGHTED, OP><<<L.vec_ctas, kBiThreads, 0, s>>>(a);
             with_sweep_shape(L.sweep_shape, [&](auto S) {
                 using Sh = decltype(S);
-                bi_mv<WEIGHTED, 1, OP, Sh::threads, Sh::unroll><<<L.sweep_ctas, Sh::threads, 0, s>>>(a);
+                if (a.unit_part)
+                    bi_mv<WEIGHTED, 1, OP, Sh::threads, Sh::unroll, true>
+                        <<<L.sweep_ctas, Sh::threads, 0, s>>>(a);
+                else
+                    bi_mv<WEIGHTED, 1, OP, Sh::threads, Sh::unroll><<<L.sweep_ctas, Sh::threads, 0, s>>>(a);
             });
             bi_mv_fix<WEIGHTED, 1, OP><<<L.fix_ctas, kBiThreads, 0, s>>>(a);
             bi_vec_x<<<L.vec_ctas, kBiThreads, 0, s>>>(a);

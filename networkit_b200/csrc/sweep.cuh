@@ -18,8 +18,11 @@
 // lane], so a warp loads 128 contiguous bytes per step and every lane sums its
 // own row sequentially, in the reference's arc order. No shared memory and no
 // barriers are needed: the whole L1 is left to cache the hot part of y.
-// Warps walk contiguous, cost-balanced ranges of slices ("units", fixed at
-// set-up), so every sum has a fixed order and a run is bit-reproducible.
+// The slices are cut into contiguous, cost-balanced ranges ("units", fixed at
+// set-up). Warps take the next unit from a device counter, so at any time
+// they work on neighbouring units and no warp is left with a share that ends
+// late. Each unit's residual and sink partials go to a slot of its own, so
+// every sum has a fixed order and a run is bit-reproducible.
 #pragma once
 
 #include <algorithm>
@@ -58,7 +61,7 @@ struct IterState {
     int done;                      // converged / max reached
     unsigned int ticket;           // last-block detection in the fix-up
     int error;
-    int pad;
+    unsigned int queue;            // next work unit of a queued sweep (reset by the fix-up)
 };
 
 template <typename T>
@@ -97,6 +100,12 @@ struct SweepArgs {
     const uint32_t *__restrict__ row_map;
     uint32_t row_base;
     uint32_t pad;
+    // Queued sweep: warps take units from IterState::queue and store each
+    // unit's residual and sink partial sums here (indexed by unit), so the
+    // sums keep a fixed order whichever warp ran the unit. Null: the static
+    // round-robin assignment with per-CTA partials in cta_res / cta_sink.
+    double *unit_res;
+    double *unit_sink;
 };
 
 template <typename T>
@@ -230,23 +239,117 @@ __device__ __forceinline__ uint4 ld_na_v4(const uint4 *p) {
     return v;
 }
 
-// The sweep: each warp walks its units; each lane accumulates one virtual
-// row of a slice in arc order. Chunk slices store partial sums; row slices
-// finish rows.
+// Slices [s_begin, s_end) of one work unit: each lane accumulates one
+// virtual row of a slice in arc order. Chunk slices store partial sums; row
+// slices finish rows, adding their residual and sink terms to res / sink.
+template <typename T, bool WEIGHTED, int UNROLL, bool HOT, bool PART>
+__device__ __forceinline__ void sweep_unit(const SweepArgs<T> &a, const T *s_y, uint32_t s_begin,
+                                           uint32_t s_end, int lane, double &res, double &sink) {
+    for (uint32_t s = s_begin; s < s_end; ++s) {
+        const uint32_t off = a.slice_off[s];
+        const uint32_t len = a.slice_off[s + 1] - off;
+        const size_t base = static_cast<size_t>(off) * 32 + lane;
+        const uint32_t *cp = a.col_sell + base;
+        T acc = T(0);
+        uint32_t j = 0;
+        for (; j + UNROLL <= len; j += UNROLL) {
+            uint32_t c[UNROLL];
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                c[k] = ld_stream(cp + static_cast<size_t>(j + k) * 32);
+            T v[UNROLL];
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                v[k] = gather_y<T, HOT, PART>(a, s_y, c[k]);
+            if (WEIGHTED) {
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    v[k] = t_mul(v[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
+            }
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                acc += v[k];
+        }
+        if (j < len) {
+            // The last len - j < UNROLL steps as one predicated batch, so
+            // their gathers are in flight together; the sum keeps the same
+            // order (absent steps add nothing).
+            uint32_t c[UNROLL];
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                c[k] = j + k < len ? ld_stream(cp + static_cast<size_t>(j + k) * 32) : 0u;
+            T v[UNROLL];
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                v[k] = j + k < len ? gather_y<T, HOT, PART>(a, s_y, c[k]) : T(0);
+            if (WEIGHTED) {
+#pragma unroll
+                for (int k = 0; k < UNROLL; ++k)
+                    if (j + k < len)
+                        v[k] = t_mul(v[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
+            }
+#pragma unroll
+            for (int k = 0; k < UNROLL; ++k)
+                if (j + k < len)
+                    acc += v[k];
+        }
+        if (s < a.s_chunk) {
+            a.chunk_val[static_cast<size_t>(s) * 32 + lane] = acc;
+        } else {
+            const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
+            if (r < a.n)
+                finish_row_sweep<T, WEIGHTED, PART>(a, r, acc, res, sink);
+        }
+    }
+}
+
+// The sweep: each warp walks its units (sweep_unit).
 // Registers are fitted to 48 warps per SM (more warps do not make the sweep
 // faster: it is bound by the rate of L1 miss requests), and to 32 for the
 // other batch depths and the weighted FP64 sweep, which would spill at 48.
 // HOT: the variant with the shared-memory tier (a.hot * sizeof(T) bytes of
 // dynamic shared memory, a multiple of 16). PART: the row slice of a
 // partitioned run (see SweepArgs.row_map).
-template <typename T, bool WEIGHTED, int THREADS, int UNROLL, bool HOT = false, bool PART = false>
+// QUEUED: warps take the next unit from a device counter instead of a fixed
+// round-robin share, so warps that run faster take more of the graph and the
+// sweep ends when the work does, not when the slowest share does (R-MAT 24,
+// FP64: 0.875 ms against 0.956 ms with 8 round-robin units per warp, same
+// scores bit for bit). Every unit's residual and sink partials go to their
+// own slots (unit_res, unit_sink) after a fixed-order warp sum, and the
+// fix-up adds them in a fixed order: the result does not depend on which
+// warp ran which unit. The regular PageRank sweep is always QUEUED; the
+// shared-memory tier and the row slices of a partitioned run keep the
+// round-robin units.
+template <typename T, bool WEIGHTED, int THREADS, int UNROLL, bool HOT = false, bool PART = false,
+          bool QUEUED = false>
 __global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T) > 4) ? 1024 / THREADS : 1536 / THREADS)
     sweep_kernel(SweepArgs<T> a) {
+    static_assert(!(QUEUED && HOT), "the queued sweep has no shared-memory tier");
     __shared__ double s_red[32];
     extern __shared__ __align__(16) unsigned char s_dyn[];
     T *s_y = reinterpret_cast<T *>(s_dyn);
     if (*(volatile int *)&a.st->done)
         return;
+    const int lane = threadIdx.x & 31;
+    if (QUEUED) {
+        for (;;) {
+            uint32_t u = 0;
+            if (lane == 0)
+                u = atomicAdd(&a.st->queue, 1u);
+            u = __shfl_sync(0xffffffffu, u, 0);
+            if (u >= a.units)
+                return;
+            double res = 0.0, sink = 0.0;
+            sweep_unit<T, WEIGHTED, UNROLL, false, PART>(a, s_y, a.unit_start[u],
+                                                          a.unit_start[u + 1], lane, res, sink);
+            res = warp_sum(res);
+            sink = warp_sum(sink);
+            if (lane == 0) {
+                a.unit_res[u] = res;
+                a.unit_sink[u] = sink;
+            }
+        }
+    }
     if (HOT) {
         const uint32_t vecs = a.hot * static_cast<uint32_t>(sizeof(T)) / 16u;
         const uint4 *src = reinterpret_cast<const uint4 *>(a.y_in);
@@ -255,70 +358,13 @@ __global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T)
             dst[i] = ld_na_v4(src + i);
         __syncthreads();
     }
-    const int lane = threadIdx.x & 31;
     const uint32_t wpc = THREADS / 32;
     const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);
     const uint32_t nw = gridDim.x * wpc;
     double res = 0.0, sink = 0.0;
-    for (uint32_t u = gw; u < a.units; u += nw) {
-        const uint32_t s_end = a.unit_start[u + 1];
-        for (uint32_t s = a.unit_start[u]; s < s_end; ++s) {
-            const uint32_t off = a.slice_off[s];
-            const uint32_t len = a.slice_off[s + 1] - off;
-            const size_t base = static_cast<size_t>(off) * 32 + lane;
-            const uint32_t *cp = a.col_sell + base;
-            T acc = T(0);
-            uint32_t j = 0;
-            for (; j + UNROLL <= len; j += UNROLL) {
-                uint32_t c[UNROLL];
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    c[k] = ld_stream(cp + static_cast<size_t>(j + k) * 32);
-                T v[UNROLL];
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    v[k] = gather_y<T, HOT, PART>(a, s_y, c[k]);
-                if (WEIGHTED) {
-#pragma unroll
-                    for (int k = 0; k < UNROLL; ++k)
-                        v[k] = t_mul(v[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
-                }
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    acc += v[k];
-            }
-            if (j < len) {
-                // The last len - j < UNROLL steps as one predicated batch, so
-                // their gathers are in flight together; the sum keeps the same
-                // order (absent steps add nothing).
-                uint32_t c[UNROLL];
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    c[k] = j + k < len ? ld_stream(cp + static_cast<size_t>(j + k) * 32) : 0u;
-                T v[UNROLL];
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    v[k] = j + k < len ? gather_y<T, HOT, PART>(a, s_y, c[k]) : T(0);
-                if (WEIGHTED) {
-#pragma unroll
-                    for (int k = 0; k < UNROLL; ++k)
-                        if (j + k < len)
-                            v[k] = t_mul(v[k], ld_stream(a.w_sell + base + static_cast<size_t>(j + k) * 32));
-                }
-#pragma unroll
-                for (int k = 0; k < UNROLL; ++k)
-                    if (j + k < len)
-                        acc += v[k];
-            }
-            if (s < a.s_chunk) {
-                a.chunk_val[static_cast<size_t>(s) * 32 + lane] = acc;
-            } else {
-                const uint32_t r = a.n_long + (s - a.s_chunk) * 32 + lane;
-                if (r < a.n)
-                    finish_row_sweep<T, WEIGHTED, PART>(a, r, acc, res, sink);
-            }
-        }
-    }
+    for (uint32_t u = gw; u < a.units; u += nw)
+        sweep_unit<T, WEIGHTED, UNROLL, HOT, PART>(a, s_y, a.unit_start[u], a.unit_start[u + 1],
+                                                   lane, res, sink);
     const double bres = block_sum<THREADS>(res, s_red);
     const double bsink = block_sum<THREADS>(sink, s_red);
     if (threadIdx.x == 0) {
@@ -392,6 +438,14 @@ __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
     const RunParams rp = *a.rp;
     const T sink_coef = static_cast<T>(a.st->sink_coef);
     double res = 0.0, sink = 0.0;
+    if (a.unit_res) {
+        // Partials of a queued sweep: a fixed share of the units per thread.
+        for (uint32_t i = blockIdx.x * kFixThreads + threadIdx.x; i < a.units;
+             i += gridDim.x * kFixThreads) {
+            res += a.unit_res[i];
+            sink += a.unit_sink[i];
+        }
+    }
     const uint32_t vctas = fix_vlong_ctas(a.n_vlong);
     if (blockIdx.x < vctas) {
         const uint32_t r = blockIdx.x * kFixWarps + (threadIdx.x >> 5);
@@ -436,7 +490,8 @@ __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
     __threadfence();
     // Fixed-order reduction of sweep-CTA and fix-up-CTA partials.
     double r = 0.0, s = 0.0;
-    for (uint32_t i = threadIdx.x; i < a.sweep_ctas; i += kFixThreads) {
+    const uint32_t sweep_parts = a.unit_res ? 0u : a.sweep_ctas;
+    for (uint32_t i = threadIdx.x; i < sweep_parts; i += kFixThreads) {
         r += ((volatile double *)a.cta_res)[i];
         s += ((volatile double *)a.cta_sink)[i];
     }
@@ -458,6 +513,7 @@ __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
         st->sink_mass = s;
         st->sink_coef = rp.distribute ? (rp.personal ? s : s / static_cast<double>(a.n)) : 0.0;
         st->ticket = 0;
+        st->queue = 0;
         __threadfence();
         st->done = (it >= rp.max_iterations || norm <= rp.tol) ? 1 : 0;
     }
