@@ -43,7 +43,8 @@ struct nkg_part {
     nkg::DeviceArray<uint32_t> unit_start;
     uint32_t units = 0;
     unsigned sweep_ctas = 0, fix_ctas = 0;
-    nkg::DeviceArray<double> chunk_val, cta_res, cta_sink, fix_res, fix_sink, part;
+    // unit_part: the residual and sink partials of each work unit (2 x units)
+    nkg::DeviceArray<double> chunk_val, unit_part, fix_res, fix_sink, part;
     nkg::DeviceArray<nkg::RunParams> rp;
     nkg::DeviceArray<nkg::IterState> st;
     nkg::PinnedHost<nkg::IterState> st_host;
@@ -256,10 +257,11 @@ nkg_part *create_part(uint64_t vec_len, uint64_t row_base, uint64_t rows, uint64
     build_sell(p->fw, n, new_ptr.get(), new_col.get(), w ? new_w.get() : nullptr, nullptr,
                len.get(), dev, s, pad);
 
-    // Launch shape of the regular sweep (512 threads, 8 gathers in flight).
-    auto kfn = sweep_kernel<double, false, kPartThreads, kPartUnroll, false, true>;
+    // Launch shape of the regular sweep (512 threads, 8 gathers in flight),
+    // warps taking units from the state's counter as in the single-GPU run.
+    auto kfn = sweep_kernel<double, false, kPartThreads, kPartUnroll, false, true, true>;
     NKG_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, 0));
-    auto kfw = sweep_kernel<double, true, kPartThreads, kPartUnroll, false, true>;
+    auto kfw = sweep_kernel<double, true, kPartThreads, kPartUnroll, false, true, true>;
     NKG_CUDA(cudaFuncSetAttribute(kfw, cudaFuncAttributePreferredSharedMemoryCarveout, 0));
     int occ = 0;
     NKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, w ? kfw : kfn, kPartThreads, 0));
@@ -270,15 +272,14 @@ nkg_part *create_part(uint64_t vec_len, uint64_t row_base, uint64_t rows, uint64
                                   kPartThreads)));
     const uint64_t warps = static_cast<uint64_t>(p->sweep_ctas) * (kPartThreads / 32);
     p->units = static_cast<uint32_t>(
-        std::max<uint64_t>(1, std::min<uint64_t>(warps * kUnitsPerWarp,
+        std::max<uint64_t>(1, std::min<uint64_t>(warps * kQueueUnitsPerWarp,
                                                  std::max<uint32_t>(p->fw.slices, 1))));
     p->unit_start.alloc(static_cast<size_t>(p->units) + 1);
     sell_units(p->fw, p->units, p->unit_start.get(), s);
     p->fix_ctas = fix_vlong_ctas(p->fw.n_vlong) +
                   ceil_div(std::max<uint32_t>(p->fw.n_long - p->fw.n_vlong, 1), kFixThreads);
     p->chunk_val.alloc(static_cast<size_t>(p->fw.s_chunk) * 32 + 1);
-    p->cta_res.alloc(p->sweep_ctas);
-    p->cta_sink.alloc(p->sweep_ctas);
+    p->unit_part.alloc(2 * static_cast<size_t>(p->units));
     p->fix_res.alloc(p->fix_ctas);
     p->fix_sink.alloc(p->fix_ctas);
     p->part.alloc(3 * kRedBlocks + 3);
@@ -303,8 +304,8 @@ SweepArgs<double> part_args(const nkg_part *p, const double *y_in, double *y_out
     a.y_in = y_in;
     a.y_out = y_out;
     a.chunk_val = p->chunk_val.get();
-    a.cta_res = p->cta_res.get();
-    a.cta_sink = p->cta_sink.get();
+    a.unit_res = p->unit_part.get();
+    a.unit_sink = p->unit_part.get() + p->units;
     a.fix_res = p->fix_res.get();
     a.fix_sink = p->fix_sink.get();
     a.rp = p->rp.get();
@@ -400,11 +401,11 @@ int nkg_part_sweep(nkg_part *p, const double *d_y_in, double sink_coef, double *
         NKG_CUDA(cudaMemcpyAsync(p->st.get(), h, sizeof(IterState), cudaMemcpyHostToDevice, s));
         const SweepArgs<double> a = part_args(p, d_y_in, d_y_out);
         if (p->weighted) {
-            sweep_kernel<double, true, kPartThreads, kPartUnroll, false, true>
+            sweep_kernel<double, true, kPartThreads, kPartUnroll, false, true, true>
                 <<<p->sweep_ctas, kPartThreads, 0, s>>>(a);
             fixup_kernel<double, true, true><<<p->fix_ctas, kFixThreads, 0, s>>>(a);
         } else {
-            sweep_kernel<double, false, kPartThreads, kPartUnroll, false, true>
+            sweep_kernel<double, false, kPartThreads, kPartUnroll, false, true, true>
                 <<<p->sweep_ctas, kPartThreads, 0, s>>>(a);
             fixup_kernel<double, false, true><<<p->fix_ctas, kFixThreads, 0, s>>>(a);
         }

@@ -33,7 +33,7 @@ namespace nkg {
 
 // Arcs per chunk of a split row; also the longest sequential loop of a lane.
 constexpr uint32_t kChunk = 256;
-// A split row with more chunks than this is summed by a whole CTA.
+// A split row with more chunks than this is summed by a whole warp in the fix-up.
 constexpr uint32_t kShortChunks = 16;
 
 // Constant per run, read from device memory so that captured CUDA graphs
@@ -317,8 +317,8 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs<T> &a, const T *s_y, 
 // scores bit for bit). Every unit's residual and sink partials go to their
 // own slots (unit_res, unit_sink) after a fixed-order warp sum, and the
 // fix-up adds them in a fixed order: the result does not depend on which
-// warp ran which unit. The regular PageRank sweep is always QUEUED; the
-// shared-memory tier and the row slices of a partitioned run keep the
+// warp ran which unit. The regular PageRank sweep and the row slices of a
+// partitioned run are always QUEUED; the shared-memory tier keeps the
 // round-robin units.
 template <typename T, bool WEIGHTED, int THREADS, int UNROLL, bool HOT = false, bool PART = false,
           bool QUEUED = false>
