@@ -301,13 +301,9 @@ __global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 512 / THREADS : WEIGHTED
     const int lane = threadIdx.x & 31;
     // Warps take units from a device counter in order (as the queued
     // PageRank sweep); every unit's two partial sums go to their own slots.
-    for (;;) {
-        uint32_t u = 0;
-        if (lane == 0)
-            u = atomicAdd(a.queue, 1u);
-        u = __shfl_sync(0xffffffffu, u, 0);
-        if (u >= a.units)
-            return;
+    const uint32_t nw = gridDim.x * (THREADS / 32);
+    for (uint32_t u = blockIdx.x * (THREADS / 32) + (threadIdx.x >> 5); u < a.units;
+         u = next_unit(a.queue, a.units, nw, lane)) {
         double res = 0.0, td = 0.0;
         const uint32_t s_end = a.unit_start[u + 1];
         for (uint32_t s = a.unit_start[u]; s < s_end; ++s) {
@@ -944,8 +940,11 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
     const int distribute = p.distribute_sinks ? 1 : 0;
     const double inv_n = 1.0 / static_cast<double>(n);
     const unsigned vec_ctas = std::max<unsigned>(1, std::min<unsigned>(sms * 4, ceil_div(n, kBiThreads)));
-    const unsigned fix_ctas = split_fix_ctas<kBiThreads>(A.tl.n_long, A.tl.n_vlong);
-    ensure_work(g, A, vec_ctas, fix_ctas);
+    const unsigned fix_ctas = fix_ctas_with_units(
+        split_fix_ctas<kBiThreads>(A.tl.n_long, A.tl.n_vlong), A.n_units32, kBiThreads);
+    const unsigned adj_fix_ctas = fix_ctas_with_units(
+        split_fix_ctas<kAdjThreads>(A.tl.n_long, A.tl.n_vlong), A.n_units64, kAdjThreads);
+    ensure_work(g, A, vec_ctas, std::max(fix_ctas, adj_fix_ctas));
     AdjWork &W = A.work;
     AdjResult R;
     NKG_CUDA(cudaEventRecord(g->ev0, s));
@@ -1006,7 +1005,6 @@ AdjResult run_adjoint(nkg_graph *g, const nkg_pr_params &p, const double *d_tele
     aa.sweep_ctas = A.ctas64;
     aa.distribute = distribute;
     aa.personal = personal;
-    const unsigned adj_fix_ctas = split_fix_ctas<kAdjThreads>(A.tl.n_long, A.tl.n_vlong);
     auto sweep64 = [&](const double *in, double *out, double *cout, unsigned long long max_it) {
         aa.lam_in = in;
         aa.lam_out = out;

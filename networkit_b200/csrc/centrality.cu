@@ -99,13 +99,9 @@ __global__ void __launch_bounds__(THREADS, WEIGHTED || UNROLL > 8 ? 1024 / THREA
     const int lane = threadIdx.x & 31;
     // Warps take units from a device counter in order (as the queued
     // PageRank sweep); every unit's sum of squares goes to its own slot.
-    for (;;) {
-        uint32_t u = 0;
-        if (lane == 0)
-            u = atomicAdd(&a.st->queue, 1u);
-        u = __shfl_sync(0xffffffffu, u, 0);
-        if (u >= a.units)
-            return;
+    const uint32_t nw = gridDim.x * (THREADS / 32);
+    for (uint32_t u = blockIdx.x * (THREADS / 32) + (threadIdx.x >> 5); u < a.units;
+         u = next_unit(&a.st->queue, a.units, nw, lane)) {
         double sq = 0.0;
         const uint32_t s_end = a.unit_start[u + 1];
         for (uint32_t s = a.unit_start[u]; s < s_end; ++s) {
@@ -281,7 +277,8 @@ CentResult cent_run(nkg_graph *g, const SellLayout &L, const double *w_sell, dou
     const uint32_t units = static_cast<uint32_t>(std::max<uint64_t>(
         1, std::min<uint64_t>(static_cast<uint64_t>(ctas) * (kCentThreads / 32) * kQueueUnitsPerWarp,
                               std::max<uint64_t>(slices, 1))));
-    const unsigned fix_ctas = split_fix_ctas<kCentFix>(L.n_long, L.n_vlong);
+    const unsigned fix_ctas =
+        fix_ctas_with_units(split_fix_ctas<kCentFix>(L.n_long, L.n_vlong), units, kCentFix);
     DeviceArray<uint32_t> unit_start(static_cast<size_t>(units) + 1);
     sell_units(L, units, unit_start.get(), s);
     DeviceArray<double> x[2] = {DeviceArray<double>(n + 1), DeviceArray<double>(n + 1)};

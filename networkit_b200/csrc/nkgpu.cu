@@ -1083,7 +1083,11 @@ static nkg_graph *build_graph(std::unique_ptr<nkg_graph> g, DeviceArray<uint64_t
     // they are never reallocated under a captured graph.
     g->cta_res.alloc(static_cast<size_t>(sms) * 32);
     g->cta_sink.alloc(static_cast<size_t>(sms) * 32);
-    const size_t fix = static_cast<size_t>(g->fw.n_vlong) + ceil_div(g->fw.n_long, kFixThreads) + 1;
+    // Fix-up grids also cover the queued sweep's unit partials (at most one
+    // unit per slice, kUnitsPerFixThread per thread).
+    const size_t fix = std::max<size_t>(
+        static_cast<size_t>(g->fw.n_vlong) + ceil_div(g->fw.n_long, kFixThreads) + 1,
+        fix_ctas_with_units(1, g->fw.slices, kFixThreads));
     g->fix_res.alloc(fix);
     g->fix_sink.alloc(fix);
     g->rp.alloc(1);
@@ -1363,6 +1367,7 @@ static void sweep_setup(nkg_graph *g) {
         unit_bounds<<<ceil_div(static_cast<uint64_t>(P.q_units) + 1, 256), 256, 0, s>>>(
             g->fw.slice_cost.get(), g->fw.slices, P.q_units, P.q_unit_start.get());
         NKG_CUDA(cudaGetLastError());
+        P.fix_ctas = fix_ctas_with_units(P.fix_ctas, P.q_units, kFixThreads);
     }
     if (P.hot) {
         const int bytes = static_cast<int>(P.hot * sizeof(T));
@@ -1666,7 +1671,8 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
     DeviceArray<float> &bx = W.x, &br = W.r, &brhat = W.rhat, &bp = W.p, &bv = W.v, &bs = W.s,
                        &bt = W.t, &bg = W.g;
     DeviceArray<double> &x64 = W.x64, &part = W.part;
-    const unsigned fix_ctas = split_fix_ctas<kBiThreads>(g->fw.n_long, g->fw.n_vlong);
+    const unsigned fix_ctas = fix_ctas_with_units(split_fix_ctas<kBiThreads>(g->fw.n_long, g->fw.n_vlong),
+                                                  P32.q_units, kBiThreads);
     if (W.fix_part.size() < 2 * static_cast<size_t>(fix_ctas))
         W.fix_part.alloc(2 * static_cast<size_t>(fix_ctas));
     DeviceArray<double> &fix_part = W.fix_part;

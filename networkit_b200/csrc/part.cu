@@ -276,8 +276,10 @@ nkg_part *create_part(uint64_t vec_len, uint64_t row_base, uint64_t rows, uint64
                                                  std::max<uint32_t>(p->fw.slices, 1))));
     p->unit_start.alloc(static_cast<size_t>(p->units) + 1);
     sell_units(p->fw, p->units, p->unit_start.get(), s);
-    p->fix_ctas = fix_vlong_ctas(p->fw.n_vlong) +
-                  ceil_div(std::max<uint32_t>(p->fw.n_long - p->fw.n_vlong, 1), kFixThreads);
+    p->fix_ctas = fix_ctas_with_units(
+        fix_vlong_ctas(p->fw.n_vlong) +
+            ceil_div(std::max<uint32_t>(p->fw.n_long - p->fw.n_vlong, 1), kFixThreads),
+        p->units, kFixThreads);
     p->chunk_val.alloc(static_cast<size_t>(p->fw.s_chunk) * 32 + 1);
     p->unit_part.alloc(2 * static_cast<size_t>(p->units));
     p->fix_res.alloc(p->fix_ctas);

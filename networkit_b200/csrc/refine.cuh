@@ -191,13 +191,9 @@ __global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 1024 / THREADS : 1536 / 
     const float *gsrc = OP == 0 ? a.g : px;
     const int lane = threadIdx.x & 31;
     if (QUEUED) {
-        for (;;) {
-            uint32_t u = 0;
-            if (lane == 0)
-                u = atomicAdd(&a.sc->queue, 1u);
-            u = __shfl_sync(0xffffffffu, u, 0);
-            if (u >= a.units)
-                return;
+        const uint32_t nw = gridDim.x * (THREADS / 32);
+        for (uint32_t u = blockIdx.x * (THREADS / 32) + (threadIdx.x >> 5); u < a.units;
+             u = next_unit(&a.sc->queue, a.units, nw, lane)) {
             double d1 = 0.0, d2 = 0.0;
             bi_mv_unit<WEIGHTED, MODE, OP, UNROLL>(a, px, out, gsrc, a.unit_start[u],
                                                    a.unit_start[u + 1], lane, d1, d2);
@@ -208,6 +204,7 @@ __global__ void __launch_bounds__(THREADS, UNROLL > 8 ? 1024 / THREADS : 1536 / 
                 a.unit_part[2 * static_cast<size_t>(u) + 1] = d2;
             }
         }
+        return;
     }
     const uint32_t wpc = THREADS / 32;
     const uint32_t gw = blockIdx.x * wpc + (threadIdx.x >> 5);

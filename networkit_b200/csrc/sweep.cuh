@@ -36,6 +36,28 @@ constexpr uint32_t kChunk = 256;
 // A split row with more chunks than this is summed by a whole warp in the fix-up.
 constexpr uint32_t kShortChunks = 16;
 
+// Work units of the queued sweeps: warp gw of nw runs unit gw first, with no
+// ticket, then units nw + t for the tickets t it takes from `queue`, while
+// any are left. A grid that covers all units takes no tickets at all, so small
+// graphs pay no atomics. Returns the warp's next unit (>= units: done).
+__device__ __forceinline__ uint32_t next_unit(unsigned int *queue, uint32_t units, uint32_t nw,
+                                              int lane) {
+    if (nw >= units)
+        return units;
+    uint32_t t = 0;
+    if (lane == 0)
+        t = atomicAdd(queue, 1u);
+    return nw + __shfl_sync(0xffffffffu, t, 0);
+}
+
+// Fix-up CTAs of a queued sweep: those its split rows need, and enough that
+// no thread adds more than kUnitsPerFixThread of the sweep's unit partials.
+constexpr uint32_t kUnitsPerFixThread = 4;
+inline unsigned fix_ctas_with_units(unsigned split_ctas, uint64_t units, unsigned threads) {
+    const uint64_t per_cta = static_cast<uint64_t>(threads) * kUnitsPerFixThread;
+    return static_cast<unsigned>(std::max<uint64_t>(split_ctas, (units + per_cta - 1) / per_cta));
+}
+
 // Constant per run, read from device memory so that captured CUDA graphs
 // stay valid across runs with different parameters.
 struct RunParams {
@@ -332,13 +354,9 @@ __global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T)
         return;
     const int lane = threadIdx.x & 31;
     if (QUEUED) {
-        for (;;) {
-            uint32_t u = 0;
-            if (lane == 0)
-                u = atomicAdd(&a.st->queue, 1u);
-            u = __shfl_sync(0xffffffffu, u, 0);
-            if (u >= a.units)
-                return;
+        const uint32_t nw = gridDim.x * (THREADS / 32);
+        for (uint32_t u = blockIdx.x * (THREADS / 32) + (threadIdx.x >> 5); u < a.units;
+             u = next_unit(&a.st->queue, a.units, nw, lane)) {
             double res = 0.0, sink = 0.0;
             sweep_unit<T, WEIGHTED, UNROLL, false, PART>(a, s_y, a.unit_start[u],
                                                           a.unit_start[u + 1], lane, res, sink);
@@ -349,6 +367,7 @@ __global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T)
                 a.unit_sink[u] = sink;
             }
         }
+        return;
     }
     if (HOT) {
         const uint32_t vecs = a.hot * static_cast<uint32_t>(sizeof(T)) / 16u;

@@ -264,6 +264,26 @@ def test_repeated_runs_are_bit_identical():
     assert a[1] == b[1]
 
 
+@pytest.mark.parametrize("norm", [0, 1])
+def test_queued_sweep_sums_do_not_depend_on_the_schedule(norm):
+    """Warps take the sweep's work units from a counter, so which warp runs
+    which unit changes from sweep to sweep. Every unit's partial sums have a
+    slot of their own and are added in a fixed order: the residual of every
+    sweep, the iteration count and the scores repeat bit for bit (R-MAT 16,
+    with rows split into chunks)."""
+    csr = generators.rmat_directed(16, 16, seed=11)
+    dg = _capi.DeviceGraph(csr)
+    assert dg.info()["split_rows"] > 0
+    p = dg.params(0.85, 1e-10, norm, False, True, 0, _capi.UINT64_MAX)
+    runs = [dg.run(p, trace=256) for _ in range(3)]
+    for s, it, mx, st in runs[1:]:
+        np.testing.assert_array_equal(s, runs[0][0])
+        assert it == runs[0][1]
+        np.testing.assert_array_equal(st["residual_trace"].view(np.uint64),
+                                      runs[0][3]["residual_trace"].view(np.uint64))
+    assert runs[0][3]["residual_trace"].shape[0] == runs[0][1]
+
+
 def test_memory_pool_reuse_and_release(oracle_mod):
     """Graphs created and destroyed in a loop reuse the library's cached
     device memory and give the same scores; nkg_release_cached_memory hands
