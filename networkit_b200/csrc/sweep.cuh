@@ -19,9 +19,9 @@
 // own row sequentially, in the reference's arc order. No shared memory and no
 // barriers are needed: the whole L1 is left to cache the hot part of y.
 // The slices are cut into contiguous, cost-balanced ranges ("units", fixed at
-// set-up). Warps take the next unit from a device counter, so at any time
-// they work on neighbouring units and no warp is left with a share that ends
-// late. Each unit's residual and sink partials go to a slot of its own, so
+// set-up). Every warp runs one unit of its own first and then takes the next
+// unit from a device counter (next_unit), so no warp is left with a share that
+// ends late. Each unit's residual and sink partials go to a slot of its own, so
 // every sum has a fixed order and a run is bit-reproducible.
 #pragma once
 
@@ -332,11 +332,11 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs<T> &a, const T *s_y, 
 // HOT: the variant with the shared-memory tier (a.hot * sizeof(T) bytes of
 // dynamic shared memory, a multiple of 16). PART: the row slice of a
 // partitioned run (see SweepArgs.row_map).
-// QUEUED: warps take the next unit from a device counter instead of a fixed
-// round-robin share, so warps that run faster take more of the graph and the
-// sweep ends when the work does, not when the slowest share does (R-MAT 24,
-// FP64: 0.875 ms against 0.956 ms with 8 round-robin units per warp, same
-// scores bit for bit). Every unit's residual and sink partials go to their
+// QUEUED: after a first unit of their own, warps take the next unit from a
+// device counter (next_unit) instead of a fixed round-robin share, so warps
+// that run faster take more of the graph and the sweep ends when the work
+// does, not when the slowest share does (R-MAT 24, FP64: 0.874 ms against
+// 0.956 ms with 8 round-robin units per warp, same scores bit for bit). Every unit's residual and sink partials go to their
 // own slots (unit_res, unit_sink) after a fixed-order warp sum, and the
 // fix-up adds them in a fixed order: the result does not depend on which
 // warp ran which unit. The regular PageRank sweep and the row slices of a
