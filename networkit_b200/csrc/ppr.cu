@@ -6,7 +6,7 @@
 //
 // Layout: the iterate is node-major, Y[r * kp + j] (kp = 32 * CPL columns,
 // CPL per lane), in gather form (x/deg, sinks x). A warp owns one virtual
-// row (a whole row, or a 256-arc chunk of a long row); per arc it broadcasts
+// row (a whole row, or a kChunk-arc chunk of a long row); per arc it broadcasts
 // the source id and every lane loads its CPL columns of that source's row:
 // kp * 4 contiguous bytes per arc, float4-coalesced. Warps walk contiguous,
 // cost-balanced ranges of virtual rows, so every sum has a fixed order.
