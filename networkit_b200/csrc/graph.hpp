@@ -92,6 +92,9 @@ struct Plane {
     DeviceArray<uint32_t> q_unit_start;
     DeviceArray<double> q_part;
     uint32_t q_units = 0;
+    // The sweep's last CTA closes each iteration (no fix-up launch): graphs
+    // with no split rows and at most kCloseInSweepUnits units.
+    bool close_in_sweep = false;
 };
 
 } // namespace nkg

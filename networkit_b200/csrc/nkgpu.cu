@@ -1368,6 +1368,7 @@ static void sweep_setup(nkg_graph *g) {
             g->fw.slice_cost.get(), g->fw.slices, P.q_units, P.q_unit_start.get());
         NKG_CUDA(cudaGetLastError());
         P.fix_ctas = fix_ctas_with_units(P.fix_ctas, P.q_units, kFixThreads);
+        P.close_in_sweep = g->fw.n_long == 0 && P.q_units <= kCloseInSweepUnits;
     }
     if (P.hot) {
         const int bytes = static_cast<int>(P.hot * sizeof(T));
@@ -1447,6 +1448,7 @@ static SweepArgs<T> sweep_args(nkg_graph *g, int in_buf) {
         a.unit_start = P.q_unit_start.get();
         a.unit_res = P.q_part.get();
         a.unit_sink = P.q_part.get() + P.q_units;
+        a.close_in_sweep = P.close_in_sweep ? 1 : 0;
     }
     a.hot = P.hot;
     a.trace = g->trace.get();
@@ -1478,7 +1480,15 @@ static void launch_sweep(nkg_graph *g, int in_buf, cudaStream_t s) {
     Plane<T> &P = plane<T>(g);
     const SweepArgs<T> a = sweep_args<T, WEIGHTED>(g, in_buf);
     launch_sweep_kernel<T, WEIGHTED>(g, a, s);
-    fixup_kernel<T, WEIGHTED><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
+    if (!P.close_in_sweep)
+        fixup_kernel<T, WEIGHTED><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
+}
+
+// Kernel launches of one iteration: the sweep, and the fix-up unless the
+// sweep closes the iteration itself.
+template <typename T>
+static uint64_t launches_per_sweep(nkg_graph *g) {
+    return plane<T>(g).close_in_sweep ? 1 : 2;
 }
 
 // Capture kSweepsPerGraph sweeps (sweep + fix-up each) as one CUDA graph.
@@ -1611,7 +1621,7 @@ static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *d
     for (;;) {
         for (int b = 0; b < batch; ++b)
             NKG_CUDA(cudaGraphLaunch(exec, s));
-        R.launches += static_cast<uint64_t>(batch) * 2 * kSweepsPerGraph;
+        R.launches += static_cast<uint64_t>(batch) * launches_per_sweep<T>(g) * kSweepsPerGraph;
         NKG_CUDA(cudaMemcpyAsync(sh, g->st.get(), sizeof(IterState), cudaMemcpyDeviceToHost, s));
         NKG_CUDA(cudaStreamSynchronize(s));
         if (sh->done)
@@ -1748,7 +1758,7 @@ static RunResult run_refine(nkg_graph *g, const nkg_pr_params &p, const double *
             bx.get(), x64.get(), P64.y[0].get(), g->degc.get(), degw64, n, add, part.get(),
             g->st.get(), &scp->ticket, a.distribute, personal);
         NKG_CUDA(cudaGraphLaunch(exec, s));
-        R.launches += 1 + 2 * kSweepsPerGraph;
+        R.launches += 1 + launches_per_sweep<double>(g) * kSweepsPerGraph;
         ++fp64;
         NKG_CUDA(cudaMemcpyAsync(sh, g->st.get(), sizeof(IterState), cudaMemcpyDeviceToHost, s));
         NKG_CUDA(cudaStreamSynchronize(s));
@@ -1846,7 +1856,8 @@ static void profile_sweeps(nkg_graph *g, int sweeps, double *ms_kernel, double *
         NKG_CUDA(cudaEventRecord(ev[2 * i], s));
         launch_sweep_kernel<T, WEIGHTED>(g, a, s);
         NKG_CUDA(cudaEventRecord(ev[2 * i + 1], s));
-        fixup_kernel<T, WEIGHTED><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
+        if (!P.close_in_sweep)
+            fixup_kernel<T, WEIGHTED><<<P.fix_ctas, kFixThreads, 0, s>>>(a);
     }
     NKG_CUDA(cudaGetLastError());
     NKG_CUDA(cudaStreamSynchronize(s));

@@ -132,7 +132,15 @@ struct SweepArgs {
     // round-robin assignment with per-CTA partials in cta_res / cta_sink.
     double *unit_res;
     double *unit_sink;
+    // The queued sweep's last CTA closes the iteration itself (graphs with no
+    // split rows and few units; no fix-up launch): see close_iteration.
+    int close_in_sweep;
+    int pad5;
 };
+
+// Graphs with no split rows and at most this many units close every
+// iteration in the sweep's last CTA instead of a fix-up launch.
+constexpr uint32_t kCloseInSweepUnits = 8192;
 
 template <typename T>
 __device__ __forceinline__ T t_mul(T a, T b);
@@ -265,6 +273,29 @@ __device__ __forceinline__ uint4 ld_na_v4(const uint4 *p) {
     return v;
 }
 
+// Closes an iteration from the reduced residual sum r and sink mass s
+// (PageRank.cpp:68-70): iteration count, stopping norm, trace, the sink term
+// of the next sweep, the convergence flag. One thread, after every partial
+// sum of the sweep is in r and s.
+template <typename T>
+__device__ __forceinline__ void close_iteration(const SweepArgs<T> &a, const RunParams &rp, double r,
+                                                double s) {
+    IterState *st = a.st;
+    const unsigned long long it = st->iteration + 1;
+    const double norm = rp.l2 ? sqrt(r) : r;
+    st->iteration = it;
+    st->residual = norm;
+    st->residual_sum = r;
+    if (it - 1 < a.trace_cap)
+        a.trace[it - 1] = norm;
+    st->sink_mass = s;
+    st->sink_coef = rp.distribute ? (rp.personal ? s : s / static_cast<double>(a.n)) : 0.0;
+    st->ticket = 0;
+    st->queue = 0;
+    __threadfence();
+    st->done = (it >= rp.max_iterations || norm <= rp.tol) ? 1 : 0;
+}
+
 // Slices [s_begin, s_end) of one work unit: each lane accumulates one
 // virtual row of a slice in arc order. Chunk slices store partial sums; row
 // slices finish rows, adding their residual and sink terms to res / sink.
@@ -371,6 +402,29 @@ __global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T)
                 a.unit_sink[u] = sink;
             }
         }
+        if (!a.close_in_sweep)
+            return;
+        // The last CTA to finish adds the units' partials in unit order (a
+        // fixed tree) and closes the iteration; no CTA waits for another.
+        __shared__ bool s_last;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            s_last = atomicAdd(&a.st->ticket, 1u) == gridDim.x - 1;
+        }
+        __syncthreads();
+        if (!s_last)
+            return;
+        __threadfence();
+        double r = 0.0, sk = 0.0;
+        for (uint32_t i = threadIdx.x; i < a.units; i += THREADS) {
+            r += ((volatile double *)a.unit_res)[i];
+            sk += ((volatile double *)a.unit_sink)[i];
+        }
+        r = block_sum<THREADS>(r, s_red);
+        sk = block_sum<THREADS>(sk, s_red);
+        if (threadIdx.x == 0)
+            close_iteration(a, *a.rp, r, sk);
         return;
     }
     if (HOT) {
@@ -524,22 +578,8 @@ __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
     }
     r = block_sum<kFixThreads>(r, s_red);
     s = block_sum<kFixThreads>(s, s_red);
-    if (threadIdx.x == 0) {
-        IterState *st = a.st;
-        const unsigned long long it = st->iteration + 1;
-        const double norm = rp.l2 ? sqrt(r) : r;
-        st->iteration = it;
-        st->residual = norm;
-        st->residual_sum = r;
-        if (it - 1 < a.trace_cap)
-            a.trace[it - 1] = norm;
-        st->sink_mass = s;
-        st->sink_coef = rp.distribute ? (rp.personal ? s : s / static_cast<double>(a.n)) : 0.0;
-        st->ticket = 0;
-        st->queue = 0;
-        __threadfence();
-        st->done = (it >= rp.max_iterations || norm <= rp.tol) ? 1 : 0;
-    }
+    if (threadIdx.x == 0)
+        close_iteration(a, rp, r, s);
 }
 
 } // namespace nkg
