@@ -1617,7 +1617,9 @@ static RunResult run_power(nkg_graph *g, const nkg_pr_params &p, const double *d
 
     cudaGraphExec_t exec = sweep_graph<T, WEIGHTED>(g, personal);
     IterState *sh = g->st_host.get();
-    int batch = 1;
+    // Graph launches between status read-backs: 2, 4, 8, 8, ... (16 sweeps
+    // first: a host round trip costs more than the no-op sweeps it saves).
+    int batch = 2;
     for (;;) {
         for (int b = 0; b < batch; ++b)
             NKG_CUDA(cudaGraphLaunch(exec, s));
