@@ -472,6 +472,29 @@ inline unsigned split_fix_ctas(uint32_t n_long, uint32_t n_vlong) {
         1, (n_vlong + w - 1) / w + (short_rows + THREADS - 1) / THREADS));
 }
 
+// Lane-strided partial sum of one split row's chunk partials
+// v[cb + lane], v[cb + lane + 32], ... in ascending order, with 16 loads in
+// flight at a time (a row has up to about a thousand chunks). Absent entries
+// add zero, so the sum equals the one-at-a-time loop bit for bit.
+template <typename V>
+__device__ __forceinline__ V lane_chunk_sum(const V *__restrict__ v, uint32_t cb, uint32_t ce,
+                                            int lane) {
+    constexpr int kBatch = 16;
+    V part = V(0);
+    for (uint32_t k0 = cb + lane; k0 < ce; k0 += 32 * kBatch) {
+        V x[kBatch];
+#pragma unroll
+        for (int q = 0; q < kBatch; ++q) {
+            const uint32_t k = k0 + 32u * q;
+            x[q] = k < ce ? v[k] : V(0);
+        }
+#pragma unroll
+        for (int q = 0; q < kBatch; ++q)
+            part += x[q];
+    }
+    return part;
+}
+
 // Split row r of this thread in that layout and its chunk sum. Returns true
 // for the thread that finishes r (lane 0 of a row's warp, or the row's own
 // thread). A warp sums lane-strided partials in V, then across lanes in double
@@ -488,11 +511,7 @@ __device__ __forceinline__ bool split_row_sum(const uint32_t *__restrict__ chunk
         if (r >= n_vlong)
             return false;
         const int lane = threadIdx.x & 31;
-        const uint32_t cb = chunk_begin[r], ce = chunk_begin[r + 1];
-        V part = V(0);
-#pragma unroll 4
-        for (uint32_t k = cb + lane; k < ce; k += 32)
-            part += chunk_val[k];
+        const V part = lane_chunk_sum(chunk_val, chunk_begin[r], chunk_begin[r + 1], lane);
         acc = static_cast<V>(warp_sum(static_cast<double>(part)));
         return lane == 0;
     }
@@ -528,11 +547,7 @@ __global__ void __launch_bounds__(kFixThreads) fixup_kernel(SweepArgs<T> a) {
         const uint32_t r = blockIdx.x * kFixWarps + (threadIdx.x >> 5);
         const int lane = threadIdx.x & 31;
         if (r < a.n_vlong) {
-            const uint32_t cb = a.chunk_begin[r], ce = a.chunk_begin[r + 1];
-            T part = T(0);
-#pragma unroll 4
-            for (uint32_t k = cb + lane; k < ce; k += 32)
-                part += a.chunk_val[k];
+            const T part = lane_chunk_sum<T>(a.chunk_val, a.chunk_begin[r], a.chunk_begin[r + 1], lane);
             const double tot = warp_sum(static_cast<double>(part));
             if (lane == 0)
                 finish_row<T, WEIGHTED, PART>(a, rp, sink_coef, r, static_cast<T>(tot), res, sink);
