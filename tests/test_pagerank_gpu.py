@@ -104,6 +104,28 @@ def test_er_config_parity(oracle_mod):
             assert_ranking_equal(ids[:100], g["rank_ids_top100"], s)
 
 
+@pytest.mark.parametrize("n, deg", [(100_000, 10), (400_000, 8)])
+def test_graphs_without_split_rows(oracle_mod, n, deg):
+    """Graphs with no row over 256 arcs: the smaller one has few enough work
+    units that the sweep's last CTA closes every iteration (no fix-up
+    launch); the larger one has more than 8,192 units, so a fix-up with no
+    split rows adds the units' partials. Both against the oracle, with and
+    without distributeSinks, and bit-identical on a second run."""
+    csr = generators.erdos_renyi(n, deg / (n - 1), seed=5)
+    assert int(np.diff(csr.in_ptr.astype(np.int64)).max()) <= 256
+    slices = (n + 31) // 32
+    assert (slices <= 8192) == (n == 100_000)
+    for distribute in (False, True):
+        o = oracle_mod.pagerank(csr, tol=1e-10, norm=0, distribute_sinks=distribute)
+        dg, s, it, mx, st = gpu_run(csr, tol=1e-10, norm=0, distribute=distribute)
+        assert dg.info()["split_rows"] == 0
+        assert np.abs(s - o.scores).sum() <= L1_FP64
+        assert abs(it - o.iterations) <= 1
+        s2, it2, _, _ = dg.run(dg.params(0.85, 1e-10, 0, False, distribute, 0, _capi.UINT64_MAX))
+        np.testing.assert_array_equal(s2, s)
+        assert it2 == it
+
+
 def test_weighted_parity(oracle_mod):
     csr = generators.with_uniform_weights(generators.rmat_directed(14, 16, seed=9), seed=43)
     for normalized in (False, True):
