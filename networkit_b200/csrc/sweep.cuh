@@ -400,6 +400,8 @@ __global__ void __launch_bounds__(THREADS, UNROLL != 8 || (WEIGHTED && sizeof(T)
             if (lane == 0) {
                 a.unit_res[u] = res;
                 a.unit_sink[u] = sink;
+                if (a.close_in_sweep)
+                    __threadfence();  // visible to the CTA that closes the iteration
             }
         }
         if (!a.close_in_sweep)
